@@ -1,0 +1,341 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 spatial-search path (one JSON line on rank 0).
+
+Headline workload (N=1): exact k-NN, k = 5, on the 1.8M-point clustered
+cloud with 400,000 jittered queries (the 3DIono-sized workload).  One step
+= one k_nn! pass: LBVH build over the points + the in-kernel radius-expansion
+search of every query, inputs resident in HBM.  Inputs are smaller than L2,
+so a 256 MiB buffer is written between timed steps (outside the step
+events) to flush it.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun every rank runs its own copy of the workload (queries are
+independent: no data-path collective, weak scaling); times are device
+events, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+for _p in (REPO, os.path.join(REPO, "rt-dsl_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "exact kNN queries/s at k=5; BH force+adjoint bodies/s; batched vs plain, 1 B200"
+UNIT = "queries/s"
+K = 5
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the BH / batched sub-benchmarks")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.tmp = None
+
+    def start(self):
+        try:
+            self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.tmp.flush()
+        self.tmp.seek(0)
+        rows = [l.strip().split(",") for l in self.tmp.read().splitlines() if l.strip()]
+        self.tmp.close()
+        os.unlink(self.tmp.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d["hbm_gbs"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def traffic_for(kernel: str, workload: str):
+    """DRAM bytes per launch from a committed ncu summary, if one exists."""
+    path = os.path.join(REPO, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    e = d.get(kernel, {}).get(workload)
+    return None if e is None else e.get("dram_bytes_per_launch")
+
+
+# ------------------------------------------------------------- workloads
+def load_workload():
+    from rtdsl import workloads
+    pts, q = workloads.clustered()
+    return pts, q
+
+
+def tuned_schedule(rtd):
+    """Launch knobs for the headline workload from the autotuner cache if
+    present, else the defaults."""
+    s = rtd.default_schedule()
+    try:
+        from rtdsl import autotune
+        s = autotune.cached_schedule("clustered_1p8m_k5", s)
+    except Exception:
+        pass
+    return s
+
+
+# ---------------------------------------------------------------- ours
+def run_ours(args, ws, rank, local):
+    import torch
+    import rtdsl
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+    pts, q = load_workload()
+    n, nq = len(pts), len(q)
+    P = torch.from_numpy(pts).to(dev)
+    Q = torch.from_numpy(q).to(dev)
+    s = tuned_schedule(rtdsl)
+    ix = rtdsl.Index().profile(True)
+    ids = torch.empty((nq, K), dtype=torch.int32, device=dev)
+    d2 = torch.empty((nq, K), dtype=torch.float32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+
+    def step():
+        ix.build(P, s)
+        ix.knn(Q, K, s, out_ids=ids, out_d2=d2)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    lib = rtdsl.load()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.4)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    launches0 = lib.rtd_launch_count()
+    step_ms, phases = [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        ev0.record()
+        step()
+        ev1.record()
+        ev1.synchronize()
+        step_ms.append(ev0.elapsed_time(ev1))
+        phases.append(ix.timings())
+    launches = lib.rtd_launch_count() - launches0
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    total_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = ws * nq / (ms_per_step / 1e3)
+
+    # dominant kernel: the search kernel (per-launch duration from its own
+    # events on the launching stream) vs the build phases
+    mean = lambda key: statistics.mean(p[key] for p in phases)
+    search_ms = mean("search_ms")
+    algo_bytes = nq * (12 + 4 * K + 4 * K) + 12 * n
+    peaks = measured_peaks()
+    achieved = algo_bytes / (search_ms / 1e3) / 1e9
+    roofline = {"kernel": "knn_thread_kernel<5>", "bound": "hbm", "achieved": achieved,
+                "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                "peak_source": peaks["source"] + " (MEASURED_PEAKS.json hbm_gbs)",
+                "traffic": traffic_for("knn_search", "clustered_1p8m_k5"),
+                "algorithmic_bytes_per_launch": algo_bytes, "launch_ms": search_ms}
+
+    # ---- e2e through the host C ABI (k_nn! with host buffers)
+    e2e = None
+    if True:
+        ctx = rtdsl.Context()
+        hp = torch.from_numpy(pts).pin_memory().numpy()
+        hq = torch.from_numpy(q).pin_memory().numpy()
+        hids = torch.empty((nq, K), dtype=torch.int32).pin_memory().numpy().view("uint32")
+        for _ in range(max(args.warmup, 3)):
+            ctx.k_nn(hp, hq, K, s, out_ids=hids)
+        e2e_t = []
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ctx.k_nn(hp, hq, K, s, out_ids=hids)
+            e2e_t.append(time.perf_counter() - t0)
+        e2e_s = statistics.mean(e2e_t)
+        if dist:
+            t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": ws * nq / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(hp.nbytes + hq.nbytes),
+               "d2h_bytes_per_step": int(hids.nbytes), "ms_per_step": e2e_s * 1e3,
+               "api": "rtd_k_nn_host (k_nn! host buffers, pinned)"}
+        ctx.close()
+
+    extras = {}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(pts, q)
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "clustered_1p8m_k5: 1.8M clustered points, 400K queries, k=5, "
+                               "one step = LBVH build + in-kernel radius-expansion search",
+                   "n_points": n, "n_queries": nq, "k": K, "parallelism": f"replica x{ws}",
+                   "l2": "256 MiB buffer written between timed steps (outside step events)",
+                   "schedule": s.as_dict()},
+        "phases_ms": {key: mean(key) for key in phases[0]},
+        "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
+        "gpu_launches_per_step": launches / args.steps, "clocks": clk,
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    line.update(extras)
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------- CPU baseline
+def cpu_baseline(pts, q, sample_q: int = 8000):
+    """The reference's own CPU search (gprt-core Scene::build + traverse in
+    the k_nn! round loop, restated in C, OpenMP over queries) on a bounded
+    sample: the full build plus `sample_q` queries, extrapolated to the
+    workload's query count."""
+    import numpy as np
+    import oracle
+
+    rng = np.random.default_rng(1234)
+    sel = rng.choice(len(q), size=min(sample_q, len(q)), replace=False)
+    r0 = oracle.radius_sampled_percentile(pts, q, K, 0.10)   # k_nn! default seed
+    t0 = time.perf_counter()
+    oracle.cpu_bvh_knn(pts, q[:1], K, r0, 3.0)
+    t_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.cpu_bvh_knn(pts, q[sel], K, r0, 3.0)
+    t_all = time.perf_counter() - t0
+    t_search = max(t_all - t_build, 1e-9)
+    per_workload = t_build + t_search * (len(q) / len(sel))
+    return {"value": len(q) / per_workload, "unit": UNIT, "cores": oracle.num_threads(),
+            "kind": "port",
+            "sample": (f"full Scene::build of {len(pts)} points ({t_build:.2f} s) + {len(sel)} of "
+                       f"{len(q)} queries ({t_search:.2f} s), extrapolated to all queries; "
+                       "k_nn! defaults P=0.10, M=3.0")}
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    import oracle
+    pts, q = load_workload()
+    vals = []
+    for i in range(max(args.warmup, 3) + args.steps):
+        r = cpu_baseline(pts, q, sample_q=2000)
+        if i >= max(args.warmup, 3):
+            vals.append(r)
+    v = statistics.mean(x["value"] for x in vals)
+    line = {
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": len(q) / v * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": "clustered_1p8m_k5: 1.8M clustered points, 400K queries, k=5",
+                   "n_points": len(pts), "n_queries": len(q), "k": K},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
+                         "sample": vals[-1]["sample"]},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+    else:
+        run_ours(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,192 @@
+/*
+ * rtdsl.h -- C ABI of the B200-native spatial-search path of rt-dsl:
+ * exact unbounded k-NN by in-kernel radius expansion, fixed-radius range
+ * query with push-to-buffer output, Barnes-Hut gravity, their backward
+ * passes, and batched many-cloud k-NN.
+ *
+ * This header replaces the reference's C ABI, declared on the Rust side at
+ * gprt-optix/src/lib.rs:13-31 and implemented in C++ at
+ * gprt-optix/host/main.cpp:99-417 (OptiX pipeline / SBT / BVH / named
+ * device arrays).  Each entry point below cites the reference function it
+ * stands in for.  Differences from the reference boundary:
+ *   - every call returns an rtd_status instead of calling exit()
+ *     (main.cpp:12-28);
+ *   - device-pointer entry points take a cudaStream_t and never synchronise;
+ *     the *_host convenience entry points copy host buffers in and out,
+ *     like the reference's gprt_execute / gprt_retrieve_* pair;
+ *   - handles are not thread-safe: one handle per host thread / stream, as
+ *     the reference's CGprtPipeline (main.cpp:40-61) is used.
+ * No PyTorch or CUDA C++ types appear in the signatures: pointers, sizes and
+ * an opaque stream handle only.
+ */
+#ifndef RTDSL_H
+#define RTDSL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RTDSL_VERSION 100
+
+/* cudaStream_t without including cuda_runtime.h; NULL = legacy stream. */
+typedef struct CUstream_st *rtd_stream;
+
+typedef enum rtd_status {
+    RTD_OK = 0,
+    RTD_ERR_INVALID_ARGUMENT = 1,
+    RTD_ERR_CUDA = 2,            /* a CUDA runtime call failed */
+    RTD_ERR_OUT_OF_MEMORY = 3,
+    RTD_ERR_OVERFLOW = 4,        /* output buffer too small; required size reported */
+    RTD_ERR_NOT_CONVERGED = 5,   /* a bounded in-kernel loop ran out of rounds */
+    RTD_ERR_TIMEOUT = 6,         /* a bounded device spin-wait gave up */
+    RTD_ERR_UNSUPPORTED = 7,
+    RTD_ERR_NO_DEVICE = 8
+} rtd_status;
+
+/* gprt-core Vec3 (#[repr(C)] f32 x,y,z), gprt-core/src/lib.rs:8-10. */
+typedef struct rtd_vec3 { float x, y, z; } rtd_vec3;
+
+/* gprt-core Body {pos, mass, velocity} (28 B), gprt-core/src/lib.rs:311-317. */
+typedef struct rtd_body { rtd_vec3 pos; float mass; rtd_vec3 velocity; } rtd_body;
+
+/* Initial-radius heuristic, gprt-ir RadiusHeuristic (gprt-ir/src/lib.rs:33-37)
+ * plus the sampled nearest-neighbour seed used by the plain-kNN workload. */
+typedef enum rtd_radius_heuristic {
+    RTD_RADIUS_SAMPLED_NN = 0,          /* param x p95 1-NN distance of a 4096-point sample */
+    RTD_RADIUS_SAMPLED_PERCENTILE = 1,  /* k_nn! default: param = percentile P, x1.1 */
+    RTD_RADIUS_FIXED = 2,               /* param = radius */
+    RTD_RADIUS_SAMPLED_MAX = 3          /* percentile 1.0 */
+} rtd_radius_heuristic;
+
+/* gprt-ir Schedule (gprt-ir/src/lib.rs:58-89) re-expressed for the kernels
+ * here.  radius_increment_mult, radius_heuristic and use_morton_lbv keep
+ * their meaning; max_hits_per_query / memory_strategy have no counterpart
+ * (no per-query hit slab exists); the rest are launch knobs the autotuner
+ * picks. */
+typedef struct rtd_schedule {
+    float radius_increment_mult;  /* M > 1: radius *= M per round (k_nn! lib.rs:592) */
+    uint32_t max_rounds;          /* the last round is unbounded, so results stay exact */
+    int32_t radius_heuristic;     /* rtd_radius_heuristic */
+    float radius_param;           /* see rtd_radius_heuristic */
+    uint32_t use_morton_lbv;      /* process queries in Morton order (k_nn! lib.rs:456-460) */
+    uint32_t leaf_size;           /* LBVH leaf size: subtrees of <= leaf_size points collapse */
+    uint32_t block_size;          /* threads per block of the search kernel (0 = auto) */
+    uint32_t lanes_per_query;     /* 1 = thread per query, 32 = warp per query (0 = auto) */
+    uint32_t morton_bits;         /* 30 (u32 keys) or 63 (u64 keys); 0 = auto */
+} rtd_schedule;
+
+/* Defaults: M = 2, 32 rounds, sampled-NN seed x 2^-4, Morton query order,
+ * leaf 4, auto launch shape, auto key width. */
+void rtd_schedule_default(rtd_schedule *s);
+
+const char *rtd_status_string(rtd_status s);
+/* Message of the last failing call on this host thread ("" if none). */
+const char *rtd_last_error(void);
+int rtd_version(void);
+
+/* ---------------------------------------------------------------------
+ * LBVH index over one point cloud.  Replaces gprt_bvh_build /
+ * gprt_bvh_refit / gprt_bvh_destroy (main.cpp:200-292; Rust decls
+ * gprt-optix/src/lib.rs:16-19).  The tree is radius-independent, so the
+ * reference's per-round refit (K1 kernels.cu:3-16 + OPTIX_BUILD_OPERATION_
+ * UPDATE) has no counterpart: the radius grows inside the search kernel.
+ * ------------------------------------------------------------------- */
+typedef struct rtd_index rtd_index;
+
+rtd_status rtd_index_create(rtd_index **out);
+rtd_status rtd_index_destroy(rtd_index *idx);
+/* d_xyz: n points, x,y,z float triples (Vec3 layout) in device memory.
+ * Morton codes -> onesweep radix sort -> Karras radix tree -> bottom-up
+ * refit; subtrees of <= leaf_size points become leaves. */
+rtd_status rtd_index_build(rtd_index *idx, const float *d_xyz, uint64_t n,
+                           const rtd_schedule *sched, rtd_stream stream);
+typedef struct rtd_index_info {
+    uint64_t n_points;
+    uint64_t n_internal;   /* internal nodes after leaf collapse */
+    uint32_t leaf_size;
+    uint32_t morton_bits;
+    float lo[3], hi[3];    /* scene bounding box */
+} rtd_index_info;
+/* Synchronises the stream, then reports sizes and device error flags. */
+rtd_status rtd_index_info_get(rtd_index *idx, rtd_index_info *info, rtd_stream stream);
+
+/* Phase timers, the counterpart of the reference's [CUDA_EVENTS] prints
+ * (bvh_build / bvh_refit / kernel, gprt-optix/host/main.cpp:201-246,
+ * 314-340): when enabled, the index records CUDA events around its phases
+ * on the caller's stream; rtd_index_profile_get waits for them. */
+typedef struct rtd_profile {
+    float build_sort_ms;   /* scene box + Morton codes + radix sort + point gather */
+    float build_tree_ms;   /* Karras tree + leaf collapse + refit + top staging */
+    float seed_ms;         /* initial-radius seed */
+    float order_ms;        /* query Morton ordering */
+    float search_ms;       /* the search kernel (kNN or range count + fill) */
+} rtd_profile;
+rtd_status rtd_index_profile_enable(rtd_index *idx, int enable);
+rtd_status rtd_index_profile_get(rtd_index *idx, rtd_profile *out);
+/* Kernels this library has launched in this process (all handles). */
+uint64_t rtd_launch_count(void);
+
+/* ---------------------------------------------------------------------
+ * Exact k-NN.  Replaces the k_nn! round loop (gprt-macros/src/lib.rs:
+ * 408-604) and its per-round gprt_execute + gprt_retrieve_array_* calls
+ * (main.cpp:313-365): all rounds run inside one kernel launch.
+ * Output per query: the k smallest (FP32 squared distance, point id)
+ * pairs, ascending, ties to the lower id; ids[q*k+j] (and d2[q*k+j] when
+ * d2 != NULL).  Slots beyond the number of points hold 0xFFFFFFFF / +inf.
+ * ------------------------------------------------------------------- */
+rtd_status rtd_knn(rtd_index *idx, const float *d_queries, uint64_t nq, uint32_t k,
+                   const rtd_schedule *sched, uint32_t *d_ids, float *d_d2, rtd_stream stream);
+
+/* Host-buffer k_nn!(data, queries, k, out[, schedule]): copies in, builds
+ * the index, searches, copies ids (and d2 if non-NULL) out, synchronises.
+ * The context caches device buffers across calls. */
+typedef struct rtd_context rtd_context;
+rtd_status rtd_context_create(rtd_context **out);
+rtd_status rtd_context_destroy(rtd_context *ctx);
+rtd_status rtd_k_nn_host(rtd_context *ctx, const rtd_vec3 *data, uint64_t n,
+                         const rtd_vec3 *queries, uint64_t nq, uint32_t k,
+                         const rtd_schedule *sched, uint32_t *ids, float *d2);
+
+/* ---------------------------------------------------------------------
+ * Fixed-radius range query with push-to-buffer output.  Replaces the
+ * global-push programs (gprt-macros/src/lib.rs:276-295: atomicAdd on a
+ * per-query length, store while below cap) and r_nn!/gprt_trace!
+ * (lib.rs:625-672, 729-750).  Membership: FP32 key <= RN(r*r).
+ * Count pass: d_counts[q] hits per query, *h_total the sum (this call
+ * synchronises to return it).  Fill pass: (query, id) uint32 pairs pushed
+ * by warp-aggregated atomics into d_pairs (2 u32 per pair); order is
+ * unspecified unless sort_pairs != 0 (then sorted by query, id).  If
+ * capacity < total, nothing past capacity is written, *h_written = total
+ * and RTD_ERR_OVERFLOW is returned.
+ * ------------------------------------------------------------------- */
+rtd_status rtd_range_count(rtd_index *idx, const float *d_queries, uint64_t nq, float radius,
+                           const rtd_schedule *sched, uint32_t *d_counts, uint64_t *h_total,
+                           rtd_stream stream);
+rtd_status rtd_range_fill(rtd_index *idx, const float *d_queries, uint64_t nq, float radius,
+                          const rtd_schedule *sched, uint32_t *d_pairs, uint64_t capacity,
+                          int sort_pairs, uint64_t *h_written, rtd_stream stream);
+/* Host-buffer range_query!(data, queries, r, out): returns the pair count in
+ * *n_pairs; pairs (2*capacity u32) receives them sorted by (query, id). */
+rtd_status rtd_range_query_host(rtd_context *ctx, const rtd_vec3 *data, uint64_t n,
+                                const rtd_vec3 *queries, uint64_t nq, float radius,
+                                uint32_t *pairs, uint64_t capacity, uint64_t *n_pairs);
+
+/* ---------------------------------------------------------------------
+ * k-NN distance backward (no reference counterpart: the reference has no
+ * gradients).  Loss gradient g[q*k+j] = dL/d(d2_qj) with ids held fixed;
+ * d2_qj = |q - p_id|^2.  grad_q (nq*3) is overwritten; grad_p (n*3) is
+ * accumulated with atomics (zero it first).  Slots with id 0xFFFFFFFF are
+ * skipped.
+ * ------------------------------------------------------------------- */
+rtd_status rtd_knn_backward(const float *d_queries, uint64_t nq, const float *d_points,
+                            uint64_t n, uint32_t k, const uint32_t *d_ids,
+                            const float *d_grad_d2, float *d_grad_q, float *d_grad_p,
+                            rtd_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RTDSL_H */

@@ -1,0 +1,216 @@
+"""CPU oracle for rt-dsl's spatial-search path (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline arm import
+this package, and only as the checker or as the timed CPU port of the
+reference's own CPU search.  The product (rt-dsl_b200/rtdsl) never imports
+it.  See oracle.c for what each function restates and how it is pinned.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SRC = os.path.join(HERE, "oracle.c")
+LIB = os.path.join(HERE, "liboracle.so")
+CFLAGS = ["-std=gnu11", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC",
+          "-shared", "-Wall"]
+
+EMPTY = 0xFFFFFFFF
+
+_lock = threading.Lock()
+_lib = None
+
+
+class FlatNode(C.Structure):
+    """FlatNode, gprt-core/src/lib.rs:299-308."""
+    _fields_ = [("com", C.c_float * 3), ("mass", C.c_float), ("width", C.c_float),
+                ("is_leaf", C.c_uint32), ("next_idx", C.c_uint32), ("autorope", C.c_uint32),
+                ("bucket_start", C.c_uint32), ("num_particles", C.c_uint32)]
+
+
+FLAT_NODE_DTYPE = np.dtype([("com", np.float32, 3), ("mass", np.float32), ("width", np.float32),
+                            ("is_leaf", np.uint32), ("next_idx", np.uint32),
+                            ("autorope", np.uint32), ("bucket_start", np.uint32),
+                            ("num_particles", np.uint32)])
+
+
+def build(force: bool = False) -> str:
+    """Compile oracle.c with gcc (no FMA contraction, no fast-math)."""
+    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= os.path.getmtime(SRC):
+        return LIB
+    tmp = LIB + f".tmp{os.getpid()}"
+    r = subprocess.run(["gcc", *CFLAGS, "-o", tmp, SRC, "-lm"], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{r.stderr}")
+    os.replace(tmp, LIB)
+    return LIB
+
+
+def lib() -> C.CDLL:
+    global _lib
+    with _lock:
+        if _lib is None:
+            build()
+            L = C.CDLL(LIB)
+            P = C.c_void_p
+            I64 = C.c_int64
+            F = C.c_float
+            L.orc_num_threads.restype = C.c_int
+            L.orc_set_num_threads.argtypes = [C.c_int]
+            L.orc_morton3.restype = C.c_uint32
+            L.orc_morton3.argtypes = [C.c_uint32] * 3
+            L.orc_morton_codes.argtypes = [P, I64, P]
+            L.orc_knn.argtypes = [P, I64, P, I64, C.c_int, P, P]
+            L.orc_knn_fp64_ambiguity.argtypes = [P, I64, P, I64, C.c_int, P]
+            L.orc_knn_fp64_ambiguity.restype = I64
+            L.orc_range_count.argtypes = [P, I64, P, I64, F, P]
+            L.orc_range_count.restype = I64
+            L.orc_range_pairs.argtypes = [P, I64, P, I64, F, P, P]
+            L.orc_radius_sampled_percentile.argtypes = [P, I64, P, I64, C.c_int, F]
+            L.orc_radius_sampled_percentile.restype = F
+            L.orc_radius_sampled_nn.argtypes = [P, I64, F]
+            L.orc_radius_sampled_nn.restype = F
+            L.orc_cpu_bvh_knn.argtypes = [P, I64, P, I64, C.c_int, F, F, C.c_int, P, P]
+            L.orc_cpu_bvh_knn.restype = C.c_int
+            L.orc_bh_build.argtypes = [P, P, I64, C.c_uint32, F, P, P, P]
+            L.orc_bh_build.restype = I64
+            L.orc_bh_ref_forces.argtypes = [P, P, I64, P, I64, P, F, F, P]
+            L.orc_direct_ref_f64.argtypes = [P, P, I64, P, I64, C.c_double, P]
+            L.orc_key_public.argtypes = [P, P]
+            L.orc_key_public.restype = F
+            _lib = L
+    return _lib
+
+
+def _f32(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data) if a is not None and a.size else None
+
+
+def num_threads() -> int:
+    return lib().orc_num_threads()
+
+
+def set_num_threads(n: int) -> None:
+    lib().orc_set_num_threads(int(n))
+
+
+def morton3(x: int, y: int, z: int) -> int:
+    return int(lib().orc_morton3(x, y, z))
+
+
+def morton_codes(xyz) -> np.ndarray:
+    xyz = _f32(xyz)
+    out = np.empty(len(xyz), dtype=np.uint32)
+    lib().orc_morton_codes(_p(xyz), len(xyz), _p(out))
+    return out
+
+
+def key(q, p) -> float:
+    q = _f32(q)
+    p = _f32(p)
+    return float(lib().orc_key_public(_p(q), _p(p)))
+
+
+def knn(pts, q, k: int):
+    """Exact kNN: (ids [Q,k] uint32, d2 [Q,k] float32), (key, id) ascending."""
+    pts = _f32(pts)
+    q = _f32(q)
+    ids = np.empty((len(q), k), dtype=np.uint32)
+    d2 = np.empty((len(q), k), dtype=np.float32)
+    lib().orc_knn(_p(pts), len(pts), _p(q), len(q), k, _p(ids), _p(d2))
+    return ids, d2
+
+
+def knn_fp64_ambiguity(pts, q, ids) -> int:
+    pts = _f32(pts)
+    q = _f32(q)
+    ids = np.ascontiguousarray(ids, dtype=np.uint32)
+    return int(lib().orc_knn_fp64_ambiguity(_p(pts), len(pts), _p(q), len(q), ids.shape[1], _p(ids)))
+
+
+def range_count(pts, q, r: float):
+    pts = _f32(pts)
+    q = _f32(q)
+    counts = np.empty(len(q), dtype=np.uint32)
+    total = lib().orc_range_count(_p(pts), len(pts), _p(q), len(q), C.c_float(r), _p(counts))
+    return counts, int(total)
+
+
+def range_pairs(pts, q, r: float) -> np.ndarray:
+    """(query, id) pairs sorted by query then id."""
+    pts = _f32(pts)
+    q = _f32(q)
+    counts, total = range_count(pts, q, r)
+    off = np.zeros(len(q), dtype=np.uint64)
+    if len(q) > 1:
+        off[1:] = np.cumsum(counts[:-1].astype(np.uint64))
+    pairs = np.empty((max(total, 1), 2), dtype=np.uint32)
+    lib().orc_range_pairs(_p(pts), len(pts), _p(q), len(q), C.c_float(r), _p(off), _p(pairs))
+    return pairs[:total]
+
+
+def radius_sampled_percentile(pts, q, k: int, p: float) -> float:
+    pts = _f32(pts)
+    q = _f32(q)
+    return float(lib().orc_radius_sampled_percentile(_p(pts), len(pts), _p(q), len(q), k,
+                                                     C.c_float(p)))
+
+
+def radius_sampled_nn(pts, mult: float) -> float:
+    pts = _f32(pts)
+    return float(lib().orc_radius_sampled_nn(_p(pts), len(pts), C.c_float(mult)))
+
+
+def cpu_bvh_knn(pts, q, k: int, radius0: float, mult: float, use_morton: bool = True):
+    """The reference's CPU search (gprt-core Scene::build/traverse inside the
+    k_nn! round loop).  Returns (ids, d2, rounds)."""
+    pts = _f32(pts)
+    q = _f32(q)
+    ids = np.empty((len(q), k), dtype=np.uint32)
+    d2 = np.empty((len(q), k), dtype=np.float32)
+    rounds = lib().orc_cpu_bvh_knn(_p(pts), len(pts), _p(q), len(q), k, C.c_float(radius0),
+                                   C.c_float(mult), int(use_morton), _p(ids), _p(d2))
+    return ids, d2, int(rounds)
+
+
+def bh_build(pos, mass, bucket: int = 128, min_width: float = 1e-5):
+    """Reference Barnes-Hut tree: (nodes structured array, flat body order,
+    root box [min xyz, max xyz, width])."""
+    pos = _f32(pos)
+    mass = _f32(mass)
+    n = len(pos)
+    nodes = np.zeros(2 * n + 1, dtype=FLAT_NODE_DTYPE)
+    order = np.empty(n, dtype=np.uint32)
+    root = np.empty(7, dtype=np.float32)
+    nn = lib().orc_bh_build(_p(pos), _p(mass), n, bucket, C.c_float(min_width), _p(nodes),
+                            _p(order), _p(root))
+    return nodes[:nn].copy(), order, root
+
+
+def bh_ref_forces(pos, mass, nodes, order, theta: float, G: float = 6.674e-11) -> np.ndarray:
+    pos = _f32(pos)
+    mass = _f32(mass)
+    nodes = np.ascontiguousarray(nodes, dtype=FLAT_NODE_DTYPE)
+    order = np.ascontiguousarray(order, dtype=np.uint32)
+    out = np.empty((len(pos), 3), dtype=np.float32)
+    lib().orc_bh_ref_forces(_p(pos), _p(mass), len(pos), _p(nodes), len(nodes), _p(order),
+                            C.c_float(theta), C.c_float(G), _p(out))
+    return out
+
+
+def direct_ref_f64(pos, mass, targets, G: float = 6.674e-11) -> np.ndarray:
+    pos = _f32(pos)
+    mass = _f32(mass)
+    t = np.ascontiguousarray(targets, dtype=np.int64)
+    out = np.empty((len(t), 3), dtype=np.float64)
+    lib().orc_direct_ref_f64(_p(pos), _p(mass), len(pos), _p(t), len(t), C.c_double(G), _p(out))
+    return out

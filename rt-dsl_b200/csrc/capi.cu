@@ -1,0 +1,298 @@
+// capi.cu -- the extern "C" boundary declared in include/rtdsl.h.
+// Every entry point validates its arguments, returns an rtd_status and
+// records a message for rtd_last_error(); nothing calls exit() (the
+// reference's CUDA_CHECK/OPTIX_CHECK do, gprt-optix/host/main.cpp:12-28).
+#include <atomic>
+#include <cstdio>
+#include <new>
+
+#include "index.cuh"
+
+namespace rtd {
+
+static thread_local std::string g_last_error;
+static std::atomic<uint64_t> g_launches{0};
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+rtd_status fail(rtd_status s, const std::string &msg) {
+    g_last_error = msg;
+    return s;
+}
+
+rtd_status cuda_fail(cudaError_t e, const char *what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    g_last_error = m;
+    if (e == cudaErrorMemoryAllocation) return RTD_ERR_OUT_OF_MEMORY;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return RTD_ERR_NO_DEVICE;
+    return RTD_ERR_CUDA;
+}
+
+rtd_status status_from_deverr(uint32_t f) {
+    if (f == 0) return RTD_OK;
+    if (f & DEVERR_TIMEOUT) return fail(RTD_ERR_TIMEOUT, "a device wait hit its iteration limit");
+    if (f & DEVERR_STACK) return fail(RTD_ERR_OVERFLOW, "traversal stack overflow");
+    if (f & DEVERR_OVERFLOW) return fail(RTD_ERR_OVERFLOW, "output buffer too small");
+    if (f & DEVERR_NOT_CONVERGED) return fail(RTD_ERR_NOT_CONVERGED, "radius expansion did not converge");
+    if (f & DEVERR_DEPTH) return fail(RTD_ERR_UNSUPPORTED, "tree deeper than the key supports");
+    return fail(RTD_ERR_CUDA, "unknown device error flag");
+}
+
+rtd_status DevBuf::reserve(size_t want) {
+    if (want <= bytes && ptr) return RTD_OK;
+    release();
+    size_t b = want < 256 ? 256 : want;
+    cudaError_t e = cudaMalloc(&ptr, b);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        bytes = 0;
+        cudaGetLastError();
+        return cuda_fail(e, "cudaMalloc");
+    }
+    bytes = b;
+    return RTD_OK;
+}
+
+void DevBuf::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+// Implemented in lbvh.cu / knn.cu / range.cu / knn_backward.cu.
+rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd_schedule *s,
+                       cudaStream_t st);
+rtd_status knn_search(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k,
+                      const rtd_schedule *sched, uint32_t *d_ids, float *d_d2, cudaStream_t st);
+rtd_status range_count(rtd_index *idx, const float *d_q, uint64_t nq, float r,
+                       const rtd_schedule *s, uint32_t *d_counts, uint64_t *h_total,
+                       cudaStream_t st);
+rtd_status range_fill(rtd_index *idx, const float *d_q, uint64_t nq, float r,
+                      const rtd_schedule *s, uint32_t *d_pairs, uint64_t capacity, int sort_pairs,
+                      uint64_t *h_written, cudaStream_t st);
+rtd_status knn_backward(const float *q, uint64_t nq, const float *pts, uint64_t n, uint32_t k,
+                        const uint32_t *ids, const float *g, float *gq, float *gp, cudaStream_t st);
+
+// Reads and clears the device error flags of an index (synchronises).
+rtd_status check_index_errors(rtd_index *idx, cudaStream_t st) {
+    if (!idx->hdr.ptr) return RTD_OK;
+    uint32_t f = 0;
+    IndexHeader *h = idx->hdr.as<IndexHeader>();
+    RTD_CUDA(cudaMemcpyAsync(&f, &h->err, sizeof(f), cudaMemcpyDeviceToHost, st));
+    RTD_CUDA(cudaStreamSynchronize(st));
+    if (f) RTD_CUDA(cudaMemsetAsync(&h->err, 0, sizeof(uint32_t), st));
+    return status_from_deverr(f);
+}
+
+}  // namespace rtd
+
+using namespace rtd;
+
+// Host-buffer context: an index plus device staging buffers and a stream.
+struct rtd_context {
+    rtd_index index;
+    DevBuf data, queries, ids, d2, pairs;
+    cudaStream_t stream = nullptr;
+};
+
+extern "C" {
+
+void rtd_schedule_default(rtd_schedule *s) {
+    if (!s) return;
+    s->radius_increment_mult = 2.0f;
+    s->max_rounds = 32;
+    s->radius_heuristic = RTD_RADIUS_SAMPLED_NN;
+    s->radius_param = 0.0625f;   // 2^-4 x p95 1-NN distance of a 4096-point sample
+    s->use_morton_lbv = 1;
+    s->leaf_size = 4;
+    s->block_size = 0;
+    s->lanes_per_query = 0;
+    s->morton_bits = 0;
+}
+
+const char *rtd_status_string(rtd_status s) {
+    switch (s) {
+    case RTD_OK: return "RTD_OK";
+    case RTD_ERR_INVALID_ARGUMENT: return "RTD_ERR_INVALID_ARGUMENT";
+    case RTD_ERR_CUDA: return "RTD_ERR_CUDA";
+    case RTD_ERR_OUT_OF_MEMORY: return "RTD_ERR_OUT_OF_MEMORY";
+    case RTD_ERR_OVERFLOW: return "RTD_ERR_OVERFLOW";
+    case RTD_ERR_NOT_CONVERGED: return "RTD_ERR_NOT_CONVERGED";
+    case RTD_ERR_TIMEOUT: return "RTD_ERR_TIMEOUT";
+    case RTD_ERR_UNSUPPORTED: return "RTD_ERR_UNSUPPORTED";
+    case RTD_ERR_NO_DEVICE: return "RTD_ERR_NO_DEVICE";
+    }
+    return "RTD_ERR_UNKNOWN";
+}
+
+const char *rtd_last_error(void) { return g_last_error.c_str(); }
+
+int rtd_version(void) { return RTDSL_VERSION; }
+
+rtd_status rtd_index_create(rtd_index **out) {
+    if (!out) return fail(RTD_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = new (std::nothrow) rtd_index();
+    if (!*out) return fail(RTD_ERR_OUT_OF_MEMORY, "host allocation failed");
+    return RTD_OK;
+}
+
+rtd_status rtd_index_destroy(rtd_index *idx) {
+    delete idx;
+    return RTD_OK;
+}
+
+rtd_status rtd_index_build(rtd_index *idx, const float *d_xyz, uint64_t n,
+                           const rtd_schedule *sched, rtd_stream stream) {
+    return index_build(idx, d_xyz, n, sched, (cudaStream_t)stream);
+}
+
+rtd_status rtd_index_info_get(rtd_index *idx, rtd_index_info *info, rtd_stream stream) {
+    if (!idx || !info) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL argument");
+    memset(info, 0, sizeof(*info));
+    info->n_points = idx->n;
+    info->leaf_size = idx->leaf_size;
+    info->morton_bits = (uint32_t)idx->morton_bits;
+    if (!idx->hdr.ptr) return RTD_OK;
+    IndexHeader h;
+    cudaStream_t st = (cudaStream_t)stream;
+    RTD_CUDA(cudaMemcpyAsync(&h, idx->hdr.ptr, sizeof(h), cudaMemcpyDeviceToHost, st));
+    RTD_CUDA(cudaStreamSynchronize(st));
+    info->n_internal = h.n_internal;
+    for (int a = 0; a < 3; ++a) {
+        info->lo[a] = float_unflip(h.box[a]);
+        info->hi[a] = float_unflip(h.box[3 + a]);
+    }
+    return check_index_errors(idx, st);
+}
+
+rtd_status rtd_index_profile_enable(rtd_index *idx, int enable) {
+    if (!idx) return fail(RTD_ERR_INVALID_ARGUMENT, "index is NULL");
+    idx->prof = enable != 0;
+    return RTD_OK;
+}
+
+static float ev_ms(rtd_index *idx, int a, int b) {
+    if (!idx->ev_set[a] || !idx->ev_set[b]) return 0.0f;
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, idx->ev[a], idx->ev[b]) != cudaSuccess) {
+        cudaGetLastError();
+        return 0.0f;
+    }
+    return ms;
+}
+
+rtd_status rtd_index_profile_get(rtd_index *idx, rtd_profile *out) {
+    if (!idx || !out) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL argument");
+    memset(out, 0, sizeof(*out));
+    for (int i = 0; i < 8; ++i)
+        if (idx->ev_set[i]) RTD_CUDA(cudaEventSynchronize(idx->ev[i]));
+    out->build_sort_ms = ev_ms(idx, EV_BUILD0, EV_BUILD_SORTED);
+    out->build_tree_ms = ev_ms(idx, EV_BUILD_SORTED, EV_BUILD1);
+    out->seed_ms = ev_ms(idx, EV_SEARCH0, EV_SEEDED);
+    out->order_ms = ev_ms(idx, EV_SEEDED, EV_ORDERED);
+    out->search_ms = ev_ms(idx, EV_ORDERED, EV_SEARCH1);
+    return RTD_OK;
+}
+
+uint64_t rtd_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+rtd_status rtd_knn(rtd_index *idx, const float *d_queries, uint64_t nq, uint32_t k,
+                   const rtd_schedule *sched, uint32_t *d_ids, float *d_d2, rtd_stream stream) {
+    return knn_search(idx, d_queries, nq, k, sched, d_ids, d_d2, (cudaStream_t)stream);
+}
+
+rtd_status rtd_context_create(rtd_context **out) {
+    if (!out) return fail(RTD_ERR_INVALID_ARGUMENT, "out is NULL");
+    rtd_context *c = new (std::nothrow) rtd_context();
+    if (!c) return fail(RTD_ERR_OUT_OF_MEMORY, "host allocation failed");
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return cuda_fail(e, "cudaStreamCreateWithFlags");
+    }
+    *out = c;
+    return RTD_OK;
+}
+
+rtd_status rtd_context_destroy(rtd_context *ctx) {
+    if (!ctx) return RTD_OK;
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return RTD_OK;
+}
+
+rtd_status rtd_k_nn_host(rtd_context *ctx, const rtd_vec3 *data, uint64_t n,
+                         const rtd_vec3 *queries, uint64_t nq, uint32_t k,
+                         const rtd_schedule *sched, uint32_t *ids, float *d2) {
+    if (!ctx) return fail(RTD_ERR_INVALID_ARGUMENT, "context is NULL");
+    if ((n && !data) || (nq && (!queries || !ids)))
+        return fail(RTD_ERR_INVALID_ARGUMENT, "NULL host buffer");
+    cudaStream_t st = ctx->stream;
+    RTD_TRY(ctx->data.reserve(n * sizeof(rtd_vec3)));
+    RTD_TRY(ctx->queries.reserve(nq * sizeof(rtd_vec3)));
+    RTD_TRY(ctx->ids.reserve(nq * (uint64_t)k * sizeof(uint32_t)));
+    if (d2) RTD_TRY(ctx->d2.reserve(nq * (uint64_t)k * sizeof(float)));
+    if (n) RTD_CUDA(cudaMemcpyAsync(ctx->data.ptr, data, n * sizeof(rtd_vec3), cudaMemcpyHostToDevice, st));
+    if (nq) RTD_CUDA(cudaMemcpyAsync(ctx->queries.ptr, queries, nq * sizeof(rtd_vec3), cudaMemcpyHostToDevice, st));
+    RTD_TRY(index_build(&ctx->index, ctx->data.as<float>(), n, sched, st));
+    RTD_TRY(knn_search(&ctx->index, ctx->queries.as<float>(), nq, k, sched, ctx->ids.as<uint32_t>(),
+                       d2 ? ctx->d2.as<float>() : nullptr, st));
+    if (nq) {
+        RTD_CUDA(cudaMemcpyAsync(ids, ctx->ids.ptr, nq * (uint64_t)k * 4, cudaMemcpyDeviceToHost, st));
+        if (d2) RTD_CUDA(cudaMemcpyAsync(d2, ctx->d2.ptr, nq * (uint64_t)k * 4, cudaMemcpyDeviceToHost, st));
+    }
+    RTD_CUDA(cudaStreamSynchronize(st));
+    return check_index_errors(&ctx->index, st);
+}
+
+rtd_status rtd_range_count(rtd_index *idx, const float *d_queries, uint64_t nq, float radius,
+                           const rtd_schedule *sched, uint32_t *d_counts, uint64_t *h_total,
+                           rtd_stream stream) {
+    return range_count(idx, d_queries, nq, radius, sched, d_counts, h_total, (cudaStream_t)stream);
+}
+
+rtd_status rtd_range_fill(rtd_index *idx, const float *d_queries, uint64_t nq, float radius,
+                          const rtd_schedule *sched, uint32_t *d_pairs, uint64_t capacity,
+                          int sort_pairs, uint64_t *h_written, rtd_stream stream) {
+    return range_fill(idx, d_queries, nq, radius, sched, d_pairs, capacity, sort_pairs, h_written,
+                      (cudaStream_t)stream);
+}
+
+rtd_status rtd_range_query_host(rtd_context *ctx, const rtd_vec3 *data, uint64_t n,
+                                const rtd_vec3 *queries, uint64_t nq, float radius,
+                                uint32_t *pairs, uint64_t capacity, uint64_t *n_pairs) {
+    if (!ctx || !n_pairs) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL argument");
+    if ((n && !data) || (nq && !queries) || (capacity && !pairs))
+        return fail(RTD_ERR_INVALID_ARGUMENT, "NULL host buffer");
+    cudaStream_t st = ctx->stream;
+    RTD_TRY(ctx->data.reserve(n * sizeof(rtd_vec3)));
+    RTD_TRY(ctx->queries.reserve(nq * sizeof(rtd_vec3)));
+    RTD_TRY(ctx->ids.reserve(nq * sizeof(uint32_t)));
+    if (n) RTD_CUDA(cudaMemcpyAsync(ctx->data.ptr, data, n * sizeof(rtd_vec3), cudaMemcpyHostToDevice, st));
+    if (nq) RTD_CUDA(cudaMemcpyAsync(ctx->queries.ptr, queries, nq * sizeof(rtd_vec3), cudaMemcpyHostToDevice, st));
+    RTD_TRY(index_build(&ctx->index, ctx->data.as<float>(), n, nullptr, st));
+    uint64_t total = 0;
+    RTD_TRY(range_count(&ctx->index, ctx->queries.as<float>(), nq, radius, nullptr,
+                        ctx->ids.as<uint32_t>(), &total, st));
+    *n_pairs = total;
+    if (total > capacity) return fail(RTD_ERR_OVERFLOW, "pair buffer smaller than the pair count");
+    RTD_TRY(ctx->pairs.reserve(total * 2 * sizeof(uint32_t)));
+    uint64_t written = 0;
+    RTD_TRY(range_fill(&ctx->index, ctx->queries.as<float>(), nq, radius, nullptr,
+                       ctx->pairs.as<uint32_t>(), total, 1, &written, st));
+    if (total) RTD_CUDA(cudaMemcpyAsync(pairs, ctx->pairs.ptr, total * 8, cudaMemcpyDeviceToHost, st));
+    RTD_CUDA(cudaStreamSynchronize(st));
+    return check_index_errors(&ctx->index, st);
+}
+
+rtd_status rtd_knn_backward(const float *d_queries, uint64_t nq, const float *d_points,
+                            uint64_t n, uint32_t k, const uint32_t *d_ids,
+                            const float *d_grad_d2, float *d_grad_q, float *d_grad_p,
+                            rtd_stream stream) {
+    return knn_backward(d_queries, nq, d_points, n, k, d_ids, d_grad_d2, d_grad_q, d_grad_p,
+                        (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,115 @@
+// index.cuh -- LBVH index layout shared by the builder and the search kernels.
+//
+// Points are stored Morton-sorted as float4 (x, y, z, bits of the original
+// id): one 128-bit load per candidate.  Internal nodes hold the boxes of
+// their two children (64 B, four 128-bit loads).  A child word is either an
+// internal-node index or a leaf (first sorted point, count stored beside it).
+// The top levels of the tree are copied into a small array that search
+// kernels stage in shared memory; child words that point into it carry
+// CHILD_TOP.
+#pragma once
+
+#include "common.cuh"
+#include "sort.cuh"
+
+namespace rtd {
+
+constexpr uint32_t CHILD_LEAF = 0x80000000u;
+constexpr uint32_t CHILD_TOP = 0x40000000u;
+constexpr uint32_t CHILD_INDEX = 0x3FFFFFFFu;
+constexpr uint32_t CHILD_NONE = 0xFFFFFFFFu;
+constexpr uint32_t EMPTY_ID = 0xFFFFFFFFu;
+constexpr int TOP_LEVELS = 6;
+constexpr int TOP_MAX = (1 << TOP_LEVELS) - 1;   // 63 nodes, 4 KB of shared memory
+
+struct __align__(16) BvhNode {
+    float4 a;  // lo.x[0] lo.y[0] lo.z[0] hi.x[0]
+    float4 b;  // hi.y[0] hi.z[0] lo.x[1] lo.y[1]
+    float4 c;  // lo.z[1] hi.x[1] hi.y[1] hi.z[1]
+    uint4 d;   // child[0] child[1] count[0] count[1]
+};
+static_assert(sizeof(BvhNode) == 64, "node is one half cache line");
+
+// Device-resident header of an index (all fields written on the device).
+struct IndexHeader {
+    uint32_t root;        // child word of the root for search kernels (CHILD_TOP|0 or a leaf)
+    uint32_t root_count;  // point count when the root is a leaf
+    uint32_t n_internal;  // compact internal nodes
+    uint32_t n_top;       // staged top nodes
+    uint32_t box[6];      // scene box as order-preserving u32: lo xyz, hi xyz
+    uint32_t err;         // DEVERR_* flags
+    float r0sq;           // squared initial radius of the last search
+    uint64_t total;       // last range-count total
+    float nn95_key;       // p95 of the squared 1-NN distance within a 4096-point sample
+    uint32_t n_sample;    // points in the radius-seed sample (<= 1000)
+};
+
+constexpr int SEED_NN_SAMPLE = 4096;
+constexpr int SEED_PCT_POINTS = 1000;
+constexpr int SEED_PCT_QUERIES = 100;
+
+}  // namespace rtd
+
+struct rtd_index {
+    uint64_t n = 0;
+    uint32_t leaf_size = 4;
+    int morton_bits = 30;
+    int device = 0;
+    rtd::DevBuf hdr;        // IndexHeader
+    rtd::DevBuf pts;        // float4 * n, Morton order
+    rtd::DevBuf nodes;      // BvhNode * (n - 1)
+    rtd::DevBuf top;        // BvhNode * TOP_MAX
+    // build scratch
+    rtd::DevBuf keys, keys_alt, vals, vals_alt;
+    rtd::DevBuf kleft, kright, kfirst, klast, kparent, flags, cidx, cparent, counter;
+    rtd::SortScratch sort;
+    rtd::ScanScratch scan;
+    // radius-seed data kept from the build: stride sample of the points in
+    // input order (<= 1000 x float4) and the 4096-point 1-NN scratch
+    rtd::DevBuf sample, seed;
+    // search scratch
+    rtd::DevBuf qkeys, qkeys_alt, qperm, qperm_alt;
+    rtd::DevBuf rcounts, roffsets, rcursor, rpairs_alt, rkeys, rkeys_alt;
+    // phase timers (rtd_index_profile_*)
+    bool prof = false;
+    cudaEvent_t ev[8] = {};
+    bool ev_set[8] = {};
+    void mark(int i, cudaStream_t st) {
+        if (!prof) return;
+        if (!ev[i] && cudaEventCreate(&ev[i]) != cudaSuccess) { ev[i] = nullptr; return; }
+        if (cudaEventRecord(ev[i], st) == cudaSuccess) ev_set[i] = true;
+    }
+    ~rtd_index() {
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+};
+
+namespace rtd {
+// Event slots of rtd_index::mark.
+enum : int { EV_BUILD0 = 0, EV_BUILD_SORTED, EV_BUILD1, EV_SEARCH0, EV_SEEDED, EV_ORDERED,
+             EV_SEARCH1 };
+}  // namespace rtd
+
+namespace rtd {
+
+// Arguments the search kernels need from an index.
+struct IndexView {
+    const float4 *pts;
+    const BvhNode *nodes;
+    const BvhNode *top;
+    const IndexHeader *hdr;
+    uint64_t n;
+};
+inline IndexView view_of(const rtd_index *idx) {
+    return IndexView{idx->pts.as<float4>(), idx->nodes.as<BvhNode>(), idx->top.as<BvhNode>(),
+                     idx->hdr.as<IndexHeader>(), idx->n};
+}
+
+// Query ordering: Morton codes of the queries against the scene box, sorted;
+// perm[i] is the i-th query to process.  Returns perm (device) or nullptr
+// when ordering is off.
+rtd_status order_queries(rtd_index *idx, const float *d_q, uint64_t nq, bool morton,
+                         const uint32_t **perm, cudaStream_t stream);
+
+}  // namespace rtd

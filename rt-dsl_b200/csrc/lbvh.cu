@@ -1,0 +1,539 @@
+// lbvh.cu -- LBVH builder: scene box -> Morton codes -> onesweep radix sort
+// -> Karras radix tree -> leaf collapse -> bottom-up box refit with atomics
+// -> top-level staging.  Replaces the OptiX GAS build/refit of
+// gprt-optix/host/main.cpp:200-292 and the sphere-AABB kernel of
+// gprt-optix/host/kernels.cu:3-16: the tree holds point boxes only and the
+// search radius is applied inside the search kernels.
+#include "index.cuh"
+
+namespace rtd {
+namespace {
+
+constexpr int BLOCK = 256;
+
+__global__ void hdr_init_kernel(IndexHeader *h) {
+    h->root = CHILD_NONE;
+    h->root_count = 0;
+    h->n_internal = 0;
+    h->n_top = 0;
+    for (int a = 0; a < 3; ++a) {
+        h->box[a] = 0xFFFFFFFFu;   // flip(+inf) side: any atomicMin lowers it
+        h->box[3 + a] = 0u;
+    }
+    h->err = 0;
+    h->r0sq = 0.0f;
+    h->total = 0;
+    h->nn95_key = -1.0f;   // "no sample": the seed falls back to radius 1
+    h->n_sample = 0;
+}
+
+// Scene box, NaN-ignoring (fminf/fmaxf), as order-preserving atomics.
+__global__ void __launch_bounds__(BLOCK) bbox_kernel(const float *__restrict__ xyz, uint64_t n,
+                                                     IndexHeader *h) {
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint64_t i = (uint64_t)blockIdx.x * BLOCK + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * BLOCK) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            float v = xyz[3 * i + a];
+            lo[a] = fminf(lo[a], v);
+            hi[a] = fmaxf(hi[a], v);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[a] = fminf(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+            hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+        }
+    __shared__ float s[BLOCK / 32][6];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int a = 0; a < 3; ++a) { s[warp][a] = lo[a]; s[warp][3 + a] = hi[a]; }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        int a = threadIdx.x;
+        float l = INFINITY, u = -INFINITY;
+        for (int w = 0; w < BLOCK / 32; ++w) { l = fminf(l, s[w][a]); u = fmaxf(u, s[w][3 + a]); }
+        atomicMin(&h->box[a], float_flip(l));
+        atomicMax(&h->box[3 + a], float_flip(u));
+    }
+}
+
+struct SceneNorm {
+    float lo[3], ext[3];
+};
+__device__ __forceinline__ SceneNorm scene_norm(const IndexHeader *h) {
+    SceneNorm s;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float lo = float_unflip(h->box[a]), hi = float_unflip(h->box[3 + a]);
+        s.lo[a] = lo;
+        // morton.rs:37-39: extent clamped to >= 1e-6
+        s.ext[a] = fmaxf(__fsub_rn(hi, lo), 1e-6f);
+    }
+    return s;
+}
+
+// 30-bit codes follow compute_morton_codes (gprt-core/src/morton.rs:19-48);
+// 63-bit codes use the same normalisation with 21 bits per axis.
+template <typename K>
+__global__ void __launch_bounds__(BLOCK) morton_kernel(const float *__restrict__ xyz, uint64_t n,
+                                                       const IndexHeader *h, K *__restrict__ keys) {
+    SceneNorm s = scene_norm(h);
+    for (uint64_t i = (uint64_t)blockIdx.x * BLOCK + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * BLOCK) {
+        float x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+        if (sizeof(K) == 4) {
+            keys[i] = (K)morton30(quantize(x, s.lo[0], s.ext[0], 1023.0f),
+                                  quantize(y, s.lo[1], s.ext[1], 1023.0f),
+                                  quantize(z, s.lo[2], s.ext[2], 1023.0f));
+        } else {
+            keys[i] = (K)morton63(quantize(x, s.lo[0], s.ext[0], 2097151.0f),
+                                  quantize(y, s.lo[1], s.ext[1], 2097151.0f),
+                                  quantize(z, s.lo[2], s.ext[2], 2097151.0f));
+        }
+    }
+}
+
+__global__ void __launch_bounds__(BLOCK) gather_points_kernel(const float *__restrict__ xyz,
+                                                              const uint32_t *__restrict__ perm,
+                                                              uint64_t n, float4 *__restrict__ pts) {
+    for (uint64_t i = (uint64_t)blockIdx.x * BLOCK + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * BLOCK) {
+        uint32_t o = perm[i];
+        pts[i] = make_float4(xyz[3 * (uint64_t)o], xyz[3 * (uint64_t)o + 1],
+                             xyz[3 * (uint64_t)o + 2], __uint_as_float(o));
+    }
+}
+
+// Common-prefix length of sorted keys i and j, ties broken by index
+// (Karras 2012, "Maximizing parallelism in the construction of BVHs").
+template <typename K>
+__device__ __forceinline__ int delta(const K *__restrict__ keys, int64_t n, int64_t i, int64_t j) {
+    if (j < 0 || j >= n) return -1;
+    K a = keys[i], b = keys[j];
+    if (a == b) return (int)(8 * sizeof(K)) + __clz((uint32_t)(i ^ j));
+    return sizeof(K) == 8 ? __clzll((unsigned long long)(a ^ b)) : __clz((uint32_t)(a ^ b));
+}
+
+template <typename K>
+__global__ void __launch_bounds__(BLOCK) karras_kernel(const K *__restrict__ keys, int64_t n,
+                                                       uint32_t leaf_size, uint32_t *kleft,
+                                                       uint32_t *kright, uint32_t *kfirst,
+                                                       uint32_t *klast, uint32_t *kparent,
+                                                       uint32_t *flags) {
+    for (int64_t i = (int64_t)blockIdx.x * BLOCK + threadIdx.x; i < n - 1;
+         i += (int64_t)gridDim.x * BLOCK) {
+        int dir = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+        int dmin = delta(keys, n, i, i - dir);
+        int64_t lmax = 2;
+        while (delta(keys, n, i, i + lmax * dir) > dmin) lmax <<= 1;
+        int64_t l = 0;
+        for (int64_t t = lmax >> 1; t >= 1; t >>= 1)
+            if (delta(keys, n, i, i + (l + t) * dir) > dmin) l += t;
+        int64_t j = i + l * dir;
+        int dnode = delta(keys, n, i, j);
+        int64_t s = 0, t = l;
+        do {
+            t = (t + 1) >> 1;
+            if (delta(keys, n, i, i + (s + t) * dir) > dnode) s += t;
+        } while (t > 1);
+        int64_t gamma = i + s * dir + (dir < 0 ? -1 : 0);
+        int64_t first = i < j ? i : j, last = i < j ? j : i;
+        uint32_t left = (uint32_t)gamma, right = (uint32_t)(gamma + 1);
+        if (first == gamma) left |= CHILD_LEAF;
+        else kparent[gamma] = (uint32_t)i;
+        if (last == gamma + 1) right |= CHILD_LEAF;
+        else kparent[gamma + 1] = (uint32_t)i;
+        kleft[i] = left;
+        kright[i] = right;
+        kfirst[i] = (uint32_t)first;
+        klast[i] = (uint32_t)last;
+        flags[i] = (uint32_t)(last - first + 1) > leaf_size ? 1u : 0u;
+    }
+}
+
+// Compact nodes: children become leaves when their subtree has <= leaf_size
+// points.  Boxes are filled by the refit kernel.
+__global__ void __launch_bounds__(BLOCK) compact_kernel(
+    int64_t n, const uint32_t *__restrict__ kleft, const uint32_t *__restrict__ kright,
+    const uint32_t *__restrict__ kfirst, const uint32_t *__restrict__ klast,
+    const uint32_t *__restrict__ kparent, const uint32_t *__restrict__ flags,
+    const uint32_t *__restrict__ cidx, BvhNode *nodes, uint32_t *cparent, uint32_t *counter) {
+    for (int64_t i = (int64_t)blockIdx.x * BLOCK + threadIdx.x; i < n - 1;
+         i += (int64_t)gridDim.x * BLOCK) {
+        if (!flags[i]) continue;
+        uint32_t c = cidx[i];
+        uint32_t ch[2] = {kleft[i], kright[i]};
+        uint32_t word[2], cnt[2];
+        for (int s = 0; s < 2; ++s) {
+            uint32_t w = ch[s];
+            if (w & CHILD_LEAF) {
+                word[s] = CHILD_LEAF | (w & CHILD_INDEX);
+                cnt[s] = 1;
+            } else if (flags[w]) {
+                word[s] = cidx[w];
+            } else {
+                word[s] = CHILD_LEAF | kfirst[w];
+                cnt[s] = klast[w] - kfirst[w] + 1;
+            }
+            if (!(word[s] & CHILD_LEAF)) cnt[s] = 0;
+        }
+        BvhNode nd;
+        nd.a = make_float4(0.f, 0.f, 0.f, 0.f);
+        nd.b = nd.a;
+        nd.c = nd.a;
+        nd.d = make_uint4(word[0], word[1], cnt[0], cnt[1]);
+        nodes[c] = nd;
+        // parent (compact) and which side this node is on
+        uint32_t par = CHILD_NONE;
+        if (i != 0) {
+            uint32_t kp = kparent[i];
+            uint32_t side = ((kright[kp] & ~CHILD_LEAF) == (uint32_t)i) ? 1u : 0u;
+            par = (cidx[kp] << 1) | side;
+        }
+        cparent[c] = par;
+        counter[c] = 0;
+    }
+}
+
+struct Box {
+    float lo[3], hi[3];
+};
+
+__device__ __forceinline__ Box leaf_box(const float4 *__restrict__ pts, uint32_t first,
+                                        uint32_t count) {
+    Box b;
+    for (int a = 0; a < 3; ++a) { b.lo[a] = INFINITY; b.hi[a] = -INFINITY; }
+    for (uint32_t j = 0; j < count; ++j) {
+        float4 p = pts[first + j];
+        b.lo[0] = fminf(b.lo[0], p.x); b.hi[0] = fmaxf(b.hi[0], p.x);
+        b.lo[1] = fminf(b.lo[1], p.y); b.hi[1] = fmaxf(b.hi[1], p.y);
+        b.lo[2] = fminf(b.lo[2], p.z); b.hi[2] = fmaxf(b.hi[2], p.z);
+    }
+    return b;
+}
+
+__device__ __forceinline__ void store_child_box(BvhNode *nd, int side, const Box &b) {
+    float *f = reinterpret_cast<float *>(nd);
+    // layout: [lo.x0 lo.y0 lo.z0 hi.x0 hi.y0 hi.z0] [lo.x1 .. hi.z1]
+    for (int a = 0; a < 3; ++a) {
+        f[side * 6 + a] = b.lo[a];
+        f[side * 6 + 3 + a] = b.hi[a];
+    }
+}
+
+__device__ __forceinline__ Box node_union_cg(const BvhNode *nd) {
+    const float *f = reinterpret_cast<const float *>(nd);
+    Box b;
+    for (int a = 0; a < 3; ++a) {
+        b.lo[a] = fminf(__ldcg(f + a), __ldcg(f + 6 + a));
+        b.hi[a] = fmaxf(__ldcg(f + 3 + a), __ldcg(f + 9 + a));
+    }
+    return b;
+}
+
+// Bottom-up refit: a thread per node with leaf children computes their
+// boxes; the second arrival at a node (atomic counter) forms its box and
+// carries it to the parent.
+__global__ void __launch_bounds__(BLOCK) refit_kernel(uint32_t n_internal_max,
+                                                      const IndexHeader *h,
+                                                      const float4 *__restrict__ pts,
+                                                      BvhNode *nodes,
+                                                      const uint32_t *__restrict__ cparent,
+                                                      uint32_t *counter) {
+    const uint32_t n_int = h->n_internal;
+    for (uint32_t c = blockIdx.x * BLOCK + threadIdx.x; c < n_int && c < n_internal_max;
+         c += gridDim.x * BLOCK) {
+        uint4 d = nodes[c].d;
+        uint32_t nleaf = 0;
+        if (d.x & CHILD_LEAF) { store_child_box(&nodes[c], 0, leaf_box(pts, d.x & CHILD_INDEX, d.z)); ++nleaf; }
+        if (d.y & CHILD_LEAF) { store_child_box(&nodes[c], 1, leaf_box(pts, d.y & CHILD_INDEX, d.w)); ++nleaf; }
+        if (nleaf == 0) continue;
+        __threadfence();
+        uint32_t old = atomicAdd(&counter[c], nleaf);
+        if (old + nleaf < 2) continue;
+        uint32_t cur = c;
+        for (int depth = 0;; ++depth) {
+            if (depth > 128) {   // deeper than any Karras tree: broken parent links
+                atomicOr(&((IndexHeader *)h)->err, DEVERR_DEPTH);
+                break;
+            }
+            __threadfence();
+            Box b = node_union_cg(&nodes[cur]);
+            uint32_t par = cparent[cur];
+            if (par == CHILD_NONE) break;
+            uint32_t p = par >> 1;
+            store_child_box(&nodes[p], (int)(par & 1u), b);
+            __threadfence();
+            if (atomicAdd(&counter[p], 1u) == 0u) break;
+            cur = p;
+        }
+    }
+}
+
+// Root word and the breadth-first top levels, copied into `top`.
+__global__ void stage_top_kernel(IndexHeader *h, const BvhNode *__restrict__ nodes, BvhNode *top,
+                                 uint64_t n, uint32_t leaf_size) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (n == 0) {
+        h->root = CHILD_NONE;
+        h->n_top = 0;
+        return;
+    }
+    if (n == 1 || n <= leaf_size) {
+        h->root = CHILD_LEAF | 0u;
+        h->root_count = (uint32_t)n;
+        h->n_top = 0;
+        return;
+    }
+    uint32_t q[TOP_MAX];
+    uint8_t depth[TOP_MAX];
+    int cnt = 0;
+    q[cnt] = 0; depth[cnt] = 0; ++cnt;
+    for (int i = 0; i < cnt; ++i) {
+        if (depth[i] + 1 >= TOP_LEVELS) continue;
+        uint4 d = nodes[q[i]].d;
+        uint32_t ch[2] = {d.x, d.y};
+        for (int s = 0; s < 2; ++s)
+            if (!(ch[s] & CHILD_LEAF) && cnt < TOP_MAX) {
+                q[cnt] = ch[s];
+                depth[cnt] = (uint8_t)(depth[i] + 1);
+                ++cnt;
+            }
+    }
+    for (int i = 0; i < cnt; ++i) {
+        BvhNode nd = nodes[q[i]];
+        uint32_t ch[2] = {nd.d.x, nd.d.y};
+        for (int s = 0; s < 2; ++s) {
+            if (ch[s] & CHILD_LEAF) continue;
+            for (int j = 0; j < cnt; ++j)
+                if (q[j] == ch[s]) { ch[s] = CHILD_TOP | (uint32_t)j; break; }
+        }
+        nd.d.x = ch[0];
+        nd.d.y = ch[1];
+        top[i] = nd;
+    }
+    h->root = CHILD_TOP | 0u;
+    h->n_top = (uint32_t)cnt;
+}
+
+// ------------------------------------------------ radius-seed sample data
+// Stride sample of <= 1000 points in input order, kept for the k_nn!
+// sampled-percentile seed (gprt-macros/src/lib.rs:433-434).
+__global__ void seed_sample_kernel(const float *__restrict__ xyz, uint64_t n, float4 *sample,
+                                   IndexHeader *h) {
+    uint64_t pstep = n / SEED_PCT_POINTS > 1 ? n / SEED_PCT_POINTS : 1;
+    uint64_t cnt = (n + pstep - 1) / pstep;
+    if (cnt > SEED_PCT_POINTS) cnt = SEED_PCT_POINTS;
+    for (uint64_t t = threadIdx.x; t < cnt; t += blockDim.x) {
+        uint64_t i = t * pstep;
+        sample[t] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], 0.0f);
+    }
+    if (threadIdx.x == 0) h->n_sample = (uint32_t)cnt;
+}
+
+// Squared 1-NN distance of each of S = min(n, 4096) stride-sampled points
+// (index a*n/S) among the other sample points.
+__global__ void __launch_bounds__(128) seed_nn_kernel(const float *__restrict__ xyz, uint64_t n,
+                                                      uint32_t S, float *__restrict__ out) {
+    __shared__ float3 s_p[128];
+    const uint32_t a = blockIdx.x * 128 + threadIdx.x;
+    float3 pa = make_float3(0.f, 0.f, 0.f);
+    if (a < S) {
+        uint64_t ia = (uint64_t)a * n / S;
+        pa = make_float3(xyz[3 * ia], xyz[3 * ia + 1], xyz[3 * ia + 2]);
+    }
+    float best = INFINITY;
+    for (uint32_t t0 = 0; t0 < S; t0 += 128) {
+        uint32_t b = t0 + threadIdx.x;
+        if (b < S) {
+            uint64_t ib = (uint64_t)b * n / S;
+            s_p[threadIdx.x] = make_float3(xyz[3 * ib], xyz[3 * ib + 1], xyz[3 * ib + 2]);
+        }
+        __syncthreads();
+        uint32_t lim = S - t0 < 128 ? S - t0 : 128;
+        for (uint32_t j = 0; j < lim; ++j) {
+            if (t0 + j == a) continue;
+            float key = exact_key(pa.x, pa.y, pa.z, s_p[j].x, s_p[j].y, s_p[j].z);
+            if (key < best) best = key;
+        }
+        __syncthreads();
+    }
+    if (a < S) out[a] = best;
+}
+
+// Sorts <= 4096 floats ascending in shared memory with one 1024-thread block.
+__device__ void block_sort4096(float *s, uint32_t n_pad) {
+    for (uint32_t k = 2; k <= n_pad; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < n_pad; i += blockDim.x) {
+                uint32_t ixj = i ^ j;
+                if (ixj > i) {
+                    float x = s[i], y = s[ixj];
+                    bool up = (i & k) == 0;
+                    if (up ? (x > y) : (x < y)) { s[i] = y; s[ixj] = x; }
+                }
+            }
+            __syncthreads();
+        }
+}
+
+__global__ void __launch_bounds__(1024) seed_nn_select_kernel(const float *__restrict__ keys,
+                                                              uint32_t S, IndexHeader *h) {
+    __shared__ float s[SEED_NN_SAMPLE];
+    uint32_t n_pad = 1;
+    while (n_pad < S) n_pad <<= 1;
+    for (uint32_t i = threadIdx.x; i < n_pad; i += blockDim.x) s[i] = i < S ? keys[i] : INFINITY;
+    __syncthreads();
+    block_sort4096(s, n_pad);
+    if (threadIdx.x == 0) {
+        uint32_t idx = (uint32_t)(0.95f * (float)S);
+        if (idx > S - 1) idx = S - 1;
+        h->nn95_key = s[idx];
+    }
+}
+
+rtd_status build_seed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStream_t st) {
+    IndexHeader *h = idx->hdr.as<IndexHeader>();
+    RTD_TRY(idx->sample.reserve(SEED_PCT_POINTS * sizeof(float4)));
+    RTD_TRY(idx->seed.reserve(SEED_NN_SAMPLE * sizeof(float)));
+    seed_sample_kernel<<<1, 256, 0, st>>>(d_xyz, n, idx->sample.as<float4>(), h);
+    RTD_LAUNCH_CHECK();
+    if (n >= 2) {
+        uint32_t S = n < SEED_NN_SAMPLE ? (uint32_t)n : (uint32_t)SEED_NN_SAMPLE;
+        seed_nn_kernel<<<(S + 127) / 128, 128, 0, st>>>(d_xyz, n, S, idx->seed.as<float>());
+        RTD_LAUNCH_CHECK();
+        seed_nn_select_kernel<<<1, 1024, 0, st>>>(idx->seed.as<float>(), S, h);
+        RTD_LAUNCH_CHECK();
+    }
+    return RTD_OK;
+}
+
+template <typename K>
+rtd_status build_typed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStream_t st) {
+    IndexHeader *h = idx->hdr.as<IndexHeader>();
+    uint32_t *d_err = &h->err;
+    const int kbits = sizeof(K) == 4 ? 30 : 63;
+    RTD_TRY(idx->keys.reserve(n * sizeof(K)));
+    RTD_TRY(idx->keys_alt.reserve(n * sizeof(K)));
+    RTD_TRY(idx->vals.reserve(n * sizeof(uint32_t)));
+    RTD_TRY(idx->vals_alt.reserve(n * sizeof(uint32_t)));
+    const int g = grid_for(n, BLOCK, 148 * 8);
+    morton_kernel<K><<<g, BLOCK, 0, st>>>(d_xyz, n, h, idx->keys.as<K>());
+    RTD_LAUNCH_CHECK();
+    bool in_alt = false;
+    RTD_TRY(radix_sort_pairs<K>(idx->keys.as<K>(), idx->keys_alt.as<K>(), idx->vals.as<uint32_t>(),
+                                idx->vals_alt.as<uint32_t>(), true, n, 0, kbits, idx->sort, d_err,
+                                st, &in_alt));
+    K *skeys = in_alt ? idx->keys_alt.as<K>() : idx->keys.as<K>();
+    uint32_t *perm = in_alt ? idx->vals_alt.as<uint32_t>() : idx->vals.as<uint32_t>();
+    gather_points_kernel<<<g, BLOCK, 0, st>>>(d_xyz, perm, n, idx->pts.as<float4>());
+    RTD_LAUNCH_CHECK();
+    idx->mark(EV_BUILD_SORTED, st);
+    if (n < 2 || n <= idx->leaf_size) return RTD_OK;
+    const uint64_t ni = n - 1;
+    for (rtd::DevBuf *b : {&idx->kleft, &idx->kright, &idx->kfirst, &idx->klast, &idx->kparent,
+                           &idx->flags, &idx->cidx, &idx->cparent, &idx->counter})
+        RTD_TRY(b->reserve(ni * sizeof(uint32_t)));
+    const int gi = grid_for(ni, BLOCK, 148 * 8);
+    karras_kernel<K><<<gi, BLOCK, 0, st>>>(skeys, (int64_t)n, idx->leaf_size,
+                                           idx->kleft.as<uint32_t>(), idx->kright.as<uint32_t>(),
+                                           idx->kfirst.as<uint32_t>(), idx->klast.as<uint32_t>(),
+                                           idx->kparent.as<uint32_t>(), idx->flags.as<uint32_t>());
+    RTD_LAUNCH_CHECK();
+    RTD_TRY(exclusive_scan_u32_32(idx->flags.as<uint32_t>(), idx->cidx.as<uint32_t>(), ni,
+                                  &h->n_internal, idx->scan, d_err, st));
+    compact_kernel<<<gi, BLOCK, 0, st>>>(
+        (int64_t)n, idx->kleft.as<uint32_t>(), idx->kright.as<uint32_t>(),
+        idx->kfirst.as<uint32_t>(), idx->klast.as<uint32_t>(), idx->kparent.as<uint32_t>(),
+        idx->flags.as<uint32_t>(), idx->cidx.as<uint32_t>(), idx->nodes.as<BvhNode>(),
+        idx->cparent.as<uint32_t>(), idx->counter.as<uint32_t>());
+    RTD_LAUNCH_CHECK();
+    refit_kernel<<<gi, BLOCK, 0, st>>>((uint32_t)ni, h, idx->pts.as<float4>(),
+                                        idx->nodes.as<BvhNode>(), idx->cparent.as<uint32_t>(),
+                                        idx->counter.as<uint32_t>());
+    RTD_LAUNCH_CHECK();
+    return RTD_OK;
+}
+
+}  // namespace
+
+rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd_schedule *s,
+                       cudaStream_t st) {
+    if (!idx) return fail(RTD_ERR_INVALID_ARGUMENT, "index is NULL");
+    if (n > 0 && !d_xyz) return fail(RTD_ERR_INVALID_ARGUMENT, "points pointer is NULL");
+    if (n >= (1ull << 30) - 1) return fail(RTD_ERR_INVALID_ARGUMENT, "at most 2^30-2 points");
+    rtd_schedule def;
+    rtd_schedule_default(&def);
+    if (!s) s = &def;
+    if (s->leaf_size < 1 || s->leaf_size > 64)
+        return fail(RTD_ERR_INVALID_ARGUMENT, "leaf_size must be in [1, 64]");
+    int mb = (int)s->morton_bits;
+    if (mb == 0) mb = n >= (1ull << 19) ? 63 : 30;
+    if (mb != 30 && mb != 63) return fail(RTD_ERR_INVALID_ARGUMENT, "morton_bits must be 30 or 63");
+    RTD_CUDA(cudaGetDevice(&idx->device));
+    idx->n = n;
+    idx->leaf_size = s->leaf_size;
+    idx->morton_bits = mb;
+    RTD_TRY(idx->hdr.reserve(sizeof(IndexHeader)));
+    RTD_TRY(idx->pts.reserve((n ? n : 1) * sizeof(float4)));
+    RTD_TRY(idx->nodes.reserve((n > 1 ? n - 1 : 1) * sizeof(BvhNode)));
+    RTD_TRY(idx->top.reserve(TOP_MAX * sizeof(BvhNode)));
+    IndexHeader *h = idx->hdr.as<IndexHeader>();
+    for (bool &e : idx->ev_set) e = false;
+    idx->mark(EV_BUILD0, st);
+    hdr_init_kernel<<<1, 1, 0, st>>>(h);
+    RTD_LAUNCH_CHECK();
+    if (n > 0) {
+        bbox_kernel<<<grid_for(n, BLOCK, 148 * 4), BLOCK, 0, st>>>(d_xyz, n, h);
+        RTD_LAUNCH_CHECK();
+        RTD_TRY(build_seed(idx, d_xyz, n, st));
+        if (mb == 30) RTD_TRY(build_typed<uint32_t>(idx, d_xyz, n, st));
+        else RTD_TRY(build_typed<uint64_t>(idx, d_xyz, n, st));
+    }
+    stage_top_kernel<<<1, 1, 0, st>>>(h, idx->nodes.as<BvhNode>(), idx->top.as<BvhNode>(), n,
+                                      idx->leaf_size);
+    RTD_LAUNCH_CHECK();
+    idx->mark(EV_BUILD1, st);
+    return RTD_OK;
+}
+
+// ------------------------------------------------------- query ordering
+namespace {
+__global__ void __launch_bounds__(BLOCK) query_morton_kernel(const float *__restrict__ q,
+                                                             uint64_t nq, const IndexHeader *h,
+                                                             uint32_t *__restrict__ keys) {
+    SceneNorm s = scene_norm(h);
+    for (uint64_t i = (uint64_t)blockIdx.x * BLOCK + threadIdx.x; i < nq;
+         i += (uint64_t)gridDim.x * BLOCK) {
+        keys[i] = morton30(quantize(q[3 * i], s.lo[0], s.ext[0], 1023.0f),
+                           quantize(q[3 * i + 1], s.lo[1], s.ext[1], 1023.0f),
+                           quantize(q[3 * i + 2], s.lo[2], s.ext[2], 1023.0f));
+    }
+}
+}  // namespace
+
+rtd_status order_queries(rtd_index *idx, const float *d_q, uint64_t nq, bool morton,
+                         const uint32_t **perm, cudaStream_t st) {
+    *perm = nullptr;
+    if (!morton || nq < 2) return RTD_OK;
+    if (nq >= (1ull << 30)) return fail(RTD_ERR_INVALID_ARGUMENT, "at most 2^30-1 queries");
+    RTD_TRY(idx->qkeys.reserve(nq * 4));
+    RTD_TRY(idx->qkeys_alt.reserve(nq * 4));
+    RTD_TRY(idx->qperm.reserve(nq * 4));
+    RTD_TRY(idx->qperm_alt.reserve(nq * 4));
+    IndexHeader *h = idx->hdr.as<IndexHeader>();
+    query_morton_kernel<<<grid_for(nq, BLOCK, 148 * 8), BLOCK, 0, st>>>(d_q, nq, h,
+                                                                        idx->qkeys.as<uint32_t>());
+    RTD_LAUNCH_CHECK();
+    bool in_alt = false;
+    RTD_TRY(radix_sort_pairs<uint32_t>(idx->qkeys.as<uint32_t>(), idx->qkeys_alt.as<uint32_t>(),
+                                       idx->qperm.as<uint32_t>(), idx->qperm_alt.as<uint32_t>(),
+                                       true, nq, 0, 30, idx->sort, &h->err, st, &in_alt));
+    *perm = in_alt ? idx->qperm_alt.as<uint32_t>() : idx->qperm.as<uint32_t>();
+    return RTD_OK;
+}
+
+}  // namespace rtd

@@ -1,0 +1,334 @@
+// range.cu -- fixed-radius range query: a count pass sizes the output, a
+// fill pass pushes (query, id) pairs into it.  Replaces the reference's
+// global-push programs (gprt-macros/src/lib.rs:276-295), where every
+// any-hit does atomicAdd(&lens[q], 1) into a capped per-query slab that the
+// host then copies back and filters (lib.rs:538-583).  Here the buffer is
+// exactly sized by the count pass, and hits are staged per warp in shared
+// memory and pushed with one global atomicAdd per flush (warp-aggregated
+// compaction), so global atomics scale with the output bytes / 8 KB instead
+// of the hit count.  Membership: exact FP32 key <= RN(r*r), as the
+// intersection program tests dist_sq <= r_val*r_val (lib.rs:283, 341).
+#include "index.cuh"
+
+namespace rtd {
+namespace {
+
+constexpr int RBLOCK = 128;
+constexpr int RWARPS = RBLOCK / 32;
+constexpr int SHORT_DEPTH = 16;  // stack entries per thread in shared memory
+constexpr int STACK_DEPTH = 104; // >= maximal tree depth
+constexpr int WBUF = 1024;       // staged pairs per warp (8 KB)
+
+struct RangeArgs {
+    IndexView ix;
+    const float *q;
+    uint64_t nq;
+    const uint32_t *perm;
+    float r2;
+    uint32_t *counts;
+    uint2 *pairs;
+    uint64_t capacity;
+    unsigned long long *cursor;
+    uint32_t *err;
+};
+
+__device__ __forceinline__ void load_node_r(const BvhNode *__restrict__ s_top,
+                                            const BvhNode *__restrict__ g, uint32_t w, float4 &a,
+                                            float4 &b, float4 &c, uint4 &d) {
+    if (w & CHILD_TOP) {
+        const BvhNode &n = s_top[w & CHILD_INDEX];
+        a = n.a; b = n.b; c = n.c; d = n.d;
+    } else {
+        const BvhNode *n = g + (w & CHILD_INDEX);
+        a = __ldg(&n->a); b = __ldg(&n->b); c = __ldg(&n->c); d = __ldg(&n->d);
+    }
+}
+
+// One traversal step state per thread.
+struct Walk {
+    uint32_t node;
+    int sp;
+};
+
+// FILL = false: count hits per query.  FILL = true: push pairs.
+// Threads of a warp advance their own traversals one node per iteration of
+// a warp-converged loop; after each iteration the warp flushes its staging
+// buffer when it might not hold another iteration's hits.
+template <bool FILL>
+__global__ void __launch_bounds__(RBLOCK) range_kernel(const RangeArgs p) {
+    __shared__ BvhNode s_top[TOP_MAX];
+    __shared__ uint32_t s_stack[SHORT_DEPTH][RBLOCK];
+    __shared__ uint2 s_buf[FILL ? RWARPS : 1][FILL ? WBUF : 1];
+    __shared__ uint32_t s_cnt[RWARPS];
+    const IndexHeader *h = p.ix.hdr;
+    const uint32_t ntop = h->n_top;
+    for (uint32_t i = threadIdx.x; i < ntop; i += RBLOCK) s_top[i] = p.ix.top[i];
+    if (threadIdx.x < RWARPS) s_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t root = h->root, root_count = h->root_count;
+    const float4 *__restrict__ pts = p.ix.pts;
+    const BvhNode *__restrict__ gn = p.ix.nodes;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const float r2 = p.r2;
+    const uint32_t visit_cap = 2u * h->n_internal + 4u;
+    uint32_t l_stack[STACK_DEPTH - SHORT_DEPTH];
+
+    const uint64_t stride = (uint64_t)gridDim.x * RBLOCK;
+    const uint64_t t0 = (uint64_t)blockIdx.x * RBLOCK + warp * 32;
+    // warp-uniform loop over query batches
+    for (uint64_t tb = t0; tb < p.nq; tb += stride) {
+        const uint64_t t = tb + lane;
+        const bool have = t < p.nq;
+        uint64_t qi = 0;
+        float qx = 0.f, qy = 0.f, qz = 0.f;
+        if (have) {
+            qi = p.perm ? p.perm[t] : t;
+            qx = p.q[3 * qi]; qy = p.q[3 * qi + 1]; qz = p.q[3 * qi + 2];
+        }
+        uint32_t node = (have && root != CHILD_NONE) ? root : CHILD_NONE;
+        int sp = 0;
+        uint32_t cnt = 0;
+        uint32_t visits = 0;
+        while (__any_sync(0xffffffffu, node != CHILD_NONE)) {
+            if (node != CHILD_NONE && ++visits > visit_cap) {   // broken tree: give up
+                atomicOr(p.err, DEVERR_STACK);
+                node = CHILD_NONE;
+                sp = 0;
+            }
+            if (node != CHILD_NONE) {
+                uint32_t lf_first[2], lf_cnt[2];
+                int nleaf = 0;
+                uint32_t next = CHILD_NONE;
+                if (node & CHILD_LEAF) {
+                    lf_first[0] = node & CHILD_INDEX;
+                    lf_cnt[0] = root_count;
+                    nleaf = 1;
+                } else {
+                    float4 a, b, c;
+                    uint4 d;
+                    load_node_r(s_top, gn, node, a, b, c, d);
+                    bool v0 = !(box_min_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y) > r2);
+                    bool v1 = !(box_min_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w) > r2);
+                    if (v0 && (d.x & CHILD_LEAF)) { lf_first[nleaf] = d.x & CHILD_INDEX; lf_cnt[nleaf] = d.z; ++nleaf; v0 = false; }
+                    if (v1 && (d.y & CHILD_LEAF)) { lf_first[nleaf] = d.y & CHILD_INDEX; lf_cnt[nleaf] = d.w; ++nleaf; v1 = false; }
+                    if (v0 && v1) {
+                        next = d.x;
+                        if (sp < SHORT_DEPTH) s_stack[sp++][threadIdx.x] = d.y;
+                        else if (sp < STACK_DEPTH) { l_stack[sp - SHORT_DEPTH] = d.y; ++sp; }
+                        else atomicOr(p.err, DEVERR_STACK);
+                    } else if (v0) {
+                        next = d.x;
+                    } else if (v1) {
+                        next = d.y;
+                    }
+                }
+                for (int l = 0; l < nleaf; ++l)
+                    for (uint32_t j = 0; j < lf_cnt[l]; ++j) {
+                        float4 pt = __ldg(&pts[lf_first[l] + j]);
+                        float key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
+                        if (key <= r2) {
+                            ++cnt;
+                            if (FILL) {
+                                uint2 pr = make_uint2((uint32_t)qi, __float_as_uint(pt.w));
+                                uint32_t slot = atomicAdd(&s_cnt[warp], 1u);
+                                if (slot < WBUF) {
+                                    s_buf[FILL ? warp : 0][FILL ? slot : 0] = pr;
+                                } else {   // staging full: push this pair alone
+                                    unsigned long long dst = atomicAdd(p.cursor, 1ull);
+                                    if (dst < p.capacity) p.pairs[dst] = pr;
+                                    else atomicOr(p.err, DEVERR_OVERFLOW);
+                                }
+                            }
+                        }
+                    }
+                if (next == CHILD_NONE && sp > 0) {
+                    --sp;
+                    next = sp < SHORT_DEPTH ? s_stack[sp][threadIdx.x] : l_stack[sp - SHORT_DEPTH];
+                }
+                node = next;
+            }
+            if (FILL) {
+                __syncwarp();
+                uint32_t c = s_cnt[warp];
+                c = c < WBUF ? c : WBUF;
+                if (c >= WBUF / 2 || !__any_sync(0xffffffffu, node != CHILD_NONE)) {
+                    unsigned long long base = 0;
+                    if (lane == 0 && c) base = atomicAdd(p.cursor, (unsigned long long)c);
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    for (uint32_t j = lane; j < c; j += 32) {
+                        uint64_t dst = base + j;
+                        if (dst < p.capacity) p.pairs[dst] = s_buf[FILL ? warp : 0][FILL ? j : 0];
+                    }
+                    if (lane == 0 && base + c > p.capacity) atomicOr(p.err, DEVERR_OVERFLOW);
+                    __syncwarp();
+                    if (lane == 0) s_cnt[warp] = 0;
+                    __syncwarp();
+                }
+            }
+        }
+        if (!FILL && have) p.counts[qi] = cnt;
+    }
+}
+
+__global__ void pairs_from_keys_kernel(const uint64_t *__restrict__ keys, uint64_t n,
+                                       uint2 *__restrict__ out) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t k = keys[i];
+        out[i] = make_uint2((uint32_t)(k >> 32), (uint32_t)k);
+    }
+}
+
+__global__ void keys_from_pairs_kernel(const uint2 *__restrict__ pairs, uint64_t n,
+                                       uint64_t *__restrict__ keys) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        uint2 p = pairs[i];
+        keys[i] = ((uint64_t)p.x << 32) | p.y;
+    }
+}
+
+rtd_status range_args(rtd_index *idx, const float *d_q, uint64_t nq, float r,
+                      const rtd_schedule *sched, RangeArgs &a, cudaStream_t st) {
+    if (!idx || !idx->hdr.ptr) return fail(RTD_ERR_INVALID_ARGUMENT, "index not built");
+    if (nq && !d_q) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL queries");
+    if (!(r >= 0.0f)) return fail(RTD_ERR_INVALID_ARGUMENT, "radius must be >= 0");
+    if (idx->leaf_size > 64) return fail(RTD_ERR_UNSUPPORTED, "leaf_size > 64");
+    rtd_schedule def;
+    rtd_schedule_default(&def);
+    const rtd_schedule &s = sched ? *sched : def;
+    const uint32_t *perm = nullptr;
+    for (int e = EV_SEARCH0; e <= EV_SEARCH1; ++e) idx->ev_set[e] = false;
+    idx->mark(EV_SEARCH0, st);
+    idx->mark(EV_SEEDED, st);
+    RTD_TRY(order_queries(idx, d_q, nq, s.use_morton_lbv != 0, &perm, st));
+    idx->mark(EV_ORDERED, st);
+    a.ix = view_of(idx);
+    a.q = d_q;
+    a.nq = nq;
+    a.perm = perm;
+    a.r2 = r * r;
+    a.counts = nullptr;
+    a.pairs = nullptr;
+    a.capacity = 0;
+    a.cursor = nullptr;
+    a.err = &idx->hdr.as<IndexHeader>()->err;
+    return RTD_OK;
+}
+
+}  // namespace
+
+rtd_status check_index_errors(rtd_index *idx, cudaStream_t st);
+
+rtd_status range_count(rtd_index *idx, const float *d_q, uint64_t nq, float r,
+                       const rtd_schedule *s, uint32_t *d_counts, uint64_t *h_total,
+                       cudaStream_t st) {
+    if (!d_counts && nq) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL counts");
+    RangeArgs a;
+    RTD_TRY(range_args(idx, d_q, nq, r, s, a, st));
+    a.counts = d_counts;
+    IndexHeader *h = idx->hdr.as<IndexHeader>();
+    if (nq) {
+        range_kernel<false><<<grid_for(nq, RBLOCK, 1 << 20), RBLOCK, 0, st>>>(a);
+        RTD_LAUNCH_CHECK();
+        idx->mark(EV_SEARCH1, st);
+        RTD_TRY(idx->roffsets.reserve(nq * sizeof(uint64_t)));
+        RTD_TRY(exclusive_scan_u32(d_counts, idx->roffsets.as<uint64_t>(), nq, &h->total,
+                                   idx->scan, &h->err, st));
+    } else {
+        RTD_CUDA(cudaMemsetAsync(&h->total, 0, sizeof(uint64_t), st));
+    }
+    uint64_t total = 0;
+    RTD_CUDA(cudaMemcpyAsync(&total, &h->total, sizeof(total), cudaMemcpyDeviceToHost, st));
+    RTD_TRY(check_index_errors(idx, st));   // synchronises
+    if (h_total) *h_total = total;
+    return RTD_OK;
+}
+
+rtd_status range_fill(rtd_index *idx, const float *d_q, uint64_t nq, float r,
+                      const rtd_schedule *s, uint32_t *d_pairs, uint64_t capacity, int sort_pairs,
+                      uint64_t *h_written, cudaStream_t st) {
+    if (capacity && !d_pairs) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL pairs");
+    RangeArgs a;
+    RTD_TRY(range_args(idx, d_q, nq, r, s, a, st));
+    RTD_TRY(idx->rcursor.reserve(sizeof(unsigned long long)));
+    RTD_CUDA(cudaMemsetAsync(idx->rcursor.ptr, 0, sizeof(unsigned long long), st));
+    a.pairs = reinterpret_cast<uint2 *>(d_pairs);
+    a.capacity = capacity;
+    a.cursor = idx->rcursor.as<unsigned long long>();
+    if (nq) {
+        range_kernel<true><<<grid_for(nq, RBLOCK, 1 << 20), RBLOCK, 0, st>>>(a);
+        RTD_LAUNCH_CHECK();
+        idx->mark(EV_SEARCH1, st);
+    }
+    unsigned long long total = 0;
+    RTD_CUDA(cudaMemcpyAsync(&total, idx->rcursor.ptr, sizeof(total), cudaMemcpyDeviceToHost, st));
+    RTD_CUDA(cudaStreamSynchronize(st));
+    if (h_written) *h_written = total;
+    if (total > capacity) {
+        IndexHeader *h = idx->hdr.as<IndexHeader>();
+        RTD_CUDA(cudaMemsetAsync(&h->err, 0, sizeof(uint32_t), st));
+        return fail(RTD_ERR_OVERFLOW, "pair buffer smaller than the pair count");
+    }
+    if (sort_pairs && total > 1) {
+        if (total >= (1ull << 30)) return fail(RTD_ERR_UNSUPPORTED, "sorting >= 2^30 pairs");
+        RTD_TRY(idx->rkeys.reserve(total * 8));
+        RTD_TRY(idx->rkeys_alt.reserve(total * 8));
+        RTD_TRY(idx->rpairs_alt.reserve(total * 8));   // dummy values, ping-pong halves
+        uint32_t *v0 = idx->rpairs_alt.as<uint32_t>();
+        uint32_t *v1 = v0 + total;
+        const int g = grid_for(total, 256, 148 * 8);
+        keys_from_pairs_kernel<<<g, 256, 0, st>>>(a.pairs, total, idx->rkeys.as<uint64_t>());
+        RTD_LAUNCH_CHECK();
+        int qbits = 1;
+        while (qbits < 32 && (1ull << qbits) < nq) ++qbits;
+        bool in_alt = false;
+        IndexHeader *h = idx->hdr.as<IndexHeader>();
+        RTD_TRY(radix_sort_pairs<uint64_t>(idx->rkeys.as<uint64_t>(), idx->rkeys_alt.as<uint64_t>(),
+                                           v0, v1, true, total, 0, 32 + qbits, idx->sort, &h->err,
+                                           st, &in_alt));
+        const uint64_t *sk = in_alt ? idx->rkeys_alt.as<uint64_t>() : idx->rkeys.as<uint64_t>();
+        pairs_from_keys_kernel<<<g, 256, 0, st>>>(sk, total, a.pairs);
+        RTD_LAUNCH_CHECK();
+    }
+    return check_index_errors(idx, st);
+}
+
+// ------------------------------------------------------- kNN backward
+namespace {
+__global__ void knn_backward_kernel(const float *__restrict__ q, uint64_t nq,
+                                    const float *__restrict__ pts, uint64_t n, uint32_t k,
+                                    const uint32_t *__restrict__ ids, const float *__restrict__ g,
+                                    float *__restrict__ gq, float *__restrict__ gp) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nq;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        float qx = q[3 * i], qy = q[3 * i + 1], qz = q[3 * i + 2];
+        float ax = 0.f, ay = 0.f, az = 0.f;
+        for (uint32_t j = 0; j < k; ++j) {
+            uint32_t id = ids[i * k + j];
+            if (id == EMPTY_ID || id >= n) continue;
+            float w = 2.0f * g[i * k + j];
+            float dx = qx - pts[3 * (uint64_t)id], dy = qy - pts[3 * (uint64_t)id + 1],
+                  dz = qz - pts[3 * (uint64_t)id + 2];
+            ax += w * dx; ay += w * dy; az += w * dz;
+            if (gp) {
+                atomicAdd(&gp[3 * (uint64_t)id], -w * dx);
+                atomicAdd(&gp[3 * (uint64_t)id + 1], -w * dy);
+                atomicAdd(&gp[3 * (uint64_t)id + 2], -w * dz);
+            }
+        }
+        if (gq) { gq[3 * i] = ax; gq[3 * i + 1] = ay; gq[3 * i + 2] = az; }
+    }
+}
+}  // namespace
+
+rtd_status knn_backward(const float *q, uint64_t nq, const float *pts, uint64_t n, uint32_t k,
+                        const uint32_t *ids, const float *g, float *gq, float *gp, cudaStream_t st) {
+    if (nq == 0 || k == 0) return RTD_OK;
+    if (!q || !pts || !ids || !g) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL input");
+    knn_backward_kernel<<<grid_for(nq, 256, 148 * 16), 256, 0, st>>>(q, nq, pts, n, k, ids, g, gq, gp);
+    RTD_LAUNCH_CHECK();
+    return RTD_OK;
+}
+
+}  // namespace rtd

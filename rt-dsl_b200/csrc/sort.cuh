@@ -1,0 +1,44 @@
+// sort.cuh -- onesweep LSD radix sort of (key, u32 value) pairs and a
+// single-pass decoupled look-back exclusive scan.
+//
+// Radix sort: one read of the keys builds the digit histograms of every
+// pass; each 8-bit pass is then a single kernel whose tiles (taken in order
+// from an atomic counter) rank their keys with warp match-any, publish the
+// per-digit tile count, look back over earlier tiles for the running digit
+// prefix, and scatter through shared memory so each digit run is written
+// contiguously.  Waits on earlier tiles are bounded (SPIN_LIMIT) and set
+// DEVERR_TIMEOUT instead of hanging.
+#pragma once
+
+#include "common.cuh"
+
+namespace rtd {
+
+struct SortScratch {
+    DevBuf hist;      // passes * 256 u32 (counts, then exclusive offsets)
+    DevBuf status;    // passes * tiles * 256 u32 (look-back words)
+    DevBuf counters;  // passes u32 (tile tickets)
+};
+
+// Sorts n pairs by bits [begin_bit, end_bit) of the key.  keys/vals hold the
+// input; keys_alt/vals_alt are scratch of the same size (all four buffers
+// are required).  With vals_iota the input values are taken to be 0..n-1
+// and vals is not read.  On return *in_alt tells whether the sorted result
+// is in the *_alt buffers.  n must be < 2^30.
+template <typename K>
+rtd_status radix_sort_pairs(K *keys, K *keys_alt, uint32_t *vals, uint32_t *vals_alt,
+                            bool vals_iota, uint64_t n, int begin_bit, int end_bit,
+                            SortScratch &scr, uint32_t *d_err, cudaStream_t stream, bool *in_alt);
+
+// out[i] = sum(in[0..i)), out has n entries; *d_total (device) = sum(in).
+struct ScanScratch {
+    DevBuf status;    // tiles u64 look-back words
+    DevBuf counter;   // tile ticket
+};
+rtd_status exclusive_scan_u32(const uint32_t *in, uint64_t *out, uint64_t n, uint64_t *d_total,
+                              ScanScratch &scr, uint32_t *d_err, cudaStream_t stream);
+// Same, 32-bit output (caller guarantees the sum fits).
+rtd_status exclusive_scan_u32_32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *d_total,
+                                 ScanScratch &scr, uint32_t *d_err, cudaStream_t stream);
+
+}  // namespace rtd

@@ -1,0 +1,15 @@
+"""rtdsl -- B200-native spatial search for rt-dsl (k-NN, range, Barnes-Hut).
+
+All compute runs in librtdsl.so (hand-written sm_100a CUDA behind the C ABI
+of include/rtdsl.h); this package binds it with ctypes and mirrors the
+reference's k_nn! / range_query! / barnes_hut! interface.
+"""
+from ._capi import (EMPTY_ID, RADIUS_FIXED, RADIUS_SAMPLED_MAX, RADIUS_SAMPLED_NN,
+                    RADIUS_SAMPLED_PERCENTILE, RtdError, Schedule, default_schedule, load)
+from .api import Context, Index, k_nn, k_nn_array, knn_backward, range_query
+
+__all__ = [
+    "EMPTY_ID", "RADIUS_FIXED", "RADIUS_SAMPLED_MAX", "RADIUS_SAMPLED_NN",
+    "RADIUS_SAMPLED_PERCENTILE", "RtdError", "Schedule", "default_schedule", "load",
+    "Context", "Index", "k_nn", "k_nn_array", "knn_backward", "range_query",
+]

@@ -1,0 +1,155 @@
+"""ctypes binding of include/rtdsl.h.
+
+The library is the product: there is no CPU fallback.  If librtdsl.so is
+missing and cannot be built, importing the binding raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+from . import _build
+
+RTD_OK = 0
+RTD_ERR_INVALID_ARGUMENT = 1
+RTD_ERR_CUDA = 2
+RTD_ERR_OUT_OF_MEMORY = 3
+RTD_ERR_OVERFLOW = 4
+RTD_ERR_NOT_CONVERGED = 5
+RTD_ERR_TIMEOUT = 6
+RTD_ERR_UNSUPPORTED = 7
+RTD_ERR_NO_DEVICE = 8
+
+RADIUS_SAMPLED_NN = 0
+RADIUS_SAMPLED_PERCENTILE = 1
+RADIUS_FIXED = 2
+RADIUS_SAMPLED_MAX = 3
+
+EMPTY_ID = 0xFFFFFFFF
+
+
+class RtdError(RuntimeError):
+    """A C-ABI call returned a status other than RTD_OK."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_status_name(status)}: {message}")
+        self.status = status
+
+
+class Schedule(C.Structure):
+    """rtd_schedule: gprt-ir Schedule (gprt-ir/src/lib.rs:58-89) re-expressed."""
+    _fields_ = [
+        ("radius_increment_mult", C.c_float),
+        ("max_rounds", C.c_uint32),
+        ("radius_heuristic", C.c_int32),
+        ("radius_param", C.c_float),
+        ("use_morton_lbv", C.c_uint32),
+        ("leaf_size", C.c_uint32),
+        ("block_size", C.c_uint32),
+        ("lanes_per_query", C.c_uint32),
+        ("morton_bits", C.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class IndexInfo(C.Structure):
+    _fields_ = [
+        ("n_points", C.c_uint64),
+        ("n_internal", C.c_uint64),
+        ("leaf_size", C.c_uint32),
+        ("morton_bits", C.c_uint32),
+        ("lo", C.c_float * 3),
+        ("hi", C.c_float * 3),
+    ]
+
+
+_P = C.c_void_p
+_U64 = C.c_uint64
+_U32 = C.c_uint32
+_F = C.c_float
+_I = C.c_int
+
+# name -> (restype, argtypes); mirrors include/rtdsl.h
+_SIGNATURES = {
+    "rtd_schedule_default": (None, [C.POINTER(Schedule)]),
+    "rtd_status_string": (C.c_char_p, [_I]),
+    "rtd_last_error": (C.c_char_p, []),
+    "rtd_version": (_I, []),
+    "rtd_index_create": (_I, [C.POINTER(_P)]),
+    "rtd_index_destroy": (_I, [_P]),
+    "rtd_index_build": (_I, [_P, _P, _U64, C.POINTER(Schedule), _P]),
+    "rtd_index_info_get": (_I, [_P, C.POINTER(IndexInfo), _P]),
+    "rtd_knn": (_I, [_P, _P, _U64, _U32, C.POINTER(Schedule), _P, _P, _P]),
+    "rtd_context_create": (_I, [C.POINTER(_P)]),
+    "rtd_context_destroy": (_I, [_P]),
+    "rtd_k_nn_host": (_I, [_P, _P, _U64, _P, _U64, _U32, C.POINTER(Schedule), _P, _P]),
+    "rtd_range_count": (_I, [_P, _P, _U64, _F, C.POINTER(Schedule), _P, C.POINTER(_U64), _P]),
+    "rtd_range_fill": (_I, [_P, _P, _U64, _F, C.POINTER(Schedule), _P, _U64, _I,
+                            C.POINTER(_U64), _P]),
+    "rtd_range_query_host": (_I, [_P, _P, _U64, _P, _U64, _F, _P, _U64, C.POINTER(_U64)]),
+    "rtd_knn_backward": (_I, [_P, _U64, _P, _U64, _U32, _P, _P, _P, _P, _P]),
+    "rtd_index_profile_enable": (_I, [_P, _I]),
+    "rtd_index_profile_get": (_I, [_P, _P]),
+    "rtd_launch_count": (_U64, []),
+}
+
+
+class Profile(C.Structure):
+    _fields_ = [("build_sort_ms", C.c_float), ("build_tree_ms", C.c_float),
+                ("seed_ms", C.c_float), ("order_ms", C.c_float), ("search_ms", C.c_float)]
+
+    def as_dict(self) -> dict:
+        return {name: float(getattr(self, name)) for name, _ in self._fields_}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def _status_name(s: int) -> str:
+    names = {0: "RTD_OK", 1: "RTD_ERR_INVALID_ARGUMENT", 2: "RTD_ERR_CUDA",
+             3: "RTD_ERR_OUT_OF_MEMORY", 4: "RTD_ERR_OVERFLOW", 5: "RTD_ERR_NOT_CONVERGED",
+             6: "RTD_ERR_TIMEOUT", 7: "RTD_ERR_UNSUPPORTED", 8: "RTD_ERR_NO_DEVICE"}
+    return names.get(s, f"status {s}")
+
+
+def declared_symbols() -> list[str]:
+    return list(_SIGNATURES)
+
+
+def load(build_if_missing: bool = True) -> C.CDLL:
+    """Load librtdsl.so, building it first if it is missing or stale."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        path = _build.LIB_PATH
+        if build_if_missing and _build.is_stale():
+            _build.build()
+        if not os.path.exists(path):
+            raise ImportError(f"librtdsl.so not found at {path}; run rtdsl._build.build()")
+        lib = C.CDLL(path, mode=C.RTLD_GLOBAL)
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def check(status: int) -> None:
+    if status != RTD_OK:
+        msg = load().rtd_last_error().decode(errors="replace")
+        raise RtdError(status, msg)
+
+
+def default_schedule(**overrides) -> Schedule:
+    s = Schedule()
+    load().rtd_schedule_default(C.byref(s))
+    for k, v in overrides.items():
+        if not hasattr(s, k):
+            raise AttributeError(f"unknown schedule field {k}")
+        setattr(s, k, v)
+    return s

@@ -1,0 +1,234 @@
+"""Host-side mirror of the reference's search API over the C ABI.
+
+``k_nn`` / ``range_query`` / ``barnes_hut`` keep the argument meaning of the
+reference macros (gprt-macros/src/lib.rs:408 ``k_nn!(data, queries, k, out
+[, schedule])``, README ``range_query!``, lib.rs:752 ``barnes_hut!(bodies,
+theta, G, out)``): data and queries are Vec3 arrays (N x 3 float32), k_nn
+returns one id list per query sorted by distance.  ``Index`` is the
+device-tensor interface (torch CUDA tensors in, torch CUDA tensors out, on
+the current stream).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+from ._capi import EMPTY_ID, RtdError, Schedule, check, default_schedule, load
+
+
+def _as_vec3(a, name: str) -> np.ndarray:
+    arr = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+    if arr.ndim != 2 or arr.shape[1] != 3:
+        raise ValueError(f"{name} must be an (N, 3) array of Vec3, got shape {arr.shape}")
+    return arr
+
+
+def _ptr(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data) if a.size else None
+
+
+class Context:
+    """rtd_context: device staging buffers + a stream for host-buffer calls."""
+
+    def __init__(self):
+        self._lib = load()
+        h = C.c_void_p()
+        check(self._lib.rtd_context_create(C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.rtd_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def k_nn(self, data, queries, k: int, schedule: Schedule | None = None,
+             with_d2: bool = False, out_ids: np.ndarray | None = None,
+             out_d2: np.ndarray | None = None):
+        data = _as_vec3(data, "data")
+        queries = _as_vec3(queries, "queries")
+        nq = queries.shape[0]
+        ids = out_ids if out_ids is not None else np.empty((nq, k), dtype=np.uint32)
+        d2 = out_d2 if out_d2 is not None else (np.empty((nq, k), dtype=np.float32) if with_d2 else None)
+        s = schedule if schedule is not None else default_schedule()
+        check(self._lib.rtd_k_nn_host(self._h, _ptr(data), data.shape[0], _ptr(queries), nq, k,
+                                      C.byref(s), _ptr(ids), _ptr(d2) if d2 is not None else None))
+        return (ids, d2) if with_d2 else ids
+
+    def range_query(self, data, queries, radius: float, capacity: int | None = None) -> np.ndarray:
+        data = _as_vec3(data, "data")
+        queries = _as_vec3(queries, "queries")
+        n_pairs = C.c_uint64(0)
+        if capacity is None:
+            # size by a first call with no room, as the count pass reports it
+            st = self._lib.rtd_range_query_host(self._h, _ptr(data), data.shape[0], _ptr(queries),
+                                                queries.shape[0], C.c_float(radius), None, 0,
+                                                C.byref(n_pairs))
+            if st not in (_capi.RTD_OK, _capi.RTD_ERR_OVERFLOW):
+                check(st)
+            capacity = n_pairs.value
+        pairs = np.empty((max(capacity, 1), 2), dtype=np.uint32)
+        check(self._lib.rtd_range_query_host(self._h, _ptr(data), data.shape[0], _ptr(queries),
+                                             queries.shape[0], C.c_float(radius), _ptr(pairs),
+                                             capacity, C.byref(n_pairs)))
+        return pairs[: n_pairs.value]
+
+
+_ctx: Context | None = None
+
+
+def _context() -> Context:
+    global _ctx
+    if _ctx is None:
+        _ctx = Context()
+    return _ctx
+
+
+def k_nn(data, queries, k: int, schedule: Schedule | None = None) -> list[list[int]]:
+    """k_nn!(data, queries, k, out[, schedule]): per query, its k nearest
+    point ids sorted by distance (ties to the lower id).  Slots past the
+    number of points are dropped, as a Vec<Vec<u32>> would be shorter."""
+    ids = _context().k_nn(data, queries, k, schedule)
+    return [[int(v) for v in row if v != EMPTY_ID] for row in ids]
+
+
+def k_nn_array(data, queries, k: int, schedule: Schedule | None = None, with_d2: bool = True):
+    """Array form of k_nn: ids [Q, k] uint32 (EMPTY_ID padded), d2 [Q, k]."""
+    return _context().k_nn(data, queries, k, schedule, with_d2=with_d2)
+
+
+def range_query(data, queries, radius: float) -> np.ndarray:
+    """range_query!(data, queries, r, out): (query, id) uint32 pairs of every
+    point within r of every query, sorted by (query, id)."""
+    return _context().range_query(data, queries, radius)
+
+
+# --------------------------------------------------------------- devices
+def _stream_handle(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _check_points_tensor(t, name: str):
+    import torch
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA tensor")
+    if t.dtype != torch.float32 or t.dim() != 2 or t.shape[1] != 3 or not t.is_contiguous():
+        raise ValueError(f"{name} must be a contiguous float32 (N, 3) tensor")
+
+
+class Index:
+    """rtd_index over a CUDA tensor of points (N x 3 float32)."""
+
+    def __init__(self):
+        self._lib = load()
+        h = C.c_void_p()
+        check(self._lib.rtd_index_create(C.byref(h)))
+        self._h = h
+        self.points = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.rtd_index_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def build(self, points, schedule: Schedule | None = None, stream=None) -> "Index":
+        _check_points_tensor(points, "points")
+        s = schedule if schedule is not None else default_schedule()
+        check(self._lib.rtd_index_build(self._h, C.c_void_p(points.data_ptr()), points.shape[0],
+                                        C.byref(s), _stream_handle(stream)))
+        self.points = points
+        return self
+
+    def profile(self, enable: bool = True) -> "Index":
+        check(self._lib.rtd_index_profile_enable(self._h, int(enable)))
+        return self
+
+    def timings(self) -> dict:
+        """Phase times (ms) of the last build and search, from CUDA events."""
+        p = _capi.Profile()
+        check(self._lib.rtd_index_profile_get(self._h, C.byref(p)))
+        return p.as_dict()
+
+    def info(self, stream=None) -> dict:
+        inf = _capi.IndexInfo()
+        check(self._lib.rtd_index_info_get(self._h, C.byref(inf), _stream_handle(stream)))
+        return {"n_points": inf.n_points, "n_internal": inf.n_internal,
+                "leaf_size": inf.leaf_size, "morton_bits": inf.morton_bits,
+                "lo": list(inf.lo), "hi": list(inf.hi)}
+
+    def knn(self, queries, k: int, schedule: Schedule | None = None, with_d2: bool = True,
+            out_ids=None, out_d2=None, stream=None):
+        import torch
+        _check_points_tensor(queries, "queries")
+        nq = queries.shape[0]
+        dev = queries.device
+        ids = out_ids if out_ids is not None else torch.empty((nq, k), dtype=torch.int32, device=dev)
+        d2 = out_d2 if out_d2 is not None else (
+            torch.empty((nq, k), dtype=torch.float32, device=dev) if with_d2 else None)
+        s = schedule if schedule is not None else default_schedule()
+        check(self._lib.rtd_knn(self._h, C.c_void_p(queries.data_ptr()), nq, k, C.byref(s),
+                                C.c_void_p(ids.data_ptr()),
+                                C.c_void_p(d2.data_ptr()) if d2 is not None else None,
+                                _stream_handle(stream)))
+        return ids, d2
+
+    def range_count(self, queries, radius: float, schedule: Schedule | None = None,
+                    out_counts=None, stream=None):
+        import torch
+        _check_points_tensor(queries, "queries")
+        nq = queries.shape[0]
+        counts = out_counts if out_counts is not None else torch.empty(
+            (nq,), dtype=torch.int32, device=queries.device)
+        total = C.c_uint64(0)
+        s = schedule if schedule is not None else default_schedule()
+        check(self._lib.rtd_range_count(self._h, C.c_void_p(queries.data_ptr()), nq,
+                                        C.c_float(radius), C.byref(s),
+                                        C.c_void_p(counts.data_ptr()), C.byref(total),
+                                        _stream_handle(stream)))
+        return counts, total.value
+
+    def range_fill(self, queries, radius: float, capacity: int, sort_pairs: bool = False,
+                   schedule: Schedule | None = None, out_pairs=None, stream=None):
+        import torch
+        _check_points_tensor(queries, "queries")
+        pairs = out_pairs if out_pairs is not None else torch.empty(
+            (max(capacity, 1), 2), dtype=torch.int32, device=queries.device)
+        written = C.c_uint64(0)
+        s = schedule if schedule is not None else default_schedule()
+        check(self._lib.rtd_range_fill(self._h, C.c_void_p(queries.data_ptr()), queries.shape[0],
+                                       C.c_float(radius), C.byref(s),
+                                       C.c_void_p(pairs.data_ptr()), capacity, int(sort_pairs),
+                                       C.byref(written), _stream_handle(stream)))
+        return pairs[: written.value]
+
+
+def knn_backward(queries, points, ids, grad_d2, grad_q=None, grad_p=None, stream=None):
+    """dL/dq (overwritten) and dL/dp (accumulated) for d2 = |q - p_id|^2."""
+    import torch
+    lib = load()
+    nq, k = ids.shape
+    if grad_q is None:
+        grad_q = torch.empty_like(queries)
+    if grad_p is None:
+        grad_p = torch.zeros_like(points)
+    check(lib.rtd_knn_backward(C.c_void_p(queries.data_ptr()), nq, C.c_void_p(points.data_ptr()),
+                               points.shape[0], k, C.c_void_p(ids.data_ptr()),
+                               C.c_void_p(grad_d2.contiguous().data_ptr()),
+                               C.c_void_p(grad_q.data_ptr()), C.c_void_p(grad_p.data_ptr()),
+                               _stream_handle(stream)))
+    return grad_q, grad_p

@@ -1,0 +1,198 @@
+"""k-NN parity: the CUDA path (through the C ABI) against the CPU oracle.
+Neighbour ids must match bit-exactly (FP32 key, ties to the lower id) and the
+returned squared distances must equal the oracle's FP32 keys bit-for-bit."""
+import numpy as np
+import pytest
+import torch
+
+from rtdsl import workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_knn(rtd, pts, q, k, **sched):
+    s = rtd.default_schedule(**sched)
+    ix = rtd.Index().build(torch.from_numpy(np.ascontiguousarray(pts)).cuda(), s)
+    ids, d2 = ix.knn(torch.from_numpy(np.ascontiguousarray(q)).cuda(), k, s)
+    torch.cuda.synchronize()
+    info = ix.info()
+    return ids.cpu().numpy().view(np.uint32), d2.cpu().numpy(), info
+
+
+def assert_same(orc_ids, orc_d2, ids, d2):
+    bad = np.nonzero(np.any(orc_ids != ids, axis=1))[0]
+    assert len(bad) == 0, (f"{len(bad)} queries differ; first {bad[:5]}: "
+                           f"oracle {orc_ids[bad[:2]]} gpu {ids[bad[:2]]}")
+    np.testing.assert_array_equal(orc_d2.view(np.uint32), d2.view(np.uint32))
+
+
+def clustered_small(n=30_000, nq=3_000, seed=11):
+    return workloads.clustered(n=n, nq=nq, seed=seed, n_clusters=12, box=10.0)
+
+
+def test_plain_knn_small_config(rtd, orc, cuda):
+    """100,000 uniform points, 10,000 jittered queries, k = 5: the CPU-runnable
+    workload, checked exhaustively."""
+    pts, q = workloads.plain_knn_small()
+    ids, d2, info = gpu_knn(rtd, pts, q, 5)
+    oi, od = orc.knn(pts, q, 5)
+    assert_same(oi, od, ids, d2)
+    assert info["n_points"] == len(pts)
+    assert orc.knn_fp64_ambiguity(pts, q[:2000], ids[:2000]) <= 2
+
+
+@pytest.mark.parametrize("k", [1, 2, 5, 8, 16, 32])
+@pytest.mark.parametrize("lanes", [1, 32])
+def test_knn_k_and_lanes(rtd, orc, cuda, k, lanes):
+    pts, q = clustered_small()
+    ids, d2, _ = gpu_knn(rtd, pts, q, k, lanes_per_query=lanes)
+    oi, od = orc.knn(pts, q, k)
+    assert_same(oi, od, ids, d2)
+
+
+@pytest.mark.parametrize("k", [33, 64, 100, 256])
+def test_knn_large_k_warp_list(rtd, orc, cuda, k):
+    pts, q = clustered_small(n=20_000, nq=1_000, seed=12)
+    ids, d2, _ = gpu_knn(rtd, pts, q, k)
+    oi, od = orc.knn(pts, q, k)
+    assert_same(oi, od, ids, d2)
+
+
+@pytest.mark.parametrize("leaf", [1, 2, 4, 8, 16, 32, 64])
+@pytest.mark.parametrize("bits", [30, 63])
+def test_knn_leaf_and_key_width(rtd, orc, cuda, leaf, bits):
+    pts, q = clustered_small(n=25_000, nq=2_000, seed=13)
+    ids, d2, info = gpu_knn(rtd, pts, q, 5, leaf_size=leaf, morton_bits=bits)
+    oi, od = orc.knn(pts, q, 5)
+    assert_same(oi, od, ids, d2)
+    assert info["morton_bits"] == bits
+
+
+@pytest.mark.parametrize("heur,param", [(0, 2 ** -4), (1, 0.10), (1, 0.02), (2, 1e-6),
+                                        (2, 100.0), (3, 0.0)])
+def test_knn_radius_heuristics_do_not_change_results(rtd, orc, cuda, heur, param):
+    pts, q = clustered_small(n=20_000, nq=2_000, seed=14)
+    ids, d2, _ = gpu_knn(rtd, pts, q, 8, radius_heuristic=heur, radius_param=param)
+    oi, od = orc.knn(pts, q, 8)
+    assert_same(oi, od, ids, d2)
+
+
+@pytest.mark.parametrize("mult,rounds", [(2.0, 1), (2.0, 2), (1.05, 32), (3.0, 30), (64.0, 4)])
+def test_knn_round_schedules(rtd, orc, cuda, mult, rounds):
+    pts, q = clustered_small(n=20_000, nq=2_000, seed=15)
+    ids, d2, _ = gpu_knn(rtd, pts, q, 5, radius_increment_mult=mult, max_rounds=rounds)
+    oi, od = orc.knn(pts, q, 5)
+    assert_same(oi, od, ids, d2)
+
+
+def test_knn_unsorted_queries(rtd, orc, cuda):
+    pts, q = clustered_small(n=20_000, nq=2_000, seed=16)
+    ids, d2, _ = gpu_knn(rtd, pts, q, 5, use_morton_lbv=0)
+    oi, od = orc.knn(pts, q, 5)
+    assert_same(oi, od, ids, d2)
+
+
+def test_knn_duplicates_and_ties(rtd, orc, cuda):
+    rng = np.random.default_rng(3)
+    base = rng.integers(0, 8, size=(500, 3)).astype(np.float32)   # integer lattice: many ties
+    pts = np.concatenate([base, base, base[:100]])
+    q = np.concatenate([base[:200], rng.integers(0, 8, size=(200, 3)).astype(np.float32) + 0.5])
+    for k in (1, 5, 16, 40):
+        for lanes in (1, 32):
+            if lanes == 1 and k > 32:
+                continue
+            ids, d2, _ = gpu_knn(rtd, pts, q, k, lanes_per_query=lanes)
+            oi, od = orc.knn(pts, q, k)
+            assert_same(oi, od, ids, d2)
+
+
+def test_knn_all_points_identical(rtd, orc, cuda):
+    pts = np.full((5000, 3), 0.25, dtype=np.float32)
+    q = np.array([[0.25, 0.25, 0.25], [1.0, 2.0, 3.0], [-5.0, 0.0, 0.0]], dtype=np.float32)
+    ids, d2, _ = gpu_knn(rtd, pts, q, 7)
+    oi, od = orc.knn(pts, q, 7)
+    assert_same(oi, od, ids, d2)
+    assert ids[0].tolist() == list(range(7))
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 7])
+def test_knn_fewer_points_than_k(rtd, orc, cuda, n):
+    rng = np.random.default_rng(n)
+    pts = rng.random((n, 3)).astype(np.float32)
+    q = rng.random((50, 3)).astype(np.float32)
+    for lanes in (1, 32):
+        ids, d2, _ = gpu_knn(rtd, pts, q, 8, lanes_per_query=lanes)
+        oi, od = orc.knn(pts, q, 8)
+        assert_same(oi, od, ids, d2)
+        assert np.all(ids[:, n:] == 0xFFFFFFFF) and np.all(np.isinf(d2[:, n:]))
+
+
+def test_knn_empty_inputs(rtd, cuda):
+    s = rtd.default_schedule()
+    ix = rtd.Index().build(torch.zeros((0, 3), device="cuda"), s)
+    ids, d2 = ix.knn(torch.rand((10, 3), device="cuda"), 4, s)
+    torch.cuda.synchronize()
+    assert np.all(ids.cpu().numpy().view(np.uint32) == 0xFFFFFFFF)
+    ix2 = rtd.Index().build(torch.rand((100, 3), device="cuda"), s)
+    ids2, _ = ix2.knn(torch.zeros((0, 3), device="cuda"), 4, s)
+    assert ids2.shape == (0, 4)
+
+
+def test_knn_non_finite(rtd, orc, cuda):
+    rng = np.random.default_rng(9)
+    pts = rng.random((3000, 3)).astype(np.float32)
+    pts[10] = [np.nan, 0.5, 0.5]
+    pts[20] = [np.inf, 0.5, 0.5]
+    pts[30] = [0.5, -np.inf, 0.5]
+    q = rng.random((300, 3)).astype(np.float32)
+    q[0] = [np.nan, 0.1, 0.1]
+    q[1] = [np.inf, 0.1, 0.1]
+    q[2] = [1e30, 1e30, 1e30]
+    for lanes in (1, 32):
+        ids, d2, _ = gpu_knn(rtd, pts, q, 6, lanes_per_query=lanes)
+        oi, od = orc.knn(pts, q, 6)
+        assert_same(oi, od, ids, d2)
+        assert np.all(ids[0] == 0xFFFFFFFF)
+
+
+def test_knn_far_queries_and_large_coordinates(rtd, orc, cuda):
+    rng = np.random.default_rng(10)
+    pts = (rng.random((4000, 3)) * 1e6).astype(np.float32)
+    q = np.concatenate([(rng.random((200, 3)) * 1e6), rng.normal(0, 1e8, (50, 3))]).astype(np.float32)
+    ids, d2, _ = gpu_knn(rtd, pts, q, 5)
+    oi, od = orc.knn(pts, q, 5)
+    assert_same(oi, od, ids, d2)
+
+
+def test_knn_host_api_k_nn(rtd, orc, cuda):
+    pts, q = clustered_small(n=10_000, nq=500, seed=17)
+    out = rtd.k_nn(pts, q, 5)
+    oi, _ = orc.knn(pts, q, 5)
+    assert out == oi.astype(np.int64).tolist()
+    few = rtd.k_nn(pts[:3], q[:4], 5)
+    assert all(len(r) == 3 for r in few)
+
+
+def test_knn_deterministic_and_reusable_index(rtd, cuda):
+    pts, q = clustered_small(n=20_000, nq=2_000, seed=18)
+    s = rtd.default_schedule()
+    ix = rtd.Index().build(torch.from_numpy(pts).cuda(), s)
+    qt = torch.from_numpy(q).cuda()
+    a, _ = ix.knn(qt, 8, s)
+    b, _ = ix.knn(qt, 8, s)
+    c, _ = ix.knn(qt[:100], 8, s)
+    torch.cuda.synchronize()
+    assert torch.equal(a, b) and torch.equal(a[:100], c)
+
+
+@pytest.mark.slow
+def test_knn_clustered_1p8m_sampled(rtd, orc, cuda):
+    """The 1.8M-point / 400K-query workload: all 400K queries on the GPU,
+    2,000 of them against the oracle; every result sorted and in range."""
+    pts, q = workloads.clustered()
+    ids, d2, _ = gpu_knn(rtd, pts, q, 5)
+    sel = np.random.default_rng(0).choice(len(q), 2000, replace=False)
+    oi, od = orc.knn(pts, q[sel], 5)
+    assert_same(oi, od, ids[sel], d2[sel])
+    assert np.all(ids < len(pts))
+    assert np.all(np.diff(d2, axis=1) >= 0)

@@ -1,0 +1,93 @@
+"""Range-query parity: counts and (query, id) pairs from the CUDA count/fill
+passes against the oracle, bit-exact membership (FP32 key <= RN(r*r))."""
+import numpy as np
+import pytest
+import torch
+
+from rtdsl import workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_range(rtd, pts, q, r, sort=True, **sched):
+    s = rtd.default_schedule(**sched)
+    ix = rtd.Index().build(torch.from_numpy(np.ascontiguousarray(pts)).cuda(), s)
+    qt = torch.from_numpy(np.ascontiguousarray(q)).cuda()
+    counts, total = ix.range_count(qt, r, s)
+    pairs = ix.range_fill(qt, r, total, sort_pairs=sort, schedule=s)
+    torch.cuda.synchronize()
+    return counts.cpu().numpy().view(np.uint32), total, pairs.cpu().numpy().view(np.uint32)
+
+
+@pytest.mark.parametrize("leaf", [1, 4, 16, 64])
+def test_range_clustered_sorted(rtd, orc, cuda, leaf):
+    pts, q = workloads.clustered(n=30_000, nq=3_000, seed=21, n_clusters=10, box=10.0)
+    r = 0.08
+    counts, total, pairs = gpu_range(rtd, pts, q, r, leaf_size=leaf)
+    oc, ot = orc.range_count(pts, q, r)
+    np.testing.assert_array_equal(counts, oc)
+    assert total == ot
+    np.testing.assert_array_equal(pairs, orc.range_pairs(pts, q, r))
+
+
+def test_range_unsorted_is_same_set(rtd, orc, cuda):
+    pts, q = workloads.clustered(n=30_000, nq=2_000, seed=22, n_clusters=10, box=10.0)
+    r = 0.2   # heavy output: exercises the staging-buffer overflow path
+    counts, total, pairs = gpu_range(rtd, pts, q, r, sort=False)
+    ref = orc.range_pairs(pts, q, r)
+    assert total == len(ref) == len(pairs)
+    key = lambda a: np.sort(a[:, 0].astype(np.uint64) << np.uint64(32) | a[:, 1].astype(np.uint64))
+    np.testing.assert_array_equal(key(pairs), key(ref))
+
+
+def test_range_radius_zero_and_duplicates(rtd, orc, cuda):
+    rng = np.random.default_rng(4)
+    base = rng.random((300, 3)).astype(np.float32)
+    pts = np.concatenate([base, base[:100]])
+    q = np.concatenate([base[:50], rng.random((50, 3)).astype(np.float32)])
+    counts, total, pairs = gpu_range(rtd, pts, q, 0.0)
+    np.testing.assert_array_equal(pairs, orc.range_pairs(pts, q, 0.0))
+    assert np.all(counts[:50] == 2) and np.all(counts[50:] == 0)
+
+
+def test_range_empty_inputs(rtd, cuda):
+    counts, total, pairs = gpu_range(rtd, np.zeros((0, 3), np.float32),
+                                     np.random.rand(20, 3).astype(np.float32), 1.0)
+    assert total == 0 and np.all(counts == 0) and len(pairs) == 0
+
+
+def test_range_overflow_reports_required_size(rtd, cuda):
+    pts, q = workloads.clustered(n=5_000, nq=500, seed=23, n_clusters=4, box=2.0)
+    s = rtd.default_schedule()
+    ix = rtd.Index().build(torch.from_numpy(pts).cuda(), s)
+    qt = torch.from_numpy(q).cuda()
+    _, total = ix.range_count(qt, 0.3, s)
+    assert total > 10
+    with pytest.raises(rtd.RtdError) as e:
+        ix.range_fill(qt, 0.3, total // 2, schedule=s)
+    assert e.value.status == 4
+    # the index stays usable afterwards
+    pairs = ix.range_fill(qt, 0.3, total, sort_pairs=True, schedule=s)
+    assert len(pairs) == total
+
+
+def test_range_host_api(rtd, orc, cuda):
+    pts, q = workloads.clustered(n=8_000, nq=400, seed=24, n_clusters=4, box=5.0)
+    pairs = rtd.range_query(pts, q, 0.15)
+    np.testing.assert_array_equal(pairs, orc.range_pairs(pts, q, 0.15))
+
+
+@pytest.mark.slow
+def test_range_large_property(rtd, orc, cuda):
+    """400K queries on 1.8M points: the count pass and the fill agree
+    (sum of counts = pairs written, per-query histogram of the pairs equals
+    the counts), and a query sample matches the oracle exactly."""
+    pts, q = workloads.clustered()
+    r = 0.35
+    counts, total, pairs = gpu_range(rtd, pts, q, r)
+    assert counts.sum() == total == len(pairs)
+    np.testing.assert_array_equal(np.bincount(pairs[:, 0], minlength=len(q)), counts)
+    assert np.all(np.diff(pairs[:, 0].astype(np.int64)) >= 0)
+    sel = np.arange(0, len(q), 997)[:300]
+    oc, _ = orc.range_count(pts, q[sel], r)
+    np.testing.assert_array_equal(counts[sel], oc)
