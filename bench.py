@@ -136,13 +136,8 @@ def load_workload():
 def tuned_schedule(rtd):
     """Launch knobs for the headline workload from the autotuner cache if
     present, else the defaults."""
-    s = rtd.default_schedule()
-    try:
-        from rtdsl import autotune
-        s = autotune.cached_schedule("clustered_1p8m_k5", s)
-    except Exception:
-        pass
-    return s
+    from rtdsl import autotune
+    return autotune.cached_schedule("clustered_1p8m_k5", rtd.default_schedule())
 
 
 # ---------------------------------------------------------------- ours

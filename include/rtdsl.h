@@ -76,7 +76,15 @@ typedef struct rtd_schedule {
     uint32_t block_size;          /* threads per block of the search kernel (0 = auto) */
     uint32_t lanes_per_query;     /* 1 = thread per query, 32 = warp per query (0 = auto) */
     uint32_t morton_bits;         /* 30 (u32 keys) or 63 (u64 keys); 0 = auto */
+    uint32_t packet_traversal;    /* thread-per-query kernels: 32 Morton-adjacent queries
+                                     share one traversal (rtd_packet_mode) */
 } rtd_schedule;
+
+typedef enum rtd_packet_mode {
+    RTD_PACKET_AUTO = 0,   /* currently: off (per-thread traversal measured faster) */
+    RTD_PACKET_ON = 1,
+    RTD_PACKET_OFF = 2
+} rtd_packet_mode;
 
 /* Defaults: M = 2, 32 rounds, sampled-NN seed x 2^-4, Morton query order,
  * leaf 4, auto launch shape, auto key width. */
@@ -185,6 +193,76 @@ rtd_status rtd_knn_backward(const float *d_queries, uint64_t nq, const float *d_
                             uint64_t n, uint32_t k, const uint32_t *d_ids,
                             const float *d_grad_d2, float *d_grad_q, float *d_grad_p,
                             rtd_stream stream);
+
+/* ---------------------------------------------------------------------
+ * Barnes-Hut gravity.  Replaces barnes_hut! (gprt-macros/src/lib.rs:
+ * 752-834): the CPU BarnesHutTree::build (gprt-core/src/lib.rs:427-539)
+ * becomes a GPU build of the same tree, and gprt_execute_autorope_soa_ffi
+ * (gprt-optix/host/main.cpp:371-415) becomes the walk kernels.
+ * ------------------------------------------------------------------- */
+typedef enum rtd_bh_law {
+    /* The reference law and MAC (gprt-macros/src/lib.rs:760-806): per-body
+     * stackless walk, a node is accepted when width < max(1e-6, theta*d) +
+     * 1e-5; leaves are summed directly, accepted cells as monopoles; force
+     * G*mi*mj*delta/(r2*sqrt(r2+1e-6)), skipped when r2 <= 1e-10.  Output:
+     * forces (n*3). */
+    RTD_BH_LAW_REFERENCE = 0,
+    /* Plummer-softened gravity: phi_i = -G sum_j m_j/sqrt(r2+eps^2),
+     * a_i = -grad phi_i; monopole + traceless quadrupole about the COM;
+     * warp-coherent walk of 32 consecutive bodies with the group MAC
+     * width^2 < theta^2 * dist^2(com, group box).  Output: accelerations
+     * (n*3) and potentials (n). */
+    RTD_BH_LAW_PLUMMER = 1
+} rtd_bh_law;
+
+typedef struct rtd_bh_params {
+    float theta;
+    float G;
+    float eps;            /* Plummer softening length */
+    int32_t law;          /* rtd_bh_law */
+    int32_t quadrupole;   /* Plummer law: 1 = monopole + quadrupole, 0 = monopole */
+    uint32_t bucket;      /* leaf bucket size; reference BUCKET_SIZE = 128 (lib.rs:275) */
+    float min_width;      /* reference MIN_SPLIT_SIZE = 1e-5 (lib.rs:276) */
+} rtd_bh_params;
+
+/* theta 0.5, G 6.674e-11, eps 1e-3, reference law, quadrupole on,
+ * bucket 128, min_width 1e-5. */
+void rtd_bh_params_default(rtd_bh_params *p);
+
+typedef struct rtd_bh rtd_bh;
+rtd_status rtd_bh_create(rtd_bh **out);
+rtd_status rtd_bh_destroy(rtd_bh *b);
+/* Builds the octree over n bodies (d_pos n*3, d_mass n, device).  The tree
+ * holds its own copy of the bodies in flat (leaf) order. */
+rtd_status rtd_bh_build(rtd_bh *b, const float *d_pos, const float *d_mass, uint64_t n,
+                        const rtd_bh_params *p, rtd_stream stream);
+/* Frees the tree (keeps the handle); a backward then needs a new build. */
+rtd_status rtd_bh_release(rtd_bh *b);
+/* Walk over the built tree.  Reference law: d_out = forces, d_phi unused.
+ * Plummer law: d_out = accelerations, d_phi = potentials (may be NULL).
+ * Outputs are in the caller's body order. */
+rtd_status rtd_bh_forward(rtd_bh *b, const rtd_bh_params *p, float *d_out, float *d_phi,
+                          rtd_stream stream);
+/* Adjoint of the Plummer-law walk (same tree, same decisions): given
+ * dL/da (n*3) and dL/dphi (n, may be NULL = 0), writes dL/dpos (n*3) and
+ * dL/dmass (n).  No reference counterpart (the reference has no gradients). */
+rtd_status rtd_bh_backward(rtd_bh *b, const rtd_bh_params *p, const float *d_g_acc,
+                           const float *d_g_phi, float *d_g_pos, float *d_g_mass,
+                           rtd_stream stream);
+typedef struct rtd_bh_info {
+    uint64_t n_bodies, n_nodes, n_leaves;
+    uint32_t depth;          /* deepest level (root = 0) */
+    float root_min[3], root_max[3];
+} rtd_bh_info;
+rtd_status rtd_bh_info_get(rtd_bh *b, rtd_bh_info *info, rtd_stream stream);
+/* Host copies of the tree in the reference's FlatNode layout
+ * (gprt-core/src/lib.rs:299-308, 40 B per node) and the flat body order
+ * (order[i] = caller index of the i-th flat body).  Synchronises. */
+rtd_status rtd_bh_export(rtd_bh *b, void *h_flat_nodes, uint32_t *h_order, rtd_stream stream);
+/* Host-buffer barnes_hut!(bodies, theta, G, out) with the reference law;
+ * bodies with mass <= 0 are kept (the CLI loader drops them). */
+rtd_status rtd_barnes_hut_host(rtd_context *ctx, const rtd_body *bodies, uint64_t n, float theta,
+                               float G, rtd_vec3 *out_forces);
 
 #ifdef __cplusplus
 }

@@ -83,6 +83,13 @@ def lib() -> C.CDLL:
             L.orc_direct_ref_f64.argtypes = [P, P, I64, P, I64, C.c_double, P]
             L.orc_key_public.argtypes = [P, P]
             L.orc_key_public.restype = F
+            L.orc_bh_group_lists.argtypes = [P, I64, P, I64, C.c_int, F, P, P, I64]
+            L.orc_bh_group_lists.restype = I64
+            L.orc_bh_plummer_eval.argtypes = [P, I64, P, P, I64, C.c_int, P, P, C.c_double,
+                                              C.c_double, C.c_int, P, P]
+            L.orc_bh_plummer_eval.restype = C.c_double
+            L.orc_direct_plummer_f64.argtypes = [P, P, I64, C.c_double, C.c_double, P, P, P, P]
+            L.orc_direct_plummer_f64.restype = C.c_double
             _lib = L
     return _lib
 
@@ -214,3 +221,60 @@ def direct_ref_f64(pos, mass, targets, G: float = 6.674e-11) -> np.ndarray:
     out = np.empty((len(t), 3), dtype=np.float64)
     lib().orc_direct_ref_f64(_p(pos), _p(mass), len(pos), _p(t), len(t), C.c_double(G), _p(out))
     return out
+
+
+class PlummerFrozen:
+    """Plummer-law BH with the group decisions of one configuration frozen
+    (reference tree of `bucket`, groups of 32 flat bodies, FP32 decisions as
+    the GPU makes them), evaluated in FP64 for perturbed inputs."""
+
+    def __init__(self, pos, mass, theta: float, bucket: int, group: int = 32,
+                 min_width: float = 1e-5):
+        pos = _f32(pos)
+        mass = _f32(mass)
+        self.nodes, self.order, _ = bh_build(pos, mass, bucket=bucket, min_width=min_width)
+        self.n = len(pos)
+        self.group = group
+        fpos = np.ascontiguousarray(pos[self.order])
+        ng = (self.n + group - 1) // group
+        self.offsets = np.zeros(ng + 1, dtype=np.int64)
+        cap = max(1024, 64 * ng)
+        while True:
+            items = np.empty(cap, dtype=np.int32)
+            tot = lib().orc_bh_group_lists(_p(self.nodes), len(self.nodes), _p(fpos), self.n, group,
+                                           C.c_float(theta), _p(self.offsets), _p(items), cap)
+            if tot >= 0:
+                self.items = items[:tot].copy()
+                break
+            cap = -tot
+        # flat position of each caller index
+        self.flat_of = np.empty(self.n, dtype=np.int64)
+        self.flat_of[self.order] = np.arange(self.n)
+
+    def eval(self, pos, mass, eps: float, G: float, quad: bool = True):
+        """(L, phi [N], acc [N,3]) in FP64, caller order."""
+        p = np.ascontiguousarray(np.asarray(pos, dtype=np.float64)[self.order])
+        m = np.ascontiguousarray(np.asarray(mass, dtype=np.float64)[self.order])
+        phi = np.empty(self.n)
+        acc = np.empty((self.n, 3))
+        L = lib().orc_bh_plummer_eval(_p(self.nodes), len(self.nodes), _p(p), _p(m), self.n,
+                                      self.group, _p(self.offsets), _p(self.items), eps, G,
+                                      int(quad), _p(phi), _p(acc))
+        out_phi = np.empty(self.n)
+        out_acc = np.empty((self.n, 3))
+        out_phi[self.order] = phi
+        out_acc[self.order] = acc
+        return float(L), out_phi, out_acc
+
+
+def direct_plummer_f64(pos, mass, eps: float, G: float, grad: bool = False):
+    """FP64 direct sum: (L, phi, acc[, g_pos, g_mass]) for L = sum phi + 0.5 sum |a|^2."""
+    p = np.ascontiguousarray(np.asarray(pos, dtype=np.float64))
+    m = np.ascontiguousarray(np.asarray(mass, dtype=np.float64))
+    n = len(p)
+    phi = np.empty(n)
+    acc = np.empty((n, 3))
+    gp = np.empty((n, 3)) if grad else None
+    gm = np.empty(n) if grad else None
+    L = lib().orc_direct_plummer_f64(_p(p), _p(m), n, eps, G, _p(phi), _p(acc), _p(gp), _p(gm))
+    return (float(L), phi, acc, gp, gm) if grad else (float(L), phi, acc)

@@ -760,3 +760,218 @@ void orc_direct_ref_f64(const float *pos, const float *mass, int64_t n, const in
         force[3 * t] = sx; force[3 * t + 1] = sy; force[3 * t + 2] = sz;
     }
 }
+
+/* ------------------------------------------------------------------------
+ * Plummer-law Barnes-Hut (the build's physics mode; no reference
+ * counterpart beyond the tree).  The tree is the reference tree built by
+ * orc_bh_build (with its own bucket size).  Groups are 32 consecutive
+ * bodies of the flat order; a node is accepted for a group when
+ *     RN(width*width) < RN(theta2 * d2),  d2 = |gap(COM, group box)|^2
+ * (all FP32, rounded per operation, theta2 = RN(theta*theta)); accepted
+ * nodes interact as monopole (+ traceless quadrupole) multipoles, rejected
+ * leaves by direct summation, rejected internal nodes are opened.
+ * orc_bh_group_lists records these decisions once; orc_bh_plummer_eval
+ * then evaluates phi, a and L = sum(phi) + 0.5*sum|a|^2 in FP64 for any
+ * (perturbed) positions / masses with the decisions and the tree
+ * membership held fixed -- the function whose derivative the GPU adjoint
+ * computes, so central finite differences of it check the adjoint.
+ * ---------------------------------------------------------------------- */
+static float orc_gap(float lo, float hi, float c) {
+    float a = lo - c, b = c - hi;
+    return fmaxf(fmaxf(a, b), 0.0f);
+}
+
+/* items: node index * 2 + (1 if direct leaf sum else 0). Returns the item
+ * count (or -needed when capacity is too small). */
+int64_t orc_bh_group_lists(const orc_flat_node *nodes, int64_t nn, const float *fpos, int64_t n,
+                           int group, float theta, int64_t *offsets, int32_t *items,
+                           int64_t capacity) {
+    const float th2 = theta * theta;
+    int64_t ng = (n + group - 1) / group;
+    int64_t total = 0;
+    offsets[0] = 0;
+    for (int64_t g = 0; g < ng; ++g) {
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int64_t i = g * group; i < (g + 1) * group && i < n; ++i)
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = fminf(lo[a], fpos[3 * i + a]);
+                hi[a] = fmaxf(hi[a], fpos[3 * i + a]);
+            }
+        int64_t p = 0;
+        while (p < nn) {
+            const orc_flat_node *nd = &nodes[p];
+            float tx = orc_gap(lo[0], hi[0], nd->com[0]);
+            float ty = orc_gap(lo[1], hi[1], nd->com[1]);
+            float tz = orc_gap(lo[2], hi[2], nd->com[2]);
+            float d2 = orc_dot3(tx, ty, tz);
+            int accept = nd->width * nd->width < th2 * d2;
+            if (accept) {
+                if (total < capacity) items[total] = (int32_t)(2 * p);
+                ++total;
+                p = nd->autorope;
+            } else if (nd->is_leaf) {
+                if (total < capacity) items[total] = (int32_t)(2 * p + 1);
+                ++total;
+                p = p + 1;
+            } else {
+                p = p + 1;
+            }
+        }
+        offsets[g + 1] = total;
+    }
+    return total <= capacity ? total : -total;
+}
+
+typedef struct { double c[3]; double m; double q[6]; } orc_cell64;
+
+/* FP64 cell moments over each node's flat body range. */
+static void orc_cells64(const orc_flat_node *nodes, int64_t nn, const double *pos,
+                        const double *mass, int64_t n, orc_cell64 *cells) {
+    int64_t *first = (int64_t *)malloc(sizeof(int64_t) * (size_t)(nn + 1));
+    int64_t nxt = n;
+    for (int64_t i = nn - 1; i >= 0; --i) {   /* first body of the subtree */
+        if (nodes[i].is_leaf) nxt = nodes[i].bucket_start;
+        first[i] = nxt;
+    }
+    first[nn] = n;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t i = 0; i < nn; ++i) {
+        int64_t s = first[i];
+        int64_t e = nodes[i].autorope < (uint32_t)nn ? first[nodes[i].autorope] : n;
+        double m = 0, c[3] = {0, 0, 0}, q[6] = {0, 0, 0, 0, 0, 0};
+        for (int64_t j = s; j < e; ++j) {
+            m += mass[j];
+            for (int a = 0; a < 3; ++a) c[a] += mass[j] * pos[3 * j + a];
+        }
+        if (m > 0) for (int a = 0; a < 3; ++a) c[a] /= m;
+        for (int64_t j = s; j < e; ++j) {
+            double dx = pos[3 * j] - c[0], dy = pos[3 * j + 1] - c[1], dz = pos[3 * j + 2] - c[2];
+            double r2 = dx * dx + dy * dy + dz * dz, w = mass[j];
+            q[0] += w * (3 * dx * dx - r2); q[1] += w * (3 * dy * dy - r2); q[2] += w * (3 * dz * dz - r2);
+            q[3] += w * 3 * dx * dy; q[4] += w * 3 * dx * dz; q[5] += w * 3 * dy * dz;
+        }
+        orc_cell64 *o = &cells[i];
+        memcpy(o->c, c, sizeof c); o->m = m; memcpy(o->q, q, sizeof q);
+    }
+    free(first);
+}
+
+/* pos/mass in flat order (n*3, n).  Returns L; phi/acc optional (flat). */
+double orc_bh_plummer_eval(const orc_flat_node *nodes, int64_t nn, const double *pos,
+                           const double *mass, int64_t n, int group, const int64_t *offsets,
+                           const int32_t *items, double eps, double G, int quad, double *phi,
+                           double *acc) {
+    orc_cell64 *cells = (orc_cell64 *)malloc(sizeof(orc_cell64) * (size_t)(nn > 0 ? nn : 1));
+    orc_cells64(nodes, nn, pos, mass, n, cells);
+    const double e2 = eps * eps;
+    int64_t ng = (n + group - 1) / group;
+    double L = 0;
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : L)
+    for (int64_t g = 0; g < ng; ++g) {
+        for (int64_t i = g * group; i < (g + 1) * group && i < n; ++i) {
+            const double *x = pos + 3 * i;
+            double ph = 0, ax = 0, ay = 0, az = 0;
+            for (int64_t t = offsets[g]; t < offsets[g + 1]; ++t) {
+                int64_t p = items[t] >> 1;
+                if (items[t] & 1) {
+                    int64_t s = nodes[p].bucket_start, c = nodes[p].num_particles;
+                    for (int64_t j = s; j < s + c; ++j) {
+                        if (j == i) continue;
+                        double rx = x[0] - pos[3 * j], ry = x[1] - pos[3 * j + 1], rz = x[2] - pos[3 * j + 2];
+                        double s2 = rx * rx + ry * ry + rz * rz + e2;
+                        double i1 = 1.0 / sqrt(s2), i3 = i1 * i1 * i1;
+                        ph -= mass[j] * i1;
+                        ax -= mass[j] * rx * i3; ay -= mass[j] * ry * i3; az -= mass[j] * rz * i3;
+                    }
+                } else {
+                    const orc_cell64 *c = &cells[p];
+                    double rx = x[0] - c->c[0], ry = x[1] - c->c[1], rz = x[2] - c->c[2];
+                    double s2 = rx * rx + ry * ry + rz * rz + e2;
+                    double i1 = 1.0 / sqrt(s2), i2 = i1 * i1, i3 = i1 * i2;
+                    ph -= c->m * i1;
+                    ax -= c->m * rx * i3; ay -= c->m * ry * i3; az -= c->m * rz * i3;
+                    if (quad) {
+                        const double *Q = c->q;
+                        double qx = Q[0] * rx + Q[3] * ry + Q[4] * rz;
+                        double qy = Q[3] * rx + Q[1] * ry + Q[5] * rz;
+                        double qz = Q[4] * rx + Q[5] * ry + Q[2] * rz;
+                        double q = rx * qx + ry * qy + rz * qz;
+                        double i5 = i3 * i2, i7 = i5 * i2;
+                        ph -= 0.5 * q * i5;
+                        ax += qx * i5 - 2.5 * q * rx * i7;
+                        ay += qy * i5 - 2.5 * q * ry * i7;
+                        az += qz * i5 - 2.5 * q * rz * i7;
+                    }
+                }
+            }
+            ph *= G; ax *= G; ay *= G; az *= G;
+            if (phi) phi[i] = ph;
+            if (acc) { acc[3 * i] = ax; acc[3 * i + 1] = ay; acc[3 * i + 2] = az; }
+            L += ph + 0.5 * (ax * ax + ay * ay + az * az);
+        }
+    }
+    free(cells);
+    return L;
+}
+
+/* FP64 Plummer direct sum: phi, acc (n, n*3) and, if g_pos != NULL, the
+ * gradient of L = sum(phi) + 0.5*sum|a|^2 with respect to positions and
+ * masses.  Returns L. */
+double orc_direct_plummer_f64(const double *pos, const double *mass, int64_t n, double eps,
+                              double G, double *phi, double *acc, double *g_pos, double *g_mass) {
+    const double e2 = eps * eps;
+    double L = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : L)
+    for (int64_t i = 0; i < n; ++i) {
+        double ph = 0, ax = 0, ay = 0, az = 0;
+        for (int64_t j = 0; j < n; ++j) {
+            if (j == i) continue;
+            double rx = pos[3 * i] - pos[3 * j], ry = pos[3 * i + 1] - pos[3 * j + 1],
+                   rz = pos[3 * i + 2] - pos[3 * j + 2];
+            double s2 = rx * rx + ry * ry + rz * rz + e2;
+            double i1 = 1.0 / sqrt(s2), i3 = i1 * i1 * i1;
+            ph -= mass[j] * i1;
+            ax -= mass[j] * rx * i3; ay -= mass[j] * ry * i3; az -= mass[j] * rz * i3;
+        }
+        phi[i] = G * ph;
+        acc[3 * i] = G * ax; acc[3 * i + 1] = G * ay; acc[3 * i + 2] = G * az;
+        L += G * ph + 0.5 * G * G * (ax * ax + ay * ay + az * az);
+    }
+    if (!g_pos) return L;
+    /* u_i = 1, v_i = a_i; pair term as field point k and as source k */
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t k = 0; k < n; ++k) {
+        double gx = 0, gy = 0, gz = 0, gm = 0;
+        for (int64_t j = 0; j < n; ++j) {
+            if (j == k) continue;
+            /* k as field point, j as source */
+            {
+                const double *v = acc + 3 * k;
+                double rx = pos[3 * k] - pos[3 * j], ry = pos[3 * k + 1] - pos[3 * j + 1],
+                       rz = pos[3 * k + 2] - pos[3 * j + 2];
+                double s2 = rx * rx + ry * ry + rz * rz + e2;
+                double i1 = 1.0 / sqrt(s2), i3 = i1 * i1 * i1, i5 = i3 * i1 * i1;
+                double vr = v[0] * rx + v[1] * ry + v[2] * rz, m = mass[j];
+                gx += G * (m * rx * i3 - m * (v[0] * i3 - 3 * vr * rx * i5));
+                gy += G * (m * ry * i3 - m * (v[1] * i3 - 3 * vr * ry * i5));
+                gz += G * (m * rz * i3 - m * (v[2] * i3 - 3 * vr * rz * i5));
+            }
+            /* j as field point, k as source */
+            {
+                const double *v = acc + 3 * j;
+                double rx = pos[3 * j] - pos[3 * k], ry = pos[3 * j + 1] - pos[3 * k + 1],
+                       rz = pos[3 * j + 2] - pos[3 * k + 2];
+                double s2 = rx * rx + ry * ry + rz * rz + e2;
+                double i1 = 1.0 / sqrt(s2), i3 = i1 * i1 * i1, i5 = i3 * i1 * i1;
+                double vr = v[0] * rx + v[1] * ry + v[2] * rz, m = mass[k];
+                gx -= G * (m * rx * i3 - m * (v[0] * i3 - 3 * vr * rx * i5));
+                gy -= G * (m * ry * i3 - m * (v[1] * i3 - 3 * vr * ry * i5));
+                gz -= G * (m * rz * i3 - m * (v[2] * i3 - 3 * vr * rz * i5));
+                gm += G * (-i1 - vr * i3);
+            }
+        }
+        g_pos[3 * k] = gx; g_pos[3 * k + 1] = gy; g_pos[3 * k + 2] = gz;
+        if (g_mass) g_mass[k] = gm;
+    }
+    return L;
+}

@@ -1,0 +1,85 @@
+// bh.cuh -- Barnes-Hut octree layout shared by the builder and the walks.
+//
+// The tree is the reference's (gprt-core/src/lib.rs:340-539): a cube root
+// around the bounding box, geometric octant splits at the cell centre, a
+// cell is a leaf when it holds <= bucket bodies or its width drops below
+// min_width, nodes in pre-order with next = self + 1 and an "autorope" to
+// the node after the subtree, leaf buckets contiguous in the flat body
+// order.  Node records (pre-order index):
+//   node_a[i] = (com.x, com.y, com.z, mass)
+//   node_b[i] = (autorope, bucket_start, count | LEAF_BIT, bits of width)
+//   node_q[i] = traceless quadrupole about the COM (xx, yy, zz, xy, xz, yz, 0, 0)
+#pragma once
+
+#include "common.cuh"
+#include "sort.cuh"
+
+namespace rtd {
+
+constexpr uint32_t BH_LEAF_BIT = 0x80000000u;
+constexpr int BH_MAX_LEVEL = 21;            // octant digits held by a 63-bit path key
+constexpr int BH_GROUP = 32;                // bodies per warp-coherent group
+
+struct BhHeader {
+    float root_min[3], root_max[3];
+    float max_extent, scale;
+    float min_b[3];
+    uint32_t box[6];          // order-preserving bbox of the positions
+    uint32_t lw;              // first level whose width < min_width
+    uint32_t n_nodes, n_leaves;
+    uint32_t err;
+    uint32_t level_count[BH_MAX_LEVEL + 2];
+    uint32_t level_off[BH_MAX_LEVEL + 3];
+};
+
+}  // namespace rtd
+
+struct rtd_bh {
+    uint64_t n = 0;
+    uint32_t bucket = 128;
+    float min_width = 1e-5f;
+    bool built = false;
+    rtd::DevBuf hdr;
+    // build scratch
+    rtd::DevBuf mkeys, mkeys_alt, mvals, mvals_alt;   // Morton sort
+    rtd::DevBuf pkeys, pkeys_alt, pvals, pvals_alt;   // path-key sort (values: Morton rank)
+    rtd::DevBuf lcp, wmin, lam, nn, base, heads, leaf_head, leaf_of;
+    rtd::DevBuf fkeys, fkeys_alt, fvals, fvals_alt;   // final regroup sort
+    rtd::DevBuf node_start, node_level, level_nodes;
+    rtd::SortScratch sort;
+    rtd::ScanScratch scan;
+    // tree
+    rtd::DevBuf order;        // flat order: original index of the i-th body
+    rtd::DevBuf fbody;        // float4 (pos, mass) in flat order
+    rtd::DevBuf node_a, node_b, node_q;
+    // adjoint scratch
+    rtd::DevBuf cell_grad, prefix, gpos_flat, gmass_flat;
+};
+
+// Device buffers a host-buffer context keeps for barnes_hut! calls.
+struct rtd_context_bh {
+    rtd_bh bh;
+    rtd::DevBuf bodies, pos, mass, out;
+};
+
+namespace rtd {
+
+struct BhView {
+    const float4 *node_a;
+    const uint4 *node_b;
+    const float4 *node_q;      // 2 float4 per node
+    const float4 *fbody;
+    const uint32_t *order;
+    const BhHeader *hdr;
+    uint64_t n;
+};
+
+inline BhView bh_view(const rtd_bh *b) {
+    return BhView{b->node_a.as<float4>(), b->node_b.as<uint4>(), b->node_q.as<float4>(),
+                  b->fbody.as<float4>(), b->order.as<uint32_t>(), b->hdr.as<BhHeader>(), b->n};
+}
+
+rtd_status bh_build(rtd_bh *b, const float *d_pos, const float *d_mass, uint64_t n,
+                    const rtd_bh_params *p, cudaStream_t st);
+
+}  // namespace rtd

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <new>
 
+#include "bh.cuh"
 #include "index.cuh"
 
 namespace rtd {
@@ -95,7 +96,16 @@ struct rtd_context {
     rtd_index index;
     DevBuf data, queries, ids, d2, pairs;
     cudaStream_t stream = nullptr;
+    rtd_context_bh *bh = nullptr;   // created on the first barnes_hut! call
+    ~rtd_context() { delete bh; }
 };
+
+rtd_context_bh *context_bh(rtd_context *ctx) {
+    if (!ctx->bh) ctx->bh = new (std::nothrow) rtd_context_bh();
+    return ctx->bh;
+}
+
+cudaStream_t context_stream(rtd_context *ctx) { return ctx->stream; }
 
 extern "C" {
 
@@ -110,6 +120,7 @@ void rtd_schedule_default(rtd_schedule *s) {
     s->block_size = 0;
     s->lanes_per_query = 0;
     s->morton_bits = 0;
+    s->packet_traversal = RTD_PACKET_AUTO;
 }
 
 const char *rtd_status_string(rtd_status s) {

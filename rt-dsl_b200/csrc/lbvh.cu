@@ -224,14 +224,30 @@ __device__ __forceinline__ void store_child_box(BvhNode *nd, int side, const Box
     }
 }
 
-__device__ __forceinline__ Box node_union_cg(const BvhNode *nd) {
-    const float *f = reinterpret_cast<const float *>(nd);
+__device__ __forceinline__ Box load_child_box_cg(const BvhNode *nd, int side) {
+    const float *f = reinterpret_cast<const float *>(nd) + side * 6;
     Box b;
     for (int a = 0; a < 3; ++a) {
-        b.lo[a] = fminf(__ldcg(f + a), __ldcg(f + 6 + a));
-        b.hi[a] = fmaxf(__ldcg(f + 3 + a), __ldcg(f + 9 + a));
+        b.lo[a] = __ldcg(f + a);
+        b.hi[a] = __ldcg(f + 3 + a);
     }
     return b;
+}
+
+__device__ __forceinline__ Box box_union(const Box &x, const Box &y) {
+    Box b;
+    for (int a = 0; a < 3; ++a) {
+        b.lo[a] = fminf(x.lo[a], y.lo[a]);
+        b.hi[a] = fmaxf(x.hi[a], y.hi[a]);
+    }
+    return b;
+}
+
+__device__ __forceinline__ uint32_t atomic_add_acq_rel(uint32_t *p, uint32_t v) {
+    uint32_t old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;"
+                 : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
 }
 
 // Bottom-up refit: a thread per node with leaf children computes their
@@ -248,75 +264,94 @@ __global__ void __launch_bounds__(BLOCK) refit_kernel(uint32_t n_internal_max,
          c += gridDim.x * BLOCK) {
         uint4 d = nodes[c].d;
         uint32_t nleaf = 0;
-        if (d.x & CHILD_LEAF) { store_child_box(&nodes[c], 0, leaf_box(pts, d.x & CHILD_INDEX, d.z)); ++nleaf; }
-        if (d.y & CHILD_LEAF) { store_child_box(&nodes[c], 1, leaf_box(pts, d.y & CHILD_INDEX, d.w)); ++nleaf; }
+        Box b;
+        if (d.x & CHILD_LEAF) {
+            b = leaf_box(pts, d.x & CHILD_INDEX, d.z);
+            store_child_box(&nodes[c], 0, b);
+            ++nleaf;
+        }
+        if (d.y & CHILD_LEAF) {
+            Box b1 = leaf_box(pts, d.y & CHILD_INDEX, d.w);
+            store_child_box(&nodes[c], 1, b1);
+            b = nleaf ? box_union(b, b1) : b1;
+            ++nleaf;
+        }
         if (nleaf == 0) continue;
-        __threadfence();
-        uint32_t old = atomicAdd(&counter[c], nleaf);
+        // acq_rel: our box stores are released before the count, and the
+        // second arrival acquires the sibling's stores.
+        uint32_t old = atomic_add_acq_rel(&counter[c], nleaf);
         if (old + nleaf < 2) continue;
+        if (nleaf == 1) b = box_union(b, load_child_box_cg(&nodes[c], (d.x & CHILD_LEAF) ? 1 : 0));
         uint32_t cur = c;
         for (int depth = 0;; ++depth) {
             if (depth > 128) {   // deeper than any Karras tree: broken parent links
                 atomicOr(&((IndexHeader *)h)->err, DEVERR_DEPTH);
                 break;
             }
-            __threadfence();
-            Box b = node_union_cg(&nodes[cur]);
             uint32_t par = cparent[cur];
             if (par == CHILD_NONE) break;
             uint32_t p = par >> 1;
-            store_child_box(&nodes[p], (int)(par & 1u), b);
-            __threadfence();
-            if (atomicAdd(&counter[p], 1u) == 0u) break;
+            int side = (int)(par & 1u);
+            store_child_box(&nodes[p], side, b);
+            if (atomic_add_acq_rel(&counter[p], 1u) == 0u) break;
+            b = box_union(b, load_child_box_cg(&nodes[p], 1 - side));
             cur = p;
         }
     }
 }
 
-// Root word and the breadth-first top levels, copied into `top`.
-__global__ void stage_top_kernel(IndexHeader *h, const BvhNode *__restrict__ nodes, BvhNode *top,
-                                 uint64_t n, uint32_t leaf_size) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    if (n == 0) {
-        h->root = CHILD_NONE;
-        h->n_top = 0;
-        return;
-    }
-    if (n == 1 || n <= leaf_size) {
-        h->root = CHILD_LEAF | 0u;
-        h->root_count = (uint32_t)n;
-        h->n_top = 0;
-        return;
-    }
-    uint32_t q[TOP_MAX];
-    uint8_t depth[TOP_MAX];
-    int cnt = 0;
-    q[cnt] = 0; depth[cnt] = 0; ++cnt;
-    for (int i = 0; i < cnt; ++i) {
-        if (depth[i] + 1 >= TOP_LEVELS) continue;
-        uint4 d = nodes[q[i]].d;
-        uint32_t ch[2] = {d.x, d.y};
-        for (int s = 0; s < 2; ++s)
-            if (!(ch[s] & CHILD_LEAF) && cnt < TOP_MAX) {
-                q[cnt] = ch[s];
-                depth[cnt] = (uint8_t)(depth[i] + 1);
-                ++cnt;
-            }
-    }
-    for (int i = 0; i < cnt; ++i) {
-        BvhNode nd = nodes[q[i]];
-        uint32_t ch[2] = {nd.d.x, nd.d.y};
-        for (int s = 0; s < 2; ++s) {
-            if (ch[s] & CHILD_LEAF) continue;
-            for (int j = 0; j < cnt; ++j)
-                if (q[j] == ch[s]) { ch[s] = CHILD_TOP | (uint32_t)j; break; }
+// Root word and the breadth-first top levels, copied into `top`.  One warp:
+// each level's nodes are loaded in parallel (level TOP_LEVELS-1 has at most
+// 32 nodes) and their internal children are placed by a warp prefix sum.
+__global__ void __launch_bounds__(32) stage_top_kernel(IndexHeader *h,
+                                                       const BvhNode *__restrict__ nodes,
+                                                       BvhNode *top, uint64_t n,
+                                                       uint32_t leaf_size) {
+    const int lane = threadIdx.x;
+    if (n == 0 || n == 1 || n <= leaf_size) {
+        if (lane == 0) {
+            h->root = n == 0 ? CHILD_NONE : (CHILD_LEAF | 0u);
+            h->root_count = (uint32_t)n;
+            h->n_top = 0;
         }
-        nd.d.x = ch[0];
-        nd.d.y = ch[1];
-        top[i] = nd;
+        return;
     }
-    h->root = CHILD_TOP | 0u;
-    h->n_top = (uint32_t)cnt;
+    __shared__ uint32_t s_q[TOP_MAX];
+    if (lane == 0) s_q[0] = 0;
+    __syncwarp();
+    int begin = 0, end = 1;
+    for (int depth = 0; depth < TOP_LEVELS; ++depth) {
+        const int i = begin + lane;
+        const bool has = i < end;
+        BvhNode nd;
+        if (has) nd = nodes[s_q[i]];
+        const bool deeper = depth + 1 < TOP_LEVELS;
+        const bool c0 = has && deeper && !(nd.d.x & CHILD_LEAF);
+        const bool c1 = has && deeper && !(nd.d.y & CHILD_LEAF);
+        const uint32_t cnt = (uint32_t)c0 + (uint32_t)c1;
+        uint32_t incl = cnt;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        const uint32_t pos = (uint32_t)end + incl - cnt;
+        if (c0) s_q[pos] = nd.d.x;
+        if (c1) s_q[pos + (c0 ? 1u : 0u)] = nd.d.y;
+        if (has) {
+            if (c0) nd.d.x = CHILD_TOP | pos;
+            if (c1) nd.d.y = CHILD_TOP | (pos + (c0 ? 1u : 0u));
+            top[i] = nd;
+        }
+        __syncwarp();
+        begin = end;
+        end += (int)total;
+        if (total == 0) break;
+    }
+    if (lane == 0) {
+        h->root = CHILD_TOP | 0u;
+        h->n_top = (uint32_t)end;
+    }
 }
 
 // ------------------------------------------------ radius-seed sample data
@@ -335,64 +370,75 @@ __global__ void seed_sample_kernel(const float *__restrict__ xyz, uint64_t n, fl
 }
 
 // Squared 1-NN distance of each of S = min(n, 4096) stride-sampled points
-// (index a*n/S) among the other sample points.
+// (index a*n/S) among the other sample points.  Grid (a-tiles x b-chunks);
+// each thread folds its chunk's minimum into out[a] (order-preserving u32,
+// pre-set to 0xFFFFFFFF).  The minimum does not depend on the order.
+constexpr int SEED_CHUNK = 256;
 __global__ void __launch_bounds__(128) seed_nn_kernel(const float *__restrict__ xyz, uint64_t n,
-                                                      uint32_t S, float *__restrict__ out) {
-    __shared__ float3 s_p[128];
+                                                      uint32_t S, uint32_t *__restrict__ out) {
+    __shared__ float3 s_p[SEED_CHUNK];
     const uint32_t a = blockIdx.x * 128 + threadIdx.x;
-    float3 pa = make_float3(0.f, 0.f, 0.f);
-    if (a < S) {
-        uint64_t ia = (uint64_t)a * n / S;
-        pa = make_float3(xyz[3 * ia], xyz[3 * ia + 1], xyz[3 * ia + 2]);
-    }
-    float best = INFINITY;
-    for (uint32_t t0 = 0; t0 < S; t0 += 128) {
-        uint32_t b = t0 + threadIdx.x;
+    const uint32_t b0 = blockIdx.y * SEED_CHUNK;
+    for (uint32_t t = threadIdx.x; t < SEED_CHUNK; t += 128) {
+        uint32_t b = b0 + t;
         if (b < S) {
             uint64_t ib = (uint64_t)b * n / S;
-            s_p[threadIdx.x] = make_float3(xyz[3 * ib], xyz[3 * ib + 1], xyz[3 * ib + 2]);
+            s_p[t] = make_float3(xyz[3 * ib], xyz[3 * ib + 1], xyz[3 * ib + 2]);
         }
-        __syncthreads();
-        uint32_t lim = S - t0 < 128 ? S - t0 : 128;
-        for (uint32_t j = 0; j < lim; ++j) {
-            if (t0 + j == a) continue;
-            float key = exact_key(pa.x, pa.y, pa.z, s_p[j].x, s_p[j].y, s_p[j].z);
-            if (key < best) best = key;
-        }
-        __syncthreads();
     }
-    if (a < S) out[a] = best;
-}
-
-// Sorts <= 4096 floats ascending in shared memory with one 1024-thread block.
-__device__ void block_sort4096(float *s, uint32_t n_pad) {
-    for (uint32_t k = 2; k <= n_pad; k <<= 1)
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < n_pad; i += blockDim.x) {
-                uint32_t ixj = i ^ j;
-                if (ixj > i) {
-                    float x = s[i], y = s[ixj];
-                    bool up = (i & k) == 0;
-                    if (up ? (x > y) : (x < y)) { s[i] = y; s[ixj] = x; }
-                }
-            }
-            __syncthreads();
-        }
-}
-
-__global__ void __launch_bounds__(1024) seed_nn_select_kernel(const float *__restrict__ keys,
-                                                              uint32_t S, IndexHeader *h) {
-    __shared__ float s[SEED_NN_SAMPLE];
-    uint32_t n_pad = 1;
-    while (n_pad < S) n_pad <<= 1;
-    for (uint32_t i = threadIdx.x; i < n_pad; i += blockDim.x) s[i] = i < S ? keys[i] : INFINITY;
     __syncthreads();
-    block_sort4096(s, n_pad);
-    if (threadIdx.x == 0) {
-        uint32_t idx = (uint32_t)(0.95f * (float)S);
-        if (idx > S - 1) idx = S - 1;
-        h->nn95_key = s[idx];
+    if (a >= S) return;
+    const uint64_t ia = (uint64_t)a * n / S;
+    const float ax = xyz[3 * ia], ay = xyz[3 * ia + 1], az = xyz[3 * ia + 2];
+    const uint32_t lim = S - b0 < (uint32_t)SEED_CHUNK ? S - b0 : (uint32_t)SEED_CHUNK;
+    float best = INFINITY;
+    for (uint32_t j = 0; j < lim; ++j) {
+        if (b0 + j == a) continue;
+        float key = exact_key(ax, ay, az, s_p[j].x, s_p[j].y, s_p[j].z);
+        if (key < best) best = key;
     }
+    if (best < INFINITY) atomicMin(&out[a], float_flip(best));
+}
+
+// rank-th smallest of S <= 4096 order-preserving u32 values: an 8-bit
+// radix select in one 1024-thread block (4 histogram passes).
+__global__ void __launch_bounds__(1024) seed_nn_select_kernel(const uint32_t *__restrict__ keys,
+                                                              uint32_t S, IndexHeader *h) {
+    __shared__ uint32_t s_hist[256];
+    __shared__ uint32_t s_sel[2];   // prefix chosen so far, remaining rank
+    uint32_t v[4];
+    for (int j = 0; j < 4; ++j) {
+        uint32_t i = threadIdx.x + 1024u * j;
+        v[j] = i < S ? keys[i] : 0xFFFFFFFFu;
+    }
+    uint32_t rank = (uint32_t)(0.95f * (float)S);
+    if (rank > S - 1) rank = S - 1;
+    uint32_t prefix = 0;
+    for (int pass = 3; pass >= 0; --pass) {
+        const int shift = 8 * pass;
+        const uint32_t hi_mask = pass == 3 ? 0u : (0xFFFFFFFFu << (shift + 8));
+        if (threadIdx.x < 256) s_hist[threadIdx.x] = 0;
+        __syncthreads();
+        for (int j = 0; j < 4; ++j) {
+            uint32_t i = threadIdx.x + 1024u * j;
+            if (i < S && (v[j] & hi_mask) == prefix) atomicAdd(&s_hist[(v[j] >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t acc = 0, d = 0;
+            for (; d < 255; ++d) {
+                if (acc + s_hist[d] > rank) break;
+                acc += s_hist[d];
+            }
+            s_sel[0] = prefix | (d << shift);
+            s_sel[1] = rank - acc;
+        }
+        __syncthreads();
+        prefix = s_sel[0];
+        rank = s_sel[1];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) h->nn95_key = float_unflip(prefix);
 }
 
 rtd_status build_seed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStream_t st) {
@@ -403,9 +449,11 @@ rtd_status build_seed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStream
     RTD_LAUNCH_CHECK();
     if (n >= 2) {
         uint32_t S = n < SEED_NN_SAMPLE ? (uint32_t)n : (uint32_t)SEED_NN_SAMPLE;
-        seed_nn_kernel<<<(S + 127) / 128, 128, 0, st>>>(d_xyz, n, S, idx->seed.as<float>());
+        RTD_CUDA(cudaMemsetAsync(idx->seed.ptr, 0xFF, S * sizeof(uint32_t), st));
+        dim3 grid((S + 127) / 128, (S + SEED_CHUNK - 1) / SEED_CHUNK);
+        seed_nn_kernel<<<grid, 128, 0, st>>>(d_xyz, n, S, idx->seed.as<uint32_t>());
         RTD_LAUNCH_CHECK();
-        seed_nn_select_kernel<<<1, 1024, 0, st>>>(idx->seed.as<float>(), S, h);
+        seed_nn_select_kernel<<<1, 1024, 0, st>>>(idx->seed.as<uint32_t>(), S, h);
         RTD_LAUNCH_CHECK();
     }
     return RTD_OK;
@@ -493,7 +541,7 @@ rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd
         if (mb == 30) RTD_TRY(build_typed<uint32_t>(idx, d_xyz, n, st));
         else RTD_TRY(build_typed<uint64_t>(idx, d_xyz, n, st));
     }
-    stage_top_kernel<<<1, 1, 0, st>>>(h, idx->nodes.as<BvhNode>(), idx->top.as<BvhNode>(), n,
+    stage_top_kernel<<<1, 32, 0, st>>>(h, idx->nodes.as<BvhNode>(), idx->top.as<BvhNode>(), n,
                                       idx->leaf_size);
     RTD_LAUNCH_CHECK();
     idx->mark(EV_BUILD1, st);

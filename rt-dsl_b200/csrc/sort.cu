@@ -142,24 +142,37 @@ __global__ void __launch_bounds__(RS_BLOCK) rs_pass_kernel(
     uint32_t excl_local = block_excl_scan256(tile_cnt, s_misc, nullptr);
     s_excl[d] = excl_local;
 
+    // Look back over earlier tiles, 8 status words in flight at a time:
+    // sum their counts up to the nearest inclusive prefix.
     uint32_t prev = 0;
     if (tile > 0) {
         int64_t t = (int64_t)tile - 1;
         uint32_t spins = 0;
-        while (t >= 0) {
-            uint32_t v = st[(uint64_t)t * 256 + d];
-            uint32_t f = v & ~VALUE_MASK;
-            if (f == 0) {
+        while (true) {
+            uint32_t w[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                w[j] = (t - j >= 0) ? (uint32_t)st[(uint64_t)(t - j) * 256 + d] : (2u << 30);
+            int used = 0;
+            bool done = false;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (done || used < j) continue;
+                uint32_t f = w[j] & ~VALUE_MASK;
+                if (f == 0) continue;          // not published yet: retry from here
+                prev += w[j] & VALUE_MASK;
+                used = j + 1;
+                if (f == FLAG_INC) done = true;
+            }
+            if (done) break;
+            t -= used;
+            if (used < 8) {
                 if (++spins > SPIN_LIMIT) {
                     atomicOr(d_err, DEVERR_TIMEOUT);
                     break;
                 }
-                __nanosleep(32);
-                continue;
+                __nanosleep(20);
             }
-            prev += v & VALUE_MASK;
-            if (f == FLAG_INC) break;
-            --t;
         }
         st[(uint64_t)tile * 256 + d] = FLAG_INC | ((prev + tile_cnt) & VALUE_MASK);
     }
@@ -246,34 +259,44 @@ __global__ void __launch_bounds__(SC_BLOCK) scan_kernel(const uint32_t *__restri
     __syncthreads();
     const uint64_t excl = s_warp[warp] + x - sum;
     const uint64_t agg = s_warp[SC_BLOCK / 32];
-    if (tid == 0) {
+    // Warp-cooperative look-back: lane j reads tile (t - j); the nearest
+    // inclusive prefix ends the sum.
+    if (warp == 0) {
         volatile uint64_t *st = status;
         uint64_t prev = 0;
         if (tile == 0) {
-            st[0] = SC_INC | (agg & SC_MASK);
+            if (lane == 0) st[0] = SC_INC | (agg & SC_MASK);
         } else {
-            st[tile] = SC_AGG | (agg & SC_MASK);
+            if (lane == 0) st[tile] = SC_AGG | (agg & SC_MASK);
             int64_t t = (int64_t)tile - 1;
             uint32_t spins = 0;
-            while (t >= 0) {
-                uint64_t w = st[t];
-                uint64_t f = w & ~SC_MASK;
-                if (f == 0) {
-                    if (++spins > SPIN_LIMIT) {
-                        atomicOr(d_err, DEVERR_TIMEOUT);
-                        break;
-                    }
-                    __nanosleep(32);
-                    continue;
+            while (true) {
+                const int64_t ti = t - lane;
+                uint64_t w = ti >= 0 ? (uint64_t)st[ti] : (2ull << 62);
+                while (__any_sync(0xffffffffu, (w & ~SC_MASK) == 0)) {
+                    if (++spins > SPIN_LIMIT) break;
+                    __nanosleep(20);
+                    if ((w & ~SC_MASK) == 0) w = st[ti];
                 }
-                prev += w & SC_MASK;
-                if (f == SC_INC) break;
-                --t;
+                if (spins > SPIN_LIMIT) {
+                    if (lane == 0) atomicOr(d_err, DEVERR_TIMEOUT);
+                    break;
+                }
+                const uint32_t inc = __ballot_sync(0xffffffffu, (w & ~SC_MASK) == SC_INC);
+                const int stop = inc ? __ffs(inc) - 1 : 31;
+                uint64_t v = lane <= stop ? (w & SC_MASK) : 0ull;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                prev += v;
+                if (inc) break;
+                t -= 32;
             }
-            st[tile] = SC_INC | ((prev + agg) & SC_MASK);
+            if (lane == 0) st[tile] = SC_INC | ((prev + agg) & SC_MASK);
         }
-        s_prefix = prev;
-        if (tile == ntiles - 1 && d_total) *d_total = (OutT)(prev + agg);
+        if (lane == 0) {
+            s_prefix = prev;
+            if (tile == ntiles - 1 && d_total) *d_total = (OutT)(prev + agg);
+        }
     }
     __syncthreads();
     uint64_t run = s_prefix + excl;

@@ -4,12 +4,15 @@ All compute runs in librtdsl.so (hand-written sm_100a CUDA behind the C ABI
 of include/rtdsl.h); this package binds it with ctypes and mirrors the
 reference's k_nn! / range_query! / barnes_hut! interface.
 """
-from ._capi import (EMPTY_ID, RADIUS_FIXED, RADIUS_SAMPLED_MAX, RADIUS_SAMPLED_NN,
-                    RADIUS_SAMPLED_PERCENTILE, RtdError, Schedule, default_schedule, load)
+from ._capi import (BH_LAW_PLUMMER, BH_LAW_REFERENCE, EMPTY_ID, RADIUS_FIXED,
+                    RADIUS_SAMPLED_MAX, RADIUS_SAMPLED_NN, RADIUS_SAMPLED_PERCENTILE, BhParams,
+                    RtdError, Schedule, default_bh_params, default_schedule, load)
 from .api import Context, Index, k_nn, k_nn_array, knn_backward, range_query
+from .bh import BarnesHut, barnes_hut
 
 __all__ = [
-    "EMPTY_ID", "RADIUS_FIXED", "RADIUS_SAMPLED_MAX", "RADIUS_SAMPLED_NN",
-    "RADIUS_SAMPLED_PERCENTILE", "RtdError", "Schedule", "default_schedule", "load",
-    "Context", "Index", "k_nn", "k_nn_array", "knn_backward", "range_query",
+    "BH_LAW_PLUMMER", "BH_LAW_REFERENCE", "EMPTY_ID", "RADIUS_FIXED", "RADIUS_SAMPLED_MAX",
+    "RADIUS_SAMPLED_NN", "RADIUS_SAMPLED_PERCENTILE", "BhParams", "RtdError", "Schedule",
+    "default_bh_params", "default_schedule", "load", "Context", "Index", "k_nn", "k_nn_array",
+    "knn_backward", "range_query", "BarnesHut", "barnes_hut",
 ]

@@ -49,6 +49,7 @@ class Schedule(C.Structure):
         ("block_size", C.c_uint32),
         ("lanes_per_query", C.c_uint32),
         ("morton_bits", C.c_uint32),
+        ("packet_traversal", C.c_uint32),
     ]
 
     def as_dict(self) -> dict:
@@ -94,7 +95,44 @@ _SIGNATURES = {
     "rtd_index_profile_enable": (_I, [_P, _I]),
     "rtd_index_profile_get": (_I, [_P, _P]),
     "rtd_launch_count": (_U64, []),
+    "rtd_bh_params_default": (None, [_P]),
+    "rtd_bh_create": (_I, [C.POINTER(_P)]),
+    "rtd_bh_destroy": (_I, [_P]),
+    "rtd_bh_build": (_I, [_P, _P, _P, _U64, _P, _P]),
+    "rtd_bh_release": (_I, [_P]),
+    "rtd_bh_forward": (_I, [_P, _P, _P, _P, _P]),
+    "rtd_bh_backward": (_I, [_P, _P, _P, _P, _P, _P, _P]),
+    "rtd_bh_info_get": (_I, [_P, _P, _P]),
+    "rtd_bh_export": (_I, [_P, _P, _P, _P]),
+    "rtd_barnes_hut_host": (_I, [_P, _P, _U64, _F, _F, _P]),
 }
+
+BH_LAW_REFERENCE = 0
+BH_LAW_PLUMMER = 1
+
+
+class BhParams(C.Structure):
+    """rtd_bh_params."""
+    _fields_ = [("theta", C.c_float), ("G", C.c_float), ("eps", C.c_float), ("law", C.c_int32),
+                ("quadrupole", C.c_int32), ("bucket", C.c_uint32), ("min_width", C.c_float)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class BhInfo(C.Structure):
+    _fields_ = [("n_bodies", C.c_uint64), ("n_nodes", C.c_uint64), ("n_leaves", C.c_uint64),
+                ("depth", C.c_uint32), ("root_min", C.c_float * 3), ("root_max", C.c_float * 3)]
+
+
+def default_bh_params(**overrides) -> BhParams:
+    p = BhParams()
+    load().rtd_bh_params_default(C.byref(p))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise AttributeError(f"unknown bh parameter {k}")
+        setattr(p, k, v)
+    return p
 
 
 class Profile(C.Structure):

@@ -217,6 +217,29 @@ class Index:
         return pairs[: written.value]
 
 
+def radius_for_mean_count(index: "Index", queries, target_mean: float, sample: int = 20000,
+                          iters: int = 30, schedule: Schedule | None = None) -> float:
+    """Radius whose mean neighbour count over a query sample is target_mean,
+    found by bisection on the GPU count pass (log-scale)."""
+    import torch
+    qs = queries[:: max(1, queries.shape[0] // sample)].contiguous()
+    lo, hi = 0.0, 1.0
+    # grow hi until it is large enough
+    for _ in range(60):
+        _, tot = index.range_count(qs, hi, schedule)
+        if tot / qs.shape[0] >= target_mean:
+            break
+        lo, hi = hi, hi * 2.0
+    for _ in range(iters):
+        mid = 0.5 * (lo + hi)
+        _, tot = index.range_count(qs, mid, schedule)
+        if tot / qs.shape[0] < target_mean:
+            lo = mid
+        else:
+            hi = mid
+    return float(hi)
+
+
 def knn_backward(queries, points, ids, grad_d2, grad_q=None, grad_p=None, stream=None):
     """dL/dq (overwritten) and dL/dp (accumulated) for d2 = |q - p_id|^2."""
     import torch

@@ -1,0 +1,137 @@
+"""Autotuner for the k-NN launch knobs, with a JSON "wisdom" cache.
+
+The reference tunes its Schedule offline and stores it as gprt_wisdom.json
+(gprt-sandbox/src/main.rs:53-77; grid + subsample funnel in
+gprt-profiler/src/main.rs:40-126; hill-climb in gprt-macros/src/lib.rs:
+120-214).  Here the knobs are the LBVH leaf size, the initial-radius
+multiplier and growth factor of the in-kernel radius expansion, the block
+size, and the traversal mode (thread per query, 32-query packets, warp per
+query).  Because every candidate returns identical results (exact search),
+the tuner only times them; it still checks each candidate's ids against the
+first candidate's and refuses one that differs.
+
+Funnel: every candidate is timed on a query subsample, the best few on all
+queries.  Results are cached per (tag, GPU name) in wisdom.json next to this
+file.
+"""
+from __future__ import annotations
+
+import itertools
+import json
+import os
+import time
+
+from . import _capi
+
+WISDOM = os.path.join(os.path.dirname(os.path.abspath(__file__)), "wisdom.json")
+
+DEFAULT_GRID = {
+    "leaf_size": [1, 2, 4, 8],
+    "radius_param": [0.0625, 0.25, 0.5, 1.0],
+    "radius_increment_mult": [2.0, 4.0],
+    "block_size": [64, 128, 256],
+    "mode": ["thread", "packet", "warp"],
+}
+
+_MODES = {"thread": dict(lanes_per_query=1, packet_traversal=2),
+          "packet": dict(lanes_per_query=1, packet_traversal=1),
+          "warp": dict(lanes_per_query=32, packet_traversal=2)}
+
+
+def gpu_name() -> str:
+    try:
+        import torch
+        return torch.cuda.get_device_name()
+    except Exception:
+        return "unknown"
+
+
+def _load() -> dict:
+    if os.path.exists(WISDOM):
+        with open(WISDOM) as f:
+            return json.load(f)
+    return {}
+
+
+def cached_schedule(tag: str, default: _capi.Schedule | None = None) -> _capi.Schedule:
+    """Schedule tuned for `tag` on this GPU type, else `default`."""
+    s = default if default is not None else _capi.default_schedule()
+    entry = _load().get(tag)
+    if not entry:
+        return s
+    for k, v in entry["schedule"].items():
+        if hasattr(s, k):
+            setattr(s, k, v)
+    return s
+
+
+def save(tag: str, schedule: _capi.Schedule, meta: dict) -> None:
+    d = _load()
+    d[tag] = {"schedule": schedule.as_dict(), **meta}
+    tmp = WISDOM + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(d, f, indent=1, sort_keys=True)
+    os.replace(tmp, WISDOM)
+
+
+def _time_knn(index_cls, P, Q, k, s, reps: int):
+    import torch
+    ix = index_cls().profile(True)
+    ids = torch.empty((Q.shape[0], k), dtype=torch.int32, device=Q.device)
+    d2 = torch.empty((Q.shape[0], k), dtype=torch.float32, device=Q.device)
+    ix.build(P, s)
+    ix.knn(Q, k, s, out_ids=ids, out_d2=d2)
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(reps):
+        ix.build(P, s)
+        ix.knn(Q, k, s, out_ids=ids, out_d2=d2)
+        t = ix.timings()
+        best = min(best, sum(t.values()))
+    return best, ids
+
+
+def tune_knn(P, Q, k: int, tag: str, grid: dict | None = None, reps: int = 3,
+             subsample: int = 8, keep: int = 6, save_result: bool = True, log=None):
+    """Times build + search for every grid point (funnel: query subsample,
+    then the best `keep` on all queries); returns (schedule, table)."""
+    from .api import Index
+    grid = grid or DEFAULT_GRID
+    keys = list(grid)
+    cands = []
+    for combo in itertools.product(*(grid[k_] for k_ in keys)):
+        kw = dict(zip(keys, combo))
+        mode = kw.pop("mode", "thread")
+        if mode != "warp" and k > 32:
+            continue
+        kw.update(_MODES[mode])
+        cands.append(kw)
+    Qs = Q[:: max(1, subsample)].contiguous()
+    ref_ids = None
+    stage1 = []
+    for kw in cands:
+        s = _capi.default_schedule(**kw)
+        ms, ids = _time_knn(Index, P, Qs, k, s, reps)
+        if ref_ids is None:
+            ref_ids = ids.clone()
+        elif not bool((ids == ref_ids).all()):
+            raise RuntimeError(f"autotune: candidate {kw} returned different neighbours")
+        stage1.append((ms, kw))
+        if log:
+            log(f"stage1 {ms:.4f} ms {kw}")
+    stage1.sort(key=lambda x: x[0])
+    stage2 = []
+    for _, kw in stage1[:keep]:
+        s = _capi.default_schedule(**kw)
+        ms, _ = _time_knn(Index, P, Q, k, s, reps)
+        stage2.append((ms, kw))
+        if log:
+            log(f"stage2 {ms:.4f} ms {kw}")
+    stage2.sort(key=lambda x: x[0])
+    best_ms, best_kw = stage2[0]
+    best = _capi.default_schedule(**best_kw)
+    if save_result:
+        save(tag, best, {"gpu": gpu_name(), "n": int(P.shape[0]), "nq": int(Q.shape[0]), "k": k,
+                         "build_plus_search_ms": best_ms,
+                         "tuned_at": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())})
+    return best, stage2

@@ -42,11 +42,23 @@ def test_plain_knn_small_config(rtd, orc, cuda):
 
 
 @pytest.mark.parametrize("k", [1, 2, 5, 8, 16, 32])
-@pytest.mark.parametrize("lanes", [1, 32])
-def test_knn_k_and_lanes(rtd, orc, cuda, k, lanes):
+@pytest.mark.parametrize("mode", ["packet", "thread", "warp"])
+def test_knn_k_and_traversal(rtd, orc, cuda, k, mode):
     pts, q = clustered_small()
-    ids, d2, _ = gpu_knn(rtd, pts, q, k, lanes_per_query=lanes)
+    kw = {"packet": dict(lanes_per_query=1, packet_traversal=1),
+          "thread": dict(lanes_per_query=1, packet_traversal=2),
+          "warp": dict(lanes_per_query=32)}[mode]
+    ids, d2, _ = gpu_knn(rtd, pts, q, k, **kw)
     oi, od = orc.knn(pts, q, k)
+    assert_same(oi, od, ids, d2)
+
+
+@pytest.mark.parametrize("packet", [1, 2])
+@pytest.mark.parametrize("block", [64, 128, 256])
+def test_knn_block_sizes(rtd, orc, cuda, packet, block):
+    pts, q = clustered_small(n=15_000, nq=1_500, seed=19)
+    ids, d2, _ = gpu_knn(rtd, pts, q, 5, packet_traversal=packet, block_size=block)
+    oi, od = orc.knn(pts, q, 5)
     assert_same(oi, od, ids, d2)
 
 
@@ -98,10 +110,10 @@ def test_knn_duplicates_and_ties(rtd, orc, cuda):
     pts = np.concatenate([base, base, base[:100]])
     q = np.concatenate([base[:200], rng.integers(0, 8, size=(200, 3)).astype(np.float32) + 0.5])
     for k in (1, 5, 16, 40):
-        for lanes in (1, 32):
+        for lanes, packet in ((1, 1), (1, 2), (32, 0)):
             if lanes == 1 and k > 32:
                 continue
-            ids, d2, _ = gpu_knn(rtd, pts, q, k, lanes_per_query=lanes)
+            ids, d2, _ = gpu_knn(rtd, pts, q, k, lanes_per_query=lanes, packet_traversal=packet)
             oi, od = orc.knn(pts, q, k)
             assert_same(oi, od, ids, d2)
 

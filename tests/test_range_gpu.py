@@ -82,9 +82,14 @@ def test_range_large_property(rtd, orc, cuda):
     """400K queries on 1.8M points: the count pass and the fill agree
     (sum of counts = pairs written, per-query histogram of the pairs equals
     the counts), and a query sample matches the oracle exactly."""
+    from rtdsl.api import radius_for_mean_count
     pts, q = workloads.clustered()
-    r = 0.35
+    s = rtd.default_schedule()
+    ix = rtd.Index().build(torch.from_numpy(pts).cuda(), s)
+    r = radius_for_mean_count(ix, torch.from_numpy(q).cuda(), 50.0)
     counts, total, pairs = gpu_range(rtd, pts, q, r)
+    assert 40 <= total / len(q) <= 60          # the workload's mean of 50 neighbours
+    assert counts.max() > 1000                 # with a heavy tail in the dense clusters
     assert counts.sum() == total == len(pairs)
     np.testing.assert_array_equal(np.bincount(pairs[:, 0], minlength=len(q)), counts)
     assert np.all(np.diff(pairs[:, 0].astype(np.int64)) >= 0)
