@@ -83,10 +83,8 @@ def lib() -> C.CDLL:
             L.orc_direct_ref_f64.argtypes = [P, P, I64, P, I64, C.c_double, P]
             L.orc_key_public.argtypes = [P, P]
             L.orc_key_public.restype = F
-            L.orc_bh_group_lists.argtypes = [P, I64, P, I64, C.c_int, F, P, P, I64]
-            L.orc_bh_group_lists.restype = I64
-            L.orc_bh_plummer_eval.argtypes = [P, I64, P, P, I64, C.c_int, P, P, C.c_double,
-                                              C.c_double, C.c_int, P, P]
+            L.orc_bh_plummer_eval.argtypes = [P, I64, P, P, P, I64, F, C.c_double, C.c_double,
+                                              C.c_int, P, P]
             L.orc_bh_plummer_eval.restype = C.c_double
             L.orc_direct_plummer_f64.argtypes = [P, P, I64, C.c_double, C.c_double, P, P, P, P]
             L.orc_direct_plummer_f64.restype = C.c_double
@@ -224,32 +222,18 @@ def direct_ref_f64(pos, mass, targets, G: float = 6.674e-11) -> np.ndarray:
 
 
 class PlummerFrozen:
-    """Plummer-law BH with the group decisions of one configuration frozen
-    (reference tree of `bucket`, groups of 32 flat bodies, FP32 decisions as
-    the GPU makes them), evaluated in FP64 for perturbed inputs."""
+    """Plummer-law BH with the decisions of one configuration frozen (the
+    reference tree of `bucket`; per-body FP32 MAC decisions as the GPU makes
+    them, from this configuration's tree and positions), evaluated in FP64
+    for perturbed positions and masses."""
 
-    def __init__(self, pos, mass, theta: float, bucket: int, group: int = 32,
-                 min_width: float = 1e-5):
+    def __init__(self, pos, mass, theta: float, bucket: int, min_width: float = 1e-5):
         pos = _f32(pos)
         mass = _f32(mass)
         self.nodes, self.order, _ = bh_build(pos, mass, bucket=bucket, min_width=min_width)
         self.n = len(pos)
-        self.group = group
-        fpos = np.ascontiguousarray(pos[self.order])
-        ng = (self.n + group - 1) // group
-        self.offsets = np.zeros(ng + 1, dtype=np.int64)
-        cap = max(1024, 64 * ng)
-        while True:
-            items = np.empty(cap, dtype=np.int32)
-            tot = lib().orc_bh_group_lists(_p(self.nodes), len(self.nodes), _p(fpos), self.n, group,
-                                           C.c_float(theta), _p(self.offsets), _p(items), cap)
-            if tot >= 0:
-                self.items = items[:tot].copy()
-                break
-            cap = -tot
-        # flat position of each caller index
-        self.flat_of = np.empty(self.n, dtype=np.int64)
-        self.flat_of[self.order] = np.arange(self.n)
+        self.theta = theta
+        self.fpos32 = np.ascontiguousarray(pos[self.order])
 
     def eval(self, pos, mass, eps: float, G: float, quad: bool = True):
         """(L, phi [N], acc [N,3]) in FP64, caller order."""
@@ -257,9 +241,9 @@ class PlummerFrozen:
         m = np.ascontiguousarray(np.asarray(mass, dtype=np.float64)[self.order])
         phi = np.empty(self.n)
         acc = np.empty((self.n, 3))
-        L = lib().orc_bh_plummer_eval(_p(self.nodes), len(self.nodes), _p(p), _p(m), self.n,
-                                      self.group, _p(self.offsets), _p(self.items), eps, G,
-                                      int(quad), _p(phi), _p(acc))
+        L = lib().orc_bh_plummer_eval(_p(self.nodes), len(self.nodes), _p(self.fpos32), _p(p),
+                                      _p(m), self.n, C.c_float(self.theta), eps, G, int(quad),
+                                      _p(phi), _p(acc))
         out_phi = np.empty(self.n)
         out_acc = np.empty((self.n, 3))
         out_phi[self.order] = phi

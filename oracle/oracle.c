@@ -764,63 +764,19 @@ void orc_direct_ref_f64(const float *pos, const float *mass, int64_t n, const in
 /* ------------------------------------------------------------------------
  * Plummer-law Barnes-Hut (the build's physics mode; no reference
  * counterpart beyond the tree).  The tree is the reference tree built by
- * orc_bh_build (with its own bucket size).  Groups are 32 consecutive
- * bodies of the flat order; a node is accepted for a group when
- *     RN(width*width) < RN(theta2 * d2),  d2 = |gap(COM, group box)|^2
- * (all FP32, rounded per operation, theta2 = RN(theta*theta)); accepted
- * nodes interact as monopole (+ traceless quadrupole) multipoles, rejected
- * leaves by direct summation, rejected internal nodes are opened.
- * orc_bh_group_lists records these decisions once; orc_bh_plummer_eval
- * then evaluates phi, a and L = sum(phi) + 0.5*sum|a|^2 in FP64 for any
- * (perturbed) positions / masses with the decisions and the tree
- * membership held fixed -- the function whose derivative the GPU adjoint
+ * orc_bh_build (with its own bucket size).  A node is accepted for body i
+ * when RN(width*width) < RN(theta2 * d2), d2 = |COM - x_i|^2 summed left to
+ * right (all FP32, rounded per operation, theta2 = RN(theta*theta)): the
+ * decision the GPU walk makes.  Accepted nodes interact as monopole (+
+ * traceless quadrupole) multipoles about their COM, rejected leaves by
+ * direct summation, rejected internal nodes are opened.
+ * orc_bh_plummer_eval takes the decisions from the FP32 tree and the FP32
+ * positions of one configuration, and evaluates phi, a and
+ * L = sum(phi) + 0.5*sum|a|^2 in FP64 for FP64 (possibly perturbed)
+ * positions and masses, with cell moments recomputed from them over the
+ * fixed tree membership: the function whose derivative the GPU adjoint
  * computes, so central finite differences of it check the adjoint.
  * ---------------------------------------------------------------------- */
-static float orc_gap(float lo, float hi, float c) {
-    float a = lo - c, b = c - hi;
-    return fmaxf(fmaxf(a, b), 0.0f);
-}
-
-/* items: node index * 2 + (1 if direct leaf sum else 0). Returns the item
- * count (or -needed when capacity is too small). */
-int64_t orc_bh_group_lists(const orc_flat_node *nodes, int64_t nn, const float *fpos, int64_t n,
-                           int group, float theta, int64_t *offsets, int32_t *items,
-                           int64_t capacity) {
-    const float th2 = theta * theta;
-    int64_t ng = (n + group - 1) / group;
-    int64_t total = 0;
-    offsets[0] = 0;
-    for (int64_t g = 0; g < ng; ++g) {
-        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-        for (int64_t i = g * group; i < (g + 1) * group && i < n; ++i)
-            for (int a = 0; a < 3; ++a) {
-                lo[a] = fminf(lo[a], fpos[3 * i + a]);
-                hi[a] = fmaxf(hi[a], fpos[3 * i + a]);
-            }
-        int64_t p = 0;
-        while (p < nn) {
-            const orc_flat_node *nd = &nodes[p];
-            float tx = orc_gap(lo[0], hi[0], nd->com[0]);
-            float ty = orc_gap(lo[1], hi[1], nd->com[1]);
-            float tz = orc_gap(lo[2], hi[2], nd->com[2]);
-            float d2 = orc_dot3(tx, ty, tz);
-            int accept = nd->width * nd->width < th2 * d2;
-            if (accept) {
-                if (total < capacity) items[total] = (int32_t)(2 * p);
-                ++total;
-                p = nd->autorope;
-            } else if (nd->is_leaf) {
-                if (total < capacity) items[total] = (int32_t)(2 * p + 1);
-                ++total;
-                p = p + 1;
-            } else {
-                p = p + 1;
-            }
-        }
-        offsets[g + 1] = total;
-    }
-    return total <= capacity ? total : -total;
-}
 
 typedef struct { double c[3]; double m; double q[6]; } orc_cell64;
 
@@ -856,59 +812,64 @@ static void orc_cells64(const orc_flat_node *nodes, int64_t nn, const double *po
     free(first);
 }
 
-/* pos/mass in flat order (n*3, n).  Returns L; phi/acc optional (flat). */
-double orc_bh_plummer_eval(const orc_flat_node *nodes, int64_t nn, const double *pos,
-                           const double *mass, int64_t n, int group, const int64_t *offsets,
-                           const int32_t *items, double eps, double G, int quad, double *phi,
-                           double *acc) {
+/* pos32: the FP32 flat-order positions the decisions use; pos/mass: FP64
+ * flat-order values.  Returns L; phi/acc optional (flat order). */
+double orc_bh_plummer_eval(const orc_flat_node *nodes, int64_t nn, const float *pos32,
+                           const double *pos, const double *mass, int64_t n, float theta,
+                           double eps, double G, int quad, double *phi, double *acc) {
     orc_cell64 *cells = (orc_cell64 *)malloc(sizeof(orc_cell64) * (size_t)(nn > 0 ? nn : 1));
     orc_cells64(nodes, nn, pos, mass, n, cells);
     const double e2 = eps * eps;
-    int64_t ng = (n + group - 1) / group;
+    const float th2 = theta * theta;
     double L = 0;
-#pragma omp parallel for schedule(dynamic, 4) reduction(+ : L)
-    for (int64_t g = 0; g < ng; ++g) {
-        for (int64_t i = g * group; i < (g + 1) * group && i < n; ++i) {
-            const double *x = pos + 3 * i;
-            double ph = 0, ax = 0, ay = 0, az = 0;
-            for (int64_t t = offsets[g]; t < offsets[g + 1]; ++t) {
-                int64_t p = items[t] >> 1;
-                if (items[t] & 1) {
-                    int64_t s = nodes[p].bucket_start, c = nodes[p].num_particles;
-                    for (int64_t j = s; j < s + c; ++j) {
-                        if (j == i) continue;
-                        double rx = x[0] - pos[3 * j], ry = x[1] - pos[3 * j + 1], rz = x[2] - pos[3 * j + 2];
-                        double s2 = rx * rx + ry * ry + rz * rz + e2;
-                        double i1 = 1.0 / sqrt(s2), i3 = i1 * i1 * i1;
-                        ph -= mass[j] * i1;
-                        ax -= mass[j] * rx * i3; ay -= mass[j] * ry * i3; az -= mass[j] * rz * i3;
-                    }
-                } else {
-                    const orc_cell64 *c = &cells[p];
-                    double rx = x[0] - c->c[0], ry = x[1] - c->c[1], rz = x[2] - c->c[2];
-                    double s2 = rx * rx + ry * ry + rz * rz + e2;
-                    double i1 = 1.0 / sqrt(s2), i2 = i1 * i1, i3 = i1 * i2;
-                    ph -= c->m * i1;
-                    ax -= c->m * rx * i3; ay -= c->m * ry * i3; az -= c->m * rz * i3;
-                    if (quad) {
-                        const double *Q = c->q;
-                        double qx = Q[0] * rx + Q[3] * ry + Q[4] * rz;
-                        double qy = Q[3] * rx + Q[1] * ry + Q[5] * rz;
-                        double qz = Q[4] * rx + Q[5] * ry + Q[2] * rz;
-                        double q = rx * qx + ry * qy + rz * qz;
-                        double i5 = i3 * i2, i7 = i5 * i2;
-                        ph -= 0.5 * q * i5;
-                        ax += qx * i5 - 2.5 * q * rx * i7;
-                        ay += qy * i5 - 2.5 * q * ry * i7;
-                        az += qz * i5 - 2.5 * q * rz * i7;
-                    }
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : L)
+    for (int64_t i = 0; i < n; ++i) {
+        const double *x = pos + 3 * i;
+        const float *x32 = pos32 + 3 * i;
+        double ph = 0, ax = 0, ay = 0, az = 0;
+        int64_t p = 0;
+        while (p < nn) {
+            const orc_flat_node *nd = &nodes[p];
+            float d2 = orc_dot3(nd->com[0] - x32[0], nd->com[1] - x32[1], nd->com[2] - x32[2]);
+            if (nd->width * nd->width < th2 * d2) {
+                const orc_cell64 *c = &cells[p];
+                double rx = x[0] - c->c[0], ry = x[1] - c->c[1], rz = x[2] - c->c[2];
+                double s2 = rx * rx + ry * ry + rz * rz + e2;
+                double i1 = 1.0 / sqrt(s2), i2 = i1 * i1, i3 = i1 * i2;
+                ph -= c->m * i1;
+                ax -= c->m * rx * i3; ay -= c->m * ry * i3; az -= c->m * rz * i3;
+                if (quad) {
+                    const double *Q = c->q;
+                    double qx = Q[0] * rx + Q[3] * ry + Q[4] * rz;
+                    double qy = Q[3] * rx + Q[1] * ry + Q[5] * rz;
+                    double qz = Q[4] * rx + Q[5] * ry + Q[2] * rz;
+                    double q = rx * qx + ry * qy + rz * qz;
+                    double i5 = i3 * i2, i7 = i5 * i2;
+                    ph -= 0.5 * q * i5;
+                    ax += qx * i5 - 2.5 * q * rx * i7;
+                    ay += qy * i5 - 2.5 * q * ry * i7;
+                    az += qz * i5 - 2.5 * q * rz * i7;
                 }
+                p = nd->autorope;
+            } else if (nd->is_leaf) {
+                int64_t s = nd->bucket_start, cnt = nd->num_particles;
+                for (int64_t j = s; j < s + cnt; ++j) {
+                    if (j == i) continue;
+                    double rx = x[0] - pos[3 * j], ry = x[1] - pos[3 * j + 1], rz = x[2] - pos[3 * j + 2];
+                    double s2 = rx * rx + ry * ry + rz * rz + e2;
+                    double i1 = 1.0 / sqrt(s2), i3 = i1 * i1 * i1;
+                    ph -= mass[j] * i1;
+                    ax -= mass[j] * rx * i3; ay -= mass[j] * ry * i3; az -= mass[j] * rz * i3;
+                }
+                p = p + 1;
+            } else {
+                p = p + 1;
             }
-            ph *= G; ax *= G; ay *= G; az *= G;
-            if (phi) phi[i] = ph;
-            if (acc) { acc[3 * i] = ax; acc[3 * i + 1] = ay; acc[3 * i + 2] = az; }
-            L += ph + 0.5 * (ax * ax + ay * ay + az * az);
         }
+        ph *= G; ax *= G; ay *= G; az *= G;
+        if (phi) phi[i] = ph;
+        if (acc) { acc[3 * i] = ax; acc[3 * i + 1] = ay; acc[3 * i + 2] = az; }
+        L += ph + 0.5 * (ax * ax + ay * ay + az * az);
     }
     free(cells);
     return L;

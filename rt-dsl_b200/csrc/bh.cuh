@@ -30,7 +30,12 @@ struct BhHeader {
     uint32_t err;
     uint32_t level_count[BH_MAX_LEVEL + 2];
     uint32_t level_off[BH_MAX_LEVEL + 3];
+    uint32_t n_groups;        // warp groups of the Plummer walks
+    uint32_t max_stack;       // deepest traversal stack seen by a walk
+    uint32_t group_counter;   // work queue of the walks (next group to take)
 };
+
+constexpr int BH_STACK_CAP = 8192;          // traversal stack entries per walking warp
 
 }  // namespace rtd
 
@@ -39,6 +44,8 @@ struct rtd_bh {
     uint32_t bucket = 128;
     float min_width = 1e-5f;
     bool built = false;
+    bool plummer_ready = false;   // child table and groups built (Plummer-law walks)
+    bool has_quad = false;        // quadrupoles computed
     rtd::DevBuf hdr;
     // build scratch
     rtd::DevBuf mkeys, mkeys_alt, mvals, mvals_alt;   // Morton sort
@@ -52,6 +59,9 @@ struct rtd_bh {
     rtd::DevBuf order;        // flat order: original index of the i-th body
     rtd::DevBuf fbody;        // float4 (pos, mass) in flat order
     rtd::DevBuf node_a, node_b, node_q;
+    // walk structures: child table (8 per node), leaf list, warp groups
+    rtd::DevBuf child8, leaf_node, groups, stack;
+    uint64_t stack_warps = 0;
     // adjoint scratch
     rtd::DevBuf cell_grad, prefix, gpos_flat, gmass_flat;
 };
@@ -72,11 +82,14 @@ struct BhView {
     const uint32_t *order;
     const BhHeader *hdr;
     uint64_t n;
+    const uint4 *child8;       // 2 uint4 per node: up to 8 children, 0xFFFFFFFF pads
+    const uint2 *groups;       // (first flat body, count <= 32)
 };
 
 inline BhView bh_view(const rtd_bh *b) {
     return BhView{b->node_a.as<float4>(), b->node_b.as<uint4>(), b->node_q.as<float4>(),
-                  b->fbody.as<float4>(), b->order.as<uint32_t>(), b->hdr.as<BhHeader>(), b->n};
+                  b->fbody.as<float4>(), b->order.as<uint32_t>(), b->hdr.as<BhHeader>(), b->n,
+                  b->child8.as<uint4>(), b->groups.as<uint2>()};
 }
 
 rtd_status bh_build(rtd_bh *b, const float *d_pos, const float *d_mass, uint64_t n,

@@ -1,0 +1,544 @@
+// bh_plummer.cu -- Plummer-law Barnes-Hut walks (forward and adjoint).
+//
+// Physics: phi_i = -G sum_j m_j / sqrt(|x_i - x_j|^2 + eps^2), a_i =
+// -grad phi_i; accepted cells act as monopole + traceless quadrupole about
+// their COM with the same softened distance.  A cell is accepted for body
+// i when width^2 < theta^2 |COM - x_i|^2 (each operation rounded, so the
+// CPU oracle makes identical decisions); rejected leaves are summed
+// directly, rejected internal cells opened.
+//
+// Execution: a warp takes a group of <= 32 bodies (packed sibling leaves,
+// so spatially compact) and walks the tree once for all of them.  Stack
+// entries carry the mask of lanes that still need the node; per step up to
+// 32 entries are loaded in parallel and each is tested by every lane in its
+// mask.  Accepted cells and the bodies of rejected leaves go to per-warp
+// lists with their lane masks; every 32 entries form a tile staged in
+// shared memory and evaluated by all lanes from broadcast reads.
+//
+// Adjoint (dL/dx, dL/dm for upstream dL/da, dL/dphi): per tile, pass 1
+// (lane = body) adds d/dx_i of the body's interactions; pass 2 (lane =
+// source) sums the source-side derivatives over the group's bodies and
+// issues one vector atomic per source.  Cell derivatives (COM, mass,
+// quadrupole) are then pushed to the bodies by a top-down pass: with Q
+// about the COM the first moment vanishes, so for a cell C holding body j
+//     dL/dx_j += m_j (g_c/M - 2 B c + 2 B x_j)
+//     dL/dm_j += g_M + g_c.(x_j - c)/M + (x_j - c)^T B (x_j - c)
+// with B = 3 sym(G_Q) - tr(G_Q) I; both split into per-node constants that
+// add up along root-to-leaf paths.
+#include <rtdsl.h>
+
+#include "bh.cuh"
+
+namespace rtd {
+namespace {
+
+constexpr int WW = 4;   // warps per block
+
+struct WarpTile {
+    float4 cell[32][3];   // (com, M), (Qxx Qyy Qzz Qxy), (Qxz Qyz 0 0)
+    uint32_t cmask_t[32];
+    float4 body[32];      // (x, y, z, m)
+    uint32_t bid[32];
+    uint32_t bmask_t[32];
+    uint32_t clist[32], cmask[32];
+    uint32_t blist[64], bmask[64];
+    float4 gpos[32];      // group bodies (adjoint source-side pass)
+    float4 gv[32];        // (dL/da, dL/dphi)
+};
+
+__device__ __forceinline__ float dot3_rn(float x, float y, float z) {
+    float s = __fmul_rn(x, x);
+    s = __fadd_rn(s, __fmul_rn(y, y));
+    s = __fadd_rn(s, __fmul_rn(z, z));
+    return s;
+}
+
+// Per-body MAC: accept when width^2 < theta^2 * |COM - x|^2.
+__device__ __forceinline__ bool body_accept(float x, float y, float z, float cx, float cy, float cz,
+                                            float width, float theta2) {
+    const float d2 = dot3_rn(__fsub_rn(cx, x), __fsub_rn(cy, y), __fsub_rn(cz, z));
+    return __fmul_rn(width, width) < __fmul_rn(theta2, d2);
+}
+
+__device__ __forceinline__ uint32_t lane_lt() {
+    uint32_t m;
+    asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Forward interaction of field point r = x - c with a cell (G omitted).
+template <bool QUAD>
+__device__ __forceinline__ void cell_fwd(float rx, float ry, float rz, const float4 &c,
+                                         const float4 &q0, const float4 &q1, float eps2,
+                                         float &ax, float &ay, float &az, float &phi) {
+    const float s = rx * rx + ry * ry + rz * rz + eps2;
+    const float i1 = rsqrtf(s), i2 = i1 * i1, i3 = i1 * i2;
+    phi -= c.w * i1;
+    ax -= c.w * rx * i3;
+    ay -= c.w * ry * i3;
+    az -= c.w * rz * i3;
+    if (QUAD) {
+        const float qx = q0.x * rx + q0.w * ry + q1.x * rz;
+        const float qy = q0.w * rx + q0.y * ry + q1.y * rz;
+        const float qz = q1.x * rx + q1.y * ry + q0.z * rz;
+        const float q = rx * qx + ry * qy + rz * qz;
+        const float i5 = i3 * i2, i7 = i5 * i2;
+        phi -= 0.5f * q * i5;
+        ax += qx * i5 - 2.5f * q * rx * i7;
+        ay += qy * i5 - 2.5f * q * ry * i7;
+        az += qz * i5 - 2.5f * q * rz * i7;
+    }
+}
+
+// Derivatives of u*phi + v.a for one cell interaction (G omitted):
+// g_r = d/dr (r = x - c), gM = d/dM, gq = d/dQ (symmetric part, 6 comps).
+template <bool QUAD>
+__device__ __forceinline__ void cell_adj(float rx, float ry, float rz, const float4 &c,
+                                         const float4 &q0, const float4 &q1, float eps2, float u,
+                                         float vx, float vy, float vz, float &grx, float &gry,
+                                         float &grz, float &gM, float gq[6]) {
+    const float s = rx * rx + ry * ry + rz * rz + eps2;
+    const float i1 = rsqrtf(s), i2 = i1 * i1, i3 = i1 * i2, i5 = i3 * i2;
+    const float M = c.w;
+    const float vr = vx * rx + vy * ry + vz * rz;
+    grx = u * M * rx * i3 - M * (vx * i3 - 3.f * vr * rx * i5);
+    gry = u * M * ry * i3 - M * (vy * i3 - 3.f * vr * ry * i5);
+    grz = u * M * rz * i3 - M * (vz * i3 - 3.f * vr * rz * i5);
+    gM = -u * i1 - vr * i3;
+    if (QUAD) {
+        const float Qxx = q0.x, Qyy = q0.y, Qzz = q0.z, Qxy = q0.w, Qxz = q1.x, Qyz = q1.y;
+        const float qrx = Qxx * rx + Qxy * ry + Qxz * rz;
+        const float qry = Qxy * rx + Qyy * ry + Qyz * rz;
+        const float qrz = Qxz * rx + Qyz * ry + Qzz * rz;
+        const float qvx = Qxx * vx + Qxy * vy + Qxz * vz;
+        const float qvy = Qxy * vx + Qyy * vy + Qyz * vz;
+        const float qvz = Qxz * vx + Qyz * vy + Qzz * vz;
+        const float q = rx * qrx + ry * qry + rz * qrz;
+        const float vqr = vx * qrx + vy * qry + vz * qrz;
+        const float i7 = i5 * i2, i9 = i7 * i2;
+        // phi_Q = -q i5 / 2, a_Q = Qr i5 - 2.5 q r i7: u dphi_Q/dr = -u a_Q
+        const float k1 = 2.5f * q * i7;
+        grx -= u * (qrx * i5 - k1 * rx);
+        gry -= u * (qry * i5 - k1 * ry);
+        grz -= u * (qrz * i5 - k1 * rz);
+        // d(v.a_Q)/dr = Qv i5 - 5 vQr i7 r - 5 vr i7 Qr - 2.5 q i7 v + 17.5 q vr i9 r
+        const float kr = -5.f * vqr * i7 + 17.5f * q * vr * i9;
+        const float kq = -5.f * vr * i7;
+        const float kv = -2.5f * q * i7;
+        grx += qvx * i5 + kr * rx + kq * qrx + kv * vx;
+        gry += qvy * i5 + kr * ry + kq * qry + kv * vy;
+        grz += qvz * i5 + kr * rz + kq * qrz + kv * vz;
+        // dL/dQ: -u i5 rr^T / 2 + i5 sym(v r^T) - 2.5 vr i7 rr^T
+        const float cr = -0.5f * u * i5 - 2.5f * vr * i7;
+        gq[0] = cr * rx * rx + i5 * vx * rx;
+        gq[1] = cr * ry * ry + i5 * vy * ry;
+        gq[2] = cr * rz * rz + i5 * vz * rz;
+        gq[3] = cr * rx * ry + 0.5f * i5 * (vx * ry + vy * rx);
+        gq[4] = cr * rx * rz + 0.5f * i5 * (vx * rz + vz * rx);
+        gq[5] = cr * ry * rz + 0.5f * i5 * (vy * rz + vz * ry);
+    }
+}
+
+// Derivatives of u*phi + v.a for one body-body interaction (G omitted),
+// r = x_target - x_source, source mass m: g_r and d/dm.
+__device__ __forceinline__ void body_adj(float rx, float ry, float rz, float m, float eps2, float u,
+                                         float vx, float vy, float vz, float &grx, float &gry,
+                                         float &grz, float &gm) {
+    const float s = rx * rx + ry * ry + rz * rz + eps2;
+    const float i1 = rsqrtf(s), i2 = i1 * i1, i3 = i1 * i2, i5 = i3 * i2;
+    const float vr = vx * rx + vy * ry + vz * rz;
+    grx = u * m * rx * i3 - m * (vx * i3 - 3.f * vr * rx * i5);
+    gry = u * m * ry * i3 - m * (vy * i3 - 3.f * vr * ry * i5);
+    grz = u * m * rz * i3 - m * (vz * i3 - 3.f * vr * rz * i5);
+    gm = -u * i1 - vr * i3;
+}
+
+template <bool QUAD, bool ADJ>
+__global__ void __launch_bounds__(WW * 32) bh_walk_kernel(
+    const BhView v, float theta2, float eps2, float G, const float *__restrict__ g_acc,
+    const float *__restrict__ g_phi, float *__restrict__ acc_out, float *__restrict__ phi_out,
+    float4 *__restrict__ cell_grad, float4 *__restrict__ body_grad, uint2 *__restrict__ stack,
+    BhHeader *hm) {
+    __shared__ WarpTile tiles[WW];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    WarpTile &T = tiles[warp];
+    const uint64_t gw = (uint64_t)blockIdx.x * WW + warp;
+    uint2 *stk = stack + gw * BH_STACK_CAP;
+    const uint32_t ngroups = v.hdr->n_groups, n_nodes = v.hdr->n_nodes;
+    const uint32_t lt = lane_lt();
+    const uint32_t *child = reinterpret_cast<const uint32_t *>(v.child8);
+    uint32_t max_sp = 0;
+    while (true) {
+        uint32_t g = 0;
+        if (lane == 0) g = atomicAdd(&hm->group_counter, 1u);
+        g = __shfl_sync(0xffffffffu, g, 0);
+        if (g >= ngroups) break;
+        const uint2 gr = v.groups[g];
+        const uint32_t gs = gr.x, gc = gr.y;
+        const uint32_t i = gs + lane;
+        const bool valid = (uint32_t)lane < gc;
+        const float4 me = valid ? v.fbody[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        float ax = 0.f, ay = 0.f, az = 0.f, phi = 0.f;   // forward sums / adjoint d/dx_i
+        float vx = 0.f, vy = 0.f, vz = 0.f, u = 0.f;
+        if (ADJ) {
+            if (valid) {
+                const uint32_t o = v.order[i];
+                vx = g_acc[3 * (uint64_t)o];
+                vy = g_acc[3 * (uint64_t)o + 1];
+                vz = g_acc[3 * (uint64_t)o + 2];
+                u = g_phi ? g_phi[o] : 0.f;
+            }
+            T.gpos[lane] = me;
+            T.gv[lane] = make_float4(vx, vy, vz, u);
+        }
+        int cn = 0, bn = 0, sp = 0;
+        const uint32_t all = __ballot_sync(0xffffffffu, valid);
+        if (n_nodes > 0) {
+            if (lane == 0) stk[0] = make_uint2(0u, all);
+            sp = 1;
+        }
+        __syncwarp();
+
+        auto eval_cells = [&](int cnt) {
+            uint32_t nid = 0, cm = 0;
+            if (lane < cnt) {
+                nid = T.clist[lane];
+                cm = T.cmask[lane];
+                T.cell[lane][0] = __ldg(&v.node_a[nid]);
+                if (QUAD) {
+                    T.cell[lane][1] = __ldg(&v.node_q[2 * nid]);
+                    T.cell[lane][2] = __ldg(&v.node_q[2 * nid + 1]);
+                }
+                T.cmask_t[lane] = cm;
+            }
+            __syncwarp();
+            const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int k = 0; k < cnt; ++k) {   // lane = body
+                if (!((T.cmask_t[k] >> lane) & 1u)) continue;
+                const float4 c = T.cell[k][0];
+                const float4 q0 = QUAD ? T.cell[k][1] : z4, q1 = QUAD ? T.cell[k][2] : z4;
+                if (!ADJ) {
+                    cell_fwd<QUAD>(me.x - c.x, me.y - c.y, me.z - c.z, c, q0, q1, eps2, ax, ay, az, phi);
+                } else {
+                    float grx, gry, grz, gM, gq[6];
+                    cell_adj<QUAD>(me.x - c.x, me.y - c.y, me.z - c.z, c, q0, q1, eps2, u, vx, vy,
+                                   vz, grx, gry, grz, gM, gq);
+                    ax += grx; ay += gry; az += grz;
+                }
+            }
+            if (ADJ && lane < cnt) {          // lane = cell, over the group's bodies
+                const float4 c = T.cell[lane][0];
+                const float4 q0 = QUAD ? T.cell[lane][1] : z4, q1 = QUAD ? T.cell[lane][2] : z4;
+                float sx = 0.f, sy = 0.f, sz = 0.f, sM = 0.f, sq[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                for (uint32_t m = cm; m; m &= m - 1) {
+                    const int bb = __ffs(m) - 1;
+                    const float4 p = T.gpos[bb], w = T.gv[bb];
+                    float grx, gry, grz, gM, gq[6];
+                    cell_adj<QUAD>(p.x - c.x, p.y - c.y, p.z - c.z, c, q0, q1, eps2, w.w, w.x, w.y,
+                                   w.z, grx, gry, grz, gM, gq);
+                    sx -= grx; sy -= gry; sz -= grz; sM += gM;
+                    if (QUAD)
+                        for (int t = 0; t < 6; ++t) sq[t] += gq[t];
+                }
+                atomicAdd(&cell_grad[3 * nid], make_float4(G * sx, G * sy, G * sz, G * sM));
+                if (QUAD) {
+                    atomicAdd(&cell_grad[3 * nid + 1], make_float4(G * sq[0], G * sq[1], G * sq[2], G * sq[3]));
+                    atomicAdd(&cell_grad[3 * nid + 2], make_float4(G * sq[4], G * sq[5], 0.f, 0.f));
+                }
+            }
+            __syncwarp();
+        };
+        auto eval_bodies = [&](int cnt) {
+            uint32_t bid = 0, bm = 0;
+            if (lane < cnt) {
+                bid = T.blist[lane];
+                bm = T.bmask[lane];
+                T.body[lane] = __ldg(&v.fbody[bid]);
+                T.bid[lane] = bid;
+                T.bmask_t[lane] = bm;
+            }
+            __syncwarp();
+            for (int k = 0; k < cnt; ++k) {   // lane = target
+                if (!((T.bmask_t[k] >> lane) & 1u) || T.bid[k] == i) continue;
+                const float4 o = T.body[k];
+                if (!ADJ) {
+                    const float rx = me.x - o.x, ry = me.y - o.y, rz = me.z - o.z;
+                    const float s = rx * rx + ry * ry + rz * rz + eps2;
+                    const float i1 = rsqrtf(s), i3 = i1 * i1 * i1;
+                    phi -= o.w * i1;
+                    ax -= o.w * rx * i3;
+                    ay -= o.w * ry * i3;
+                    az -= o.w * rz * i3;
+                } else {
+                    float grx, gry, grz, gm;
+                    body_adj(me.x - o.x, me.y - o.y, me.z - o.z, o.w, eps2, u, vx, vy, vz, grx, gry, grz, gm);
+                    ax += grx; ay += gry; az += grz;
+                }
+            }
+            if (ADJ && lane < cnt) {          // lane = source, over the group's bodies
+                const float4 o = T.body[lane];
+                float sx = 0.f, sy = 0.f, sz = 0.f, sm = 0.f;
+                for (uint32_t m = bm; m; m &= m - 1) {
+                    const int bb = __ffs(m) - 1;
+                    if (gs + bb == bid) continue;
+                    const float4 p = T.gpos[bb], w = T.gv[bb];
+                    float grx, gry, grz, gm;
+                    body_adj(p.x - o.x, p.y - o.y, p.z - o.z, o.w, eps2, w.w, w.x, w.y, w.z, grx, gry, grz, gm);
+                    sx -= grx; sy -= gry; sz -= grz; sm += gm;
+                }
+                atomicAdd(&body_grad[bid], make_float4(G * sx, G * sy, G * sz, G * sm));
+            }
+            __syncwarp();
+        };
+
+        while (sp > 0) {
+            const int t = sp < 32 ? sp : 32;
+            sp -= t;
+            uint2 e = make_uint2(0u, 0u);
+            float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+            uint4 b = make_uint4(0u, 0u, 0u, 0u);
+            if (lane < t) {
+                e = stk[sp + lane];
+                a = __ldg(&v.node_a[e.x]);
+                b = __ldg(&v.node_b[e.x]);
+            }
+            __syncwarp();
+            for (int k = 0; k < t; ++k) {
+                const uint32_t nk = __shfl_sync(0xffffffffu, e.x, k);
+                const uint32_t mk = __shfl_sync(0xffffffffu, e.y, k);
+                const float cx = __shfl_sync(0xffffffffu, a.x, k);
+                const float cy = __shfl_sync(0xffffffffu, a.y, k);
+                const float cz = __shfl_sync(0xffffffffu, a.z, k);
+                const uint32_t bz = __shfl_sync(0xffffffffu, b.z, k);
+                const uint32_t bw = __shfl_sync(0xffffffffu, b.w, k);
+                const bool in = (mk >> lane) & 1u;
+                const bool acc = in && body_accept(me.x, me.y, me.z, cx, cy, cz, __uint_as_float(bw), theta2);
+                const uint32_t A = __ballot_sync(0xffffffffu, acc);
+                const uint32_t R = mk & ~A;
+                if (A) {
+                    if (lane == 0) { T.clist[cn] = nk; T.cmask[cn] = A; }
+                    ++cn;
+                    __syncwarp();
+                    if (cn == 32) { eval_cells(32); cn = 0; }
+                }
+                if (!R) continue;
+                if (bz & BH_LEAF_BIT) {
+                    const uint32_t bs = __shfl_sync(0xffffffffu, b.y, k);
+                    const uint32_t bc = bz & ~BH_LEAF_BIT;
+                    for (uint32_t off = 0; off < bc; off += 32) {
+                        const uint32_t kk = bc - off < 32u ? bc - off : 32u;
+                        if ((uint32_t)lane < kk) {
+                            T.blist[bn + lane] = bs + off + lane;
+                            T.bmask[bn + lane] = R;
+                        }
+                        bn += (int)kk;
+                        __syncwarp();
+                        if (bn >= 32) {
+                            eval_bodies(32);
+                            if (lane < bn - 32) {
+                                T.blist[lane] = T.blist[32 + lane];
+                                T.bmask[lane] = T.bmask[32 + lane];
+                            }
+                            bn -= 32;
+                            __syncwarp();
+                        }
+                    }
+                } else {
+                    const uint32_t c = lane < 8 ? __ldg(&child[8 * (uint64_t)nk + lane]) : 0xFFFFFFFFu;
+                    const uint32_t pm = __ballot_sync(0xffffffffu, c != 0xFFFFFFFFu);
+                    const int np = __popc(pm);
+                    if (sp + np <= BH_STACK_CAP) {
+                        if (c != 0xFFFFFFFFu) stk[sp + __popc(pm & lt)] = make_uint2(c, R);
+                        sp += np;
+                    } else if (lane == 0) {
+                        atomicOr(&hm->err, DEVERR_STACK);
+                    }
+                    __syncwarp();
+                }
+            }
+            max_sp = max(max_sp, (uint32_t)sp);
+        }
+        if (cn > 0) eval_cells(cn);
+        if (bn > 0) eval_bodies(bn);
+        if (valid) {
+            if (!ADJ) {
+                const uint32_t o = v.order[i];
+                acc_out[3 * (uint64_t)o] = G * ax;
+                acc_out[3 * (uint64_t)o + 1] = G * ay;
+                acc_out[3 * (uint64_t)o + 2] = G * az;
+                if (phi_out) phi_out[o] = G * phi;
+            } else {
+                atomicAdd(&body_grad[i], make_float4(G * ax, G * ay, G * az, 0.f));
+            }
+        }
+        __syncwarp();
+    }
+    if (lane == 0) atomicMax(&hm->max_stack, max_sp);
+}
+
+// Per-node constants of the cell-to-body rule (Pvec.xyz, Pconst | Pmat xx
+// yy zz xy | xz yz) from the cell's derivatives (g_c, g_M | G_Q).
+__device__ __forceinline__ void cell_constants(const float4 a, const float4 *cg, float out[10]) {
+    const float4 g0 = cg[0], g1 = cg[1], g2 = cg[2];
+    const float M = a.w, cx = a.x, cy = a.y, cz = a.z;
+    const float Gxx = g1.x, Gyy = g1.y, Gzz = g1.z, Gxy = g1.w, Gxz = g2.x, Gyz = g2.y;
+    const float tr = Gxx + Gyy + Gzz;
+    const float Bxx = 3.f * Gxx - tr, Byy = 3.f * Gyy - tr, Bzz = 3.f * Gzz - tr;
+    const float Bxy = 3.f * Gxy, Bxz = 3.f * Gxz, Byz = 3.f * Gyz;
+    const float Bcx = Bxx * cx + Bxy * cy + Bxz * cz;
+    const float Bcy = Bxy * cx + Byy * cy + Byz * cz;
+    const float Bcz = Bxz * cx + Byz * cy + Bzz * cz;
+    const float invM = M > 0.f ? 1.f / M : 0.f;
+    out[0] = g0.x * invM - 2.f * Bcx;
+    out[1] = g0.y * invM - 2.f * Bcy;
+    out[2] = g0.z * invM - 2.f * Bcz;
+    out[3] = g0.w - (g0.x * cx + g0.y * cy + g0.z * cz) * invM + (cx * Bcx + cy * Bcy + cz * Bcz);
+    out[4] = Bxx; out[5] = Byy; out[6] = Bzz; out[7] = Bxy; out[8] = Bxz; out[9] = Byz;
+}
+
+// Top-down path sums of the per-node constants (one block, level by level).
+__global__ void __launch_bounds__(1024) bh_prefix_kernel(const BhView v,
+                                                         const uint32_t *__restrict__ level_nodes,
+                                                         const float4 *__restrict__ cell_grad,
+                                                         float4 *prefix) {
+    const BhHeader *h = v.hdr;
+    for (int l = 0; l <= BH_MAX_LEVEL + 1; ++l) {
+        const uint32_t off = h->level_off[l], cnt = h->level_count[l];
+        for (uint32_t t = threadIdx.x; t < cnt; t += blockDim.x) {
+            const uint32_t i = level_nodes[off + t];
+            float own[10];
+            cell_constants(v.node_a[i], cell_grad + 3 * i, own);
+            const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+            float4 p0 = l == 0 ? z : prefix[3 * i];      // the parent's path sum
+            float4 p1 = l == 0 ? z : prefix[3 * i + 1];
+            float4 p2 = l == 0 ? z : prefix[3 * i + 2];
+            p0 = make_float4(p0.x + own[0], p0.y + own[1], p0.z + own[2], p0.w + own[3]);
+            p1 = make_float4(p1.x + own[4], p1.y + own[5], p1.z + own[6], p1.w + own[7]);
+            p2 = make_float4(p2.x + own[8], p2.y + own[9], 0.f, 0.f);
+            prefix[3 * i] = p0;
+            prefix[3 * i + 1] = p1;
+            prefix[3 * i + 2] = p2;
+            const uint4 b = v.node_b[i];
+            if (!(b.z & BH_LEAF_BIT))
+                for (uint32_t c = i + 1; c < b.x; c = v.node_b[c].x) {
+                    prefix[3 * c] = p0;
+                    prefix[3 * c + 1] = p1;
+                    prefix[3 * c + 2] = p2;
+                }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(128) bh_finish_grad_kernel(const BhView v,
+                                                             const float4 *__restrict__ prefix,
+                                                             const float4 *__restrict__ body_grad,
+                                                             float *__restrict__ g_pos,
+                                                             float *__restrict__ g_mass) {
+    const uint32_t n_nodes = v.hdr->n_nodes;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_nodes; i += gridDim.x * blockDim.x) {
+        const uint4 b = v.node_b[i];
+        if (!(b.z & BH_LEAF_BIT)) continue;
+        const float4 p0 = prefix[3 * i], p1 = prefix[3 * i + 1], p2 = prefix[3 * i + 2];
+        const float Pxx = p1.x, Pyy = p1.y, Pzz = p1.z, Pxy = p1.w, Pxz = p2.x, Pyz = p2.y;
+        const uint32_t s0 = b.y, c = b.z & ~BH_LEAF_BIT;
+        for (uint32_t k = 0; k < c; ++k) {
+            const float4 o = v.fbody[s0 + k];
+            const float Px = Pxx * o.x + Pxy * o.y + Pxz * o.z;
+            const float Py = Pxy * o.x + Pyy * o.y + Pyz * o.z;
+            const float Pz = Pxz * o.x + Pyz * o.y + Pzz * o.z;
+            const float4 bg = body_grad[s0 + k];
+            const uint32_t orig = v.order[s0 + k];
+            g_pos[3 * (uint64_t)orig] = bg.x + o.w * (p0.x + 2.f * Px);
+            g_pos[3 * (uint64_t)orig + 1] = bg.y + o.w * (p0.y + 2.f * Py);
+            g_pos[3 * (uint64_t)orig + 2] = bg.z + o.w * (p0.z + 2.f * Pz);
+            if (g_mass)
+                g_mass[orig] = bg.w + p0.w + (p0.x * o.x + p0.y * o.y + p0.z * o.z) +
+                               (o.x * Px + o.y * Py + o.z * Pz);
+        }
+    }
+}
+
+template <bool QUAD, bool ADJ>
+rtd_status launch_walk(rtd_bh *b, const rtd_bh_params *p, const float *g_acc, const float *g_phi,
+                       float *acc, float *phi, cudaStream_t st) {
+    int dev = 0, sms = 148, per_sm = 4;
+    RTD_CUDA(cudaGetDevice(&dev));
+    RTD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    RTD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bh_walk_kernel<QUAD, ADJ>,
+                                                           WW * 32, 0));
+    if (per_sm < 1) per_sm = 1;
+    uint64_t blocks = (uint64_t)sms * (uint64_t)per_sm;
+    const uint64_t need = (b->n + WW - 1) / WW;   // groups <= bodies
+    if (blocks > need) blocks = need;
+    if (blocks < 1) blocks = 1;
+    const uint64_t warps = blocks * WW;
+    if (b->stack_warps < warps) {
+        RTD_TRY(b->stack.reserve(warps * BH_STACK_CAP * sizeof(uint2)));
+        b->stack_warps = warps;
+    }
+    BhHeader *h = b->hdr.as<BhHeader>();
+    RTD_CUDA(cudaMemsetAsync(&h->group_counter, 0, sizeof(uint32_t), st));
+    const BhView v = bh_view(b);
+    bh_walk_kernel<QUAD, ADJ><<<(unsigned)blocks, WW * 32, 0, st>>>(
+        v, p->theta * p->theta, p->eps * p->eps, p->G, g_acc, g_phi, acc, phi,
+        b->cell_grad.as<float4>(), b->gpos_flat.as<float4>(), b->stack.as<uint2>(), h);
+    RTD_LAUNCH_CHECK();
+    return RTD_OK;
+}
+
+}  // namespace
+
+rtd_status bh_ref_forward(rtd_bh *b, const rtd_bh_params *p, float *d_out, cudaStream_t st);
+
+rtd_status bh_forward(rtd_bh *b, const rtd_bh_params *p, float *d_out, float *d_phi,
+                      cudaStream_t st) {
+    if (!b || !b->built) return fail(RTD_ERR_INVALID_ARGUMENT, "bh tree not built");
+    if (b->n && !d_out) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL output");
+    rtd_bh_params def;
+    rtd_bh_params_default(&def);
+    if (!p) p = &def;
+    if (b->n == 0) return RTD_OK;
+    if (p->law == RTD_BH_LAW_REFERENCE) return bh_ref_forward(b, p, d_out, st);
+    if (p->law != RTD_BH_LAW_PLUMMER) return fail(RTD_ERR_INVALID_ARGUMENT, "unknown law");
+    if (!b->plummer_ready)
+        return fail(RTD_ERR_INVALID_ARGUMENT, "tree was not built for the Plummer law");
+    if (p->quadrupole && !b->has_quad)
+        return fail(RTD_ERR_INVALID_ARGUMENT, "tree was built without quadrupoles");
+    if (p->quadrupole) return launch_walk<true, false>(b, p, nullptr, nullptr, d_out, d_phi, st);
+    return launch_walk<false, false>(b, p, nullptr, nullptr, d_out, d_phi, st);
+}
+
+rtd_status bh_backward(rtd_bh *b, const rtd_bh_params *p, const float *g_acc, const float *g_phi,
+                       float *g_pos, float *g_mass, cudaStream_t st) {
+    if (!b || !b->built) return fail(RTD_ERR_INVALID_ARGUMENT, "bh tree not built");
+    rtd_bh_params def;
+    rtd_bh_params_default(&def);
+    if (!p) p = &def;
+    if (p->law != RTD_BH_LAW_PLUMMER)
+        return fail(RTD_ERR_UNSUPPORTED, "the adjoint is defined for the Plummer law");
+    if (b->n == 0) return RTD_OK;
+    if (!g_acc || !g_pos) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL gradient buffer");
+    if (!b->plummer_ready)
+        return fail(RTD_ERR_INVALID_ARGUMENT, "tree was not built for the Plummer law");
+    if (p->quadrupole && !b->has_quad)
+        return fail(RTD_ERR_INVALID_ARGUMENT, "tree was built without quadrupoles");
+    const uint64_t n = b->n;
+    RTD_TRY(b->cell_grad.reserve(n * 3 * sizeof(float4) + 64 * sizeof(uint32_t)));
+    RTD_TRY(b->prefix.reserve(n * 3 * sizeof(float4)));
+    RTD_TRY(b->gpos_flat.reserve(n * sizeof(float4)));
+    RTD_CUDA(cudaMemsetAsync(b->cell_grad.ptr, 0, n * 3 * sizeof(float4), st));
+    RTD_CUDA(cudaMemsetAsync(b->gpos_flat.ptr, 0, n * sizeof(float4), st));
+    if (p->quadrupole) RTD_TRY((launch_walk<true, true>(b, p, g_acc, g_phi, nullptr, nullptr, st)));
+    else RTD_TRY((launch_walk<false, true>(b, p, g_acc, g_phi, nullptr, nullptr, st)));
+    const BhView v = bh_view(b);
+    bh_prefix_kernel<<<1, 1024, 0, st>>>(v, b->level_nodes.as<uint32_t>(), b->cell_grad.as<float4>(),
+                                          b->prefix.as<float4>());
+    RTD_LAUNCH_CHECK();
+    bh_finish_grad_kernel<<<grid_for(n, 128, 1 << 20), 128, 0, st>>>(
+        v, b->prefix.as<float4>(), b->gpos_flat.as<float4>(), g_pos, g_mass);
+    RTD_LAUNCH_CHECK();
+    return RTD_OK;
+}
+
+}  // namespace rtd

@@ -216,7 +216,8 @@ __global__ void __launch_bounds__(BLOCK) bh_nodes_kernel(
     const uint8_t *__restrict__ lcp, const uint8_t *__restrict__ lam,
     const uint32_t *__restrict__ nn, const uint32_t *__restrict__ base,
     const uint32_t *__restrict__ leafidx, uint64_t n, uint32_t *__restrict__ node_start,
-    uint8_t *__restrict__ node_level, uint32_t *__restrict__ leaf_head, BhHeader *h) {
+    uint8_t *__restrict__ node_level, uint32_t *__restrict__ leaf_head,
+    uint32_t *__restrict__ leaf_node, BhHeader *h) {
     for (uint64_t j = (uint64_t)blockIdx.x * BLOCK + threadIdx.x; j < n;
          j += (uint64_t)gridDim.x * BLOCK) {
         uint32_t c = nn[j];
@@ -228,7 +229,97 @@ __global__ void __launch_bounds__(BLOCK) bh_nodes_kernel(
             atomicAdd(&h->level_count[l0 + t], 1u);
         }
         leaf_head[leafidx[j]] = (uint32_t)j;
+        leaf_node[leafidx[j]] = base[j] + c - 1;   // the deepest node starting at j
         (void)lam;
+    }
+}
+
+// Child table: up to 8 children per internal node (first child = i + 1,
+// next sibling = autorope), padded with 0xFFFFFFFF.
+__global__ void __launch_bounds__(BLOCK) bh_child_kernel(const BhHeader *h,
+                                                         const uint4 *__restrict__ node_b,
+                                                         uint4 *__restrict__ child8) {
+    const uint32_t n_nodes = h->n_nodes;
+    for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < n_nodes; i += gridDim.x * BLOCK) {
+        uint32_t c[8];
+        for (int k = 0; k < 8; ++k) c[k] = 0xFFFFFFFFu;
+        const uint4 b = node_b[i];
+        if (!(b.z & BH_LEAF_BIT)) {
+            int k = 0;
+            for (uint32_t x = i + 1; x < b.x && k < 8; x = node_b[x].x) c[k++] = x;
+        }
+        child8[2 * i] = make_uint4(c[0], c[1], c[2], c[3]);
+        child8[2 * i + 1] = make_uint4(c[4], c[5], c[6], c[7]);
+    }
+}
+
+// Warp groups for the Plummer walks: runs of sibling leaves (consecutive
+// pre-order nodes at the same level) packed greedily up to 32 bodies;
+// a leaf of more than 32 bodies is split into chunks of 32.  The run head
+// writes, per leaf, the number of groups starting there (gcnt) and the
+// body count of a packed group starting there (gsize).
+__device__ __forceinline__ bool next_sibling_leaf(const uint32_t *leaf_node, const uint8_t *lvl,
+                                                  uint32_t m) {
+    return leaf_node[m] == leaf_node[m - 1] + 1 && lvl[leaf_node[m]] == lvl[leaf_node[m - 1]];
+}
+
+__global__ void __launch_bounds__(BLOCK) bh_group_plan_kernel(const BhHeader *h,
+                                                              const uint32_t *__restrict__ leaf_node,
+                                                              const uint8_t *__restrict__ lvl,
+                                                              const uint4 *__restrict__ node_b,
+                                                              uint32_t *__restrict__ gcnt,
+                                                              uint32_t *__restrict__ gsize) {
+    const uint32_t nl = h->n_leaves;
+    for (uint32_t m = blockIdx.x * BLOCK + threadIdx.x; m < nl; m += gridDim.x * BLOCK) {
+        if (m > 0 && next_sibling_leaf(leaf_node, lvl, m)) continue;   // not a run head
+        uint32_t open = 0xFFFFFFFFu, acc = 0;
+        for (uint32_t t = m; t < nl && (t == m || next_sibling_leaf(leaf_node, lvl, t)); ++t) {
+            const uint32_t c = node_b[leaf_node[t]].z & ~BH_LEAF_BIT;
+            if (c > (uint32_t)BH_GROUP) {
+                if (open != 0xFFFFFFFFu) gsize[open] = acc;
+                open = 0xFFFFFFFFu;
+                acc = 0;
+                gcnt[t] = (c + BH_GROUP - 1) / BH_GROUP;
+                gsize[t] = 0;
+                continue;
+            }
+            if (open != 0xFFFFFFFFu && acc + c <= (uint32_t)BH_GROUP) {
+                acc += c;
+                gcnt[t] = 0;
+            } else {
+                if (open != 0xFFFFFFFFu) gsize[open] = acc;
+                open = t;
+                acc = c;
+                gcnt[t] = 1;
+            }
+        }
+        if (open != 0xFFFFFFFFu) gsize[open] = acc;
+    }
+}
+
+__global__ void __launch_bounds__(BLOCK) bh_group_write_kernel(BhHeader *h,
+                                                               const uint32_t *__restrict__ leaf_node,
+                                                               const uint4 *__restrict__ node_b,
+                                                               const uint32_t *__restrict__ gcnt,
+                                                               const uint32_t *__restrict__ gsize,
+                                                               const uint32_t *__restrict__ goff,
+                                                               const uint32_t *__restrict__ gtotal,
+                                                               uint2 *__restrict__ groups) {
+    const uint32_t nl = h->n_leaves;
+    if (blockIdx.x == 0 && threadIdx.x == 0) h->n_groups = *gtotal;
+    for (uint32_t m = blockIdx.x * BLOCK + threadIdx.x; m < nl; m += gridDim.x * BLOCK) {
+        const uint32_t k = gcnt[m];
+        if (!k) continue;
+        const uint4 b = node_b[leaf_node[m]];
+        const uint32_t s = b.y, c = b.z & ~BH_LEAF_BIT;
+        if (c > (uint32_t)BH_GROUP) {
+            for (uint32_t t = 0; t < k; ++t) {
+                const uint32_t cs = t * BH_GROUP;
+                groups[goff[m] + t] = make_uint2(s + cs, min((uint32_t)BH_GROUP, c - cs));
+            }
+        } else {
+            groups[goff[m]] = make_uint2(s, gsize[m]);
+        }
     }
 }
 
@@ -436,6 +527,8 @@ rtd_status bh_build(rtd_bh *b, const float *d_pos, const float *d_mass, uint64_t
     if (!p) p = &def;
     if (p->bucket < 1 || p->bucket > 4096) return fail(RTD_ERR_INVALID_ARGUMENT, "bucket must be in [1, 4096]");
     b->built = false;
+    b->plummer_ready = false;
+    b->has_quad = false;
     b->n = n;
     b->bucket = p->bucket;
     b->min_width = p->min_width;
@@ -451,7 +544,8 @@ rtd_status bh_build(rtd_bh *b, const float *d_pos, const float *d_mass, uint64_t
     const uint64_t n1 = n;
     for (DevBuf *d : {&b->mkeys, &b->mkeys_alt, &b->mvals, &b->mvals_alt, &b->pvals, &b->pvals_alt,
                       &b->nn, &b->base, &b->heads, &b->leaf_head, &b->fkeys, &b->fkeys_alt,
-                      &b->fvals, &b->fvals_alt, &b->node_start, &b->order, &b->level_nodes})
+                      &b->fvals, &b->fvals_alt, &b->node_start, &b->order, &b->level_nodes,
+                      &b->leaf_node})
         RTD_TRY(d->reserve(n1 * 4 + 16));
     RTD_TRY(b->pkeys.reserve(n1 * 8));
     RTD_TRY(b->pkeys_alt.reserve(n1 * 8));
@@ -512,7 +606,7 @@ rtd_status bh_build(rtd_bh *b, const float *d_pos, const float *d_mass, uint64_t
     bh_nodes_kernel<<<g, BLOCK, 0, st>>>(lcp, b->lam.as<uint8_t>(), b->nn.as<uint32_t>(),
                                          b->base.as<uint32_t>(), leafidx, n,
                                          b->node_start.as<uint32_t>(), node_level,
-                                         b->leaf_head.as<uint32_t>(), h);
+                                         b->leaf_head.as<uint32_t>(), b->leaf_node.as<uint32_t>(), h);
     RTD_LAUNCH_CHECK();
     bh_level_offsets_kernel<<<1, 1, 0, st>>>(h);
     RTD_LAUNCH_CHECK();
@@ -542,6 +636,29 @@ rtd_status bh_build(rtd_bh *b, const float *d_pos, const float *d_mass, uint64_t
                                                b->level_nodes.as<uint32_t>(),
                                                b->node_a.as<float4>(), b->node_q.as<float4>(), quad);
     RTD_LAUNCH_CHECK();
+    if (p->law == RTD_BH_LAW_PLUMMER) {
+        // child table and warp groups for the tiled walks (scratch reuse:
+        // mkeys = gsize, mkeys_alt = gcnt, nn = group offsets)
+        RTD_TRY(b->child8.reserve(n1 * 2 * sizeof(uint4) + 64));
+        RTD_TRY(b->groups.reserve(n1 * sizeof(uint2) + 64));
+        bh_child_kernel<<<g, BLOCK, 0, st>>>(h, b->node_b.as<uint4>(), b->child8.as<uint4>());
+        RTD_LAUNCH_CHECK();
+        uint32_t *gsize = b->mkeys.as<uint32_t>(), *gcnt = b->mkeys_alt.as<uint32_t>();
+        RTD_CUDA(cudaMemsetAsync(gcnt, 0, n1 * 4, st));
+        bh_group_plan_kernel<<<g, BLOCK, 0, st>>>(h, b->leaf_node.as<uint32_t>(), node_level,
+                                                  b->node_b.as<uint4>(), gcnt, gsize);
+        RTD_LAUNCH_CHECK();
+        // scan over all n slots (leaves beyond n_leaves hold 0)
+        RTD_TRY(exclusive_scan_u32_32(gcnt, b->nn.as<uint32_t>(), n, totals + 1, b->scan, &h->err,
+                                      st));
+        bh_group_write_kernel<<<g, BLOCK, 0, st>>>(h, b->leaf_node.as<uint32_t>(),
+                                                   b->node_b.as<uint4>(), gcnt, gsize,
+                                                   b->nn.as<uint32_t>(), totals + 1,
+                                                   b->groups.as<uint2>());
+        RTD_LAUNCH_CHECK();
+        b->plummer_ready = true;
+        b->has_quad = quad != 0;
+    }
     b->built = true;
     return RTD_OK;
 }
