@@ -195,6 +195,42 @@ rtd_status rtd_knn_backward(const float *d_queries, uint64_t nq, const float *d_
                             rtd_stream stream);
 
 /* ---------------------------------------------------------------------
+ * Batched k-NN over many independent point clouds, each with its own
+ * queries and k (no reference counterpart: the reference searches one scene
+ * per k_nn! call).  One pass builds every cloud's LBVH as one forest (a
+ * single sort over (cloud, Morton) keys) and searches every query in one
+ * persistent launch fed from a device work queue; with use_graph the pass is
+ * captured once as a CUDA graph and replayed.
+ * ------------------------------------------------------------------- */
+typedef struct rtd_cloud {
+    uint64_t point_offset;  /* first point of the cloud in the packed point array */
+    uint64_t query_offset;  /* first query of the cloud in the packed query array */
+    uint64_t out_offset;    /* results of the cloud's query j at out_offset + j*k */
+    uint32_t n_points;
+    uint32_t n_queries;
+    uint32_t k;             /* 1 .. 256 */
+    uint32_t pad;
+} rtd_cloud;
+
+typedef struct rtd_batch rtd_batch;
+rtd_status rtd_batch_create(rtd_batch **out);
+rtd_status rtd_batch_destroy(rtd_batch *b);
+/* Clouds must be packed in order: point_offset and query_offset of cloud c
+ * are the sums of n_points / n_queries of clouds 0..c-1.  radius_param of
+ * the schedule scales the per-cloud initial radius (mean point spacing of
+ * the cloud's box); leaf_size, radius_increment_mult, max_rounds apply. */
+rtd_status rtd_batch_plan(rtd_batch *b, const rtd_cloud *clouds, uint32_t n_clouds,
+                          const rtd_schedule *sched);
+/* Ids are cloud-local point indices; d_d2 may be NULL. */
+rtd_status rtd_knn_batched(rtd_batch *b, const float *d_points, const float *d_queries,
+                           uint32_t *d_ids, float *d_d2, int use_graph, rtd_stream stream);
+/* Backward of a loss on the batched squared distances with ids fixed:
+ * grad_q (all queries * 3) overwritten, grad_p (all points * 3) accumulated. */
+rtd_status rtd_knn_batched_backward(rtd_batch *b, const float *d_points, const float *d_queries,
+                                    const uint32_t *d_ids, const float *d_grad_d2,
+                                    float *d_grad_q, float *d_grad_p, rtd_stream stream);
+
+/* ---------------------------------------------------------------------
  * Barnes-Hut gravity.  Replaces barnes_hut! (gprt-macros/src/lib.rs:
  * 752-834): the CPU BarnesHutTree::build (gprt-core/src/lib.rs:427-539)
  * becomes a GPU build of the same tree, and gprt_execute_autorope_soa_ffi

@@ -106,6 +106,11 @@ inline IndexView view_of(const rtd_index *idx) {
                      idx->hdr.as<IndexHeader>(), idx->n};
 }
 
+// Karras tree, leaf collapse and bottom-up refit over n keys already sorted
+// (idx->pts holds the points in key order; idx->leaf_size set).
+template <typename K>
+rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStream_t st);
+
 // Query ordering: Morton codes of the queries against the scene box, sorted;
 // perm[i] is the i-th query to process.  Returns perm (device) or nullptr
 // when ordering is off.

@@ -2,25 +2,12 @@
 // kernel.  Replaces the k_nn! round loop (gprt-macros/src/lib.rs:462-595)
 // and its OptiX register-heap programs (lib.rs:305-377): where the
 // reference relaunches per round, copies a Q x 2k slab back to the host and
-// filters there, every query here runs its rounds in registers:
-//
-//   round i accepts points with prev < key <= bound_i, bound_{i+1} =
-//   bound_i * M^2, prev = bound_{i-1}; a query stops once it holds k
-//   points (then they are its exact k nearest) and the last allowed round
-//   is unbounded, so results are exact for every input.
-//
-// Nodes whose box lies entirely inside the previous radius are skipped
-// (their points were all collected already), nodes whose nearest box
-// distance exceeds min(bound, current k-th key) are pruned, and children are
-// visited near-first.  Keys use the exact FP32 arithmetic of the reference
-// intersection program; ties go to the lower point id.
-#include "index.cuh"
+// filters there, every query here runs all its rounds inside one launch
+// (knn_traverse.cuh).
+#include "knn_traverse.cuh"
 
 namespace rtd {
 namespace {
-
-constexpr int SHORT_STACK = 16;   // per-thread stack entries kept in shared memory
-constexpr int STACK_MAX = 104;    // >= maximal tree depth (63 key bits + 32 index bits)
 
 struct KnnArgs {
     IndexView ix;
@@ -35,35 +22,6 @@ struct KnnArgs {
     uint32_t *err;
 };
 
-__device__ __forceinline__ void load_node(const BvhNode *__restrict__ s_top,
-                                          const BvhNode *__restrict__ g, uint32_t w, float4 &a,
-                                          float4 &b, float4 &c, uint4 &d) {
-    if (w & CHILD_TOP) {
-        const BvhNode &n = s_top[w & CHILD_INDEX];
-        a = n.a; b = n.b; c = n.c; d = n.d;
-    } else {
-        const BvhNode *n = g + (w & CHILD_INDEX);
-        a = __ldg(&n->a); b = __ldg(&n->b); c = __ldg(&n->c); d = __ldg(&n->d);
-    }
-}
-
-// Sorted (key, id) list of KC slots in registers; slot KC-1 is the k-th best.
-// For k < KC the first KC-k slots hold -inf and never move.
-template <int KC>
-__device__ __forceinline__ void list_insert(float (&bk)[KC], uint32_t (&bi)[KC], float key,
-                                            uint32_t id) {
-#pragma unroll
-    for (int j = KC - 1; j > 0; --j) {
-        bool bp = key_less(key, id, bk[j - 1], bi[j - 1]);
-        bool bc = key_less(key, id, bk[j], bi[j]);
-        float nk = bp ? bk[j - 1] : (bc ? key : bk[j]);
-        uint32_t ni = bp ? bi[j - 1] : (bc ? id : bi[j]);
-        bk[j] = nk;
-        bi[j] = ni;
-    }
-    if (key_less(key, id, bk[0], bi[0])) { bk[0] = key; bi[0] = id; }
-}
-
 // One thread per query.
 template <int KC, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) knn_thread_kernel(const KnnArgs p) {
@@ -73,14 +31,11 @@ __global__ void __launch_bounds__(BLOCK) knn_thread_kernel(const KnnArgs p) {
     const uint32_t ntop = h->n_top;
     for (uint32_t i = threadIdx.x; i < ntop; i += BLOCK) s_top[i] = p.ix.top[i];
     __syncthreads();
-    const uint32_t root = h->root, root_count = h->root_count;
-    float r0sq = h->r0sq;
-    if (!(r0sq > 0.0f)) r0sq = 1e-30f;
-    const float4 *__restrict__ pts = p.ix.pts;
-    const BvhNode *__restrict__ gn = p.ix.nodes;
-    const int kk = (int)p.k;
     // a round visits each internal node at most once; more means a broken tree
-    const uint32_t visit_cap = 2u * h->n_internal + 4u;
+    const TreeRef tree{p.ix.pts, p.ix.nodes, s_top, h->root, h->root_count,
+                       2u * h->n_internal + 4u};
+    const RoundSpec rs{h->r0sq, p.mult2, p.max_rounds};
+    const int kk = (int)p.k;
     uint2 l_stack[STACK_MAX - SHORT_STACK];
 
     for (uint64_t t = (uint64_t)blockIdx.x * BLOCK + threadIdx.x; t < p.nq;
@@ -89,103 +44,8 @@ __global__ void __launch_bounds__(BLOCK) knn_thread_kernel(const KnnArgs p) {
         const float qx = p.q[3 * qi], qy = p.q[3 * qi + 1], qz = p.q[3 * qi + 2];
         float bk[KC];
         uint32_t bi[KC];
-#pragma unroll
-        for (int j = 0; j < KC; ++j) {
-            bool pad = j < KC - kk;
-            bk[j] = pad ? -INFINITY : INFINITY;
-            bi[j] = pad ? 0u : EMPTY_ID;
-        }
-        const bool valid = root != CHILD_NONE && !isnan(qx) && !isnan(qy) && !isnan(qz);
-        float bound = r0sq, prev = -1.0f;
-        for (uint32_t round = 0; valid; ++round) {
-            const bool last = round + 1 >= p.max_rounds || !(bound < INFINITY);
-            if (last) bound = INFINITY;
-            float lim = fminf(bound, bk[KC - 1]);
-            // ---- traversal of one round
-            uint32_t node = root;
-            int sp = 0;
-            uint32_t visits = 0;
-            while (true) {
-                uint32_t lf_first[2], lf_cnt[2];
-                int nleaf = 0;
-                uint32_t next = CHILD_NONE;
-                if (++visits > visit_cap) {
-                    atomicOr(p.err, DEVERR_STACK);
-                    break;
-                }
-                if (node & CHILD_LEAF) {
-                    lf_first[0] = node & CHILD_INDEX;
-                    lf_cnt[0] = root_count;
-                    nleaf = 1;
-                } else {
-                    float4 a, b, c;
-                    uint4 d;
-                    load_node(s_top, gn, node, a, b, c, d);
-                    float k0 = box_min_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y);
-                    float k1 = box_min_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w);
-                    bool v0 = !(k0 > lim), v1 = !(k1 > lim);
-                    if (prev >= 0.0f) {
-                        if (v0) v0 = !(box_max_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y) <= prev);
-                        if (v1) v1 = !(box_max_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w) <= prev);
-                    }
-                    if (v0 && (d.x & CHILD_LEAF)) { lf_first[nleaf] = d.x & CHILD_INDEX; lf_cnt[nleaf] = d.z; ++nleaf; v0 = false; }
-                    if (v1 && (d.y & CHILD_LEAF)) { lf_first[nleaf] = d.y & CHILD_INDEX; lf_cnt[nleaf] = d.w; ++nleaf; v1 = false; }
-                    // leaves of this node
-                    for (int l = 0; l < nleaf; ++l) {
-                        for (uint32_t j = 0; j < lf_cnt[l]; ++j) {
-                            float4 pt = __ldg(&pts[lf_first[l] + j]);
-                            float key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
-                            uint32_t id = __float_as_uint(pt.w);
-                            if (key <= bound && key > prev && key_less(key, id, bk[KC - 1], bi[KC - 1]))
-                                list_insert<KC>(bk, bi, key, id);
-                        }
-                    }
-                    nleaf = 0;
-                    lim = fminf(bound, bk[KC - 1]);
-                    v0 = v0 && !(k0 > lim);
-                    v1 = v1 && !(k1 > lim);
-                    if (v0 && v1) {
-                        bool near0 = k0 <= k1;
-                        uint2 far = near0 ? make_uint2(d.y, __float_as_uint(k1))
-                                          : make_uint2(d.x, __float_as_uint(k0));
-                        next = near0 ? d.x : d.y;
-                        if (sp < SHORT_STACK) s_stack[sp][threadIdx.x] = far;
-                        else if (sp < STACK_MAX) l_stack[sp - SHORT_STACK] = far;
-                        else atomicOr(p.err, DEVERR_STACK);
-                        if (sp < STACK_MAX) ++sp;
-                    } else if (v0) {
-                        next = d.x;
-                    } else if (v1) {
-                        next = d.y;
-                    }
-                }
-                // root-leaf case
-                for (int l = 0; l < nleaf; ++l) {
-                    for (uint32_t j = 0; j < lf_cnt[l]; ++j) {
-                        float4 pt = __ldg(&pts[lf_first[l] + j]);
-                        float key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
-                        uint32_t id = __float_as_uint(pt.w);
-                        if (key <= bound && key > prev && key_less(key, id, bk[KC - 1], bi[KC - 1]))
-                            list_insert<KC>(bk, bi, key, id);
-                    }
-                    lim = fminf(bound, bk[KC - 1]);
-                }
-                if (next == CHILD_NONE) {
-                    while (sp > 0) {
-                        --sp;
-                        uint2 e = sp < SHORT_STACK ? s_stack[sp][threadIdx.x]
-                                                   : l_stack[sp - SHORT_STACK];
-                        if (!(__uint_as_float(e.y) > lim)) { next = e.x; break; }
-                    }
-                    if (next == CHILD_NONE) break;
-                }
-                node = next;
-            }
-            // ---- end of round
-            if (bi[KC - 1] != EMPTY_ID || last) break;
-            prev = bound;
-            bound = __fmul_rn(bound, p.mult2);
-        }
+        knn_query_thread<KC>(tree, rs, qx, qy, qz, kk, &s_stack[0][threadIdx.x], BLOCK, l_stack,
+                             p.err, bk, bi);
         const uint64_t ob = qi * (uint64_t)kk;
 #pragma unroll
         for (int j = 0; j < KC; ++j) {
@@ -358,16 +218,12 @@ __global__ void __launch_bounds__(WARPS * 32) knn_warp_kernel(const KnnArgs p) {
     const uint32_t ntop = h->n_top;
     for (uint32_t i = threadIdx.x; i < ntop; i += WARPS * 32) s_top[i] = p.ix.top[i];
     __syncthreads();
-    const uint32_t root = h->root, root_count = h->root_count;
-    float r0sq = h->r0sq;
-    if (!(r0sq > 0.0f)) r0sq = 1e-30f;
-    const float4 *__restrict__ pts = p.ix.pts;
-    const BvhNode *__restrict__ gn = p.ix.nodes;
+    const TreeRef tree{p.ix.pts, p.ix.nodes, s_top, h->root, h->root_count,
+                       2u * h->n_internal + 4u};
+    const RoundSpec rs{h->r0sq, p.mult2, p.max_rounds};
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t kk = p.k;
-    const int wslot = (int)((kk - 1) >> 5), wlane = (int)((kk - 1) & 31);
     uint2 *stk = s_stack[warp];
-    const uint32_t visit_cap = 2u * h->n_internal + 4u;
 
     for (uint64_t t = (uint64_t)blockIdx.x * WARPS + warp; t < p.nq;
          t += (uint64_t)gridDim.x * WARPS) {
@@ -375,135 +231,7 @@ __global__ void __launch_bounds__(WARPS * 32) knn_warp_kernel(const KnnArgs p) {
         const float qx = p.q[3 * qi], qy = p.q[3 * qi + 1], qz = p.q[3 * qi + 2];
         float lk[S];
         uint32_t li[S];
-#pragma unroll
-        for (int s = 0; s < S; ++s) { lk[s] = INFINITY; li[s] = EMPTY_ID; }
-        float wk = INFINITY;
-        uint32_t wi = EMPTY_ID;
-        const bool valid = root != CHILD_NONE && !isnan(qx) && !isnan(qy) && !isnan(qz);
-        float bound = r0sq, prev = -1.0f;
-        for (uint32_t round = 0; valid; ++round) {
-            const bool last = round + 1 >= p.max_rounds || !(bound < INFINITY);
-            if (last) bound = INFINITY;
-            float lim = fminf(bound, wk);
-            uint32_t node = root;
-            int sp = 0;
-            uint32_t visits = 0;
-            while (true) {
-                uint32_t lf_first[2], lf_cnt[2];
-                int nleaf = 0;
-                uint32_t next = CHILD_NONE;
-                float k0 = 0.f, k1 = 0.f;
-                uint4 d = make_uint4(0, 0, 0, 0);
-                bool v0 = false, v1 = false;
-                if (++visits > visit_cap) {   // warp-uniform
-                    if (lane == 0) atomicOr(p.err, DEVERR_STACK);
-                    break;
-                }
-                if (node & CHILD_LEAF) {
-                    lf_first[0] = node & CHILD_INDEX;
-                    lf_cnt[0] = root_count;
-                    nleaf = 1;
-                } else {
-                    float4 a, b, c;
-                    load_node(s_top, gn, node, a, b, c, d);
-                    k0 = box_min_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y);
-                    k1 = box_min_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w);
-                    v0 = !(k0 > lim);
-                    v1 = !(k1 > lim);
-                    if (prev >= 0.0f) {
-                        if (v0) v0 = !(box_max_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y) <= prev);
-                        if (v1) v1 = !(box_max_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w) <= prev);
-                    }
-                    if (v0 && (d.x & CHILD_LEAF)) { lf_first[nleaf] = d.x & CHILD_INDEX; lf_cnt[nleaf] = d.z; ++nleaf; v0 = false; }
-                    if (v1 && (d.y & CHILD_LEAF)) { lf_first[nleaf] = d.y & CHILD_INDEX; lf_cnt[nleaf] = d.w; ++nleaf; v1 = false; }
-                }
-                for (int l = 0; l < nleaf; ++l) {
-                    for (uint32_t j0 = 0; j0 < lf_cnt[l]; j0 += 32) {
-                        float key = INFINITY;
-                        uint32_t id = EMPTY_ID;
-                        bool acc = false;
-                        if (j0 + lane < lf_cnt[l]) {
-                            float4 pt = __ldg(&pts[lf_first[l] + j0 + lane]);
-                            key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
-                            id = __float_as_uint(pt.w);
-                            acc = key <= bound && key > prev && key_less(key, id, wk, wi);
-                        }
-                        uint32_t m = __ballot_sync(0xffffffffu, acc);
-                        while (m) {
-                            int src = __ffs(m) - 1;
-                            m &= m - 1;
-                            float ck = __shfl_sync(0xffffffffu, key, src);
-                            uint32_t ci = __shfl_sync(0xffffffffu, id, src);
-                            if (!key_less(ck, ci, wk, wi)) continue;   // warp-uniform
-                            // position = number of slots ordered before the candidate
-                            int pos = 0;
-#pragma unroll
-                            for (int s = 0; s < S; ++s)
-                                pos += __popc(__ballot_sync(0xffffffffu, key_less(lk[s], li[s], ck, ci)));
-                            // shift slots >= pos up by one
-                            float carry_k = INFINITY;
-                            uint32_t carry_i = EMPTY_ID;
-#pragma unroll
-                            for (int s = 0; s < S; ++s) {
-                                float upk = __shfl_up_sync(0xffffffffu, lk[s], 1);
-                                uint32_t upi = __shfl_up_sync(0xffffffffu, li[s], 1);
-                                float topk = __shfl_sync(0xffffffffu, lk[s], 31);
-                                uint32_t topi = __shfl_sync(0xffffffffu, li[s], 31);
-                                if (lane == 0) { upk = carry_k; upi = carry_i; }
-                                int j = s * 32 + lane;
-                                if (j > pos) { lk[s] = upk; li[s] = upi; }
-                                else if (j == pos) { lk[s] = ck; li[s] = ci; }
-                                carry_k = topk;
-                                carry_i = topi;
-                            }
-                            // new k-th slot
-                            float nk = 0.f;
-                            uint32_t ni = 0;
-#pragma unroll
-                            for (int s = 0; s < S; ++s)
-                                if (s == wslot) { nk = lk[s]; ni = li[s]; }
-                            wk = __shfl_sync(0xffffffffu, nk, wlane);
-                            wi = __shfl_sync(0xffffffffu, ni, wlane);
-                        }
-                    }
-                    lim = fminf(bound, wk);
-                }
-                if (!(node & CHILD_LEAF)) {
-                    v0 = v0 && !(k0 > lim);
-                    v1 = v1 && !(k1 > lim);
-                    if (v0 && v1) {
-                        bool near0 = k0 <= k1;
-                        uint2 far = near0 ? make_uint2(d.y, __float_as_uint(k1))
-                                          : make_uint2(d.x, __float_as_uint(k0));
-                        next = near0 ? d.x : d.y;
-                        if (sp < STACK_MAX) {
-                            if (lane == 0) stk[sp] = far;
-                            ++sp;
-                        } else if (lane == 0) {
-                            atomicOr(p.err, DEVERR_STACK);
-                        }
-                    } else if (v0) {
-                        next = d.x;
-                    } else if (v1) {
-                        next = d.y;
-                    }
-                }
-                __syncwarp();
-                if (next == CHILD_NONE) {
-                    while (sp > 0) {
-                        --sp;
-                        uint2 e = stk[sp];
-                        if (!(__uint_as_float(e.y) > lim)) { next = e.x; break; }
-                    }
-                    if (next == CHILD_NONE) break;
-                }
-                __syncwarp();
-                node = next;
-            }
-            if (wi != EMPTY_ID || last) break;
-            prev = bound;
-            bound = __fmul_rn(bound, p.mult2);
-        }
+        knn_query_warp<S>(tree, rs, qx, qy, qz, kk, stk, p.err, lk, li);
         const uint64_t ob = qi * (uint64_t)kk;
 #pragma unroll
         for (int s = 0; s < S; ++s) {

@@ -1,0 +1,305 @@
+// knn_traverse.cuh -- one query's exact k-NN by in-kernel radius expansion,
+// shared by the single-cloud kernels (knn.cu) and the batched many-cloud
+// kernel (batch.cu).
+//
+// Round i accepts points with prev < key <= bound_i (bound_{i+1} = bound_i *
+// M^2, prev = bound_{i-1}); a query stops once it holds k points (they are
+// then its exact k nearest) and the last allowed round is unbounded, so the
+// result is exact for every input.  Nodes whose box lies inside the
+// previous radius are skipped (their points were all collected), nodes
+// whose nearest box key exceeds min(bound, current k-th key) are pruned,
+// and children are visited near-first.  Keys are the exact FP32 keys of
+// the reference intersection program; ties go to the lower point id.
+#pragma once
+
+#include "index.cuh"
+
+namespace rtd {
+
+constexpr int SHORT_STACK = 16;   // per-thread stack entries kept in shared memory
+constexpr int STACK_MAX = 104;    // >= maximal tree depth (63 key bits + 32 index bits)
+
+// One tree to search: a whole index, or one cloud's subtree of a forest.
+struct TreeRef {
+    const float4 *pts;
+    const BvhNode *nodes;
+    const BvhNode *s_top;    // staged top levels (nullptr: no CHILD_TOP words)
+    uint32_t root;           // child word of the root
+    uint32_t root_count;     // points when the root is a leaf
+    uint32_t visit_cap;      // more node visits than this per round = broken tree
+};
+
+struct RoundSpec {
+    float r0sq;              // squared radius of round 0
+    float mult2;             // growth of the squared radius per round
+    uint32_t max_rounds;     // the last round is unbounded
+};
+
+__device__ __forceinline__ void load_node(const BvhNode *__restrict__ s_top,
+                                          const BvhNode *__restrict__ g, uint32_t w, float4 &a,
+                                          float4 &b, float4 &c, uint4 &d) {
+    if (w & CHILD_TOP) {
+        const BvhNode &n = s_top[w & CHILD_INDEX];
+        a = n.a; b = n.b; c = n.c; d = n.d;
+    } else {
+        const BvhNode *n = g + (w & CHILD_INDEX);
+        a = __ldg(&n->a); b = __ldg(&n->b); c = __ldg(&n->c); d = __ldg(&n->d);
+    }
+}
+
+// Sorted (key, id) list of KC slots in registers; slot KC-1 is the k-th best.
+// For k < KC the first KC-k slots hold -inf and never move.
+template <int KC>
+__device__ __forceinline__ void list_insert(float (&bk)[KC], uint32_t (&bi)[KC], float key,
+                                            uint32_t id) {
+#pragma unroll
+    for (int j = KC - 1; j > 0; --j) {
+        bool bp = key_less(key, id, bk[j - 1], bi[j - 1]);
+        bool bc = key_less(key, id, bk[j], bi[j]);
+        float nk = bp ? bk[j - 1] : (bc ? key : bk[j]);
+        uint32_t ni = bp ? bi[j - 1] : (bc ? id : bi[j]);
+        bk[j] = nk;
+        bi[j] = ni;
+    }
+    if (key_less(key, id, bk[0], bi[0])) { bk[0] = key; bi[0] = id; }
+}
+
+// Thread per query: the register list ends holding the k best (key, id)
+// pairs in slots KC-k .. KC-1.  The stack keeps SHORT_STACK entries in this
+// thread's shared-memory column (s_col[sp * s_stride]) and the rest in
+// l_stack (local memory).
+template <int KC>
+__device__ __forceinline__ void knn_query_thread(const TreeRef &t, const RoundSpec &rs, float qx,
+                                                 float qy, float qz, int kk, uint2 *s_col,
+                                                 int s_stride, uint2 *l_stack, uint32_t *err,
+                                                 float (&bk)[KC], uint32_t (&bi)[KC]) {
+#pragma unroll
+    for (int j = 0; j < KC; ++j) {
+        bool pad = j < KC - kk;
+        bk[j] = pad ? -INFINITY : INFINITY;
+        bi[j] = pad ? 0u : EMPTY_ID;
+    }
+    const bool valid = t.root != CHILD_NONE && !isnan(qx) && !isnan(qy) && !isnan(qz);
+    float bound = rs.r0sq > 0.0f ? rs.r0sq : 1e-30f, prev = -1.0f;
+    for (uint32_t round = 0; valid; ++round) {
+        const bool last = round + 1 >= rs.max_rounds || !(bound < INFINITY);
+        if (last) bound = INFINITY;
+        float lim = fminf(bound, bk[KC - 1]);
+        uint32_t node = t.root;
+        int sp = 0;
+        uint32_t visits = 0;
+        while (true) {
+            uint32_t lf_first[2], lf_cnt[2];
+            int nleaf = 0;
+            uint32_t next = CHILD_NONE;
+            if (++visits > t.visit_cap) {
+                atomicOr(err, DEVERR_STACK);
+                break;
+            }
+            float k0 = 0.f, k1 = 0.f;
+            bool v0 = false, v1 = false;
+            uint4 d = make_uint4(0, 0, 0, 0);
+            if (node & CHILD_LEAF) {
+                lf_first[0] = node & CHILD_INDEX;
+                lf_cnt[0] = t.root_count;
+                nleaf = 1;
+            } else {
+                float4 a, b, c;
+                load_node(t.s_top, t.nodes, node, a, b, c, d);
+                k0 = box_min_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y);
+                k1 = box_min_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w);
+                v0 = !(k0 > lim);
+                v1 = !(k1 > lim);
+                if (prev >= 0.0f) {
+                    if (v0) v0 = !(box_max_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y) <= prev);
+                    if (v1) v1 = !(box_max_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w) <= prev);
+                }
+                if (v0 && (d.x & CHILD_LEAF)) { lf_first[nleaf] = d.x & CHILD_INDEX; lf_cnt[nleaf] = d.z; ++nleaf; v0 = false; }
+                if (v1 && (d.y & CHILD_LEAF)) { lf_first[nleaf] = d.y & CHILD_INDEX; lf_cnt[nleaf] = d.w; ++nleaf; v1 = false; }
+            }
+            for (int l = 0; l < nleaf; ++l) {
+                for (uint32_t j = 0; j < lf_cnt[l]; ++j) {
+                    float4 pt = __ldg(&t.pts[lf_first[l] + j]);
+                    float key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
+                    uint32_t id = __float_as_uint(pt.w);
+                    if (key <= bound && key > prev && key_less(key, id, bk[KC - 1], bi[KC - 1]))
+                        list_insert<KC>(bk, bi, key, id);
+                }
+            }
+            if (nleaf) lim = fminf(bound, bk[KC - 1]);
+            if (!(node & CHILD_LEAF)) {
+                v0 = v0 && !(k0 > lim);
+                v1 = v1 && !(k1 > lim);
+                if (v0 && v1) {
+                    bool near0 = k0 <= k1;
+                    uint2 far = near0 ? make_uint2(d.y, __float_as_uint(k1))
+                                      : make_uint2(d.x, __float_as_uint(k0));
+                    next = near0 ? d.x : d.y;
+                    if (sp < SHORT_STACK) s_col[sp * s_stride] = far;
+                    else if (sp < STACK_MAX) l_stack[sp - SHORT_STACK] = far;
+                    else atomicOr(err, DEVERR_STACK);
+                    if (sp < STACK_MAX) ++sp;
+                } else if (v0) {
+                    next = d.x;
+                } else if (v1) {
+                    next = d.y;
+                }
+            }
+            if (next == CHILD_NONE) {
+                while (sp > 0) {
+                    --sp;
+                    uint2 e = sp < SHORT_STACK ? s_col[sp * s_stride] : l_stack[sp - SHORT_STACK];
+                    if (!(__uint_as_float(e.y) > lim)) { next = e.x; break; }
+                }
+                if (next == CHILD_NONE) break;
+            }
+            node = next;
+        }
+        if (bi[KC - 1] != EMPTY_ID || last) break;
+        prev = bound;
+        bound = __fmul_rn(bound, rs.mult2);
+    }
+}
+
+// Warp per query: the sorted list of S*32 slots is striped over the lanes
+// (slot j in lane j % 32, register j / 32); candidates from a leaf are
+// tested one per lane and inserted with ballots and shuffles.  stk is the
+// warp's shared-memory stack (STACK_MAX entries).  All arguments must be
+// warp-uniform.
+template <int S>
+__device__ __forceinline__ void knn_query_warp(const TreeRef &t, const RoundSpec &rs, float qx,
+                                               float qy, float qz, uint32_t kk, uint2 *stk,
+                                               uint32_t *err, float (&lk)[S], uint32_t (&li)[S]) {
+    const int lane = threadIdx.x & 31;
+    const int wslot = (int)((kk - 1) >> 5), wlane = (int)((kk - 1) & 31);
+#pragma unroll
+    for (int s = 0; s < S; ++s) { lk[s] = INFINITY; li[s] = EMPTY_ID; }
+    float wk = INFINITY;
+    uint32_t wi = EMPTY_ID;
+    const bool valid = t.root != CHILD_NONE && !isnan(qx) && !isnan(qy) && !isnan(qz);
+    float bound = rs.r0sq > 0.0f ? rs.r0sq : 1e-30f, prev = -1.0f;
+    for (uint32_t round = 0; valid; ++round) {
+        const bool last = round + 1 >= rs.max_rounds || !(bound < INFINITY);
+        if (last) bound = INFINITY;
+        float lim = fminf(bound, wk);
+        uint32_t node = t.root;
+        int sp = 0;
+        uint32_t visits = 0;
+        while (true) {
+            uint32_t lf_first[2], lf_cnt[2];
+            int nleaf = 0;
+            uint32_t next = CHILD_NONE;
+            float k0 = 0.f, k1 = 0.f;
+            uint4 d = make_uint4(0, 0, 0, 0);
+            bool v0 = false, v1 = false;
+            if (++visits > t.visit_cap) {   // warp-uniform
+                if (lane == 0) atomicOr(err, DEVERR_STACK);
+                break;
+            }
+            if (node & CHILD_LEAF) {
+                lf_first[0] = node & CHILD_INDEX;
+                lf_cnt[0] = t.root_count;
+                nleaf = 1;
+            } else {
+                float4 a, b, c;
+                load_node(t.s_top, t.nodes, node, a, b, c, d);
+                k0 = box_min_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y);
+                k1 = box_min_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w);
+                v0 = !(k0 > lim);
+                v1 = !(k1 > lim);
+                if (prev >= 0.0f) {
+                    if (v0) v0 = !(box_max_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y) <= prev);
+                    if (v1) v1 = !(box_max_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w) <= prev);
+                }
+                if (v0 && (d.x & CHILD_LEAF)) { lf_first[nleaf] = d.x & CHILD_INDEX; lf_cnt[nleaf] = d.z; ++nleaf; v0 = false; }
+                if (v1 && (d.y & CHILD_LEAF)) { lf_first[nleaf] = d.y & CHILD_INDEX; lf_cnt[nleaf] = d.w; ++nleaf; v1 = false; }
+            }
+            for (int l = 0; l < nleaf; ++l) {
+                for (uint32_t j0 = 0; j0 < lf_cnt[l]; j0 += 32) {
+                    float key = INFINITY;
+                    uint32_t id = EMPTY_ID;
+                    bool acc = false;
+                    if (j0 + lane < lf_cnt[l]) {
+                        float4 pt = __ldg(&t.pts[lf_first[l] + j0 + lane]);
+                        key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
+                        id = __float_as_uint(pt.w);
+                        acc = key <= bound && key > prev && key_less(key, id, wk, wi);
+                    }
+                    uint32_t m = __ballot_sync(0xffffffffu, acc);
+                    while (m) {
+                        int src = __ffs(m) - 1;
+                        m &= m - 1;
+                        float ck = __shfl_sync(0xffffffffu, key, src);
+                        uint32_t ci = __shfl_sync(0xffffffffu, id, src);
+                        if (!key_less(ck, ci, wk, wi)) continue;   // warp-uniform
+                        // position = number of slots ordered before the candidate
+                        int pos = 0;
+#pragma unroll
+                        for (int s = 0; s < S; ++s)
+                            pos += __popc(__ballot_sync(0xffffffffu, key_less(lk[s], li[s], ck, ci)));
+                        // shift slots >= pos up by one
+                        float carry_k = INFINITY;
+                        uint32_t carry_i = EMPTY_ID;
+#pragma unroll
+                        for (int s = 0; s < S; ++s) {
+                            float upk = __shfl_up_sync(0xffffffffu, lk[s], 1);
+                            uint32_t upi = __shfl_up_sync(0xffffffffu, li[s], 1);
+                            float topk = __shfl_sync(0xffffffffu, lk[s], 31);
+                            uint32_t topi = __shfl_sync(0xffffffffu, li[s], 31);
+                            if (lane == 0) { upk = carry_k; upi = carry_i; }
+                            int j = s * 32 + lane;
+                            if (j > pos) { lk[s] = upk; li[s] = upi; }
+                            else if (j == pos) { lk[s] = ck; li[s] = ci; }
+                            carry_k = topk;
+                            carry_i = topi;
+                        }
+                        float nk = 0.f;
+                        uint32_t ni = 0;
+#pragma unroll
+                        for (int s = 0; s < S; ++s)
+                            if (s == wslot) { nk = lk[s]; ni = li[s]; }
+                        wk = __shfl_sync(0xffffffffu, nk, wlane);
+                        wi = __shfl_sync(0xffffffffu, ni, wlane);
+                    }
+                }
+                lim = fminf(bound, wk);
+            }
+            if (!(node & CHILD_LEAF)) {
+                v0 = v0 && !(k0 > lim);
+                v1 = v1 && !(k1 > lim);
+                if (v0 && v1) {
+                    bool near0 = k0 <= k1;
+                    uint2 far = near0 ? make_uint2(d.y, __float_as_uint(k1))
+                                      : make_uint2(d.x, __float_as_uint(k0));
+                    next = near0 ? d.x : d.y;
+                    if (sp < STACK_MAX) {
+                        if (lane == 0) stk[sp] = far;
+                        ++sp;
+                    } else if (lane == 0) {
+                        atomicOr(err, DEVERR_STACK);
+                    }
+                } else if (v0) {
+                    next = d.x;
+                } else if (v1) {
+                    next = d.y;
+                }
+            }
+            __syncwarp();
+            if (next == CHILD_NONE) {
+                while (sp > 0) {
+                    --sp;
+                    uint2 e = stk[sp];
+                    if (!(__uint_as_float(e.y) > lim)) { next = e.x; break; }
+                }
+                if (next == CHILD_NONE) break;
+            }
+            __syncwarp();
+            node = next;
+        }
+        if (wi != EMPTY_ID || last) break;
+        prev = bound;
+        bound = __fmul_rn(bound, rs.mult2);
+    }
+}
+
+}  // namespace rtd

@@ -459,6 +459,13 @@ rtd_status build_seed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStream
     return RTD_OK;
 }
 
+}  // namespace
+
+template <typename K>
+rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStream_t st);
+
+namespace {
+
 template <typename K>
 rtd_status build_typed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStream_t st) {
     IndexHeader *h = idx->hdr.as<IndexHeader>();
@@ -480,6 +487,17 @@ rtd_status build_typed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStrea
     gather_points_kernel<<<g, BLOCK, 0, st>>>(d_xyz, perm, n, idx->pts.as<float4>());
     RTD_LAUNCH_CHECK();
     idx->mark(EV_BUILD_SORTED, st);
+    return build_tree_sorted<K>(idx, skeys, n, st);
+}
+
+}  // namespace
+
+// Karras tree, leaf collapse and refit over keys already sorted, with
+// idx->pts holding the points in key order.
+template <typename K>
+rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStream_t st) {
+    IndexHeader *h = idx->hdr.as<IndexHeader>();
+    uint32_t *d_err = &h->err;
     if (n < 2 || n <= idx->leaf_size) return RTD_OK;
     const uint64_t ni = n - 1;
     for (rtd::DevBuf *b : {&idx->kleft, &idx->kright, &idx->kfirst, &idx->klast, &idx->kparent,
@@ -506,7 +524,10 @@ rtd_status build_typed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStrea
     return RTD_OK;
 }
 
-}  // namespace
+template rtd_status build_tree_sorted<uint32_t>(rtd_index *, const uint32_t *, uint64_t,
+                                                cudaStream_t);
+template rtd_status build_tree_sorted<uint64_t>(rtd_index *, const uint64_t *, uint64_t,
+                                                cudaStream_t);
 
 rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd_schedule *s,
                        cudaStream_t st) {

@@ -105,7 +105,19 @@ _SIGNATURES = {
     "rtd_bh_info_get": (_I, [_P, _P, _P]),
     "rtd_bh_export": (_I, [_P, _P, _P, _P]),
     "rtd_barnes_hut_host": (_I, [_P, _P, _U64, _F, _F, _P]),
+    "rtd_batch_create": (_I, [C.POINTER(_P)]),
+    "rtd_batch_destroy": (_I, [_P]),
+    "rtd_batch_plan": (_I, [_P, _P, _U32, C.POINTER(Schedule)]),
+    "rtd_knn_batched": (_I, [_P, _P, _P, _P, _P, _I, _P]),
+    "rtd_knn_batched_backward": (_I, [_P, _P, _P, _P, _P, _P, _P, _P]),
 }
+
+
+class Cloud(C.Structure):
+    """rtd_cloud: one cloud of a packed batch."""
+    _fields_ = [("point_offset", C.c_uint64), ("query_offset", C.c_uint64),
+                ("out_offset", C.c_uint64), ("n_points", C.c_uint32),
+                ("n_queries", C.c_uint32), ("k", C.c_uint32), ("pad", C.c_uint32)]
 
 BH_LAW_REFERENCE = 0
 BH_LAW_PLUMMER = 1
