@@ -279,6 +279,24 @@ rtd_status rtd_bh_release(rtd_bh *b);
  * Outputs are in the caller's body order. */
 rtd_status rtd_bh_forward(rtd_bh *b, const rtd_bh_params *p, float *d_out, float *d_phi,
                           rtd_stream stream);
+/* rtd_bh_forward for the Plummer law that allocates no device memory; no
+ * counterpart in the reference.  For callers that cannot let a library call
+ * cudaMalloc once their tree is built: hosts whose own memory manager owns
+ * the device memory, and step loops that must not stall on the device-wide
+ * synchronisation cudaMalloc / cudaFree can cause.  The walk's per-warp
+ * traversal stack, which rtd_bh_forward reserves on first use, comes here
+ * from a fixed 37 MiB array (592 warp stacks) that each device loading the
+ * library holds until the process exits.  The array limits how many warps
+ * walk at once, not the number of bodies, so no tree is refused for its
+ * size; a traversal deeper than a warp's stack is reported as
+ * RTD_ERR_OVERFLOW like rtd_bh_forward.  The first call on a device looks up
+ * the array's device address (with that device current); make that first
+ * call before any stream capture.  Every call shares the array: calls that
+ * overlap on the GPU (other streams, other threads) race and must be
+ * serialised by the caller.  Results equal rtd_bh_forward's bit for bit.
+ * RTD_BH_LAW_REFERENCE is refused with RTD_ERR_UNSUPPORTED. */
+rtd_status rtd_bh_forward_noalloc(rtd_bh *b, const rtd_bh_params *p, float *d_out, float *d_phi,
+                                  rtd_stream stream);
 /* Adjoint of the Plummer-law walk (same tree, same decisions): given
  * dL/da (n*3) and dL/dphi (n, may be NULL = 0), writes dL/dpos (n*3) and
  * dL/dmass (n).  No reference counterpart (the reference has no gradients). */

@@ -541,4 +541,57 @@ rtd_status bh_backward(rtd_bh *b, const rtd_bh_params *p, const float *g_acc, co
     return RTD_OK;
 }
 
+namespace {
+
+// Forward walk on a traversal stack supplied by the caller: `stack` holds
+// max_warps slices of BH_STACK_CAP entries and the launch is capped to that
+// many warps.  Nothing is allocated.
+template <bool QUAD>
+rtd_status launch_walk_on_stack(rtd_bh *b, const rtd_bh_params *p, float *acc, float *phi,
+                                uint2 *stack, uint64_t max_warps, cudaStream_t st) {
+    int dev = 0, sms = 148, per_sm = 4;
+    RTD_CUDA(cudaGetDevice(&dev));
+    RTD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    RTD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bh_walk_kernel<QUAD, false>,
+                                                           WW * 32, 0));
+    if (per_sm < 1) per_sm = 1;
+    uint64_t blocks = (uint64_t)sms * (uint64_t)per_sm;
+    const uint64_t need = (b->n + WW - 1) / WW;
+    if (blocks > need) blocks = need;
+    if (blocks > max_warps / WW) blocks = max_warps / WW;
+    if (blocks < 1) return fail(RTD_ERR_INVALID_ARGUMENT, "stack holds less than one block of warps");
+    BhHeader *h = b->hdr.as<BhHeader>();
+    RTD_CUDA(cudaMemsetAsync(&h->group_counter, 0, sizeof(uint32_t), st));
+    const BhView v = bh_view(b);
+    bh_walk_kernel<QUAD, false><<<(unsigned)blocks, WW * 32, 0, st>>>(
+        v, p->theta * p->theta, p->eps * p->eps, p->G, nullptr, nullptr, acc, phi, nullptr,
+        nullptr, stack, h);
+    RTD_LAUNCH_CHECK();
+    return RTD_OK;
+}
+
+}  // namespace
+
+// Plummer-law forward walk with the traversal stack given by the caller
+// (max_warps slices of BH_STACK_CAP uint2 entries); same checks and results
+// as bh_forward for the Plummer law.
+rtd_status bh_forward_on_stack(rtd_bh *b, const rtd_bh_params *p, float *d_out, float *d_phi,
+                               uint2 *stack, uint64_t max_warps, cudaStream_t st) {
+    if (!b || !b->built) return fail(RTD_ERR_INVALID_ARGUMENT, "bh tree not built");
+    if (b->n && !d_out) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL output");
+    if (!stack) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL stack");
+    rtd_bh_params def;
+    rtd_bh_params_default(&def);
+    if (!p) p = &def;
+    if (p->law != RTD_BH_LAW_PLUMMER)
+        return fail(RTD_ERR_UNSUPPORTED, "this walk implements the Plummer law only");
+    if (b->n == 0) return RTD_OK;
+    if (!b->plummer_ready)
+        return fail(RTD_ERR_INVALID_ARGUMENT, "tree was not built for the Plummer law");
+    if (p->quadrupole && !b->has_quad)
+        return fail(RTD_ERR_INVALID_ARGUMENT, "tree was built without quadrupoles");
+    if (p->quadrupole) return launch_walk_on_stack<true>(b, p, d_out, d_phi, stack, max_warps, st);
+    return launch_walk_on_stack<false>(b, p, d_out, d_phi, stack, max_warps, st);
+}
+
 }  // namespace rtd

@@ -101,6 +101,7 @@ _SIGNATURES = {
     "rtd_bh_build": (_I, [_P, _P, _P, _U64, _P, _P]),
     "rtd_bh_release": (_I, [_P]),
     "rtd_bh_forward": (_I, [_P, _P, _P, _P, _P]),
+    "rtd_bh_forward_noalloc": (_I, [_P, _P, _P, _P, _P]),
     "rtd_bh_backward": (_I, [_P, _P, _P, _P, _P, _P, _P]),
     "rtd_bh_info_get": (_I, [_P, _P, _P]),
     "rtd_bh_export": (_I, [_P, _P, _P, _P]),

@@ -1,0 +1,85 @@
+"""rtd_bh_forward_noalloc: the Plummer-law Barnes-Hut forward walk for
+callers that cannot let the library allocate device memory (a host memory
+manager that owns the device memory, or a step loop that must not stall on
+cudaMalloc / cudaFree).  Its traversal stacks come from a fixed array in the
+library instead of the allocator.
+
+Checked through the C ABI: two calls in a row, on two different trees, each
+equal bit for bit to rtd_bh_forward on the same tree (both run the same walk
+kernel with the same per-body arithmetic; only the stack memory and the
+number of warps differ), and device free memory unchanged across a call on a
+tree whose stack rtd_bh_forward never reserved.  This file is collected last
+so that a run stopping at the first failure has run every other test."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from rtdsl import workloads
+
+pytestmark = pytest.mark.gpu
+
+MIB = 1 << 20
+
+
+def plummer_tree(n, seed, quad):
+    from rtdsl._capi import BH_LAW_PLUMMER, default_bh_params
+    from rtdsl.bh import BarnesHut
+    pos, mass = workloads.plummer(n, seed=seed)
+    p = default_bh_params(law=BH_LAW_PLUMMER, theta=0.5, eps=1e-3, G=1.0, bucket=16,
+                          quadrupole=int(quad))
+    bh = BarnesHut().build(torch.from_numpy(pos).cuda(), torch.from_numpy(mass).cuda(), p)
+    return bh, p
+
+
+def noalloc_forward(lib, bh, p, acc, phi):
+    st = torch.cuda.current_stream()
+    return lib.rtd_bh_forward_noalloc(bh._h, C.byref(p), C.c_void_p(acc.data_ptr()),
+                                      C.c_void_p(phi.data_ptr()), C.c_void_p(st.cuda_stream))
+
+
+def test_noalloc_forward_equals_forward_on_two_calls(rtd, cuda):
+    lib = rtd.load()
+    bh_a, p_a = plummer_tree(100_000, seed=21, quad=True)
+    bh_b, p_b = plummer_tree(60_000, seed=22, quad=False)
+    acc_a = torch.full((bh_a.n, 3), float("nan"), device=cuda)
+    phi_a = torch.full((bh_a.n,), float("nan"), device=cuda)
+    acc_b = torch.full((bh_b.n, 3), float("nan"), device=cuda)
+    phi_b = torch.full((bh_b.n,), float("nan"), device=cuda)
+    torch.cuda.synchronize()
+
+    # call 1 (looks up the array's device address on first use)
+    assert noalloc_forward(lib, bh_a, p_a, acc_a, phi_a) == 0, lib.rtd_last_error()
+    torch.cuda.synchronize()
+    # call 2, right after, on another tree: no device memory may be taken
+    free0, _ = torch.cuda.mem_get_info()
+    assert noalloc_forward(lib, bh_b, p_b, acc_b, phi_b) == 0, lib.rtd_last_error()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free0 - free1 < 2 * MIB, f"free device memory fell by {(free0 - free1) / MIB:.1f} MiB"
+
+    # the allocating entry point on the same trees (it reserves its stacks now)
+    ref_acc_a, ref_phi_a = bh_a.forward(p_a)
+    ref_acc_b, ref_phi_b = bh_b.forward(p_b)
+    torch.cuda.synchronize()
+    # tolerance: none, the per-body arithmetic is the same kernel's
+    for got, ref in ((acc_a, ref_acc_a), (phi_a, ref_phi_a), (acc_b, ref_acc_b),
+                     (phi_b, ref_phi_b)):
+        g = got.cpu().numpy()
+        r = ref.cpu().numpy()
+        assert np.isfinite(g).all()
+        np.testing.assert_array_equal(g.view(np.uint32), r.view(np.uint32))
+    info = bh_a.info()
+    assert info["n_bodies"] == 100_000
+
+
+def test_noalloc_forward_refuses_reference_law(rtd, cuda):
+    from rtdsl._capi import BH_LAW_REFERENCE
+    lib = rtd.load()
+    bh, p = plummer_tree(1_000, seed=3, quad=True)
+    acc = torch.empty((bh.n, 3), device=cuda)
+    phi = torch.empty((bh.n,), device=cuda)
+    p.law = BH_LAW_REFERENCE
+    assert noalloc_forward(lib, bh, p, acc, phi) == 7   # RTD_ERR_UNSUPPORTED
+    assert lib.rtd_bh_forward_noalloc(None, None, None, None, None) == 1   # INVALID_ARGUMENT
