@@ -43,6 +43,8 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the BH / batched sub-benchmarks")
+    ap.add_argument("--only", choices=["bh", "batch"], default=None,
+                    help="run one sub-benchmark alone (one GPU) and print its JSON")
     return ap.parse_args()
 
 
@@ -242,6 +244,9 @@ def run_ours(args, ws, rank, local):
         ctx.close()
 
     extras = {}
+    if not args.no_extras and ws == 1:
+        extras["barnes_hut"] = bench_bh(args, dev, flush)
+        extras["batched"] = bench_batch(args, dev, flush)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -269,6 +274,186 @@ def run_ours(args, ws, rank, local):
         line["cpu_baseline"] = cpu
     line.update(extras)
     print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------- Barnes-Hut sub-bench
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def bench_bh(args, dev, flush) -> dict:
+    """1M-body Plummer sphere, theta 0.5, eps 1e-3, monopole + quadrupole.
+    One step = tree build + forward (a, phi) + adjoint of
+    L = sum(phi) + 0.5 sum|a|^2 (dL/da = a, dL/dphi = 1) w.r.t. positions and
+    masses.  Roofline of the walks in logical bytes streamed: per body
+    40 B per accepted cell + 16 B per body of an opened leaf + 32 B of I/O
+    (forward); the adjoint streams both twice plus 48 B of I/O."""
+    import torch
+    import rtdsl
+    from rtdsl import autotune, workloads
+    from rtdsl._capi import BH_LAW_PLUMMER, default_bh_params
+
+    n = 1_000_000
+    pos, mass = workloads.plummer(n, seed=7)
+    P = torch.from_numpy(pos).to(dev)
+    M = torch.from_numpy(mass).to(dev)
+    bucket = 32
+    cached = autotune._load().get("plummer_1m_bucket")
+    if cached:
+        bucket = int(cached["bucket"])
+    p = default_bh_params(law=BH_LAW_PLUMMER, theta=0.5, eps=1e-3, G=1.0, quadrupole=1,
+                          bucket=bucket)
+    bh = rtdsl.BarnesHut()
+    acc = torch.empty((n, 3), device=dev)
+    phi = torch.empty((n,), device=dev)
+    g_pos = torch.empty((n, 3), device=dev)
+    g_mass = torch.empty((n,), device=dev)
+    ones = torch.ones((n,), device=dev)
+
+    def step(ev=None):
+        if ev:
+            ev[0].record()
+        bh.build(P, M, p)
+        if ev:
+            ev[1].record()
+        bh.forward(p, out=acc, phi=phi)
+        if ev:
+            ev[2].record()
+        bh.backward(acc, ones, p, out_pos=g_pos, out_mass=g_mass)
+        if ev:
+            ev[3].record()
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    t_build, t_fwd, t_adj = [], [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        step(ev)
+        ev[3].synchronize()
+        t_build.append(ev[0].elapsed_time(ev[1]))
+        t_fwd.append(ev[1].elapsed_time(ev[2]))
+        t_adj.append(ev[2].elapsed_time(ev[3]))
+    mb, mf, ma = (statistics.mean(t) for t in (t_build, t_fwd, t_adj))
+    cnt = bh.interaction_counts(0.5, stride=16)
+    C_, B_ = cnt["cells_per_body"], cnt["bodies_per_body"]
+    fwd_bytes = n * (40 * C_ + 16 * B_ + 32)
+    adj_bytes = n * (2 * (40 * C_ + 16 * B_) + 48)
+    peak = measured_peaks()
+    walk = (fwd_bytes + adj_bytes) / ((mf + ma) / 1e3) / 1e9
+    flops_fwd = n * (C_ * 65 + B_ * 23)
+    return {
+        "metric": "BH force+adjoint bodies/s", "value": n / ((mb + mf + ma) / 1e3),
+        "unit": "bodies/s",
+        "config": {"workload": "plummer_1m: 1M-body Plummer sphere (a=1, M=1, seed 7), theta 0.5, "
+                               "eps 1e-3, monopole+quadrupole, G=1; step = build + forward + adjoint",
+                   "bucket": bucket, "l2": "256 MiB buffer written between timed steps"},
+        "ms": {"build": mb, "forward": mf, "adjoint": ma, "step": mb + mf + ma},
+        "interactions_per_body": {"cells": C_, "bodies": B_, "sampled": cnt["sampled"]},
+        "roofline": {"kernel": "bh_walk_kernel (forward + adjoint)", "bound": "hbm",
+                     "achieved": walk, "peak": peak["hbm_gbs"], "unit": "GB/s",
+                     "frac": walk / peak["hbm_gbs"],
+                     "peak_source": peak["source"] + " (MEASURED_PEAKS.json hbm_gbs)",
+                     "bytes": "logical bytes streamed (40 B per cell, 16 B per leaf body)",
+                     "forward_gbs": fwd_bytes / (mf / 1e3) / 1e9,
+                     "adjoint_gbs": adj_bytes / (ma / 1e3) / 1e9,
+                     "traffic": traffic_for("bh_walk", "plummer_1m")},
+        "fp32_tflops_forward": flops_fwd / (mf / 1e3) / 1e12,
+    }
+
+
+# --------------------------------------------------- batched sub-bench
+def bench_batch(args, dev, flush) -> dict:
+    """256 clouds (log-uniform 1e3..2e5 points, uniform / 8-Gaussian
+    alternating, 0.25x queries, k in {1,5,16,64}): the batched pass (forest
+    build + persistent search, CUDA graph replay) against plain per-cloud
+    build + search launches, with full id agreement checked."""
+    import numpy as np
+    import torch
+    import rtdsl
+    from rtdsl import autotune, workloads
+
+    cl = workloads.clouds()
+    pts = np.concatenate([c["points"] for c in cl])
+    q = np.concatenate([c["queries"] for c in cl])
+    sizes = [(len(c["points"]), len(c["queries"]), c["k"]) for c in cl]
+    P = torch.from_numpy(pts).to(dev)
+    Q = torch.from_numpy(q).to(dev)
+    s = autotune.cached_schedule("clouds_256", rtdsl.default_batch_schedule())
+    b = rtdsl.Batch(sizes, s)
+    ids = torch.empty(b.n_out, dtype=torch.int32, device=dev)
+    d2 = torch.empty(b.n_out, dtype=torch.float32, device=dev)
+    st = torch.cuda.Stream(device=dev)
+    ixs = [rtdsl.Index() for _ in cl]
+    views = []
+    for c, (npnt, nq, k) in enumerate(sizes):
+        po, qo = int(b.point_offset[c]), int(b.query_offset[c])
+        views.append((P[po:po + npnt], Q[qo:qo + nq], k))
+    plain_ids = [torch.empty((v[1].shape[0], v[2]), dtype=torch.int32, device=dev) for v in views]
+    plain_sched = rtdsl.default_schedule()
+
+    def batched():
+        b.knn(P, Q, out_ids=ids, out_d2=d2, use_graph=True, stream=st)
+
+    def plain():
+        for ix, (p_, q_, k), o in zip(ixs, views, plain_ids):
+            ix.build(p_, plain_sched, stream=st)
+            ix.knn(q_, k, plain_sched, out_ids=o, with_d2=False, stream=st)
+
+    def timed(fn, steps):
+        with torch.cuda.stream(st):
+            for _ in range(max(args.warmup, 3)):
+                fn()
+            st.synchronize()
+            ms = []
+            for _ in range(steps):
+                flush.zero_()
+                st.wait_stream(torch.cuda.current_stream())
+                e0, e1 = _events()
+                e0.record(st)
+                fn()
+                e1.record(st)
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+        return statistics.mean(ms)
+
+    t_batched = timed(batched, args.steps)
+    t_plain = timed(plain, max(3, args.steps // 3))
+    torch.cuda.synchronize()
+    agree = 0
+    for c, o in enumerate(plain_ids):
+        off = int(b.out_offset[c])
+        agree += int((ids[off:off + o.numel()].view(o.shape) == o).all(dim=1).sum())
+    # backward of L = sum_q mean_j d2_qj (ids fixed)
+    g = torch.empty(b.n_out, device=dev)
+    for c, (_, nq, k) in enumerate(sizes):
+        off = int(b.out_offset[c])
+        g[off:off + nq * k] = 1.0 / k
+    gq = torch.empty_like(Q)
+    gp = torch.zeros_like(P)
+    e0, e1 = _events()
+    with torch.cuda.stream(st):
+        b.backward(P, Q, ids, g, gq, gp, stream=st)
+        st.synchronize()
+        e0.record(st)
+        gp.zero_()
+        b.backward(P, Q, ids, g, gq, gp, stream=st)
+        e1.record(st)
+        e1.synchronize()
+    nq = len(q)
+    return {
+        "metric": "batched vs plain", "value": t_plain / t_batched, "unit": "x",
+        "config": {"workload": f"clouds_256: {len(cl)} clouds, {len(pts)} points, {nq} queries, "
+                               "k in {1,5,16,64}; batched = forest build + persistent search "
+                               "(CUDA graph), plain = one build + one search per cloud",
+                   "schedule": s.as_dict()},
+        "batched_ms": t_batched, "plain_ms": t_plain,
+        "batched_queries_per_s": nq / (t_batched / 1e3),
+        "plain_queries_per_s": nq / (t_plain / 1e3),
+        "id_agreement": agree / nq, "backward_ms": e0.elapsed_time(e1),
+    }
 
 
 # ---------------------------------------------------------- CPU baseline
@@ -328,6 +513,13 @@ def main():
     ws, rank, local = dist_env()
     if args.impl == "reference":
         run_reference(args, ws, rank)
+    elif args.only:
+        import torch
+        dev = torch.device("cuda", local)
+        torch.cuda.set_device(dev)
+        flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+        out = bench_bh(args, dev, flush) if args.only == "bh" else bench_batch(args, dev, flush)
+        print(json.dumps(out), flush=True)
     else:
         run_ours(args, ws, rank, local)
 

@@ -216,11 +216,18 @@ typedef struct rtd_batch rtd_batch;
 rtd_status rtd_batch_create(rtd_batch **out);
 rtd_status rtd_batch_destroy(rtd_batch *b);
 /* Clouds must be packed in order: point_offset and query_offset of cloud c
- * are the sums of n_points / n_queries of clouds 0..c-1.  radius_param of
- * the schedule scales the per-cloud initial radius (mean point spacing of
- * the cloud's box); leaf_size, radius_increment_mult, max_rounds apply. */
+ * are the sums of n_points / n_queries of clouds 0..c-1.  The initial radius
+ * of a cloud is radius_param when radius_heuristic is RTD_RADIUS_FIXED, else
+ * radius_param x the radius of a ball expected to hold k points at the
+ * cloud's mean density (box volume / n_points, box extents clamped to >= max
+ * extent / sqrt(n)).  leaf_size, radius_increment_mult and max_rounds apply
+ * as for rtd_knn; lanes_per_query = 32 sends clouds with k <= 32 to the
+ * warp-per-query search (else thread per query for k <= 16).  sched = NULL
+ * means rtd_batch_schedule_default. */
 rtd_status rtd_batch_plan(rtd_batch *b, const rtd_cloud *clouds, uint32_t n_clouds,
                           const rtd_schedule *sched);
+/* rtd_schedule_default with radius_param = 1 (one expected k-ball). */
+void rtd_batch_schedule_default(rtd_schedule *s);
 /* Ids are cloud-local point indices; d_d2 may be NULL. */
 rtd_status rtd_knn_batched(rtd_batch *b, const float *d_points, const float *d_queries,
                            uint32_t *d_ids, float *d_d2, int use_graph, rtd_stream stream);
@@ -309,6 +316,13 @@ typedef struct rtd_bh_info {
     float root_min[3], root_max[3];
 } rtd_bh_info;
 rtd_status rtd_bh_info_get(rtd_bh *b, rtd_bh_info *info, rtd_stream stream);
+/* Interaction counts of the Plummer-law walk at opening angle theta, for
+ * every stride-th body in tree order: *cells = accepted cells, *bodies =
+ * bodies of opened leaves, summed over the *sampled bodies.  Measurement aid
+ * (bytes and flops the walk streams per body); no reference counterpart.
+ * Synchronises. */
+rtd_status rtd_bh_interaction_counts(rtd_bh *b, float theta, uint64_t stride, uint64_t *cells,
+                                     uint64_t *bodies, uint64_t *sampled, rtd_stream stream);
 /* Host copies of the tree in the reference's FlatNode layout
  * (gprt-core/src/lib.rs:299-308, 40 B per node) and the flat body order
  * (order[i] = caller index of the i-th flat body).  Synchronises. */

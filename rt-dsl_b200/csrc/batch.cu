@@ -94,12 +94,13 @@ __global__ void __launch_bounds__(BLOCK) batch_bbox_kernel(const float *__restri
     }
 }
 
-// Initial radius of a cloud: `fixed` when > 0, else the radius of a ball
-// expected to hold k points at the cloud's mean density, (3 k V / 4 pi n)^(1/3).
-// Box extents are clamped to >= max extent / sqrt(n), which makes the
-// estimate the mean spacing of a flat (2-D) cloud; an estimate that is too
-// large only costs pruning, one that is too small costs extra rounds.
-__global__ void batch_seed_kernel(CloudDesc *cd, uint32_t n_clouds, float fixed) {
+// Initial radius of a cloud: `fixed` when > 0, else `mult` x the radius of
+// a ball expected to hold k points at the cloud's mean density,
+// (3 k V / 4 pi n)^(1/3).  Box extents are clamped to >= max extent /
+// sqrt(n), which makes the estimate the mean spacing of a flat (2-D) cloud;
+// an estimate that is too large only costs pruning, one that is too small
+// costs extra rounds.
+__global__ void batch_seed_kernel(CloudDesc *cd, uint32_t n_clouds, float fixed, float mult) {
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n_clouds; c += gridDim.x * blockDim.x) {
         float r = fixed;
         if (!(r > 0.0f)) {
@@ -113,7 +114,7 @@ __global__ void batch_seed_kernel(CloudDesc *cd, uint32_t n_clouds, float fixed)
             }
             const float emin = fmaxf(emax / sqrtf(n), 1e-20f);
             const float v = fmaxf(e[0], emin) * fmaxf(e[1], emin) * fmaxf(e[2], emin);
-            r = cbrtf(3.0f * (float)cd[c].k * v / (4.0f * 3.14159265f * n));
+            r = mult * cbrtf(3.0f * (float)cd[c].k * v / (4.0f * 3.14159265f * n));
         }
         if (!(r > 0.0f) || !(r < INFINITY)) r = 1.0f;
         cd[c].r0sq = r * r;
@@ -343,7 +344,8 @@ static rtd_status batch_pass(rtd_batch *b, const float *d_pts, const float *d_q,
         RTD_LAUNCH_CHECK();
     }
     batch_seed_kernel<<<grid_for(b->n_clouds, 128, 1024), 128, 0, st>>>(
-        cd, b->n_clouds, b->sched.radius_heuristic == RTD_RADIUS_FIXED ? b->sched.radius_param : 0.0f);
+        cd, b->n_clouds, b->sched.radius_heuristic == RTD_RADIUS_FIXED ? b->sched.radius_param : 0.0f,
+        b->sched.radius_param);
     RTD_LAUNCH_CHECK();
     const int kbits = 3 * b->bpa + b->cbits;
     if (n) {
@@ -415,11 +417,17 @@ static rtd_status batch_pass(rtd_batch *b, const float *d_pts, const float *d_q,
 
 extern "C" {
 
+void rtd_batch_schedule_default(rtd_schedule *s) {
+    if (!s) return;
+    rtd_schedule_default(s);
+    s->radius_param = 1.0f;
+}
+
 rtd_status rtd_batch_create(rtd_batch **out) {
     if (!out) return fail(RTD_ERR_INVALID_ARGUMENT, "out is NULL");
     *out = new (std::nothrow) rtd_batch();
     if (!*out) return fail(RTD_ERR_OUT_OF_MEMORY, "host allocation failed");
-    rtd_schedule_default(&(*out)->sched);
+    rtd_batch_schedule_default(&(*out)->sched);
     return RTD_OK;
 }
 
@@ -432,7 +440,7 @@ rtd_status rtd_batch_plan(rtd_batch *b, const rtd_cloud *clouds, uint32_t n_clou
                           const rtd_schedule *sched) {
     if (!b || (n_clouds && !clouds)) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL argument");
     rtd_schedule s;
-    rtd_schedule_default(&s);
+    rtd_batch_schedule_default(&s);
     if (sched) s = *sched;
     if (!(s.radius_increment_mult > 1.0f)) return fail(RTD_ERR_INVALID_ARGUMENT, "radius_increment_mult must be > 1");
     if (s.max_rounds < 1) return fail(RTD_ERR_INVALID_ARGUMENT, "max_rounds must be >= 1");
@@ -448,7 +456,7 @@ rtd_status rtd_batch_plan(rtd_batch *b, const rtd_cloud *clouds, uint32_t n_clou
         cd[c] = CloudDesc{(uint32_t)np, x.n_points, (uint32_t)nq, x.n_queries, x.k, 0u, 0u, {}, 0.f,
                           x.out_offset};
         for (uint32_t s0 = 0; s0 < x.n_queries; s0 += 32)
-            cls_items[k_class(x.k)].push_back(
+            cls_items[s.lanes_per_query == 32 && x.k <= 32 ? 2 : k_class(x.k)].push_back(
                 WorkItem{c, (uint32_t)nq + s0, x.n_queries - s0 < 32u ? x.n_queries - s0 : 32u, 0u});
         np += x.n_points;
         nq += x.n_queries;

@@ -188,3 +188,15 @@ rtd_status rtd_barnes_hut_host(rtd_context *ctx, const rtd_body *bodies, uint64_
 }
 
 }  // extern "C"
+
+namespace rtd {
+rtd_status bh_interaction_counts(rtd_bh *b, float theta, uint64_t stride, uint64_t *h_cells,
+                                 uint64_t *h_bodies, uint64_t *h_sampled, cudaStream_t st);
+}  // namespace rtd
+
+extern "C" rtd_status rtd_bh_interaction_counts(rtd_bh *b, float theta, uint64_t stride,
+                                                uint64_t *cells, uint64_t *bodies,
+                                                uint64_t *sampled, rtd_stream stream) {
+    return rtd::bh_interaction_counts(b, theta, stride, cells, bodies, sampled,
+                                      (cudaStream_t)stream);
+}

@@ -595,3 +595,59 @@ rtd_status bh_forward_on_stack(rtd_bh *b, const rtd_bh_params *p, float *d_out, 
 }
 
 }  // namespace rtd
+
+namespace rtd {
+namespace {
+
+// Interaction counts of the Plummer walk for every stride-th flat body: the
+// same per-body MAC over the pre-order tree (autoropes), counting accepted
+// cells and the bodies of opened leaves.  out[0] += cells, out[1] += bodies.
+__global__ void bh_count_kernel(const BhView v, float theta2, uint64_t stride,
+                                unsigned long long *out) {
+    const uint32_t n_nodes = v.hdr->n_nodes;
+    unsigned long long cells = 0, bodies = 0;
+    for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s * stride < v.n;
+         s += (uint64_t)gridDim.x * blockDim.x) {
+        const float4 me = v.fbody[s * stride];
+        uint32_t p = 0;
+        while (p < n_nodes) {
+            const float4 a = __ldg(&v.node_a[p]);
+            const uint4 b = __ldg(&v.node_b[p]);
+            if (body_accept(me.x, me.y, me.z, a.x, a.y, a.z, __uint_as_float(b.w), theta2)) {
+                ++cells;
+                p = b.x;
+            } else {
+                if (b.z & BH_LEAF_BIT) bodies += b.z & ~BH_LEAF_BIT;
+                ++p;
+            }
+        }
+    }
+    atomicAdd(&out[0], cells);
+    atomicAdd(&out[1], bodies);
+}
+
+}  // namespace
+
+rtd_status bh_interaction_counts(rtd_bh *b, float theta, uint64_t stride, uint64_t *h_cells,
+                                 uint64_t *h_bodies, uint64_t *h_sampled, cudaStream_t st) {
+    if (!b || !b->built) return fail(RTD_ERR_INVALID_ARGUMENT, "bh tree not built");
+    if (stride < 1) return fail(RTD_ERR_INVALID_ARGUMENT, "stride must be >= 1");
+    RTD_TRY(b->cell_grad.reserve(2 * sizeof(unsigned long long)));
+    unsigned long long *d = b->cell_grad.as<unsigned long long>();
+    RTD_CUDA(cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), st));
+    const uint64_t ns = b->n ? (b->n + stride - 1) / stride : 0;
+    if (ns) {
+        bh_count_kernel<<<grid_for(ns, 128, 148 * 8), 128, 0, st>>>(bh_view(b), theta * theta,
+                                                                     stride, d);
+        RTD_LAUNCH_CHECK();
+    }
+    unsigned long long h[2] = {0, 0};
+    RTD_CUDA(cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, st));
+    RTD_CUDA(cudaStreamSynchronize(st));
+    if (h_cells) *h_cells = h[0];
+    if (h_bodies) *h_bodies = h[1];
+    if (h_sampled) *h_sampled = ns;
+    return RTD_OK;
+}
+
+}  // namespace rtd

@@ -6,7 +6,8 @@ reference's k_nn! / range_query! / barnes_hut! interface.
 """
 from ._capi import (BH_LAW_PLUMMER, BH_LAW_REFERENCE, EMPTY_ID, RADIUS_FIXED,
                     RADIUS_SAMPLED_MAX, RADIUS_SAMPLED_NN, RADIUS_SAMPLED_PERCENTILE, BhParams,
-                    RtdError, Schedule, default_bh_params, default_schedule, load)
+                    RtdError, Schedule, default_batch_schedule, default_bh_params,
+                    default_schedule, load)
 from .api import Context, Index, k_nn, k_nn_array, knn_backward, range_query
 from .batch import Batch
 from .bh import BarnesHut, barnes_hut
@@ -14,6 +15,6 @@ from .bh import BarnesHut, barnes_hut
 __all__ = [
     "BH_LAW_PLUMMER", "BH_LAW_REFERENCE", "EMPTY_ID", "RADIUS_FIXED", "RADIUS_SAMPLED_MAX",
     "RADIUS_SAMPLED_NN", "RADIUS_SAMPLED_PERCENTILE", "BhParams", "RtdError", "Schedule",
-    "default_bh_params", "default_schedule", "load", "Context", "Index", "k_nn", "k_nn_array",
+    "default_batch_schedule", "default_bh_params", "default_schedule", "load", "Context", "Index", "k_nn", "k_nn_array",
     "knn_backward", "range_query", "Batch", "BarnesHut", "barnes_hut",
 ]

@@ -104,11 +104,14 @@ _SIGNATURES = {
     "rtd_bh_forward_noalloc": (_I, [_P, _P, _P, _P, _P]),
     "rtd_bh_backward": (_I, [_P, _P, _P, _P, _P, _P, _P]),
     "rtd_bh_info_get": (_I, [_P, _P, _P]),
+    "rtd_bh_interaction_counts": (_I, [_P, _F, _U64, C.POINTER(_U64), C.POINTER(_U64),
+                                       C.POINTER(_U64), _P]),
     "rtd_bh_export": (_I, [_P, _P, _P, _P]),
     "rtd_barnes_hut_host": (_I, [_P, _P, _U64, _F, _F, _P]),
     "rtd_batch_create": (_I, [C.POINTER(_P)]),
     "rtd_batch_destroy": (_I, [_P]),
     "rtd_batch_plan": (_I, [_P, _P, _U32, C.POINTER(Schedule)]),
+    "rtd_batch_schedule_default": (None, [C.POINTER(Schedule)]),
     "rtd_knn_batched": (_I, [_P, _P, _P, _P, _P, _I, _P]),
     "rtd_knn_batched_backward": (_I, [_P, _P, _P, _P, _P, _P, _P, _P]),
 }
@@ -194,6 +197,17 @@ def check(status: int) -> None:
     if status != RTD_OK:
         msg = load().rtd_last_error().decode(errors="replace")
         raise RtdError(status, msg)
+
+
+def default_batch_schedule(**overrides) -> Schedule:
+    """rtd_batch_schedule_default with keyword overrides."""
+    s = Schedule()
+    load().rtd_batch_schedule_default(C.byref(s))
+    for k, v in overrides.items():
+        if not hasattr(s, k):
+            raise AttributeError(f"unknown schedule field {k}")
+        setattr(s, k, v)
+    return s
 
 
 def default_schedule(**overrides) -> Schedule:

@@ -135,3 +135,128 @@ def tune_knn(P, Q, k: int, tag: str, grid: dict | None = None, reps: int = 3,
                          "build_plus_search_ms": best_ms,
                          "tuned_at": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())})
     return best, stage2
+
+
+BATCH_GRID = {
+    "leaf_size": [2, 4, 8],
+    "radius_param": [0.5, 1.0, 2.0],
+    "radius_increment_mult": [2.0, 4.0],
+    "lanes_per_query": [0, 32],
+}
+
+
+def tune_batch(P, Q, sizes, tag: str, grid: dict | None = None, reps: int = 3,
+               save_result: bool = True, log=None):
+    """Times the batched pass (forest build + persistent search) for every
+    grid point; every candidate must return the first candidate's ids."""
+    import torch
+    from .batch import Batch
+    grid = grid or BATCH_GRID
+    keys = list(grid)
+    table = []
+    ref_ids = None
+    for combo in itertools.product(*(grid[k_] for k_ in keys)):
+        kw = dict(zip(keys, combo))
+        s = _capi.default_batch_schedule(**kw)
+        b = Batch(sizes, s)
+        ids = torch.empty(max(b.n_out, 1), dtype=torch.int32, device=Q.device)
+        b.knn(P, Q, out_ids=ids, with_d2=False)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        best = float("inf")
+        for _ in range(reps):
+            e0.record()
+            b.knn(P, Q, out_ids=ids, with_d2=False)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        if ref_ids is None:
+            ref_ids = ids.clone()
+        elif not bool((ids == ref_ids).all()):
+            raise RuntimeError(f"autotune: batch candidate {kw} returned different neighbours")
+        table.append((best, kw))
+        b.close()
+        if log:
+            log(f"batch {best:.4f} ms {kw}")
+    table.sort(key=lambda x: x[0])
+    best_ms, best_kw = table[0]
+    best = _capi.default_batch_schedule(**best_kw)
+    if save_result:
+        save(tag, best, {"gpu": gpu_name(), "n": int(P.shape[0]), "nq": int(Q.shape[0]),
+                         "clouds": len(sizes), "batch_ms": best_ms,
+                         "tuned_at": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())})
+    return best, table
+
+
+def tune_bh_bucket(pos, mass, tag: str, buckets=(16, 32, 64), theta: float = 0.5,
+                   eps: float = 1e-3, reps: int = 3, save_result: bool = True, log=None):
+    """Leaf bucket of the Plummer-law tree minimising build + forward +
+    adjoint time."""
+    import torch
+    from .bh import BarnesHut
+    from ._capi import BH_LAW_PLUMMER, default_bh_params
+    n = pos.shape[0]
+    ones = torch.ones((n,), device=pos.device)
+    table = []
+    for bucket in buckets:
+        p = default_bh_params(law=BH_LAW_PLUMMER, theta=theta, eps=eps, G=1.0, quadrupole=1,
+                              bucket=bucket)
+        bh = BarnesHut()
+        best = float("inf")
+        for r in range(reps + 1):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            bh.build(pos, mass, p)
+            acc, _ = bh.forward(p)
+            bh.backward(acc, ones, p)
+            e1.record()
+            e1.synchronize()
+            if r:
+                best = min(best, e0.elapsed_time(e1))
+        bh.close()
+        table.append((best, bucket))
+        if log:
+            log(f"bh bucket {bucket}: {best:.3f} ms")
+    table.sort()
+    if save_result:
+        d = _load()
+        d[tag] = {"bucket": table[0][1], "step_ms": table[0][0], "gpu": gpu_name(), "n": int(n),
+                  "tuned_at": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())}
+        tmp = WISDOM + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(d, f, indent=1, sort_keys=True)
+        os.replace(tmp, WISDOM)
+    return table[0][1], table
+
+
+def main():
+    """Tunes the three bench workloads and writes wisdom.json:
+    python -m rtdsl.autotune"""
+    import numpy as np
+    import torch
+    from . import workloads
+    log = lambda m: print(m, flush=True)   # noqa: E731
+    pts, q = workloads.clustered()
+    P = torch.from_numpy(pts).cuda()
+    Q = torch.from_numpy(q).cuda()
+    grid = {"leaf_size": [2, 4, 8], "radius_param": [0.0625, 0.25, 0.5, 1.0],
+            "radius_increment_mult": [2.0, 4.0], "block_size": [64, 128, 256],
+            "mode": ["thread", "warp"]}
+    best, table = tune_knn(P, Q, 5, "clustered_1p8m_k5", grid=grid, log=log)
+    log(f"clustered_1p8m_k5 best {table[0]}")
+    cl = workloads.clouds()
+    P = torch.from_numpy(np.concatenate([c["points"] for c in cl])).cuda()
+    Q = torch.from_numpy(np.concatenate([c["queries"] for c in cl])).cuda()
+    sizes = [(len(c["points"]), len(c["queries"]), c["k"]) for c in cl]
+    best, table = tune_batch(P, Q, sizes, "clouds_256", log=log)
+    log(f"clouds_256 best {table[0]}")
+    pos, mass = workloads.plummer(1_000_000, seed=7)
+    bucket, table = tune_bh_bucket(torch.from_numpy(pos).cuda(), torch.from_numpy(mass).cuda(),
+                                   "plummer_1m_bucket", log=log)
+    log(f"plummer_1m_bucket best {bucket}")
+
+
+if __name__ == "__main__":
+    main()

@@ -12,17 +12,17 @@ import ctypes as C
 
 import numpy as np
 
-from ._capi import Cloud, Schedule, check, default_schedule, load
+from ._capi import Cloud, Schedule, check, default_batch_schedule, load
 from .api import _check_points_tensor, _stream_handle
 
 
 class Batch:
     """A plan for clouds packed in order in one point and one query tensor.
 
-    ``sizes`` is a sequence of (n_points, n_queries, k) per cloud; the results
-    of cloud c's query j are row ``out_offset[c] + j`` of the (sum n_q, k_max)
-    output when every k is equal, else the flat output at
-    ``out_offset[c] + j * k_c``.  Ids are cloud-local point indices.
+    ``sizes`` is a sequence of (n_points, n_queries, k) per cloud; the k
+    results of cloud c's query j start at ``out_offset[c] + j * k_c`` of the
+    flat outputs (``split`` gives per-cloud (n_q, k) views).  Ids are
+    cloud-local point indices.
     """
 
     def __init__(self, sizes, schedule: Schedule | None = None):
@@ -46,7 +46,7 @@ class Batch:
             oo += nq * k
         self.sizes = sizes
         self.n_points, self.n_queries, self.n_out = po, qo, oo
-        self.schedule = schedule if schedule is not None else default_schedule()
+        self.schedule = schedule if schedule is not None else default_batch_schedule()
         check(self._lib.rtd_batch_plan(self._h, arr, n, C.byref(self.schedule)))
 
     def close(self):

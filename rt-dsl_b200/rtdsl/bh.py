@@ -74,13 +74,16 @@ class BarnesHut:
         check(self._lib.rtd_bh_forward(self._h, C.byref(p), _ptr(out), _ptr(phi), _stream(stream)))
         return out, phi
 
-    def backward(self, g_acc, g_phi=None, params: _capi.BhParams | None = None, stream=None):
+    def backward(self, g_acc, g_phi=None, params: _capi.BhParams | None = None, stream=None,
+                 out_pos=None, out_mass=None):
         import torch
         p = params if params is not None else default_bh_params(law=BH_LAW_PLUMMER)
         g_acc = g_acc.contiguous()
         g_phi = g_phi.contiguous() if g_phi is not None else None
-        g_pos = torch.empty((self.n, 3), dtype=torch.float32, device=g_acc.device)
-        g_mass = torch.empty((self.n,), dtype=torch.float32, device=g_acc.device)
+        g_pos = out_pos if out_pos is not None else torch.empty(
+            (self.n, 3), dtype=torch.float32, device=g_acc.device)
+        g_mass = out_mass if out_mass is not None else torch.empty(
+            (self.n,), dtype=torch.float32, device=g_acc.device)
         check(self._lib.rtd_bh_backward(self._h, C.byref(p), _ptr(g_acc), _ptr(g_phi),
                                         _ptr(g_pos), _ptr(g_mass), _stream(stream)))
         return g_pos, g_mass
@@ -90,6 +93,17 @@ class BarnesHut:
         check(self._lib.rtd_bh_info_get(self._h, C.byref(inf), _stream(stream)))
         return {"n_bodies": inf.n_bodies, "n_nodes": inf.n_nodes, "n_leaves": inf.n_leaves,
                 "depth": inf.depth, "root_min": list(inf.root_min), "root_max": list(inf.root_max)}
+
+    def interaction_counts(self, theta: float, stride: int = 64, stream=None) -> dict:
+        """Mean accepted cells and leaf bodies per body of the Plummer walk
+        (every stride-th body in tree order)."""
+        cells, bodies, ns = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        check(self._lib.rtd_bh_interaction_counts(self._h, C.c_float(theta), int(stride),
+                                                  C.byref(cells), C.byref(bodies), C.byref(ns),
+                                                  _stream(stream)))
+        n = max(ns.value, 1)
+        return {"cells_per_body": cells.value / n, "bodies_per_body": bodies.value / n,
+                "sampled": ns.value}
 
     def export(self, stream=None):
         """(FlatNode structured array, flat body order)."""

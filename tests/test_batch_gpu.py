@@ -143,3 +143,68 @@ def test_batched_backward(rtd, cuda):
             np.add.at(ep, pi, -w * diff)
     np.testing.assert_allclose(gq.cpu().numpy(), eq, rtol=1e-4, atol=1e-5)
     np.testing.assert_allclose(gp.cpu().numpy(), ep, rtol=1e-4, atol=1e-5)
+
+
+@pytest.mark.parametrize("lanes,param,mult", [(32, 1.0, 2.0), (0, 0.25, 4.0), (0, 4.0, 2.0)])
+def test_batched_schedules(rtd, orc, cuda, lanes, param, mult):
+    """Warp-per-query search for every k <= 32 and other radius settings give
+    the same exact result."""
+    cl = mixed_clouds(seed=8)
+    pts, q, sizes = packed(cl)
+    s = rtd.default_batch_schedule(lanes_per_query=lanes, radius_param=param,
+                                   radius_increment_mult=mult)
+    b = rtd.Batch(sizes, s)
+    ids, d2 = b.knn(torch.from_numpy(pts).cuda(), torch.from_numpy(q).cuda())
+    torch.cuda.synchronize()
+    check_against_oracle(orc, b, cl, ids, d2)
+
+
+def test_batched_backward_central_differences(rtd, cuda):
+    """The loss of the many-cloud workload, L = sum_q mean_j d2_qj with ids
+    fixed, differentiated by the batched backward, against FP64 central
+    differences (h = 1e-4) on 64 sampled query and point coordinates."""
+    cl = workloads.clouds(n_clouds=16, seed=17, lo=200, hi=4000)
+    pts, q, sizes = packed(cl)
+    b = rtd.Batch(sizes)
+    dp = torch.from_numpy(pts).cuda()
+    dq = torch.from_numpy(q).cuda()
+    ids, _ = b.knn(dp, dq)
+    g = torch.empty(b.n_out, device=cuda)
+    for c, (_, nq, k) in enumerate(sizes):
+        o = int(b.out_offset[c])
+        g[o:o + nq * k] = 1.0 / k
+    gq, gp = b.backward(dp, dq, ids, g)
+    torch.cuda.synchronize()
+    ids_h = ids.cpu().numpy().view(np.uint32)
+    # flat (query row, point row) index of every output slot
+    qrow = np.empty(b.n_out, np.int64)
+    prow = np.empty(b.n_out, np.int64)
+    wt = np.empty(b.n_out)
+    for c, (_, nq, k) in enumerate(sizes):
+        o = int(b.out_offset[c])
+        qrow[o:o + nq * k] = int(b.query_offset[c]) + np.repeat(np.arange(nq), k)
+        loc = ids_h[o:o + nq * k].astype(np.int64)
+        prow[o:o + nq * k] = int(b.point_offset[c]) + np.where(loc == 0xFFFFFFFF, 0, loc)
+        wt[o:o + nq * k] = np.where(loc == 0xFFFFFFFF, 0.0, 1.0 / k)
+
+    def loss(Q, P):
+        d = Q[qrow] - P[prow]
+        return float(np.sum(wt * np.sum(d * d, axis=1)))
+
+    Q64 = q.astype(np.float64)
+    P64 = pts.astype(np.float64)
+    rng = np.random.default_rng(0)
+    h = 1e-4
+    for which, arr, grad in (("q", Q64, gq.cpu().numpy()), ("p", P64, gp.cpu().numpy())):
+        used = np.unique(qrow if which == "q" else prow[wt > 0])
+        for _ in range(32):
+            r = int(rng.choice(used))
+            a = int(rng.integers(0, 3))
+            old = arr[r, a]
+            arr[r, a] = old + h
+            lp = loss(Q64, P64)
+            arr[r, a] = old - h
+            lm = loss(Q64, P64)
+            arr[r, a] = old
+            fd = (lp - lm) / (2 * h)
+            assert abs(grad[r, a] - fd) <= 1e-4 * max(1.0, abs(fd)), (which, r, a, grad[r, a], fd)

@@ -213,3 +213,38 @@ def test_bh_errors_and_empty(cuda):
     bh2 = BarnesHut().build(torch.rand((100, 3), device="cuda"), torch.rand(100, device="cuda"))
     with pytest.raises(RtdError):
         bh2.backward(torch.zeros((100, 3), device="cuda"), None, default_bh_params(law=0))
+
+
+def test_plummer_interaction_counts(cuda):
+    """The walk's interaction counts: at theta = 0 no cell is accepted and
+    every body meets all n bodies; at theta = 0.5 the counts equal an FP32
+    numpy walk of the exported tree with the same per-body MAC
+    (width^2 < theta^2 |COM - x|^2, each operation rounded)."""
+    pos, mass = workloads.plummer(6_000, seed=4)
+    bh, p = gpu_tree(pos, mass, law=1, theta=0.5, eps=1e-3, G=1.0, bucket=16)
+    c0 = bh.interaction_counts(0.0, stride=1)
+    assert c0["sampled"] == 6000 and c0["cells_per_body"] == 0 and c0["bodies_per_body"] == 6000
+    stride = 97
+    c = bh.interaction_counts(0.5, stride=stride)
+    nodes, order = bh.export()
+    fpos = pos[order].astype(np.float32)
+    th2 = np.float32(0.25)
+    cells = bodies = 0
+    for i in range(0, len(fpos), stride):
+        x = fpos[i]
+        q = 0
+        while q < len(nodes):
+            nd = nodes[q]
+            d = (nd["com"].astype(np.float32) - x).astype(np.float32)
+            d2 = np.float32(np.float32(np.float32(d[0] * d[0]) + np.float32(d[1] * d[1])) + np.float32(d[2] * d[2]))
+            w = np.float32(nd["width"])
+            if np.float32(w * w) < np.float32(th2 * d2):
+                cells += 1
+                q = int(nd["autorope"])
+            else:
+                if nd["is_leaf"]:
+                    bodies += int(nd["num_particles"])
+                q += 1
+    ns = (len(fpos) + stride - 1) // stride
+    assert c["sampled"] == ns
+    assert round(c["cells_per_body"] * ns) == cells and round(c["bodies_per_body"] * ns) == bodies
