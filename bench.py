@@ -43,7 +43,7 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the BH / batched sub-benchmarks")
-    ap.add_argument("--only", choices=["bh", "batch"], default=None,
+    ap.add_argument("--only", choices=["range", "bh", "batch"], default=None,
                     help="run one sub-benchmark alone (one GPU) and print its JSON")
     return ap.parse_args()
 
@@ -245,6 +245,7 @@ def run_ours(args, ws, rank, local):
 
     extras = {}
     if not args.no_extras and ws == 1:
+        extras["range"] = bench_range(args, dev, flush, P, Q, s)
         extras["barnes_hut"] = bench_bh(args, dev, flush)
         extras["batched"] = bench_batch(args, dev, flush)
 
@@ -274,6 +275,62 @@ def run_ours(args, ws, rank, local):
         line["cpu_baseline"] = cpu
     line.update(extras)
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------- range sub-bench
+def bench_range(args, dev, flush, P, Q, s) -> dict:
+    """Fixed-radius range query on the headline cloud at the radius whose
+    mean neighbour count is 50: count pass, then the push fill of exactly
+    sized (query, id) pairs (unsorted), on a built index."""
+    import torch
+    import rtdsl
+    from rtdsl.api import radius_for_mean_count
+
+    ix = rtdsl.Index().build(P, s)
+    r = radius_for_mean_count(ix, Q, 50.0, schedule=s)
+    counts = torch.empty((Q.shape[0],), dtype=torch.int32, device=dev)
+    _, total = ix.range_count(Q, r, s, out_counts=counts)
+    pairs = torch.empty((total + 1024, 2), dtype=torch.int32, device=dev)
+
+    def step():
+        _, t = ix.range_count(Q, r, s, out_counts=counts)
+        ix.range_fill(Q, r, t + 1024, False, s, out_pairs=pairs)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    ms, cnt_ms, fill_ms = [], [], []
+    ix.profile(True)
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = _events()
+        e0.record()
+        _, t = ix.range_count(Q, r, s, out_counts=counts)
+        cnt_ms.append(ix.timings()["search_ms"])
+        ix.range_fill(Q, r, t + 1024, False, s, out_pairs=pairs)
+        fill_ms.append(ix.timings()["search_ms"])
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    m = statistics.mean(ms)
+    mc, mf = statistics.mean(cnt_ms), statistics.mean(fill_ms)
+    nq = Q.shape[0]
+    fill_bytes = nq * 12 + total * 8 + P.shape[0] * 12
+    peak = measured_peaks()
+    return {
+        "metric": "range query pairs/s (count + fill)", "value": total / (m / 1e3),
+        "unit": "pairs/s",
+        "config": {"workload": "clustered_1p8m_r50: the headline cloud, radius for a mean of 50 "
+                               "neighbours per query, unsorted (query, id) u32 pairs",
+                   "radius": r, "pairs": int(total)},
+        "ms": {"count_kernel": mc, "fill_kernel": mf, "step": m},
+        "queries_per_s": nq / (m / 1e3),
+        "roofline": {"kernel": "range_kernel<true> (fill)", "bound": "hbm",
+                     "achieved": fill_bytes / (mf / 1e3) / 1e9, "peak": peak["hbm_gbs"],
+                     "unit": "GB/s", "frac": fill_bytes / (mf / 1e3) / 1e9 / peak["hbm_gbs"],
+                     "algorithmic_bytes_per_launch": fill_bytes,
+                     "traffic": traffic_for("range_fill", "clustered_1p8m_r50")},
+    }
 
 
 # ----------------------------------------------------- Barnes-Hut sub-bench
@@ -518,7 +575,15 @@ def main():
         dev = torch.device("cuda", local)
         torch.cuda.set_device(dev)
         flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
-        out = bench_bh(args, dev, flush) if args.only == "bh" else bench_batch(args, dev, flush)
+        if args.only == "range":
+            import rtdsl
+            pts, q = load_workload()
+            out = bench_range(args, dev, flush, torch.from_numpy(pts).to(dev),
+                              torch.from_numpy(q).to(dev), tuned_schedule(rtdsl))
+        elif args.only == "bh":
+            out = bench_bh(args, dev, flush)
+        else:
+            out = bench_batch(args, dev, flush)
         print(json.dumps(out), flush=True)
     else:
         run_ours(args, ws, rank, local)

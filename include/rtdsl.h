@@ -78,7 +78,16 @@ typedef struct rtd_schedule {
     uint32_t morton_bits;         /* 30 (u32 keys) or 63 (u64 keys); 0 = auto */
     uint32_t packet_traversal;    /* thread-per-query kernels: 32 Morton-adjacent queries
                                      share one traversal (rtd_packet_mode) */
+    uint32_t lane_refill;         /* thread-per-query kernels: persistent warps whose lanes
+                                     take the next query as soon as theirs ends
+                                     (rtd_refill_mode) */
 } rtd_schedule;
+
+typedef enum rtd_refill_mode {
+    RTD_REFILL_AUTO = 0,   /* currently: off (measured 2x slower on clustered data) */
+    RTD_REFILL_ON = 1,
+    RTD_REFILL_OFF = 2     /* one query per thread, the warp ends with its slowest lane */
+} rtd_refill_mode;
 
 typedef enum rtd_packet_mode {
     RTD_PACKET_AUTO = 0,   /* currently: off (per-thread traversal measured faster) */

@@ -121,6 +121,7 @@ void rtd_schedule_default(rtd_schedule *s) {
     s->lanes_per_query = 0;
     s->morton_bits = 0;
     s->packet_traversal = RTD_PACKET_AUTO;
+    s->lane_refill = RTD_REFILL_AUTO;
 }
 
 const char *rtd_status_string(rtd_status s) {

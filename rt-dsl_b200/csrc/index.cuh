@@ -42,6 +42,7 @@ struct IndexHeader {
     uint64_t total;       // last range-count total
     float nn95_key;       // p95 of the squared 1-NN distance within a 4096-point sample
     uint32_t n_sample;    // points in the radius-seed sample (<= 1000)
+    unsigned long long qcounter;   // work counter of the refilling search kernels
 };
 
 constexpr int SEED_NN_SAMPLE = 4096;

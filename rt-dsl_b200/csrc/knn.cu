@@ -57,6 +57,191 @@ __global__ void __launch_bounds__(BLOCK) knn_thread_kernel(const KnnArgs p) {
     }
 }
 
+// One thread per query with lane refill: persistent warps whose lanes take
+// the next query as soon as their own one finishes, so a warp does not idle
+// until its slowest query ends.  A warp takes chunks of REFILL_CHUNK
+// consecutive (Morton-ordered) queries from a global counter and hands them
+// to its idle lanes; every lane runs the same per-query algorithm as
+// knn_query_thread, one node per loop trip.
+constexpr uint32_t REFILL_CHUNK = 64;
+
+template <int KC, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) knn_refill_kernel(const KnnArgs p,
+                                                           unsigned long long *counter) {
+    __shared__ BvhNode s_top[TOP_MAX];
+    __shared__ uint2 s_stack[SHORT_STACK][BLOCK];
+    const IndexHeader *h = p.ix.hdr;
+    const uint32_t ntop = h->n_top;
+    for (uint32_t i = threadIdx.x; i < ntop; i += BLOCK) s_top[i] = p.ix.top[i];
+    __syncthreads();
+    const uint32_t root = h->root, root_count = h->root_count;
+    const uint32_t visit_cap = 2u * h->n_internal + 4u;
+    float r0sq = h->r0sq;
+    if (!(r0sq > 0.0f)) r0sq = 1e-30f;
+    const int kk = (int)p.k;
+    const int lane = threadIdx.x & 31;
+    uint32_t lt;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+    uint2 *s_col = &s_stack[0][threadIdx.x];
+    uint2 l_stack[STACK_MAX - SHORT_STACK];
+
+    unsigned long long c_next = 0, c_end = 0;   // the warp's chunk (warp-uniform)
+    bool exhausted = false;                      // warp-uniform
+    bool active = false;
+    uint64_t qi = 0;
+    float qx = 0.f, qy = 0.f, qz = 0.f;
+    float bk[KC];
+    uint32_t bi[KC];
+    float bound = 0.f, prev = -1.f, lim = 0.f;
+    uint32_t node = 0, visits = 0, round = 0;
+    int sp = 0;
+    bool last = false;
+
+    while (true) {
+        // hand queries of the warp's chunk to idle lanes
+        uint32_t idle = __ballot_sync(0xffffffffu, !active);
+        while (idle && !exhausted) {
+            if (c_next == c_end) {
+                unsigned long long base = 0;
+                if (lane == 0) base = atomicAdd(counter, (unsigned long long)REFILL_CHUNK);
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (base >= p.nq) {
+                    exhausted = true;
+                    break;
+                }
+                c_next = base;
+                c_end = base + REFILL_CHUNK < p.nq ? base + REFILL_CHUNK : p.nq;
+            }
+            const uint32_t avail = (uint32_t)(c_end - c_next);
+            const uint32_t rank = __popc(idle & lt);
+            const bool mine = !active && rank < avail;
+            if (mine) {
+                const uint64_t t = c_next + rank;
+                qi = p.perm ? p.perm[t] : t;
+                qx = p.q[3 * qi];
+                qy = p.q[3 * qi + 1];
+                qz = p.q[3 * qi + 2];
+#pragma unroll
+                for (int j = 0; j < KC; ++j) {
+                    const bool pad = j < KC - kk;
+                    bk[j] = pad ? -INFINITY : INFINITY;
+                    bi[j] = pad ? 0u : EMPTY_ID;
+                }
+                bound = r0sq;
+                prev = -1.0f;
+                round = 0;
+                last = 1u >= p.max_rounds || !(bound < INFINITY);
+                if (last) bound = INFINITY;
+                lim = fminf(bound, bk[KC - 1]);
+                node = root;
+                sp = 0;
+                visits = 0;
+                active = true;
+            }
+            const uint32_t took = min(avail, (uint32_t)__popc(idle));
+            c_next += took;
+            idle = __ballot_sync(0xffffffffu, !active);
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (!active) continue;
+
+        // one node of this lane's traversal
+        bool done = false;
+        if (root == CHILD_NONE || isnan(qx) || isnan(qy) || isnan(qz)) {
+            done = true;
+        } else if (++visits > visit_cap) {
+            atomicOr(p.err, DEVERR_STACK);
+            done = true;
+        } else {
+            uint32_t lf_first[2], lf_cnt[2];
+            int nleaf = 0;
+            uint32_t next = CHILD_NONE;
+            float k0 = 0.f, k1 = 0.f;
+            bool v0 = false, v1 = false;
+            uint4 d = make_uint4(0, 0, 0, 0);
+            if (node & CHILD_LEAF) {
+                lf_first[0] = node & CHILD_INDEX;
+                lf_cnt[0] = root_count;
+                nleaf = 1;
+            } else {
+                float4 a, b, c;
+                load_node(s_top, p.ix.nodes, node, a, b, c, d);
+                k0 = box_min_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y);
+                k1 = box_min_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w);
+                v0 = !(k0 > lim);
+                v1 = !(k1 > lim);
+                if (prev >= 0.0f) {
+                    if (v0) v0 = !(box_max_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y) <= prev);
+                    if (v1) v1 = !(box_max_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w) <= prev);
+                }
+                if (v0 && (d.x & CHILD_LEAF)) { lf_first[nleaf] = d.x & CHILD_INDEX; lf_cnt[nleaf] = d.z; ++nleaf; v0 = false; }
+                if (v1 && (d.y & CHILD_LEAF)) { lf_first[nleaf] = d.y & CHILD_INDEX; lf_cnt[nleaf] = d.w; ++nleaf; v1 = false; }
+            }
+            for (int l = 0; l < nleaf; ++l) {
+                for (uint32_t j = 0; j < lf_cnt[l]; ++j) {
+                    const float4 pt = __ldg(&p.ix.pts[lf_first[l] + j]);
+                    const float key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
+                    const uint32_t id = __float_as_uint(pt.w);
+                    if (key <= bound && key > prev && key_less(key, id, bk[KC - 1], bi[KC - 1]))
+                        list_insert<KC>(bk, bi, key, id);
+                }
+            }
+            if (nleaf) lim = fminf(bound, bk[KC - 1]);
+            if (!(node & CHILD_LEAF)) {
+                v0 = v0 && !(k0 > lim);
+                v1 = v1 && !(k1 > lim);
+                if (v0 && v1) {
+                    const bool near0 = k0 <= k1;
+                    const uint2 far = near0 ? make_uint2(d.y, __float_as_uint(k1))
+                                            : make_uint2(d.x, __float_as_uint(k0));
+                    next = near0 ? d.x : d.y;
+                    if (sp < SHORT_STACK) s_col[sp * BLOCK] = far;
+                    else if (sp < STACK_MAX) l_stack[sp - SHORT_STACK] = far;
+                    else atomicOr(p.err, DEVERR_STACK);
+                    if (sp < STACK_MAX) ++sp;
+                } else if (v0) {
+                    next = d.x;
+                } else if (v1) {
+                    next = d.y;
+                }
+            }
+            if (next == CHILD_NONE) {
+                while (sp > 0) {
+                    --sp;
+                    const uint2 e = sp < SHORT_STACK ? s_col[sp * BLOCK] : l_stack[sp - SHORT_STACK];
+                    if (!(__uint_as_float(e.y) > lim)) { next = e.x; break; }
+                }
+            }
+            if (next != CHILD_NONE) {
+                node = next;
+            } else if (bi[KC - 1] != EMPTY_ID || last) {
+                done = true;
+            } else {   // next round: grow the radius, restart at the root
+                prev = bound;
+                bound = __fmul_rn(bound, p.mult2);
+                ++round;
+                last = round + 1 >= p.max_rounds || !(bound < INFINITY);
+                if (last) bound = INFINITY;
+                lim = fminf(bound, bk[KC - 1]);
+                node = root;
+                sp = 0;
+                visits = 0;
+            }
+        }
+        if (done) {
+            const uint64_t ob = qi * (uint64_t)kk;
+#pragma unroll
+            for (int j = 0; j < KC; ++j) {
+                if (j >= KC - kk) {
+                    p.ids[ob + j - (KC - kk)] = bi[j];
+                    if (p.d2) p.d2[ob + j - (KC - kk)] = bk[j];
+                }
+            }
+            active = false;
+        }
+    }
+}
+
 // Packet traversal: a warp walks the tree once for 32 consecutive
 // (Morton-ordered) queries.  A child is visited when any lane's query wants
 // it; node loads are warp-uniform (broadcast) and the node stack is shared,
@@ -330,6 +515,31 @@ rtd_status launch_thread(const KnnArgs &a, uint32_t block, cudaStream_t st) {
     return RTD_OK;
 }
 
+template <int KC, int BLOCK>
+rtd_status launch_refill_b(const KnnArgs &a, unsigned long long *counter, cudaStream_t st) {
+    int dev = 0, sms = 148, per_sm = 1;
+    RTD_CUDA(cudaGetDevice(&dev));
+    RTD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    RTD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, knn_refill_kernel<KC, BLOCK>,
+                                                           BLOCK, 0));
+    if (per_sm < 1) per_sm = 1;
+    uint64_t blocks = (uint64_t)sms * (uint64_t)per_sm;
+    const uint64_t need = (a.nq + BLOCK - 1) / BLOCK;
+    if (blocks > need) blocks = need;
+    RTD_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
+    knn_refill_kernel<KC, BLOCK><<<(unsigned)blocks, BLOCK, 0, st>>>(a, counter);
+    RTD_LAUNCH_CHECK();
+    return RTD_OK;
+}
+
+template <int KC>
+rtd_status launch_refill(const KnnArgs &a, uint32_t block, unsigned long long *counter,
+                         cudaStream_t st) {
+    if (block == 256) return launch_refill_b<KC, 256>(a, counter, st);
+    if (block == 64) return launch_refill_b<KC, 64>(a, counter, st);
+    return launch_refill_b<KC, 128>(a, counter, st);
+}
+
 template <int KC>
 rtd_status launch_packet(const KnnArgs &a, uint32_t block, cudaStream_t st) {
     const uint64_t warps = (a.nq + 31) / 32;
@@ -429,6 +639,18 @@ rtd_status knn_search(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k,
         else if (k <= 8) r = launch_packet<8>(a, block, st);
         else if (k <= 16) r = launch_packet<16>(a, block, st);
         else r = launch_packet<32>(a, block, st);
+    } else if (lanes == 1 && s.lane_refill == RTD_REFILL_ON) {
+        // Lane refill measured 2x slower than one query per thread on the
+        // clustered workload (lanes of a warp drift apart in the tree), so
+        // AUTO means off.
+        unsigned long long *ctr = &idx->hdr.as<IndexHeader>()->qcounter;
+        if (k <= 1) r = launch_refill<1>(a, block, ctr, st);
+        else if (k <= 2) r = launch_refill<2>(a, block, ctr, st);
+        else if (k <= 4) r = launch_refill<4>(a, block, ctr, st);
+        else if (k == 5) r = launch_refill<5>(a, block, ctr, st);
+        else if (k <= 8) r = launch_refill<8>(a, block, ctr, st);
+        else if (k <= 16) r = launch_refill<16>(a, block, ctr, st);
+        else r = launch_refill<32>(a, block, ctr, st);
     } else if (lanes == 1) {
         if (k <= 1) r = launch_thread<1>(a, block, st);
         else if (k <= 2) r = launch_thread<2>(a, block, st);

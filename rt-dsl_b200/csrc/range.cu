@@ -17,7 +17,7 @@ constexpr int RBLOCK = 128;
 constexpr int RWARPS = RBLOCK / 32;
 constexpr int SHORT_DEPTH = 16;  // stack entries per thread in shared memory
 constexpr int STACK_DEPTH = 104; // >= maximal tree depth
-constexpr int WBUF = 1024;       // staged pairs per warp (8 KB)
+constexpr int WBUF = 256;        // staged pairs per warp (2 KB)
 
 struct RangeArgs {
     IndexView ix;
@@ -52,26 +52,47 @@ struct Walk {
 
 // FILL = false: count hits per query.  FILL = true: push pairs.
 // Threads of a warp advance their own traversals one node per iteration of
-// a warp-converged loop; after each iteration the warp flushes its staging
-// buffer when it might not hold another iteration's hits.
+// a warp-converged loop.  The (up to two) leaves a lane reaches in an
+// iteration are tested in a warp-uniform loop over candidate slots, so each
+// slot's hits are compacted with one ballot: a warp-private staging buffer
+// in shared memory takes them at consecutive positions, and the warp pushes
+// the buffer to the output with one global atomic per flush.
 template <bool FILL>
-__global__ void __launch_bounds__(RBLOCK) range_kernel(const RangeArgs p) {
+__global__ void __launch_bounds__(RBLOCK, FILL ? 8 : 12) range_kernel(const RangeArgs p) {
     __shared__ BvhNode s_top[TOP_MAX];
     __shared__ uint32_t s_stack[SHORT_DEPTH][RBLOCK];
     __shared__ uint2 s_buf[FILL ? RWARPS : 1][FILL ? WBUF : 1];
-    __shared__ uint32_t s_cnt[RWARPS];
     const IndexHeader *h = p.ix.hdr;
     const uint32_t ntop = h->n_top;
     for (uint32_t i = threadIdx.x; i < ntop; i += RBLOCK) s_top[i] = p.ix.top[i];
-    if (threadIdx.x < RWARPS) s_cnt[threadIdx.x] = 0;
     __syncthreads();
     const uint32_t root = h->root, root_count = h->root_count;
     const float4 *__restrict__ pts = p.ix.pts;
     const BvhNode *__restrict__ gn = p.ix.nodes;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t lt;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
     const float r2 = p.r2;
     const uint32_t visit_cap = 2u * h->n_internal + 4u;
     uint32_t l_stack[STACK_DEPTH - SHORT_DEPTH];
+    uint2 *buf = s_buf[FILL ? warp : 0];
+    uint32_t fill = 0;   // staged pairs of this warp (warp-uniform)
+
+    // pushes the staged pairs with one reservation on the global cursor
+    auto flush = [&]() {
+        if (!FILL || fill == 0) return;
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(p.cursor, (unsigned long long)fill);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        __syncwarp();
+        for (uint32_t j = lane; j < fill; j += 32) {
+            const uint64_t dst = base + j;
+            if (dst < p.capacity) p.pairs[dst] = buf[j];
+        }
+        if (lane == 0 && base + fill > p.capacity) atomicOr(p.err, DEVERR_OVERFLOW);
+        __syncwarp();
+        fill = 0;
+    };
 
     const uint64_t stride = (uint64_t)gridDim.x * RBLOCK;
     const uint64_t t0 = (uint64_t)blockIdx.x * RBLOCK + warp * 32;
@@ -95,22 +116,24 @@ __global__ void __launch_bounds__(RBLOCK) range_kernel(const RangeArgs p) {
                 node = CHILD_NONE;
                 sp = 0;
             }
+            uint32_t f0 = 0, c0 = 0, f1 = 0, c1 = 0;   // this iteration's leaves
             if (node != CHILD_NONE) {
-                uint32_t lf_first[2], lf_cnt[2];
-                int nleaf = 0;
                 uint32_t next = CHILD_NONE;
                 if (node & CHILD_LEAF) {
-                    lf_first[0] = node & CHILD_INDEX;
-                    lf_cnt[0] = root_count;
-                    nleaf = 1;
+                    f0 = node & CHILD_INDEX;
+                    c0 = root_count;
                 } else {
                     float4 a, b, c;
                     uint4 d;
                     load_node_r(s_top, gn, node, a, b, c, d);
                     bool v0 = !(box_min_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y) > r2);
                     bool v1 = !(box_min_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w) > r2);
-                    if (v0 && (d.x & CHILD_LEAF)) { lf_first[nleaf] = d.x & CHILD_INDEX; lf_cnt[nleaf] = d.z; ++nleaf; v0 = false; }
-                    if (v1 && (d.y & CHILD_LEAF)) { lf_first[nleaf] = d.y & CHILD_INDEX; lf_cnt[nleaf] = d.w; ++nleaf; v1 = false; }
+                    if (v0 && (d.x & CHILD_LEAF)) { f0 = d.x & CHILD_INDEX; c0 = d.z; v0 = false; }
+                    if (v1 && (d.y & CHILD_LEAF)) {
+                        if (c0) { f1 = d.y & CHILD_INDEX; c1 = d.w; }
+                        else { f0 = d.y & CHILD_INDEX; c0 = d.w; }
+                        v1 = false;
+                    }
                     if (v0 && v1) {
                         next = d.x;
                         if (sp < SHORT_DEPTH) s_stack[sp++][threadIdx.x] = d.y;
@@ -122,52 +145,37 @@ __global__ void __launch_bounds__(RBLOCK) range_kernel(const RangeArgs p) {
                         next = d.y;
                     }
                 }
-                for (int l = 0; l < nleaf; ++l)
-                    for (uint32_t j = 0; j < lf_cnt[l]; ++j) {
-                        float4 pt = __ldg(&pts[lf_first[l] + j]);
-                        float key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
-                        if (key <= r2) {
-                            ++cnt;
-                            if (FILL) {
-                                uint2 pr = make_uint2((uint32_t)qi, __float_as_uint(pt.w));
-                                uint32_t slot = atomicAdd(&s_cnt[warp], 1u);
-                                if (slot < WBUF) {
-                                    s_buf[FILL ? warp : 0][FILL ? slot : 0] = pr;
-                                } else {   // staging full: push this pair alone
-                                    unsigned long long dst = atomicAdd(p.cursor, 1ull);
-                                    if (dst < p.capacity) p.pairs[dst] = pr;
-                                    else atomicOr(p.err, DEVERR_OVERFLOW);
-                                }
-                            }
-                        }
-                    }
                 if (next == CHILD_NONE && sp > 0) {
                     --sp;
                     next = sp < SHORT_DEPTH ? s_stack[sp][threadIdx.x] : l_stack[sp - SHORT_DEPTH];
                 }
                 node = next;
             }
-            if (FILL) {
-                __syncwarp();
-                uint32_t c = s_cnt[warp];
-                c = c < WBUF ? c : WBUF;
-                if (c >= WBUF / 2 || !__any_sync(0xffffffffu, node != CHILD_NONE)) {
-                    unsigned long long base = 0;
-                    if (lane == 0 && c) base = atomicAdd(p.cursor, (unsigned long long)c);
-                    base = __shfl_sync(0xffffffffu, base, 0);
-                    for (uint32_t j = lane; j < c; j += 32) {
-                        uint64_t dst = base + j;
-                        if (dst < p.capacity) p.pairs[dst] = s_buf[FILL ? warp : 0][FILL ? j : 0];
+            // candidate slots of both leaves, tested warp-uniformly
+            const uint32_t tot = c0 + c1;
+            const uint32_t maxt = __reduce_max_sync(0xffffffffu, tot);
+            for (uint32_t j = 0; j < maxt; ++j) {
+                bool hit = false;
+                uint32_t id = 0;
+                if (j < tot) {
+                    const float4 pt = __ldg(&pts[j < c0 ? f0 + j : f1 + (j - c0)]);
+                    hit = exact_key(qx, qy, qz, pt.x, pt.y, pt.z) <= r2;
+                    id = __float_as_uint(pt.w);
+                }
+                cnt += hit;
+                if (FILL) {
+                    const uint32_t m = __ballot_sync(0xffffffffu, hit);
+                    if (m) {
+                        if (hit) buf[fill + __popc(m & lt)] = make_uint2((uint32_t)qi, id);
+                        fill += __popc(m);
+                        if (fill > WBUF - 32) flush();
                     }
-                    if (lane == 0 && base + c > p.capacity) atomicOr(p.err, DEVERR_OVERFLOW);
-                    __syncwarp();
-                    if (lane == 0) s_cnt[warp] = 0;
-                    __syncwarp();
                 }
             }
         }
         if (!FILL && have) p.counts[qi] = cnt;
     }
+    flush();
 }
 
 __global__ void pairs_from_keys_kernel(const uint64_t *__restrict__ keys, uint64_t n,

@@ -49,7 +49,7 @@ class Schedule(C.Structure):
         ("block_size", C.c_uint32),
         ("lanes_per_query", C.c_uint32),
         ("morton_bits", C.c_uint32),
-        ("packet_traversal", C.c_uint32),
+        ("packet_traversal", C.c_uint32), ("lane_refill", C.c_uint32),
     ]
 
     def as_dict(self) -> dict:

@@ -33,7 +33,8 @@ DEFAULT_GRID = {
     "mode": ["thread", "packet", "warp"],
 }
 
-_MODES = {"thread": dict(lanes_per_query=1, packet_traversal=2),
+_MODES = {"thread": dict(lanes_per_query=1, packet_traversal=2, lane_refill=2),
+          "refill": dict(lanes_per_query=1, packet_traversal=2, lane_refill=1),
           "packet": dict(lanes_per_query=1, packet_traversal=1),
           "warp": dict(lanes_per_query=32, packet_traversal=2)}
 

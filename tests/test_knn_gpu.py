@@ -42,11 +42,12 @@ def test_plain_knn_small_config(rtd, orc, cuda):
 
 
 @pytest.mark.parametrize("k", [1, 2, 5, 8, 16, 32])
-@pytest.mark.parametrize("mode", ["packet", "thread", "warp"])
+@pytest.mark.parametrize("mode", ["packet", "thread", "refill", "warp"])
 def test_knn_k_and_traversal(rtd, orc, cuda, k, mode):
     pts, q = clustered_small()
     kw = {"packet": dict(lanes_per_query=1, packet_traversal=1),
-          "thread": dict(lanes_per_query=1, packet_traversal=2),
+          "thread": dict(lanes_per_query=1, packet_traversal=2, lane_refill=2),
+          "refill": dict(lanes_per_query=1, packet_traversal=2, lane_refill=1),
           "warp": dict(lanes_per_query=32)}[mode]
     ids, d2, _ = gpu_knn(rtd, pts, q, k, **kw)
     oi, od = orc.knn(pts, q, k)
