@@ -3,7 +3,9 @@
 // Points are stored Morton-sorted as float4 (x, y, z, bits of the original
 // id): one 128-bit load per candidate.  Internal nodes hold the boxes of
 // their two children (64 B, four 128-bit loads).  A child word is either an
-// internal-node index or a leaf (first sorted point, count stored beside it).
+// internal-node index or a leaf (first sorted point); the number of points
+// below each child is stored beside the words, so a traversal that carries
+// a node's first point knows every subtree's contiguous point range.
 // The top levels of the tree are copied into a small array that search
 // kernels stage in shared memory; child words that point into it carry
 // CHILD_TOP.
@@ -26,7 +28,7 @@ struct __align__(16) BvhNode {
     float4 a;  // lo.x[0] lo.y[0] lo.z[0] hi.x[0]
     float4 b;  // hi.y[0] hi.z[0] lo.x[1] lo.y[1]
     float4 c;  // lo.z[1] hi.x[1] hi.y[1] hi.z[1]
-    uint4 d;   // child[0] child[1] count[0] count[1]
+    uint4 d;   // child[0] child[1] count[0] count[1] (points below each child)
 };
 static_assert(sizeof(BvhNode) == 64, "node is one half cache line");
 

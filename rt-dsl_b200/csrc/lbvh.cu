@@ -155,7 +155,10 @@ __global__ void __launch_bounds__(BLOCK) karras_kernel(const K *__restrict__ key
 }
 
 // Compact nodes: children become leaves when their subtree has <= leaf_size
-// points.  Boxes are filled by the refit kernel.
+// points.  Every child carries the number of points below it (a subtree's
+// points are contiguous in sorted order, starting at the parent's first
+// point for the left child and after the left child's points for the
+// right one).  Boxes are filled by the refit kernel.
 __global__ void __launch_bounds__(BLOCK) compact_kernel(
     int64_t n, const uint32_t *__restrict__ kleft, const uint32_t *__restrict__ kright,
     const uint32_t *__restrict__ kfirst, const uint32_t *__restrict__ klast,
@@ -174,11 +177,11 @@ __global__ void __launch_bounds__(BLOCK) compact_kernel(
                 cnt[s] = 1;
             } else if (flags[w]) {
                 word[s] = cidx[w];
+                cnt[s] = klast[w] - kfirst[w] + 1;
             } else {
                 word[s] = CHILD_LEAF | kfirst[w];
                 cnt[s] = klast[w] - kfirst[w] + 1;
             }
-            if (!(word[s] & CHILD_LEAF)) cnt[s] = 0;
         }
         BvhNode nd;
         nd.a = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -206,12 +209,20 @@ __device__ __forceinline__ Box leaf_box(const float4 *__restrict__ pts, uint32_t
                                         uint32_t count) {
     Box b;
     for (int a = 0; a < 3; ++a) { b.lo[a] = INFINITY; b.hi[a] = -INFINITY; }
+    bool nan = false;
     for (uint32_t j = 0; j < count; ++j) {
         float4 p = pts[first + j];
         b.lo[0] = fminf(b.lo[0], p.x); b.hi[0] = fmaxf(b.hi[0], p.x);
         b.lo[1] = fminf(b.lo[1], p.y); b.hi[1] = fmaxf(b.hi[1], p.y);
         b.lo[2] = fminf(b.lo[2], p.z); b.hi[2] = fmaxf(b.hi[2], p.z);
+        nan |= isnan(p.x) || isnan(p.y) || isnan(p.z);
     }
+    // A point with a NaN coordinate is never a neighbour, but no finite box
+    // holds it: the leaf (and, through the unions, every ancestor) gets an
+    // unbounded box, so no search treats such a subtree as lying wholly
+    // inside a ball.
+    if (nan)
+        for (int a = 0; a < 3; ++a) { b.lo[a] = -INFINITY; b.hi[a] = INFINITY; }
     return b;
 }
 

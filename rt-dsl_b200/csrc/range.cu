@@ -52,15 +52,18 @@ struct Walk {
 
 // FILL = false: count hits per query.  FILL = true: push pairs.
 // Threads of a warp advance their own traversals one node per iteration of
-// a warp-converged loop.  The (up to two) leaves a lane reaches in an
-// iteration are tested in a warp-uniform loop over candidate slots, so each
-// slot's hits are compacted with one ballot: a warp-private staging buffer
-// in shared memory takes them at consecutive positions, and the warp pushes
-// the buffer to the output with one global atomic per flush.
+// a warp-converged loop; a stack entry carries the node and the first
+// sorted point below it.  A child whose whole box lies inside the ball
+// (farthest-corner key <= r^2, a bound on every point's key) contributes
+// all its points without a test: its count in the count pass, a
+// warp-cooperative copy of its contiguous ids in the fill pass.  Leaves
+// that straddle the sphere are tested in a warp-uniform loop over candidate
+// slots, and each slot's hits are compacted with one ballot into the warp's
+// staging buffer, which the warp pushes with one global atomic per flush.
 template <bool FILL>
 __global__ void __launch_bounds__(RBLOCK, FILL ? 8 : 12) range_kernel(const RangeArgs p) {
     __shared__ BvhNode s_top[TOP_MAX];
-    __shared__ uint32_t s_stack[SHORT_DEPTH][RBLOCK];
+    __shared__ uint2 s_stack[SHORT_DEPTH][RBLOCK];
     __shared__ uint2 s_buf[FILL ? RWARPS : 1][FILL ? WBUF : 1];
     const IndexHeader *h = p.ix.hdr;
     const uint32_t ntop = h->n_top;
@@ -74,7 +77,7 @@ __global__ void __launch_bounds__(RBLOCK, FILL ? 8 : 12) range_kernel(const Rang
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
     const float r2 = p.r2;
     const uint32_t visit_cap = 2u * h->n_internal + 4u;
-    uint32_t l_stack[STACK_DEPTH - SHORT_DEPTH];
+    uint2 l_stack[STACK_DEPTH - SHORT_DEPTH];
     uint2 *buf = s_buf[FILL ? warp : 0];
     uint32_t fill = 0;   // staged pairs of this warp (warp-uniform)
 
@@ -106,7 +109,10 @@ __global__ void __launch_bounds__(RBLOCK, FILL ? 8 : 12) range_kernel(const Rang
             qi = p.perm ? p.perm[t] : t;
             qx = p.q[3 * qi]; qy = p.q[3 * qi + 1]; qz = p.q[3 * qi + 2];
         }
-        uint32_t node = (have && root != CHILD_NONE) ? root : CHILD_NONE;
+        // a query with a NaN coordinate has no neighbours (its keys are NaN)
+        const bool live = have && !isnan(qx) && !isnan(qy) && !isnan(qz);
+        uint32_t node = (live && root != CHILD_NONE) ? root : CHILD_NONE;
+        uint32_t first = 0;   // first sorted point below `node`
         int sp = 0;
         uint32_t cnt = 0;
         uint32_t visits = 0;
@@ -116,9 +122,10 @@ __global__ void __launch_bounds__(RBLOCK, FILL ? 8 : 12) range_kernel(const Rang
                 node = CHILD_NONE;
                 sp = 0;
             }
-            uint32_t f0 = 0, c0 = 0, f1 = 0, c1 = 0;   // this iteration's leaves
+            uint32_t f0 = 0, c0 = 0, f1 = 0, c1 = 0;   // leaves to test
+            uint32_t g0 = 0, n0 = 0, g1 = 0, n1 = 0;   // subtrees inside the ball
             if (node != CHILD_NONE) {
-                uint32_t next = CHILD_NONE;
+                uint32_t next = CHILD_NONE, next_first = 0;
                 if (node & CHILD_LEAF) {
                     f0 = node & CHILD_INDEX;
                     c0 = root_count;
@@ -126,32 +133,66 @@ __global__ void __launch_bounds__(RBLOCK, FILL ? 8 : 12) range_kernel(const Rang
                     float4 a, b, c;
                     uint4 d;
                     load_node_r(s_top, gn, node, a, b, c, d);
+                    const uint32_t fl = first, fr = first + d.z;
                     bool v0 = !(box_min_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y) > r2);
                     bool v1 = !(box_min_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w) > r2);
-                    if (v0 && (d.x & CHILD_LEAF)) { f0 = d.x & CHILD_INDEX; c0 = d.z; v0 = false; }
+                    if (v0 && !(box_max_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y) > r2)) {
+                        g0 = fl; n0 = d.z; v0 = false;
+                    }
+                    if (v1 && !(box_max_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w) > r2)) {
+                        g1 = fr; n1 = d.w; v1 = false;
+                    }
+                    if (v0 && (d.x & CHILD_LEAF)) { f0 = fl; c0 = d.z; v0 = false; }
                     if (v1 && (d.y & CHILD_LEAF)) {
-                        if (c0) { f1 = d.y & CHILD_INDEX; c1 = d.w; }
-                        else { f0 = d.y & CHILD_INDEX; c0 = d.w; }
+                        if (c0) { f1 = fr; c1 = d.w; }
+                        else { f0 = fr; c0 = d.w; }
                         v1 = false;
                     }
                     if (v0 && v1) {
                         next = d.x;
-                        if (sp < SHORT_DEPTH) s_stack[sp++][threadIdx.x] = d.y;
-                        else if (sp < STACK_DEPTH) { l_stack[sp - SHORT_DEPTH] = d.y; ++sp; }
+                        next_first = fl;
+                        const uint2 e = make_uint2(d.y, fr);
+                        if (sp < SHORT_DEPTH) s_stack[sp++][threadIdx.x] = e;
+                        else if (sp < STACK_DEPTH) { l_stack[sp - SHORT_DEPTH] = e; ++sp; }
                         else atomicOr(p.err, DEVERR_STACK);
                     } else if (v0) {
                         next = d.x;
+                        next_first = fl;
                     } else if (v1) {
                         next = d.y;
+                        next_first = fr;
                     }
                 }
                 if (next == CHILD_NONE && sp > 0) {
                     --sp;
-                    next = sp < SHORT_DEPTH ? s_stack[sp][threadIdx.x] : l_stack[sp - SHORT_DEPTH];
+                    const uint2 e = sp < SHORT_DEPTH ? s_stack[sp][threadIdx.x] : l_stack[sp - SHORT_DEPTH];
+                    next = e.x;
+                    next_first = e.y;
                 }
                 node = next;
+                first = next_first;
             }
-            // candidate slots of both leaves, tested warp-uniformly
+            cnt += n0 + n1;
+            if (FILL) {   // contained subtrees: the warp copies each lane's ranges
+                uint32_t m = __ballot_sync(0xffffffffu, (n0 | n1) != 0);
+                while (m) {
+                    const int src = __ffs(m) - 1;
+                    m &= m - 1;
+                    const uint32_t sq = (uint32_t)__shfl_sync(0xffffffffu, (uint32_t)qi, src);
+                    for (int r = 0; r < 2; ++r) {
+                        const uint32_t gs = __shfl_sync(0xffffffffu, r ? g1 : g0, src);
+                        const uint32_t ns = __shfl_sync(0xffffffffu, r ? n1 : n0, src);
+                        for (uint32_t base = 0; base < ns; base += 32) {
+                            const uint32_t take = ns - base < 32u ? ns - base : 32u;
+                            if ((uint32_t)lane < take)
+                                buf[fill + lane] = make_uint2(sq, __float_as_uint(__ldg(&pts[gs + base + lane].w)));
+                            fill += take;
+                            if (fill > WBUF - 32) flush();
+                        }
+                    }
+                }
+            }
+            // straddling leaves, tested warp-uniformly
             const uint32_t tot = c0 + c1;
             const uint32_t maxt = __reduce_max_sync(0xffffffffu, tot);
             for (uint32_t j = 0; j < maxt; ++j) {

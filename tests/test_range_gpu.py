@@ -96,3 +96,42 @@ def test_range_large_property(rtd, orc, cuda):
     sel = np.arange(0, len(q), 997)[:300]
     oc, _ = orc.range_count(pts, q[sel], r)
     np.testing.assert_array_equal(counts[sel], oc)
+
+
+@pytest.mark.parametrize("r", [0.05, 0.3, 2.0])
+@pytest.mark.parametrize("leaf", [1, 8])
+def test_range_dense_clusters_contained_subtrees(rtd, orc, cuda, r, leaf):
+    """Tight clusters and radii up to the whole cloud: most hits come from
+    subtrees whose box lies inside the ball (counted and copied without a
+    per-point test); counts and pairs must still equal the oracle's."""
+    pts, q = workloads.clustered(n=20_000, nq=1_500, seed=31, n_clusters=6, box=1.0)
+    counts, total, pairs = gpu_range(rtd, pts, q, r, leaf_size=leaf)
+    oc, ot = orc.range_count(pts, q, r)
+    np.testing.assert_array_equal(counts, oc)
+    assert total == ot
+    np.testing.assert_array_equal(pairs, orc.range_pairs(pts, q, r))
+    counts_u, total_u, pairs_u = gpu_range(rtd, pts, q, r, sort=False, leaf_size=leaf)
+    assert total_u == ot
+    key = lambda a: np.sort(a[:, 0].astype(np.uint64) << np.uint64(32) | a[:, 1].astype(np.uint64))
+    np.testing.assert_array_equal(key(pairs_u), key(pairs))
+
+
+@pytest.mark.parametrize("r", [0.1, 10.0])
+def test_range_non_finite(rtd, orc, cuda, r):
+    """NaN / infinite points are never neighbours, also when their subtree
+    would otherwise lie inside the ball; a NaN query has none."""
+    rng = np.random.default_rng(12)
+    pts = rng.random((4000, 3)).astype(np.float32)
+    pts[10] = [np.nan, 0.5, 0.5]
+    pts[11] = [0.5, 0.5, np.nan]
+    pts[20] = [np.inf, 0.5, 0.5]
+    pts[30] = [0.5, -np.inf, 0.5]
+    q = rng.random((200, 3)).astype(np.float32)
+    q[0] = [np.nan, 0.1, 0.1]
+    q[1] = [np.inf, 0.1, 0.1]
+    q[2] = [1e30, 1e30, 1e30]
+    counts, total, pairs = gpu_range(rtd, pts, q, r)
+    oc, ot = orc.range_count(pts, q, r)
+    np.testing.assert_array_equal(counts, oc)
+    assert total == ot and counts[0] == 0
+    np.testing.assert_array_equal(pairs, orc.range_pairs(pts, q, r))
