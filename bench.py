@@ -108,6 +108,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest of every rank's value (every rank takes this collective
+    in the same order); x itself without a process group."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peaks() -> dict:
     path = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -196,11 +207,7 @@ def run_ours(args, ws, rank, local):
     if dist:
         dist.barrier()
     clk = clocks.stop()
-    total_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(step_ms), dist, dev)
     ms_per_step = total_ms / args.steps
     value = ws * nq / (ms_per_step / 1e3)
 
@@ -233,11 +240,7 @@ def run_ours(args, ws, rank, local):
             t0 = time.perf_counter()
             ctx.k_nn(hp, hq, K, s, out_ids=hids)
             e2e_t.append(time.perf_counter() - t0)
-        e2e_s = statistics.mean(e2e_t)
-        if dist:
-            t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = max_over_ranks(statistics.mean(e2e_t), dist, dev)
         e2e = {"value": ws * nq / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(hp.nbytes + hq.nbytes),
                "d2h_bytes_per_step": int(hids.nbytes), "ms_per_step": e2e_s * 1e3,
                "api": "rtd_k_nn_host (k_nn! host buffers, pinned)"}
