@@ -75,7 +75,8 @@ typedef struct rtd_schedule {
     uint32_t leaf_size;           /* LBVH leaf size: subtrees of <= leaf_size points collapse */
     uint32_t block_size;          /* threads per block of the search kernel (0 = auto) */
     uint32_t lanes_per_query;     /* 1 = thread per query, 32 = warp per query (0 = auto) */
-    uint32_t morton_bits;         /* 30 (u32 keys) or 63 (u64 keys); 0 = auto */
+    uint32_t morton_bits;         /* 30 (u32 keys, the reference layout) or 33..63 in steps
+                                     of 3 (u64 keys, bits/3 per axis); 0 = auto */
     uint32_t packet_traversal;    /* thread-per-query kernels: 32 Morton-adjacent queries
                                      share one traversal (rtd_packet_mode) */
     uint32_t lane_refill;         /* thread-per-query kernels: persistent warps whose lanes

@@ -129,11 +129,15 @@ __global__ void __launch_bounds__(BLOCK) batch_keys_kernel(const float *__restri
     for (uint64_t i = (uint64_t)blockIdx.x * BLOCK + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * BLOCK) {
         const uint32_t c = cloud_of[i];
-        uint32_t u[3];
+        // one cubic extent per cloud (the largest axis), as for single indexes
+        float lo[3], ext = 1e-6f;
         for (int a = 0; a < 3; ++a) {
-            const float lo = float_unflip(cd[c].box[a]), hi = float_unflip(cd[c].box[3 + a]);
-            u[a] = quantize(xyz[3 * i + a], lo, fmaxf(__fsub_rn(hi, lo), 1e-6f), scale);
+            const float hi = float_unflip(cd[c].box[3 + a]);
+            lo[a] = float_unflip(cd[c].box[a]);
+            ext = fmaxf(ext, __fsub_rn(hi, lo[a]));
         }
+        uint32_t u[3];
+        for (int a = 0; a < 3; ++a) u[a] = quantize(xyz[3 * i + a], lo[a], ext, scale);
         keys[i] = ((uint64_t)c << (3 * bpa)) | morton63(u[0], u[1], u[2]);
     }
 }

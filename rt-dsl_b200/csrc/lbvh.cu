@@ -75,12 +75,26 @@ __device__ __forceinline__ SceneNorm scene_norm(const IndexHeader *h) {
     return s;
 }
 
-// 30-bit codes follow compute_morton_codes (gprt-core/src/morton.rs:19-48);
-// 63-bit codes use the same normalisation with 21 bits per axis.
+// One extent for all three axes (the largest): every Morton bit level then
+// halves the same length on each axis, so a flat or elongated cloud is split
+// along its long axes first.  With an extent per axis, the top levels of a
+// thin sheet's tree would split its thickness and give every node a box
+// spanning the whole sheet.
+__device__ __forceinline__ SceneNorm scene_norm_cubic(const IndexHeader *h) {
+    SceneNorm s = scene_norm(h);
+    const float e = fmaxf(s.ext[0], fmaxf(s.ext[1], s.ext[2]));
+    s.ext[0] = s.ext[1] = s.ext[2] = e;
+    return s;
+}
+
+// 30-bit codes follow compute_morton_codes (gprt-core/src/morton.rs:19-48),
+// extent per axis; wider codes (B = bits / 3 per axis, scale = 2^B - 1,
+// B <= 21, interleaved in the low 3B bits of a u64) use one cubic extent.
 template <typename K>
 __global__ void __launch_bounds__(BLOCK) morton_kernel(const float *__restrict__ xyz, uint64_t n,
-                                                       const IndexHeader *h, K *__restrict__ keys) {
-    SceneNorm s = scene_norm(h);
+                                                       const IndexHeader *h, float scale,
+                                                       K *__restrict__ keys) {
+    const SceneNorm s = sizeof(K) == 4 ? scene_norm(h) : scene_norm_cubic(h);
     for (uint64_t i = (uint64_t)blockIdx.x * BLOCK + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * BLOCK) {
         float x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
@@ -89,9 +103,9 @@ __global__ void __launch_bounds__(BLOCK) morton_kernel(const float *__restrict__
                                   quantize(y, s.lo[1], s.ext[1], 1023.0f),
                                   quantize(z, s.lo[2], s.ext[2], 1023.0f));
         } else {
-            keys[i] = (K)morton63(quantize(x, s.lo[0], s.ext[0], 2097151.0f),
-                                  quantize(y, s.lo[1], s.ext[1], 2097151.0f),
-                                  quantize(z, s.lo[2], s.ext[2], 2097151.0f));
+            keys[i] = (K)morton63(quantize(x, s.lo[0], s.ext[0], scale),
+                                  quantize(y, s.lo[1], s.ext[1], scale),
+                                  quantize(z, s.lo[2], s.ext[2], scale));
         }
     }
 }
@@ -481,13 +495,14 @@ template <typename K>
 rtd_status build_typed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStream_t st) {
     IndexHeader *h = idx->hdr.as<IndexHeader>();
     uint32_t *d_err = &h->err;
-    const int kbits = sizeof(K) == 4 ? 30 : 63;
+    const int kbits = sizeof(K) == 4 ? 30 : idx->morton_bits;
+    const float scale = sizeof(K) == 4 ? 1023.0f : (float)((1u << (kbits / 3)) - 1u);
     RTD_TRY(idx->keys.reserve(n * sizeof(K)));
     RTD_TRY(idx->keys_alt.reserve(n * sizeof(K)));
     RTD_TRY(idx->vals.reserve(n * sizeof(uint32_t)));
     RTD_TRY(idx->vals_alt.reserve(n * sizeof(uint32_t)));
     const int g = grid_for(n, BLOCK, 148 * 8);
-    morton_kernel<K><<<g, BLOCK, 0, st>>>(d_xyz, n, h, idx->keys.as<K>());
+    morton_kernel<K><<<g, BLOCK, 0, st>>>(d_xyz, n, h, scale, idx->keys.as<K>());
     RTD_LAUNCH_CHECK();
     bool in_alt = false;
     RTD_TRY(radix_sort_pairs<K>(idx->keys.as<K>(), idx->keys_alt.as<K>(), idx->vals.as<uint32_t>(),
@@ -551,8 +566,11 @@ rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd
     if (s->leaf_size < 1 || s->leaf_size > 64)
         return fail(RTD_ERR_INVALID_ARGUMENT, "leaf_size must be in [1, 64]");
     int mb = (int)s->morton_bits;
-    if (mb == 0) mb = n >= (1ull << 19) ? 63 : 30;
-    if (mb != 30 && mb != 63) return fail(RTD_ERR_INVALID_ARGUMENT, "morton_bits must be 30 or 63");
+    // auto: 48-bit cubic keys (16 bits per axis); measured as fast to search as
+    // 63-bit keys on the clustered and sheet workloads, with two fewer sort passes
+    if (mb == 0) mb = 48;
+    if (mb != 30 && (mb < 33 || mb > 63 || mb % 3 != 0))
+        return fail(RTD_ERR_INVALID_ARGUMENT, "morton_bits must be 30 or a multiple of 3 in [33, 63]");
     RTD_CUDA(cudaGetDevice(&idx->device));
     idx->n = n;
     idx->leaf_size = s->leaf_size;
@@ -585,7 +603,7 @@ namespace {
 __global__ void __launch_bounds__(BLOCK) query_morton_kernel(const float *__restrict__ q,
                                                              uint64_t nq, const IndexHeader *h,
                                                              uint32_t *__restrict__ keys) {
-    SceneNorm s = scene_norm(h);
+    const SceneNorm s = scene_norm_cubic(h);   // processing order only
     for (uint64_t i = (uint64_t)blockIdx.x * BLOCK + threadIdx.x; i < nq;
          i += (uint64_t)gridDim.x * BLOCK) {
         keys[i] = morton30(quantize(q[3 * i], s.lo[0], s.ext[0], 1023.0f),

@@ -72,7 +72,7 @@ def test_knn_large_k_warp_list(rtd, orc, cuda, k):
 
 
 @pytest.mark.parametrize("leaf", [1, 2, 4, 8, 16, 32, 64])
-@pytest.mark.parametrize("bits", [30, 63])
+@pytest.mark.parametrize("bits", [30, 36, 48, 63])
 def test_knn_leaf_and_key_width(rtd, orc, cuda, leaf, bits):
     pts, q = clustered_small(n=25_000, nq=2_000, seed=13)
     ids, d2, info = gpu_knn(rtd, pts, q, 5, leaf_size=leaf, morton_bits=bits)

@@ -34,7 +34,7 @@ def test_sheet_knn(rtd, orc, sheet, sheet_index, k):
     ids, d2 = ix.knn(Q, k, s)
     torch.cuda.synchronize()
     info = ix.info()
-    assert info["morton_bits"] == 63
+    assert info["morton_bits"] == 48
     ids = ids.cpu().numpy().view(np.uint32)
     d2 = d2.cpu().numpy()
     assert np.all(ids < len(pts))
