@@ -484,7 +484,10 @@ rtd_status rtd_batch_plan(rtd_batch *b, const rtd_cloud *clouds, uint32_t n_clou
     int cb = 0;
     while (cb < 32 && (1ull << cb) < n_clouds) ++cb;
     b->cbits = cb;
-    b->bpa = (63 - cb) / 3 < 21 ? (63 - cb) / 3 : 21;
+    // bits per axis: the schedule's key width (auto 48 = 16 per axis), within what the
+    // 63-bit key leaves beside the cloud id
+    const int want = s.morton_bits ? (int)s.morton_bits / 3 : 16;
+    b->bpa = (63 - cb) / 3 < want ? (63 - cb) / 3 : want;
     if (b->bpa < 8) return fail(RTD_ERR_INVALID_ARGUMENT, "too many clouds");
     rtd_index &f = b->forest;
     f.n = np;

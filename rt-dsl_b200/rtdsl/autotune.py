@@ -143,6 +143,7 @@ BATCH_GRID = {
     "radius_param": [0.5, 1.0, 2.0],
     "radius_increment_mult": [2.0, 4.0],
     "lanes_per_query": [0, 32],
+    "morton_bits": [42, 48, 63],
 }
 
 
@@ -242,9 +243,9 @@ def main():
     pts, q = workloads.clustered()
     P = torch.from_numpy(pts).cuda()
     Q = torch.from_numpy(q).cuda()
-    grid = {"leaf_size": [2, 4, 8], "radius_param": [0.0625, 0.25, 0.5, 1.0],
+    grid = {"leaf_size": [2, 4, 8], "radius_param": [0.25, 0.5, 1.0],
             "radius_increment_mult": [2.0, 4.0], "block_size": [64, 128, 256],
-            "mode": ["thread", "warp"]}
+            "morton_bits": [42, 48, 63], "mode": ["thread", "warp"]}
     best, table = tune_knn(P, Q, 5, "clustered_1p8m_k5", grid=grid, log=log)
     log(f"clustered_1p8m_k5 best {table[0]}")
     cl = workloads.clouds()
