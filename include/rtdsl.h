@@ -192,6 +192,20 @@ rtd_status rtd_range_query_host(rtd_context *ctx, const rtd_vec3 *data, uint64_t
                                 const rtd_vec3 *queries, uint64_t nq, float radius,
                                 uint32_t *pairs, uint64_t capacity, uint64_t *n_pairs);
 
+/* DBSCAN over the range query: the reference advertises DBSCAN on its
+ * push-to-buffer range search (README.md:13) but ships no implementation.
+ * idx must be built over d_points (n points); membership is the range
+ * query's (FP32 key <= RN(eps*eps), the point itself included).  Core
+ * points have >= min_pts neighbours; clusters are numbered 0.. in the order
+ * of their smallest core point; a non-core neighbour of core points takes
+ * the smallest of their cluster numbers; all other points get -1.  These
+ * are the labels of the sequential algorithm expanding clusters from core
+ * points in index order.  Writes d_labels (n int32) and *h_n_clusters;
+ * synchronises.  Holds every neighbour pair in device memory meanwhile. */
+rtd_status rtd_dbscan(rtd_index *idx, const float *d_points, uint64_t n, float eps,
+                      uint32_t min_pts, int32_t *d_labels, uint64_t *h_n_clusters,
+                      rtd_stream stream);
+
 /* ---------------------------------------------------------------------
  * k-NN distance backward (no reference counterpart: the reference has no
  * gradients).  Loss gradient g[q*k+j] = dL/d(d2_qj) with ids held fixed;

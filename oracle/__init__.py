@@ -71,6 +71,8 @@ def lib() -> C.CDLL:
             L.orc_range_count.argtypes = [P, I64, P, I64, F, P]
             L.orc_range_count.restype = I64
             L.orc_range_pairs.argtypes = [P, I64, P, I64, F, P, P]
+            L.orc_dbscan.argtypes = [P, I64, F, C.c_uint32, P]
+            L.orc_dbscan.restype = I64
             L.orc_radius_sampled_percentile.argtypes = [P, I64, P, I64, C.c_int, F]
             L.orc_radius_sampled_percentile.restype = F
             L.orc_radius_sampled_nn.argtypes = [P, I64, F]
@@ -148,6 +150,16 @@ def range_count(pts, q, r: float):
     counts = np.empty(len(q), dtype=np.uint32)
     total = lib().orc_range_count(_p(pts), len(pts), _p(q), len(q), C.c_float(r), _p(counts))
     return counts, int(total)
+
+
+def dbscan(pts, eps: float, min_pts: int):
+    """(labels int32 [N], n_clusters): DBSCAN over the FP32 range membership,
+    clusters numbered in the order of their smallest core point, border
+    points in the first cluster that reaches them, noise -1."""
+    pts = _f32(pts)
+    labels = np.empty(len(pts), dtype=np.int32)
+    nc = lib().orc_dbscan(_p(pts), len(pts), C.c_float(eps), int(min_pts), _p(labels))
+    return labels, int(nc)
 
 
 def range_pairs(pts, q, r: float) -> np.ndarray:

@@ -936,3 +936,56 @@ double orc_direct_plummer_f64(const double *pos, const double *mass, int64_t n, 
     }
     return L;
 }
+
+/* ------------------------------------------------------------------------
+ * DBSCAN over the range-query membership (FP32 key <= RN(eps*eps), the
+ * point itself included).  The reference advertises DBSCAN on top of its
+ * push-to-buffer range search (README.md:13) but ships no implementation;
+ * this follows the published algorithm (Ester et al., 1996) with the
+ * labelling order of scikit-learn's DBSCAN, the reference validators'
+ * library:
+ *   - core point: at least min_pts neighbours;
+ *   - clusters are numbered 0, 1, ... in the order of their smallest core
+ *     point, expanded one at a time;
+ *   - a non-core neighbour of a core point takes the first cluster that
+ *     reaches it, i.e. the smallest label among its core neighbours;
+ *   - everything else is noise (-1).
+ * Brute force, O(n^2): test sizes only.  Returns the number of clusters.
+ * ---------------------------------------------------------------------- */
+int64_t orc_dbscan(const float *pts, int64_t n, float eps, uint32_t min_pts, int32_t *labels) {
+    const float r2 = eps * eps;
+    uint8_t *core = (uint8_t *)calloc((size_t)(n > 0 ? n : 1), 1);
+    int64_t *stack = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n > 0 ? n : 1));
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t i = 0; i < n; ++i) {
+        uint32_t c = 0;
+        for (int64_t j = 0; j < n; ++j)
+            if (orc_key(pts + 3 * i, pts + 3 * j) <= r2) ++c;
+        core[i] = c >= min_pts;
+    }
+    for (int64_t i = 0; i < n; ++i) labels[i] = -1;
+    int32_t next = 0;
+    for (int64_t s = 0; s < n; ++s) {
+        if (labels[s] != -1 || !core[s]) continue;
+        // a point takes the label of the cluster whose expansion first
+        // reaches it; labelling it when it is pushed keeps each point on the
+        // stack at most once (only one cluster expands at a time, so the
+        // label is the same as labelling it when popped)
+        int64_t sp = 0;
+        labels[s] = next;
+        stack[sp++] = s;
+        while (sp > 0) {
+            const int64_t i = stack[--sp];
+            if (!core[i]) continue;
+            for (int64_t j = 0; j < n; ++j)
+                if (labels[j] == -1 && orc_key(pts + 3 * i, pts + 3 * j) <= r2) {
+                    labels[j] = next;
+                    stack[sp++] = j;
+                }
+        }
+        ++next;
+    }
+    free(core);
+    free(stack);
+    return next;
+}

@@ -240,6 +240,40 @@ def radius_for_mean_count(index: "Index", queries, target_mean: float, sample: i
     return float(hi)
 
 
+def spatial_join(a, b, radius: float, schedule: Schedule | None = None, exclude_self: bool = False,
+                 stream=None):
+    """All (i, j) with |b_i - a_j| <= radius (FP32 key <= RN(r*r)), sorted by
+    (i, j): the range query with b as queries over an index of a.  With
+    exclude_self (a and b the same set) the pairs (i, i) are dropped."""
+    _check_points_tensor(a, "a")
+    _check_points_tensor(b, "b")
+    s = schedule if schedule is not None else default_schedule()
+    ix = Index().build(a, s, stream=stream)
+    _, total = ix.range_count(b, radius, s, stream=stream)
+    pairs = ix.range_fill(b, radius, total, sort_pairs=True, schedule=s, stream=stream)
+    if exclude_self:
+        pairs = pairs[pairs[:, 0] != pairs[:, 1]]
+    return pairs
+
+
+def dbscan(points, eps: float, min_pts: int, schedule: Schedule | None = None, index=None,
+           stream=None):
+    """(labels int32 CUDA tensor, n_clusters): DBSCAN over the range query;
+    clusters numbered by their smallest core point, noise -1."""
+    import torch
+    _check_points_tensor(points, "points")
+    lib = load()
+    if index is None:
+        index = Index().build(points, schedule if schedule is not None else default_schedule(),
+                              stream=stream)
+    labels = torch.empty((points.shape[0],), dtype=torch.int32, device=points.device)
+    nc = C.c_uint64(0)
+    check(lib.rtd_dbscan(index._h, C.c_void_p(points.data_ptr()), points.shape[0], C.c_float(eps),
+                         int(min_pts), C.c_void_p(labels.data_ptr()), C.byref(nc),
+                         _stream_handle(stream)))
+    return labels, nc.value
+
+
 def knn_backward(queries, points, ids, grad_d2, grad_q=None, grad_p=None, stream=None):
     """dL/dq (overwritten) and dL/dp (accumulated) for d2 = |q - p_id|^2."""
     import torch

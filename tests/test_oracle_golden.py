@@ -104,3 +104,22 @@ def test_bh_ref_walk_theta0_is_direct_sum(orc):
     f = orc.bh_ref_forces(pos, mass, nodes, order, 0.0, 1.0)
     ref = orc.direct_ref_f64(pos, mass, np.arange(700), 1.0)
     np.testing.assert_allclose(f, ref, rtol=2e-4, atol=1e-4 * np.abs(ref).max())
+
+
+def test_dbscan_matches_scikit_learn(orc):
+    """The oracle's DBSCAN (FP32 range membership) labels points exactly as
+    scikit-learn's DBSCAN does on data with no pair at distance ~ eps."""
+    from sklearn.cluster import DBSCAN
+    rng = np.random.default_rng(3)
+    blobs = [rng.normal(c, s, size=(700, 3)) for c, s in ((0.2, 0.03), (0.6, 0.05), (0.8, 0.02))]
+    pts = np.concatenate(blobs + [rng.random((900, 3))]).astype(np.float32)
+    rng.shuffle(pts)
+    d = np.sqrt(((pts[:, None, :].astype(np.float64) - pts[None, :, :]) ** 2).sum(-1))
+    for eps0, mp in ((0.04, 8), (0.08, 5), (0.02, 3)):
+        # nudge eps until no pair distance lies within FP32 rounding of it
+        eps = next(e for e in (eps0 * (1 + 1e-4 * j) for j in range(100))
+                   if np.abs(d - e).min() > 1e-6 * e)
+        ref = DBSCAN(eps=eps, min_samples=mp).fit(pts.astype(np.float64)).labels_
+        labels, nc = orc.dbscan(pts, eps, mp)
+        np.testing.assert_array_equal(labels, ref)
+        assert nc == ref.max() + 1
