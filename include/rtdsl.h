@@ -192,6 +192,15 @@ rtd_status rtd_range_query_host(rtd_context *ctx, const rtd_vec3 *data, uint64_t
                                 const rtd_vec3 *queries, uint64_t nq, float radius,
                                 uint32_t *pairs, uint64_t capacity, uint64_t *n_pairs);
 
+/* The reference's point files (load_points_fast, gprt-sandbox/src/io.rs:
+ * 8-30): "x,y,z" lines, empty lines and lines whose first three fields do
+ * not parse as f32 skipped, extra fields ignored, line order kept.  Writes
+ * up to `capacity` points (3 floats each) to the host buffer `out` and the
+ * file's point count to *n_points; RTD_ERR_OVERFLOW when it exceeds
+ * capacity (call with capacity 0 to size the buffer). */
+rtd_status rtd_load_points_csv(const char *path, float *out, uint64_t capacity,
+                               uint64_t *n_points);
+
 /* DBSCAN over the range query: the reference advertises DBSCAN on its
  * push-to-buffer range search (README.md:13) but ships no implementation.
  * idx must be built over d_points (n points); membership is the range

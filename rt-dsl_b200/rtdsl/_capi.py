@@ -92,6 +92,7 @@ _SIGNATURES = {
                             C.POINTER(_U64), _P]),
     "rtd_range_query_host": (_I, [_P, _P, _U64, _P, _U64, _F, _P, _U64, C.POINTER(_U64)]),
     "rtd_dbscan": (_I, [_P, _P, _U64, _F, _U32, _P, C.POINTER(_U64), _P]),
+    "rtd_load_points_csv": (_I, [C.c_char_p, _P, _U64, C.POINTER(_U64)]),
     "rtd_knn_backward": (_I, [_P, _U64, _P, _U64, _U32, _P, _P, _P, _P, _P]),
     "rtd_index_profile_enable": (_I, [_P, _I]),
     "rtd_index_profile_get": (_I, [_P, _P]),
