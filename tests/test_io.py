@@ -72,3 +72,35 @@ def test_knn_results_round_trip(tmp_path):
         neighbors = eval(line.strip().split(":")[1])
         assert neighbors == [int(v) for v in ids[i] if v != 0xFFFFFFFF]
     assert result_line("data.csv", 3, 3, 1.23456, 7) == "data.csv,3,3,1.235,7"
+
+
+def test_reference_wisdom_round_trip(tmp_path, rtd):
+    """gprt_wisdom.json (serde JSON of gprt_ir::Schedule) maps onto
+    rtd_schedule and back."""
+    from rtdsl import wisdom
+    text = """{
+  "radius_increment_mult": 2.5,
+  "max_hits_per_query": 512,
+  "use_morton_lbv": true,
+  "radius_heuristic": {"SampledPercentile": 0.05},
+  "memory_strategy": "GlobalMemory",
+  "build_strategy": "PreferFastBuild",
+  "geom_type": "Spheres"
+}"""
+    s = wisdom.schedule_from_wisdom(text)
+    assert s.radius_increment_mult == 2.5 and s.use_morton_lbv == 1
+    assert s.radius_heuristic == rtd.RADIUS_SAMPLED_PERCENTILE and abs(s.radius_param - 0.05) < 1e-7
+    for h, (mode, param) in (("\"SampledMax\"", (rtd.RADIUS_SAMPLED_MAX, 1.0)),
+                             ("{\"Fixed\": 0.25}", (rtd.RADIUS_FIXED, 0.25))):
+        s2 = wisdom.schedule_from_wisdom('{"radius_heuristic": %s}' % h)
+        assert (s2.radius_heuristic, s2.radius_param) == (mode, param)
+    p = tmp_path / "gprt_wisdom.json"
+    wisdom.save(str(p), s)
+    back = wisdom.load(str(p))
+    assert back.as_dict() == s.as_dict()
+    import json
+    d = json.loads(p.read_text())
+    assert d["radius_heuristic"] == {"SampledPercentile": float(np.float32(0.05))}
+    assert set(d) == set(wisdom.REFERENCE_DEFAULTS)
+    with pytest.raises(ValueError):
+        wisdom.schedule_from_wisdom('{"radius_heuristic": {"Bogus": 1}}')
