@@ -343,6 +343,16 @@ rtd_status rtd_bh_forward_noalloc(rtd_bh *b, const rtd_bh_params *p, float *d_ou
 rtd_status rtd_bh_backward(rtd_bh *b, const rtd_bh_params *p, const float *d_g_acc,
                            const float *d_g_phi, float *d_g_pos, float *d_g_mass,
                            rtd_stream stream);
+/* Time integration with the Plummer law: `steps` kick-drift-kick leapfrog
+ * steps of size dt on d_pos / d_vel (n*3 each, caller order; the reference's
+ * Body.velocity, gprt-core/src/lib.rs:311-317, which the reference never
+ * advances), rebuilding the tree every step.  d_acc (n*3) holds a(x) of the
+ * positions passed in when acc_valid != 0 (else it is computed first) and
+ * a(x) of the final positions on return, so consecutive calls chain.
+ * G, eps, theta, quadrupole and bucket come from p. */
+rtd_status rtd_bh_leapfrog(rtd_bh *b, const rtd_bh_params *p, float *d_pos, float *d_vel,
+                           const float *d_mass, uint64_t n, float dt, uint32_t steps,
+                           float *d_acc, int acc_valid, rtd_stream stream);
 typedef struct rtd_bh_info {
     uint64_t n_bodies, n_nodes, n_leaves;
     uint32_t depth;          /* deepest level (root = 0) */

@@ -106,6 +106,7 @@ _SIGNATURES = {
     "rtd_bh_forward_noalloc": (_I, [_P, _P, _P, _P, _P]),
     "rtd_bh_backward": (_I, [_P, _P, _P, _P, _P, _P, _P]),
     "rtd_bh_info_get": (_I, [_P, _P, _P]),
+    "rtd_bh_leapfrog": (_I, [_P, _P, _P, _P, _P, _U64, _F, _U32, _P, _I, _P]),
     "rtd_bh_interaction_counts": (_I, [_P, _F, _U64, C.POINTER(_U64), C.POINTER(_U64),
                                        C.POINTER(_U64), _P]),
     "rtd_bh_export": (_I, [_P, _P, _P, _P]),

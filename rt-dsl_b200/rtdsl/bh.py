@@ -94,6 +94,26 @@ class BarnesHut:
         return {"n_bodies": inf.n_bodies, "n_nodes": inf.n_nodes, "n_leaves": inf.n_leaves,
                 "depth": inf.depth, "root_min": list(inf.root_min), "root_max": list(inf.root_max)}
 
+    def leapfrog(self, pos, vel, mass, dt: float, steps: int,
+                 params: _capi.BhParams | None = None, acc=None, stream=None):
+        """Advances pos / vel (CUDA tensors, in place) by `steps` leapfrog
+        steps of the Plummer law; returns the acceleration at the final
+        positions (pass it back as `acc` to continue without recomputing)."""
+        import torch
+        p = params if params is not None else default_bh_params(law=BH_LAW_PLUMMER)
+        for t, name in ((pos, "pos"), (vel, "vel"), (mass, "mass")):
+            if not (t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()):
+                raise ValueError(f"{name} must be a contiguous float32 CUDA tensor")
+        valid = acc is not None
+        if acc is None:
+            acc = torch.empty_like(pos)
+        check(self._lib.rtd_bh_leapfrog(self._h, C.byref(p), _ptr(pos), _ptr(vel), _ptr(mass),
+                                        pos.shape[0], C.c_float(dt), int(steps), _ptr(acc),
+                                        int(valid), _stream(stream)))
+        self.n = pos.shape[0]
+        self._keep = (pos, mass)
+        return acc
+
     def interaction_counts(self, theta: float, stride: int = 64, stream=None) -> dict:
         """Mean accepted cells and leaf bodies per body of the Plummer walk
         (every stride-th body in tree order)."""

@@ -248,3 +248,65 @@ def test_plummer_interaction_counts(cuda):
     ns = (len(fpos) + stride - 1) // stride
     assert c["sampled"] == ns
     assert round(c["cells_per_body"] * ns) == cells and round(c["bodies_per_body"] * ns) == bodies
+
+
+def test_leapfrog_matches_fp64_direct_sum(orc, cuda):
+    """theta = 0 makes every interaction direct, so a few leapfrog steps must
+    follow an FP64 leapfrog driven by the FP64 direct sum (FP32 rounding)."""
+    from rtdsl.bh import BarnesHut
+    from rtdsl._capi import default_bh_params
+    pos, mass = workloads.plummer(2_000, seed=12)
+    rng = np.random.default_rng(1)
+    vel = (rng.normal(size=pos.shape) * 0.3).astype(np.float32)
+    p = default_bh_params(law=1, theta=0.0, eps=0.05, G=1.0, bucket=16)
+    P = torch.from_numpy(pos).cuda()
+    V = torch.from_numpy(vel).cuda()
+    M = torch.from_numpy(mass).cuda()
+    dt, steps = 1e-3, 5
+    BarnesHut().leapfrog(P, V, M, dt, steps, p)
+    x = pos.astype(np.float64)
+    v = vel.astype(np.float64)
+    m = mass.astype(np.float64)
+    a = orc.direct_plummer_f64(x, m, 0.05, 1.0)[2]
+    for _ in range(steps):
+        v += 0.5 * dt * a
+        x += dt * v
+        a = orc.direct_plummer_f64(x, m, 0.05, 1.0)[2]
+        v += 0.5 * dt * a
+    np.testing.assert_allclose(P.cpu().numpy(), x, rtol=2e-6, atol=2e-5)
+    np.testing.assert_allclose(V.cpu().numpy(), v, rtol=0, atol=2e-4 * np.abs(v).max())
+
+
+def test_leapfrog_energy_and_chaining(orc, cuda):
+    """Energy of a Plummer sphere in virial equilibrium is conserved to
+    1e-3 over 40 steps at theta 0.5, and two calls of 20 steps chained
+    through the returned accelerations equal one call of 40."""
+    from rtdsl.bh import BarnesHut
+    from rtdsl._capi import default_bh_params
+    n = 8_192
+    pos, mass = workloads.plummer(n, seed=5)
+    r = np.linalg.norm(pos.astype(np.float64), axis=1)
+    rng = np.random.default_rng(2)
+    # isotropic velocities with the local Plummer dispersion sigma^2 = 1/(6 sqrt(1+r^2))
+    sig = np.sqrt(1.0 / (6.0 * np.sqrt(1.0 + r * r)))
+    vel = (rng.normal(size=pos.shape) * sig[:, None]).astype(np.float32)
+    p = default_bh_params(law=1, theta=0.5, eps=0.01, G=1.0, bucket=16)
+
+    def energy(P, V, M):
+        x = P.cpu().numpy().astype(np.float64)
+        v = V.cpu().numpy().astype(np.float64)
+        m = M.cpu().numpy().astype(np.float64)
+        _, phi, _ = orc.direct_plummer_f64(x, m, 0.01, 1.0)
+        return 0.5 * np.sum(m * np.sum(v * v, axis=1)) + 0.5 * np.sum(m * phi)
+
+    M = torch.from_numpy(mass).cuda()
+    P1, V1 = torch.from_numpy(pos).cuda(), torch.from_numpy(vel).cuda()
+    e0 = energy(P1, V1, M)
+    bh = BarnesHut()
+    acc = bh.leapfrog(P1, V1, M, 2e-3, 20, p)
+    bh.leapfrog(P1, V1, M, 2e-3, 20, p, acc=acc)
+    e1 = energy(P1, V1, M)
+    assert abs(e1 - e0) / abs(e0) < 1e-3, (e0, e1)
+    P2, V2 = torch.from_numpy(pos).cuda(), torch.from_numpy(vel).cuda()
+    BarnesHut().leapfrog(P2, V2, M, 2e-3, 40, p)
+    assert torch.equal(P1, P2) and torch.equal(V1, V2)
