@@ -289,8 +289,9 @@ def run_ours(args, ws, rank, local):
 # ------------------------------------------------------- range sub-bench
 def bench_range(args, dev, flush, P, Q, s) -> dict:
     """Fixed-radius range query on the headline cloud at the radius whose
-    mean neighbour count is 50: count pass, then the push fill of exactly
-    sized (query, id) pairs (unsorted), on a built index."""
+    mean neighbour count is 50: count pass, then the fill of exactly sized
+    (query, id) pairs (unsorted; each query's pairs written into its own
+    segment at the count's offsets), on a built index."""
     import torch
     import rtdsl
     from rtdsl.api import radius_for_mean_count
@@ -334,7 +335,7 @@ def bench_range(args, dev, flush, P, Q, s) -> dict:
                    "radius": r, "pairs": int(total)},
         "ms": {"count_kernel": mc, "fill_kernel": mf, "step": m},
         "queries_per_s": nq / (m / 1e3),
-        "roofline": {"kernel": "range_kernel<true> (fill)", "bound": "hbm",
+        "roofline": {"kernel": "range_kernel<MODE_SEG> (fill)", "bound": "hbm",
                      "achieved": fill_bytes / (mf / 1e3) / 1e9, "peak": peak["hbm_gbs"],
                      "unit": "GB/s", "frac": fill_bytes / (mf / 1e3) / 1e9 / peak["hbm_gbs"],
                      "algorithmic_bytes_per_launch": fill_bytes,

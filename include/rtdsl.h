@@ -174,9 +174,14 @@ rtd_status rtd_k_nn_host(rtd_context *ctx, const rtd_vec3 *data, uint64_t n,
  * per-query length, store while below cap) and r_nn!/gprt_trace!
  * (lib.rs:625-672, 729-750).  Membership: FP32 key <= RN(r*r).
  * Count pass: d_counts[q] hits per query, *h_total the sum (this call
- * synchronises to return it).  Fill pass: (query, id) uint32 pairs pushed
- * by warp-aggregated atomics into d_pairs (2 u32 per pair); order is
- * unspecified unless sort_pairs != 0 (then sorted by query, id).  If
+ * synchronises to return it).  Fill pass: (query, id) uint32 pairs into
+ * d_pairs (2 u32 per pair).  When the last count on this index was over the
+ * same d_queries / nq / radius (and no build, k-NN search or other count
+ * came between) and capacity >= its total, every query's pairs go into its
+ * own segment at the count's offsets: grouped by query in the caller's
+ * order, and RTD_ERR_INVALID_ARGUMENT if the hit counts no longer match
+ * (queries changed in place).  Otherwise they are pushed by warp-aggregated
+ * atomics in unspecified order.  sort_pairs != 0 sorts by (query, id).  If
  * capacity < total, nothing past capacity is written, *h_written = total
  * and RTD_ERR_OVERFLOW is returned.
  * ------------------------------------------------------------------- */

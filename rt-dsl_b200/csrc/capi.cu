@@ -38,6 +38,9 @@ rtd_status status_from_deverr(uint32_t f) {
     if (f & DEVERR_OVERFLOW) return fail(RTD_ERR_OVERFLOW, "output buffer too small");
     if (f & DEVERR_NOT_CONVERGED) return fail(RTD_ERR_NOT_CONVERGED, "radius expansion did not converge");
     if (f & DEVERR_DEPTH) return fail(RTD_ERR_UNSUPPORTED, "tree deeper than the key supports");
+    if (f & DEVERR_MISMATCH)
+        return fail(RTD_ERR_INVALID_ARGUMENT, "range fill: hit counts differ from the count pass "
+                                              "(queries changed between count and fill)");
     return fail(RTD_ERR_CUDA, "unknown device error flag");
 }
 

@@ -45,6 +45,7 @@ enum : uint32_t {
     DEVERR_NOT_CONVERGED = 1u << 2, // radius expansion ran out of rounds
     DEVERR_OVERFLOW = 1u << 3,      // output buffer too small
     DEVERR_DEPTH = 1u << 4,         // tree deeper than the key supports
+    DEVERR_MISMATCH = 1u << 5,      // a fill found other hit counts than its count pass
 };
 rtd_status status_from_deverr(uint32_t flags);
 

@@ -73,6 +73,17 @@ struct rtd_index {
     // search scratch
     rtd::DevBuf qkeys, qkeys_alt, qperm, qperm_alt;
     rtd::DevBuf rcounts, roffsets, rcursor, rpairs_alt, rkeys, rkeys_alt;
+    // What the last range count left behind for a fill of the same queries:
+    // per-query exclusive offsets (roffsets), the total, and the query order.
+    // Cleared by a build and by any other query ordering on this index.
+    struct RangeToken {
+        bool valid = false;
+        const float *q = nullptr;
+        uint64_t nq = 0;
+        float radius = 0.f;
+        uint64_t total = 0;
+        const uint32_t *perm = nullptr;
+    } rtoken;
     // phase timers (rtd_index_profile_*)
     bool prof = false;
     cudaEvent_t ev[8] = {};

@@ -572,6 +572,7 @@ rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd
     if (mb != 30 && (mb < 33 || mb > 63 || mb % 3 != 0))
         return fail(RTD_ERR_INVALID_ARGUMENT, "morton_bits must be 30 or a multiple of 3 in [33, 63]");
     RTD_CUDA(cudaGetDevice(&idx->device));
+    idx->rtoken.valid = false;
     idx->n = n;
     idx->leaf_size = s->leaf_size;
     idx->morton_bits = mb;
@@ -616,6 +617,7 @@ __global__ void __launch_bounds__(BLOCK) query_morton_kernel(const float *__rest
 rtd_status order_queries(rtd_index *idx, const float *d_q, uint64_t nq, bool morton,
                          const uint32_t **perm, cudaStream_t st) {
     *perm = nullptr;
+    idx->rtoken.valid = false;   // the query-order buffers are about to change
     if (!morton || nq < 2) return RTD_OK;
     if (nq >= (1ull << 30)) return fail(RTD_ERR_INVALID_ARGUMENT, "at most 2^30-1 queries");
     RTD_TRY(idx->qkeys.reserve(nq * 4));

@@ -1,13 +1,16 @@
 // range.cu -- fixed-radius range query: a count pass sizes the output, a
-// fill pass pushes (query, id) pairs into it.  Replaces the reference's
+// fill pass writes (query, id) pairs into it.  Replaces the reference's
 // global-push programs (gprt-macros/src/lib.rs:276-295), where every
 // any-hit does atomicAdd(&lens[q], 1) into a capped per-query slab that the
 // host then copies back and filters (lib.rs:538-583).  Here the buffer is
-// exactly sized by the count pass, and hits are staged per warp in shared
-// memory and pushed with one global atomicAdd per flush (warp-aggregated
-// compaction), so global atomics scale with the output bytes / 8 KB instead
-// of the hit count.  Membership: exact FP32 key <= RN(r*r), as the
-// intersection program tests dist_sq <= r_val*r_val (lib.rs:283, 341).
+// exactly sized by the count pass.  A fill that follows the count of the
+// same queries writes every query's hits into its own segment of the
+// buffer, at the offsets the count's exclusive scan left on the index (no
+// atomics; pairs come out grouped by query in the caller's order).  Any
+// other fill stages hits per warp in shared memory and pushes them with one
+// global atomicAdd per flush (warp-aggregated compaction).  Membership:
+// exact FP32 key <= RN(r*r), as the intersection program tests
+// dist_sq <= r_val*r_val (lib.rs:283, 341).
 #include "index.cuh"
 
 namespace rtd {
@@ -15,9 +18,14 @@ namespace {
 
 constexpr int RBLOCK = 128;
 constexpr int RWARPS = RBLOCK / 32;
-constexpr int SHORT_DEPTH = 16;  // stack entries per thread in shared memory
+constexpr int SHORT_DEPTH = 12;  // stack entries per thread in shared memory
 constexpr int STACK_DEPTH = 104; // >= maximal tree depth
 constexpr int WBUF = 256;        // staged pairs per warp (2 KB)
+constexpr uint32_t BIG_SUB = 32;  // contained subtrees of this size or more: copied by the warp
+
+// Kernel modes: count hits, push pairs through warp staging and a global
+// cursor, or write pairs into per-query segments at known offsets.
+enum : int { MODE_COUNT = 0, MODE_PUSH = 1, MODE_SEG = 2 };
 
 struct RangeArgs {
     IndexView ix;
@@ -29,6 +37,8 @@ struct RangeArgs {
     uint2 *pairs;
     uint64_t capacity;
     unsigned long long *cursor;
+    const uint64_t *offsets;   // MODE_SEG: exclusive offsets of the count pass
+    uint64_t total;            // MODE_SEG: end of the last segment
     uint32_t *err;
 };
 
@@ -50,21 +60,41 @@ struct Walk {
     int sp;
 };
 
-// FILL = false: count hits per query.  FILL = true: push pairs.
+// Fields of the per-lane work a traversal step stages for the warp (one
+// 32-word row per field, so lanes reading different owners hit different
+// banks).
+enum : int { F_QX = 0, F_QY, F_QZ, F_F0, F_C0, F_F1, F_T, F_DONE,   // count needs these
+             F_QI, F_G0, F_N0, F_G1, F_WLEN, F_WBLO, F_WBHI, F_COUNT_ALL };
+constexpr int F_COUNT_ONLY = F_DONE + 1;
+
+// MODE_COUNT: count hits per query.  MODE_PUSH / MODE_SEG: write pairs.
 // Threads of a warp advance their own traversals one node per iteration of
 // a warp-converged loop; a stack entry carries the node and the first
 // sorted point below it.  A child whose whole box lies inside the ball
 // (farthest-corner key <= r^2, a bound on every point's key) contributes
-// all its points without a test: its count in the count pass, a
-// warp-cooperative copy of its contiguous ids in the fill pass.  Leaves
-// that straddle the sphere are tested in a warp-uniform loop over candidate
-// slots, and each slot's hits are compacted with one ballot into the warp's
-// staging buffer, which the warp pushes with one global atomic per flush.
-template <bool FILL>
-__global__ void __launch_bounds__(RBLOCK, FILL ? 8 : 12) range_kernel(const RangeArgs p) {
+// all its points without a test: its count in the count pass, its
+// contiguous ids in the fills (by the whole warp, one pair per lane, for
+// subtrees of BIG_SUB points or more).  After each step the lanes' other
+// work -- points of the leaves that straddle the sphere, to test, and
+// (fills) points of small contained subtrees, to take -- is flattened over the warp by a prefix sum
+// and processed 32 candidates at a time with every lane busy: a lane finds
+// its candidate's owner by a binary search over the prefix (shuffles) and
+// reads the owner's query and ranges from shared memory.  One ballot per
+// batch gives every hit its rank among its owner's hits in the batch.
+// MODE_COUNT adds each owner's hits; MODE_SEG writes them at the owner's
+// next slots of its segment and checks that the query fills it exactly;
+// MODE_PUSH compacts them into the warp's staging buffer, which the warp
+// pushes with one global atomic per flush.
+template <int MODE>
+__global__ void __launch_bounds__(RBLOCK, MODE == MODE_COUNT ? 10 : 8) range_kernel(const RangeArgs p) {
+    constexpr bool PUSH = MODE == MODE_PUSH;
+    constexpr bool SEG = MODE == MODE_SEG;
+    constexpr bool FILL = PUSH || SEG;
+    constexpr int NF = FILL ? F_COUNT_ALL : F_COUNT_ONLY;
     __shared__ BvhNode s_top[TOP_MAX];
     __shared__ uint2 s_stack[SHORT_DEPTH][RBLOCK];
-    __shared__ uint2 s_buf[FILL ? RWARPS : 1][FILL ? WBUF : 1];
+    __shared__ uint2 s_buf[PUSH ? RWARPS : 1][PUSH ? WBUF : 1];
+    __shared__ uint32_t s_work[RWARPS][NF][32];
     const IndexHeader *h = p.ix.hdr;
     const uint32_t ntop = h->n_top;
     for (uint32_t i = threadIdx.x; i < ntop; i += RBLOCK) s_top[i] = p.ix.top[i];
@@ -78,12 +108,13 @@ __global__ void __launch_bounds__(RBLOCK, FILL ? 8 : 12) range_kernel(const Rang
     const float r2 = p.r2;
     const uint32_t visit_cap = 2u * h->n_internal + 4u;
     uint2 l_stack[STACK_DEPTH - SHORT_DEPTH];
-    uint2 *buf = s_buf[FILL ? warp : 0];
+    uint2 *buf = s_buf[PUSH ? warp : 0];
+    uint32_t (*W)[32] = s_work[warp];
     uint32_t fill = 0;   // staged pairs of this warp (warp-uniform)
 
     // pushes the staged pairs with one reservation on the global cursor
     auto flush = [&]() {
-        if (!FILL || fill == 0) return;
+        if (!PUSH || fill == 0) return;
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(p.cursor, (unsigned long long)fill);
         base = __shfl_sync(0xffffffffu, base, 0);
@@ -109,13 +140,31 @@ __global__ void __launch_bounds__(RBLOCK, FILL ? 8 : 12) range_kernel(const Rang
             qi = p.perm ? p.perm[t] : t;
             qx = p.q[3 * qi]; qy = p.q[3 * qi + 1]; qz = p.q[3 * qi + 2];
         }
+        __syncwarp();   // the previous batch's readers of W are done
+        W[F_QX][lane] = __float_as_uint(qx);
+        W[F_QY][lane] = __float_as_uint(qy);
+        W[F_QZ][lane] = __float_as_uint(qz);
+        W[F_DONE][lane] = 0;
+        uint64_t wend = 0;
+        if (FILL) W[F_QI][lane] = (uint32_t)qi;
+        if (SEG) {   // this query's segment of the pair buffer
+            uint64_t wb = 0;
+            if (have) {
+                wb = p.offsets[qi];
+                wend = qi + 1 < p.nq ? p.offsets[qi + 1] : p.total;
+            }
+            W[F_WLEN][lane] = (uint32_t)(wend - wb);
+            W[F_WBLO][lane] = (uint32_t)wb;
+            W[F_WBHI][lane] = (uint32_t)(wb >> 32);
+        }
         // a query with a NaN coordinate has no neighbours (its keys are NaN)
         const bool live = have && !isnan(qx) && !isnan(qy) && !isnan(qz);
         uint32_t node = (live && root != CHILD_NONE) ? root : CHILD_NONE;
         uint32_t first = 0;   // first sorted point below `node`
         int sp = 0;
-        uint32_t cnt = 0;
+        uint32_t cnt = 0;     // points of contained subtrees (count pass)
         uint32_t visits = 0;
+        bool seg_bad = false;
         while (__any_sync(0xffffffffu, node != CHILD_NONE)) {
             if (node != CHILD_NONE && ++visits > visit_cap) {   // broken tree: give up
                 atomicOr(p.err, DEVERR_STACK);
@@ -172,49 +221,138 @@ __global__ void __launch_bounds__(RBLOCK, FILL ? 8 : 12) range_kernel(const Rang
                 node = next;
                 first = next_first;
             }
-            cnt += n0 + n1;
-            if (FILL) {   // contained subtrees: the warp copies each lane's ranges
-                uint32_t m = __ballot_sync(0xffffffffu, (n0 | n1) != 0);
+            if (!FILL) cnt += n0 + n1;
+            if (FILL) {
+                // contained subtrees of BIG_SUB points or more: the whole
+                // warp copies each one's contiguous ids, one pair per lane
+                const uint32_t b0 = n0 >= BIG_SUB ? n0 : 0u, b1 = n1 >= BIG_SUB ? n1 : 0u;
+                if (b0) n0 = 0;
+                if (b1) n1 = 0;
+                uint32_t m = __ballot_sync(0xffffffffu, (b0 | b1) != 0);
                 while (m) {
                     const int src = __ffs(m) - 1;
                     m &= m - 1;
                     const uint32_t sq = (uint32_t)__shfl_sync(0xffffffffu, (uint32_t)qi, src);
                     for (int r = 0; r < 2; ++r) {
                         const uint32_t gs = __shfl_sync(0xffffffffu, r ? g1 : g0, src);
-                        const uint32_t ns = __shfl_sync(0xffffffffu, r ? n1 : n0, src);
-                        for (uint32_t base = 0; base < ns; base += 32) {
-                            const uint32_t take = ns - base < 32u ? ns - base : 32u;
-                            if ((uint32_t)lane < take)
-                                buf[fill + lane] = make_uint2(sq, __float_as_uint(__ldg(&pts[gs + base + lane].w)));
-                            fill += take;
-                            if (fill > WBUF - 32) flush();
+                        const uint32_t ns = __shfl_sync(0xffffffffu, r ? b1 : b0, src);
+                        if (ns == 0) continue;
+                        if (SEG) {
+                            const uint32_t done = W[F_DONE][src];
+                            if ((uint64_t)done + ns <= W[F_WLEN][src]) {
+                                const uint64_t dst =
+                                    (((uint64_t)W[F_WBHI][src] << 32) | W[F_WBLO][src]) + done;
+                                for (uint32_t k = lane; k < ns; k += 32)
+                                    p.pairs[dst + k] = make_uint2(sq, __float_as_uint(__ldg(&pts[gs + k].w)));
+                            } else {
+                                seg_bad = true;
+                            }
+                            __syncwarp();
+                            if (lane == src) W[F_DONE][src] = done + ns;
+                            __syncwarp();
+                        } else {
+                            for (uint32_t base = 0; base < ns; base += 32) {
+                                const uint32_t take = ns - base < 32u ? ns - base : 32u;
+                                if ((uint32_t)lane < take)
+                                    buf[fill + lane] = make_uint2(sq, __float_as_uint(__ldg(&pts[gs + base + lane].w)));
+                                fill += take;
+                                if (fill > WBUF - 32) flush();
+                            }
                         }
                     }
                 }
             }
-            // straddling leaves, tested warp-uniformly
-            const uint32_t tot = c0 + c1;
-            const uint32_t maxt = __reduce_max_sync(0xffffffffu, tot);
-            for (uint32_t j = 0; j < maxt; ++j) {
+            // flatten this step's remaining candidates over the warp
+            const uint32_t tl = c0 + c1;
+            const uint32_t items = tl + (FILL ? n0 + n1 : 0u);
+            uint32_t incl = items;
+#pragma unroll
+            for (int dlt = 1; dlt < 32; dlt <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xffffffffu, incl, dlt);
+                if (lane >= dlt) incl += v;
+            }
+            const uint32_t excl = incl - items;
+            const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+            if (total == 0) continue;
+            W[F_F0][lane] = f0;
+            W[F_C0][lane] = c0;
+            W[F_F1][lane] = f1;
+            W[F_T][lane] = tl;
+            if (FILL) {
+                W[F_G0][lane] = g0;
+                W[F_N0][lane] = n0;
+                W[F_G1][lane] = g1;
+            }
+            __syncwarp();
+            for (uint32_t base = 0; base < total; base += 32) {
+                const uint32_t ci = base + lane;
+                const bool valid = ci < total;
+                // owner: the last lane whose prefix is <= ci
+                int o = 0;
+#pragma unroll
+                for (int step = 16; step >= 1; step >>= 1) {
+                    const uint32_t pv = __shfl_sync(0xffffffffu, excl, o + step);
+                    if (pv <= ci) o += step;
+                }
+                const uint32_t oexcl = __shfl_sync(0xffffffffu, excl, o);
+                const uint32_t oitems = __shfl_sync(0xffffffffu, items, o);
                 bool hit = false;
                 uint32_t id = 0;
-                if (j < tot) {
-                    const float4 pt = __ldg(&pts[j < c0 ? f0 + j : f1 + (j - c0)]);
-                    hit = exact_key(qx, qy, qz, pt.x, pt.y, pt.z) <= r2;
-                    id = __float_as_uint(pt.w);
-                }
-                cnt += hit;
-                if (FILL) {
-                    const uint32_t m = __ballot_sync(0xffffffffu, hit);
-                    if (m) {
-                        if (hit) buf[fill + __popc(m & lt)] = make_uint2((uint32_t)qi, id);
-                        fill += __popc(m);
-                        if (fill > WBUF - 32) flush();
+                if (valid) {
+                    const uint32_t j = ci - oexcl;
+                    const uint32_t ot = W[F_T][o];
+                    if (j < ot) {
+                        const uint32_t oc0 = W[F_C0][o];
+                        const uint32_t pi = j < oc0 ? W[F_F0][o] + j : W[F_F1][o] + (j - oc0);
+                        const float4 pt = __ldg(&pts[pi]);
+                        hit = exact_key(__uint_as_float(W[F_QX][o]), __uint_as_float(W[F_QY][o]),
+                                        __uint_as_float(W[F_QZ][o]), pt.x, pt.y, pt.z) <= r2;
+                        id = __float_as_uint(pt.w);
+                    } else if (FILL) {
+                        const uint32_t j2 = j - ot, on0 = W[F_N0][o];
+                        const uint32_t pi = j2 < on0 ? W[F_G0][o] + j2 : W[F_G1][o] + (j2 - on0);
+                        id = __float_as_uint(__ldg(&pts[pi].w));
+                        hit = true;
                     }
                 }
+                const uint32_t hm = __ballot_sync(0xffffffffu, hit);
+                // this owner's lanes in the batch: [rs, re]
+                const int rs = oexcl > base ? (int)(oexcl - base) : 0;
+                const uint32_t rend = oexcl + oitems - base;
+                const int re = (int)(rend < 32u ? rend : 32u) - 1;
+                const uint32_t below_rs = (1u << rs) - 1u;
+                const uint32_t upto_re = re >= 31 ? 0xffffffffu : ((1u << (re + 1)) - 1u);
+                const uint32_t run_hits = __popc(hm & upto_re & ~below_rs);
+                if (SEG) {
+                    const uint32_t done = W[F_DONE][o];
+                    if (hit) {
+                        const uint32_t dst = done + __popc(hm & lt & ~below_rs);
+                        if (dst < W[F_WLEN][o]) {
+                            const uint64_t wb = ((uint64_t)W[F_WBHI][o] << 32) | W[F_WBLO][o];
+                            p.pairs[wb + dst] = make_uint2(W[F_QI][o], id);
+                        } else {
+                            seg_bad = true;
+                        }
+                    }
+                    __syncwarp();
+                    if (valid && lane == re) W[F_DONE][o] = done + run_hits;
+                } else if (PUSH) {
+                    if (hm) {
+                        if (hit) buf[fill + __popc(hm & lt)] = make_uint2(W[F_QI][o], id);
+                        fill += __popc(hm);
+                        if (fill > WBUF - 32) flush();
+                    }
+                } else {
+                    if (valid && lane == re) W[F_DONE][o] += run_hits;
+                }
+                __syncwarp();
             }
         }
-        if (!FILL && have) p.counts[qi] = cnt;
+        __syncwarp();
+        if (MODE == MODE_COUNT && have) p.counts[qi] = cnt + W[F_DONE][lane];
+        // a segment left short or overrun: the queries changed since the count
+        if (SEG && (seg_bad || (have && W[F_DONE][lane] != W[F_WLEN][lane])))
+            atomicOr(p.err, DEVERR_MISMATCH);
     }
     flush();
 }
@@ -261,7 +399,16 @@ rtd_status range_args(rtd_index *idx, const float *d_q, uint64_t nq, float r,
     a.pairs = nullptr;
     a.capacity = 0;
     a.cursor = nullptr;
+    a.offsets = nullptr;
+    a.total = 0;
     a.err = &idx->hdr.as<IndexHeader>()->err;
+    return RTD_OK;
+}
+
+template <int MODE>
+rtd_status launch_range(RangeArgs &a, cudaStream_t st) {
+    range_kernel<MODE><<<grid_for(a.nq, RBLOCK, 1 << 20), RBLOCK, 0, st>>>(a);
+    RTD_LAUNCH_CHECK();
     return RTD_OK;
 }
 
@@ -278,8 +425,7 @@ rtd_status range_count(rtd_index *idx, const float *d_q, uint64_t nq, float r,
     a.counts = d_counts;
     IndexHeader *h = idx->hdr.as<IndexHeader>();
     if (nq) {
-        range_kernel<false><<<grid_for(nq, RBLOCK, 1 << 20), RBLOCK, 0, st>>>(a);
-        RTD_LAUNCH_CHECK();
+        RTD_TRY(launch_range<MODE_COUNT>(a, st));
         idx->mark(EV_SEARCH1, st);
         RTD_TRY(idx->roffsets.reserve(nq * sizeof(uint64_t)));
         RTD_TRY(exclusive_scan_u32(d_counts, idx->roffsets.as<uint64_t>(), nq, &h->total,
@@ -291,6 +437,13 @@ rtd_status range_count(rtd_index *idx, const float *d_q, uint64_t nq, float r,
     RTD_CUDA(cudaMemcpyAsync(&total, &h->total, sizeof(total), cudaMemcpyDeviceToHost, st));
     RTD_TRY(check_index_errors(idx, st));   // synchronises
     if (h_total) *h_total = total;
+    // a fill of the same queries can write straight into per-query segments
+    idx->rtoken.valid = true;
+    idx->rtoken.q = d_q;
+    idx->rtoken.nq = nq;
+    idx->rtoken.radius = r;
+    idx->rtoken.total = total;
+    idx->rtoken.perm = a.perm;
     return RTD_OK;
 }
 
@@ -298,21 +451,51 @@ rtd_status range_fill(rtd_index *idx, const float *d_q, uint64_t nq, float r,
                       const rtd_schedule *s, uint32_t *d_pairs, uint64_t capacity, int sort_pairs,
                       uint64_t *h_written, cudaStream_t st) {
     if (capacity && !d_pairs) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL pairs");
+    // Segment mode: the last count pass on this index was over these queries
+    // at this radius, its offsets and query order are still on the index,
+    // and the buffer holds every pair.
+    const auto &tk = idx->rtoken;
+    const bool seg = tk.valid && tk.q == d_q && tk.nq == nq && tk.radius == r && nq > 0 &&
+                     capacity >= tk.total;
     RangeArgs a;
-    RTD_TRY(range_args(idx, d_q, nq, r, s, a, st));
-    RTD_TRY(idx->rcursor.reserve(sizeof(unsigned long long)));
-    RTD_CUDA(cudaMemsetAsync(idx->rcursor.ptr, 0, sizeof(unsigned long long), st));
+    if (seg) {
+        if (!idx->hdr.ptr) return fail(RTD_ERR_INVALID_ARGUMENT, "index not built");
+        for (int e = EV_SEARCH0; e <= EV_SEARCH1; ++e) idx->ev_set[e] = false;
+        idx->mark(EV_SEARCH0, st);
+        idx->mark(EV_SEEDED, st);
+        idx->mark(EV_ORDERED, st);
+        a.ix = view_of(idx);
+        a.q = d_q;
+        a.nq = nq;
+        a.perm = tk.perm;
+        a.r2 = r * r;
+        a.counts = nullptr;
+        a.cursor = nullptr;
+            a.offsets = idx->roffsets.as<uint64_t>();
+        a.total = tk.total;
+        a.err = &idx->hdr.as<IndexHeader>()->err;
+    } else {
+        RTD_TRY(range_args(idx, d_q, nq, r, s, a, st));
+        RTD_TRY(idx->rcursor.reserve(sizeof(unsigned long long)));
+        RTD_CUDA(cudaMemsetAsync(idx->rcursor.ptr, 0, sizeof(unsigned long long), st));
+        a.cursor = idx->rcursor.as<unsigned long long>();
+    }
     a.pairs = reinterpret_cast<uint2 *>(d_pairs);
     a.capacity = capacity;
-    a.cursor = idx->rcursor.as<unsigned long long>();
-    if (nq) {
-        range_kernel<true><<<grid_for(nq, RBLOCK, 1 << 20), RBLOCK, 0, st>>>(a);
-        RTD_LAUNCH_CHECK();
+    if (seg) {
+        RTD_TRY(launch_range<MODE_SEG>(a, st));
+        idx->mark(EV_SEARCH1, st);
+    } else if (nq) {
+        RTD_TRY(launch_range<MODE_PUSH>(a, st));
         idx->mark(EV_SEARCH1, st);
     }
     unsigned long long total = 0;
-    RTD_CUDA(cudaMemcpyAsync(&total, idx->rcursor.ptr, sizeof(total), cudaMemcpyDeviceToHost, st));
-    RTD_CUDA(cudaStreamSynchronize(st));
+    if (seg) {
+        total = tk.total;
+    } else {
+        RTD_CUDA(cudaMemcpyAsync(&total, idx->rcursor.ptr, sizeof(total), cudaMemcpyDeviceToHost, st));
+        RTD_CUDA(cudaStreamSynchronize(st));
+    }
     if (h_written) *h_written = total;
     if (total > capacity) {
         IndexHeader *h = idx->hdr.as<IndexHeader>();

@@ -135,3 +135,64 @@ def test_range_non_finite(rtd, orc, cuda, r):
     np.testing.assert_array_equal(counts, oc)
     assert total == ot and counts[0] == 0
     np.testing.assert_array_equal(pairs, orc.range_pairs(pts, q, r))
+
+
+def _pair_keys(a):
+    return np.sort(a[:, 0].astype(np.uint64) << np.uint64(32) | a[:, 1].astype(np.uint64))
+
+
+def test_range_fill_after_count_is_grouped_by_query(rtd, orc, cuda):
+    """A fill that follows the count of the same queries writes each query's
+    pairs into its own segment: even unsorted, the pairs come out grouped
+    by query in the caller's order, and the set equals the oracle's."""
+    pts, q = workloads.clustered(n=30_000, nq=2_000, seed=41, n_clusters=10, box=10.0)
+    r = 0.2
+    counts, total, pairs = gpu_range(rtd, pts, q, r, sort=False)
+    assert np.all(np.diff(pairs[:, 0].astype(np.int64)) >= 0)
+    np.testing.assert_array_equal(np.bincount(pairs[:, 0], minlength=len(q)), counts)
+    np.testing.assert_array_equal(_pair_keys(pairs), _pair_keys(orc.range_pairs(pts, q, r)))
+
+
+def test_range_fill_without_matching_count(rtd, orc, cuda):
+    """Fills that do not follow a count of the same queries at the same
+    radius (no count at all, another radius, a k-NN search in between, other
+    queries) push pairs through the warp-staged cursor and give the same
+    set."""
+    pts, q = workloads.clustered(n=30_000, nq=2_000, seed=42, n_clusters=10, box=10.0)
+    s = rtd.default_schedule()
+    ix = rtd.Index().build(torch.from_numpy(pts).cuda(), s)
+    qt = torch.from_numpy(q).cuda()
+    ref = _pair_keys(orc.range_pairs(pts, q, 0.15))
+    n_ref = len(ref)
+    # no count on this index yet
+    np.testing.assert_array_equal(_pair_keys(ix.range_fill(qt, 0.15, n_ref, schedule=s).cpu().numpy().view(np.uint32)), ref)
+    # the last count was at another radius
+    ix.range_count(qt, 0.1, s)
+    np.testing.assert_array_equal(_pair_keys(ix.range_fill(qt, 0.15, n_ref, schedule=s).cpu().numpy().view(np.uint32)), ref)
+    # a k-NN search reordered queries after the count
+    ix.range_count(qt, 0.15, s)
+    ix.knn(qt, 5, s)
+    np.testing.assert_array_equal(_pair_keys(ix.range_fill(qt, 0.15, n_ref, schedule=s).cpu().numpy().view(np.uint32)), ref)
+    # the count was over another query buffer
+    ix.range_count(qt[:1000].clone(), 0.15, s)
+    np.testing.assert_array_equal(_pair_keys(ix.range_fill(qt, 0.15, n_ref, schedule=s).cpu().numpy().view(np.uint32)), ref)
+
+
+def test_range_fill_detects_queries_changed_after_count(rtd, orc, cuda):
+    """Queries overwritten in place between the count and the fill: the fill
+    stays inside each query's segment, reports the mismatch, and the index
+    keeps working."""
+    pts, q = workloads.clustered(n=20_000, nq=1_000, seed=43, n_clusters=6, box=5.0)
+    s = rtd.default_schedule()
+    ix = rtd.Index().build(torch.from_numpy(pts).cuda(), s)
+    qt = torch.from_numpy(q).cuda()
+    _, total = ix.range_count(qt, 0.2, s)
+    qt.copy_(torch.from_numpy(np.ascontiguousarray(q[::-1])).cuda())   # other hit counts per slot
+    pairs = torch.zeros((total + 1024, 2), dtype=torch.int32, device="cuda")
+    with pytest.raises(rtd.RtdError) as e:
+        ix.range_fill(qt, 0.2, total, schedule=s, out_pairs=pairs)
+    assert e.value.status == 1
+    assert torch.all(pairs[total:] == 0)      # nothing written past the counted total
+    _, total2 = ix.range_count(qt, 0.2, s)
+    got = ix.range_fill(qt, 0.2, total2, sort_pairs=True, schedule=s).cpu().numpy().view(np.uint32)
+    np.testing.assert_array_equal(got, orc.range_pairs(pts, q[::-1].copy(), 0.2))
