@@ -131,4 +131,21 @@ rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStr
 rtd_status order_queries(rtd_index *idx, const float *d_q, uint64_t nq, bool morton,
                          const uint32_t **perm, cudaStream_t stream);
 
+// The same order computed against the queries' own box with scratch of its
+// own, so that it can run on another stream while an index is being built.
+// Device errors land in the scratch header's err word.
+struct QueryOrderScratch {
+    DevBuf hdr;   // IndexHeader: the query box and err
+    DevBuf keys, keys_alt, perm, perm_alt;
+    SortScratch sort;
+};
+rtd_status order_queries_own(QueryOrderScratch &qs, const float *d_q, uint64_t nq,
+                             const uint32_t **perm, cudaStream_t stream);
+
+// k-NN search (knn.cu); with have_perm the query order is given (perm, or
+// nullptr for caller order) instead of computed on the index.
+rtd_status knn_search_ex(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k,
+                         const rtd_schedule *sched, uint32_t *d_ids, float *d_d2,
+                         cudaStream_t st, bool have_perm, const uint32_t *perm);
+
 }  // namespace rtd

@@ -591,6 +591,12 @@ rtd_status seed_radius(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k
 
 rtd_status knn_search(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k,
                       const rtd_schedule *sched, uint32_t *d_ids, float *d_d2, cudaStream_t st) {
+    return knn_search_ex(idx, d_q, nq, k, sched, d_ids, d_d2, st, false, nullptr);
+}
+
+rtd_status knn_search_ex(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k,
+                         const rtd_schedule *sched, uint32_t *d_ids, float *d_d2,
+                         cudaStream_t st, bool have_perm, const uint32_t *given_perm) {
     if (!idx || !idx->hdr.ptr) return fail(RTD_ERR_INVALID_ARGUMENT, "index not built");
     if (nq == 0) return RTD_OK;
     if (!d_q || !d_ids) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL queries or ids");
@@ -608,8 +614,8 @@ rtd_status knn_search(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k,
     idx->mark(EV_SEARCH0, st);
     RTD_TRY(seed_radius(idx, d_q, nq, k, s, st));
     idx->mark(EV_SEEDED, st);
-    const uint32_t *perm = nullptr;
-    RTD_TRY(order_queries(idx, d_q, nq, s.use_morton_lbv != 0, &perm, st));
+    const uint32_t *perm = given_perm;
+    if (!have_perm) RTD_TRY(order_queries(idx, d_q, nq, s.use_morton_lbv != 0, &perm, st));
     idx->mark(EV_ORDERED, st);
     KnnArgs a;
     a.ix = view_of(idx);

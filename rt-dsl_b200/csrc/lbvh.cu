@@ -636,4 +636,30 @@ rtd_status order_queries(rtd_index *idx, const float *d_q, uint64_t nq, bool mor
     return RTD_OK;
 }
 
+rtd_status order_queries_own(QueryOrderScratch &qs, const float *d_q, uint64_t nq,
+                             const uint32_t **perm, cudaStream_t st) {
+    *perm = nullptr;
+    if (nq < 2) return RTD_OK;
+    if (nq >= (1ull << 30)) return fail(RTD_ERR_INVALID_ARGUMENT, "at most 2^30-1 queries");
+    RTD_TRY(qs.hdr.reserve(sizeof(IndexHeader)));
+    RTD_TRY(qs.keys.reserve(nq * 4));
+    RTD_TRY(qs.keys_alt.reserve(nq * 4));
+    RTD_TRY(qs.perm.reserve(nq * 4));
+    RTD_TRY(qs.perm_alt.reserve(nq * 4));
+    IndexHeader *h = qs.hdr.as<IndexHeader>();
+    hdr_init_kernel<<<1, 1, 0, st>>>(h);
+    RTD_LAUNCH_CHECK();
+    bbox_kernel<<<grid_for(nq, BLOCK, 148 * 4), BLOCK, 0, st>>>(d_q, nq, h);
+    RTD_LAUNCH_CHECK();
+    query_morton_kernel<<<grid_for(nq, BLOCK, 148 * 8), BLOCK, 0, st>>>(d_q, nq, h,
+                                                                        qs.keys.as<uint32_t>());
+    RTD_LAUNCH_CHECK();
+    bool in_alt = false;
+    RTD_TRY(radix_sort_pairs<uint32_t>(qs.keys.as<uint32_t>(), qs.keys_alt.as<uint32_t>(),
+                                       qs.perm.as<uint32_t>(), qs.perm_alt.as<uint32_t>(), true,
+                                       nq, 0, 30, qs.sort, &h->err, st, &in_alt));
+    *perm = in_alt ? qs.perm_alt.as<uint32_t>() : qs.perm.as<uint32_t>();
+    return RTD_OK;
+}
+
 }  // namespace rtd

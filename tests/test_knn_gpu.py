@@ -186,6 +186,22 @@ def test_knn_host_api_k_nn(rtd, orc, cuda):
     assert all(len(r) == 3 for r in few)
 
 
+@pytest.mark.parametrize("order", [0, 1])
+def test_knn_host_context_overlap(rtd, orc, cuda, order):
+    """rtd_k_nn_host copies and orders the queries on a second stream while
+    the index is built: ids and d2 equal the oracle's with and without query
+    ordering, across repeated calls of different sizes on one context."""
+    ctx = rtd.Context()
+    s = rtd.default_schedule(use_morton_lbv=order, leaf_size=8, morton_bits=42)
+    for n, nq, seed in [(30_000, 3_000, 51), (5_000, 7_000, 52), (30_000, 1, 53), (1, 300, 54)]:
+        pts, q = clustered_small(n=n, nq=nq, seed=seed)
+        if nq == 1:
+            q = q[:1]
+        ids, d2 = ctx.k_nn(pts, q, 5, s, with_d2=True)
+        oi, od = orc.knn(pts, q, 5)
+        assert_same(oi, od, ids, d2)
+
+
 def test_knn_deterministic_and_reusable_index(rtd, cuda):
     pts, q = clustered_small(n=20_000, nq=2_000, seed=18)
     s = rtd.default_schedule()
