@@ -64,7 +64,8 @@ struct rtd_index {
     rtd::DevBuf top;        // BvhNode * TOP_MAX
     // build scratch
     rtd::DevBuf keys, keys_alt, vals, vals_alt;
-    rtd::DevBuf kleft, kright, kfirst, klast, kparent, flags, cidx, cparent, counter;
+    rtd::DevBuf kleft, kright, kfirst, klast, kparent, flags, cidx, csel;
+    rtd::DevBuf pyramid;    // run boxes over the sorted points (2 float4 per run)
     rtd::SortScratch sort;
     rtd::ScanScratch scan;
     // radius-seed data kept from the build: stride sample of the points in
@@ -120,7 +121,7 @@ inline IndexView view_of(const rtd_index *idx) {
                      idx->hdr.as<IndexHeader>(), idx->n};
 }
 
-// Karras tree, leaf collapse and bottom-up refit over n keys already sorted
+// Karras tree, leaf collapse and child boxes over n keys already sorted
 // (idx->pts holds the points in key order; idx->leaf_size set).
 template <typename K>
 rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStream_t st);

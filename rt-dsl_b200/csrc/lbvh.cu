@@ -1,6 +1,7 @@
 // lbvh.cu -- LBVH builder: scene box -> Morton codes -> onesweep radix sort
-// -> Karras radix tree -> leaf collapse -> bottom-up box refit with atomics
-// -> top-level staging.  Replaces the OptiX GAS build/refit of
+// -> Karras radix tree -> leaf collapse with every child box taken from a
+// pyramid of run boxes over the sorted points -> top-level staging.
+// Replaces the OptiX GAS build/refit of
 // gprt-optix/host/main.cpp:200-292 and the sphere-AABB kernel of
 // gprt-optix/host/kernels.cu:3-16: the tree holds point boxes only and the
 // search radius is applied inside the search kernels.
@@ -168,24 +169,192 @@ __global__ void __launch_bounds__(BLOCK) karras_kernel(const K *__restrict__ key
     }
 }
 
+// ---------------------------------------------------- box pyramid
+// Boxes of aligned runs of the sorted points: level j entry e covers points
+// [e * 32^j, (e+1) * 32^j) as (lo.xyz, -) (hi.xyz, -).  A run holding a
+// point with a NaN coordinate gets an unbounded box: such a point is never
+// a neighbour, but no finite box holds it, so no search may treat a
+// subtree containing it as lying wholly inside a ball.
+constexpr int PYR_MAX = 6;   // levels 1..6 cover 32^6 = 2^30 points
+struct Pyramid {
+    const float4 *pts;
+    const float4 *lvl[PYR_MAX + 1];   // lvl[j]: 2 float4 per entry; lvl[0] unused
+    int nlev;                         // highest level built (its size is <= 32)
+};
+
+struct Box {
+    float lo[3], hi[3];
+};
+
+__device__ __forceinline__ void box_empty(Box &b) {
+    for (int a = 0; a < 3; ++a) { b.lo[a] = INFINITY; b.hi[a] = -INFINITY; }
+}
+__device__ __forceinline__ void box_add_point(Box &b, bool &nan, const float4 p) {
+    b.lo[0] = fminf(b.lo[0], p.x); b.hi[0] = fmaxf(b.hi[0], p.x);
+    b.lo[1] = fminf(b.lo[1], p.y); b.hi[1] = fmaxf(b.hi[1], p.y);
+    b.lo[2] = fminf(b.lo[2], p.z); b.hi[2] = fmaxf(b.hi[2], p.z);
+    nan |= isnan(p.x) || isnan(p.y) || isnan(p.z);
+}
+__device__ __forceinline__ void box_add(Box &b, const float4 lo, const float4 hi) {
+    b.lo[0] = fminf(b.lo[0], lo.x); b.hi[0] = fmaxf(b.hi[0], hi.x);
+    b.lo[1] = fminf(b.lo[1], lo.y); b.hi[1] = fmaxf(b.hi[1], hi.y);
+    b.lo[2] = fminf(b.lo[2], lo.z); b.hi[2] = fmaxf(b.hi[2], hi.z);
+}
+__device__ __forceinline__ void box_unbounded(Box &b) {
+    for (int a = 0; a < 3; ++a) { b.lo[a] = -INFINITY; b.hi[a] = INFINITY; }
+}
+
+// Warp-wide min / max of one box per lane.
+__device__ __forceinline__ void warp_box_reduce(Box &b, bool &nan) {
+    for (int o = 16; o > 0; o >>= 1) {
+        for (int a = 0; a < 3; ++a) {
+            b.lo[a] = fminf(b.lo[a], __shfl_xor_sync(0xffffffffu, b.lo[a], o));
+            b.hi[a] = fmaxf(b.hi[a], __shfl_xor_sync(0xffffffffu, b.hi[a], o));
+        }
+    }
+    nan = __any_sync(0xffffffffu, nan);
+}
+
+// Levels 1 and 2 from the points: a 1024-thread block per 1024 points, a
+// warp per 32-point run, warp 0 folding the block's 32 runs.
+__global__ void __launch_bounds__(1024) pyramid_base_kernel(const float4 *__restrict__ pts,
+                                                            uint64_t n, float4 *l1, float4 *l2) {
+    __shared__ float4 s_lo[32], s_hi[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t i = (uint64_t)blockIdx.x * 1024 + threadIdx.x;
+    Box b;
+    box_empty(b);
+    bool nan = false;
+    if (i < n) box_add_point(b, nan, pts[i]);
+    warp_box_reduce(b, nan);
+    if (nan) box_unbounded(b);
+    const uint64_t e1 = (uint64_t)blockIdx.x * 32 + warp;
+    const bool has1 = e1 * 32 < n;
+    if (lane == 0) {
+        const float4 lo = make_float4(b.lo[0], b.lo[1], b.lo[2], 0.f);
+        const float4 hi = make_float4(b.hi[0], b.hi[1], b.hi[2], 0.f);
+        if (has1) { l1[2 * e1] = lo; l1[2 * e1 + 1] = hi; }
+        s_lo[warp] = lo;
+        s_hi[warp] = hi;
+    }
+    __syncthreads();
+    if (warp == 0 && l2) {
+        Box c;
+        box_empty(c);
+        box_add(c, s_lo[lane], s_hi[lane]);   // empty runs past n hold the empty box
+        bool cn = false;
+        warp_box_reduce(c, cn);
+        if (lane == 0) {
+            l2[2 * blockIdx.x] = make_float4(c.lo[0], c.lo[1], c.lo[2], 0.f);
+            l2[2 * blockIdx.x + 1] = make_float4(c.hi[0], c.hi[1], c.hi[2], 0.f);
+        }
+    }
+}
+
+// Level j from level j-1 (count_prev entries): a warp per entry.
+__global__ void __launch_bounds__(256) pyramid_level_kernel(const float4 *__restrict__ prev,
+                                                            uint64_t count_prev, float4 *out,
+                                                            uint64_t count) {
+    const int lane = threadIdx.x & 31;
+    for (uint64_t e = ((uint64_t)blockIdx.x * 256 + threadIdx.x) >> 5; e < count;
+         e += ((uint64_t)gridDim.x * 256) >> 5) {
+        Box b;
+        box_empty(b);
+        const uint64_t src = e * 32 + lane;
+        if (src < count_prev) box_add(b, prev[2 * src], prev[2 * src + 1]);
+        bool nan = false;
+        warp_box_reduce(b, nan);
+        if (lane == 0) {
+            out[2 * e] = make_float4(b.lo[0], b.lo[1], b.lo[2], 0.f);
+            out[2 * e + 1] = make_float4(b.hi[0], b.hi[1], b.hi[2], 0.f);
+        }
+    }
+}
+
+// Adds entries [a, b) of one level (the points when PTS) to a box, loading
+// BATCH entries at a time so that their loads are in flight together.  The
+// last batch repeats entry b - 1 in place of entries past b: a min / max
+// does not change when an entry is added twice.
+template <bool PTS>
+__device__ __forceinline__ void add_run(Box &bx, bool &nan, const float4 *__restrict__ base,
+                                        uint32_t a, uint32_t b) {
+    constexpr int BATCH = PTS ? 8 : 4;
+#pragma unroll 1
+    for (uint32_t t = a; t < b; t += BATCH) {
+        float4 lo[BATCH], hi[BATCH];
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u) {
+            const uint32_t e = t + u < b ? t + u : b - 1;
+            if (PTS) {
+                lo[u] = __ldg(&base[e]);
+            } else {
+                lo[u] = __ldg(&base[2 * (uint64_t)e]);
+                hi[u] = __ldg(&base[2 * (uint64_t)e + 1]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u) {
+            if (PTS) box_add_point(bx, nan, lo[u]);
+            else box_add(bx, lo[u], hi[u]);
+        }
+    }
+}
+
+// Box of the sorted points [first, first + count): partial runs at both
+// ends point by point, then whole runs from the pyramid level by level (at
+// most 31 entries per end and level); the highest level is taken whole.
+__device__ __noinline__ Box range_box(const Pyramid &P, uint32_t first, uint32_t count) {
+    Box b;
+    box_empty(b);
+    bool nan = false;
+    uint32_t l = first, r = first + count;   // n < 2^30: no overflow
+#pragma unroll 1
+    for (int j = 0; j <= PYR_MAX; ++j) {
+        if (l >= r) break;
+        if (j == P.nlev) {
+            if (j == 0) add_run<true>(b, nan, P.pts, l, r);
+            else add_run<false>(b, nan, P.lvl[j], l, r);
+            break;
+        }
+        uint32_t head = (l + 31) & ~31u;
+        if (head > r) head = r;
+        uint32_t tail = r & ~31u;
+        if (tail < head) tail = head;
+        if (j == 0) {
+            add_run<true>(b, nan, P.pts, l, head);
+            add_run<true>(b, nan, P.pts, tail, r);
+        } else {
+            add_run<false>(b, nan, P.lvl[j], l, head);
+            add_run<false>(b, nan, P.lvl[j], tail, r);
+        }
+        l = head >> 5;
+        r = tail >> 5;
+    }
+    if (nan) box_unbounded(b);
+    return b;
+}
+
 // Compact nodes: children become leaves when their subtree has <= leaf_size
-// points.  Every child carries the number of points below it (a subtree's
-// points are contiguous in sorted order, starting at the parent's first
-// point for the left child and after the left child's points for the
-// right one).  Boxes are filled by the refit kernel.
+// points.  A thread per kept node (sel[c] = its Karras index).  Every child
+// carries the number of points below it (a subtree's points are contiguous
+// in sorted order, starting at the parent's first point for the left child
+// and after the left child's points for the right one), and its box: the
+// box of its contiguous points, from the pyramid.  Every node's boxes are
+// computed independently, so no bottom-up pass over the tree follows.
 __global__ void __launch_bounds__(BLOCK) compact_kernel(
-    int64_t n, const uint32_t *__restrict__ kleft, const uint32_t *__restrict__ kright,
+    uint32_t n_internal_max, const IndexHeader *h, const uint32_t *__restrict__ sel,
+    const uint32_t *__restrict__ kleft, const uint32_t *__restrict__ kright,
     const uint32_t *__restrict__ kfirst, const uint32_t *__restrict__ klast,
-    const uint32_t *__restrict__ kparent, const uint32_t *__restrict__ flags,
-    const uint32_t *__restrict__ cidx, BvhNode *nodes, uint32_t *cparent, uint32_t *counter) {
-    for (int64_t i = (int64_t)blockIdx.x * BLOCK + threadIdx.x; i < n - 1;
-         i += (int64_t)gridDim.x * BLOCK) {
-        if (!flags[i]) continue;
-        uint32_t c = cidx[i];
-        uint32_t ch[2] = {kleft[i], kright[i]};
+    const uint32_t *__restrict__ flags, const uint32_t *__restrict__ cidx, const Pyramid P,
+    BvhNode *nodes) {
+    const uint32_t n_int = h->n_internal;
+    for (uint32_t c = blockIdx.x * BLOCK + threadIdx.x; c < n_int && c < n_internal_max;
+         c += gridDim.x * BLOCK) {
+        const uint32_t i = sel[c];
+        const uint32_t ch[2] = {kleft[i], kright[i]};
         uint32_t word[2], cnt[2];
         for (int s = 0; s < 2; ++s) {
-            uint32_t w = ch[s];
+            const uint32_t w = ch[s];
             if (w & CHILD_LEAF) {
                 word[s] = CHILD_LEAF | (w & CHILD_INDEX);
                 cnt[s] = 1;
@@ -197,131 +366,16 @@ __global__ void __launch_bounds__(BLOCK) compact_kernel(
                 cnt[s] = klast[w] - kfirst[w] + 1;
             }
         }
+        const uint32_t f0 = kfirst[i];
+        const Box b0 = range_box(P, f0, cnt[0]);
+        const Box b1 = range_box(P, f0 + cnt[0], cnt[1]);
         BvhNode nd;
-        nd.a = make_float4(0.f, 0.f, 0.f, 0.f);
-        nd.b = nd.a;
-        nd.c = nd.a;
+        // layout: [lo.x0 lo.y0 lo.z0 hi.x0] [hi.y0 hi.z0 lo.x1 lo.y1] [lo.z1 hi.x1 hi.y1 hi.z1]
+        nd.a = make_float4(b0.lo[0], b0.lo[1], b0.lo[2], b0.hi[0]);
+        nd.b = make_float4(b0.hi[1], b0.hi[2], b1.lo[0], b1.lo[1]);
+        nd.c = make_float4(b1.lo[2], b1.hi[0], b1.hi[1], b1.hi[2]);
         nd.d = make_uint4(word[0], word[1], cnt[0], cnt[1]);
         nodes[c] = nd;
-        // parent (compact) and which side this node is on
-        uint32_t par = CHILD_NONE;
-        if (i != 0) {
-            uint32_t kp = kparent[i];
-            uint32_t side = ((kright[kp] & ~CHILD_LEAF) == (uint32_t)i) ? 1u : 0u;
-            par = (cidx[kp] << 1) | side;
-        }
-        cparent[c] = par;
-        counter[c] = 0;
-    }
-}
-
-struct Box {
-    float lo[3], hi[3];
-};
-
-__device__ __forceinline__ Box leaf_box(const float4 *__restrict__ pts, uint32_t first,
-                                        uint32_t count) {
-    Box b;
-    for (int a = 0; a < 3; ++a) { b.lo[a] = INFINITY; b.hi[a] = -INFINITY; }
-    bool nan = false;
-    for (uint32_t j = 0; j < count; ++j) {
-        float4 p = pts[first + j];
-        b.lo[0] = fminf(b.lo[0], p.x); b.hi[0] = fmaxf(b.hi[0], p.x);
-        b.lo[1] = fminf(b.lo[1], p.y); b.hi[1] = fmaxf(b.hi[1], p.y);
-        b.lo[2] = fminf(b.lo[2], p.z); b.hi[2] = fmaxf(b.hi[2], p.z);
-        nan |= isnan(p.x) || isnan(p.y) || isnan(p.z);
-    }
-    // A point with a NaN coordinate is never a neighbour, but no finite box
-    // holds it: the leaf (and, through the unions, every ancestor) gets an
-    // unbounded box, so no search treats such a subtree as lying wholly
-    // inside a ball.
-    if (nan)
-        for (int a = 0; a < 3; ++a) { b.lo[a] = -INFINITY; b.hi[a] = INFINITY; }
-    return b;
-}
-
-__device__ __forceinline__ void store_child_box(BvhNode *nd, int side, const Box &b) {
-    float *f = reinterpret_cast<float *>(nd);
-    // layout: [lo.x0 lo.y0 lo.z0 hi.x0 hi.y0 hi.z0] [lo.x1 .. hi.z1]
-    for (int a = 0; a < 3; ++a) {
-        f[side * 6 + a] = b.lo[a];
-        f[side * 6 + 3 + a] = b.hi[a];
-    }
-}
-
-__device__ __forceinline__ Box load_child_box_cg(const BvhNode *nd, int side) {
-    const float *f = reinterpret_cast<const float *>(nd) + side * 6;
-    Box b;
-    for (int a = 0; a < 3; ++a) {
-        b.lo[a] = __ldcg(f + a);
-        b.hi[a] = __ldcg(f + 3 + a);
-    }
-    return b;
-}
-
-__device__ __forceinline__ Box box_union(const Box &x, const Box &y) {
-    Box b;
-    for (int a = 0; a < 3; ++a) {
-        b.lo[a] = fminf(x.lo[a], y.lo[a]);
-        b.hi[a] = fmaxf(x.hi[a], y.hi[a]);
-    }
-    return b;
-}
-
-__device__ __forceinline__ uint32_t atomic_add_acq_rel(uint32_t *p, uint32_t v) {
-    uint32_t old;
-    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;"
-                 : "=r"(old) : "l"(p), "r"(v) : "memory");
-    return old;
-}
-
-// Bottom-up refit: a thread per node with leaf children computes their
-// boxes; the second arrival at a node (atomic counter) forms its box and
-// carries it to the parent.
-__global__ void __launch_bounds__(BLOCK) refit_kernel(uint32_t n_internal_max,
-                                                      const IndexHeader *h,
-                                                      const float4 *__restrict__ pts,
-                                                      BvhNode *nodes,
-                                                      const uint32_t *__restrict__ cparent,
-                                                      uint32_t *counter) {
-    const uint32_t n_int = h->n_internal;
-    for (uint32_t c = blockIdx.x * BLOCK + threadIdx.x; c < n_int && c < n_internal_max;
-         c += gridDim.x * BLOCK) {
-        uint4 d = nodes[c].d;
-        uint32_t nleaf = 0;
-        Box b;
-        if (d.x & CHILD_LEAF) {
-            b = leaf_box(pts, d.x & CHILD_INDEX, d.z);
-            store_child_box(&nodes[c], 0, b);
-            ++nleaf;
-        }
-        if (d.y & CHILD_LEAF) {
-            Box b1 = leaf_box(pts, d.y & CHILD_INDEX, d.w);
-            store_child_box(&nodes[c], 1, b1);
-            b = nleaf ? box_union(b, b1) : b1;
-            ++nleaf;
-        }
-        if (nleaf == 0) continue;
-        // acq_rel: our box stores are released before the count, and the
-        // second arrival acquires the sibling's stores.
-        uint32_t old = atomic_add_acq_rel(&counter[c], nleaf);
-        if (old + nleaf < 2) continue;
-        if (nleaf == 1) b = box_union(b, load_child_box_cg(&nodes[c], (d.x & CHILD_LEAF) ? 1 : 0));
-        uint32_t cur = c;
-        for (int depth = 0;; ++depth) {
-            if (depth > 128) {   // deeper than any Karras tree: broken parent links
-                atomicOr(&((IndexHeader *)h)->err, DEVERR_DEPTH);
-                break;
-            }
-            uint32_t par = cparent[cur];
-            if (par == CHILD_NONE) break;
-            uint32_t p = par >> 1;
-            int side = (int)(par & 1u);
-            store_child_box(&nodes[p], side, b);
-            if (atomic_add_acq_rel(&counter[p], 1u) == 0u) break;
-            b = box_union(b, load_child_box_cg(&nodes[p], 1 - side));
-            cur = p;
-        }
     }
 }
 
@@ -518,7 +572,7 @@ rtd_status build_typed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStrea
 
 }  // namespace
 
-// Karras tree, leaf collapse and refit over keys already sorted, with
+// Karras tree, leaf collapse and child boxes over keys already sorted, with
 // idx->pts holding the points in key order.
 template <typename K>
 rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStream_t st) {
@@ -527,25 +581,48 @@ rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStr
     if (n < 2 || n <= idx->leaf_size) return RTD_OK;
     const uint64_t ni = n - 1;
     for (rtd::DevBuf *b : {&idx->kleft, &idx->kright, &idx->kfirst, &idx->klast, &idx->kparent,
-                           &idx->flags, &idx->cidx, &idx->cparent, &idx->counter})
+                           &idx->flags, &idx->cidx, &idx->csel})
         RTD_TRY(b->reserve(ni * sizeof(uint32_t)));
+    // box pyramid over the sorted points (levels until one has <= 32 entries)
+    Pyramid P;
+    P.pts = idx->pts.as<float4>();
+    uint64_t sizes[PYR_MAX + 1] = {n}, offs[PYR_MAX + 1] = {0}, total = 0;
+    int nlev = 0;
+    while (sizes[nlev] > 32 && nlev < PYR_MAX) {
+        ++nlev;
+        sizes[nlev] = ceil_div(sizes[nlev - 1], 32);
+        offs[nlev] = total;
+        total += sizes[nlev];
+    }
+    P.nlev = nlev;
+    RTD_TRY(idx->pyramid.reserve((total ? total : 1) * 2 * sizeof(float4)));
+    float4 *pyr = idx->pyramid.as<float4>();
+    for (int j = 0; j <= PYR_MAX; ++j) P.lvl[j] = j >= 1 && j <= nlev ? pyr + 2 * offs[j] : nullptr;
+    if (nlev >= 1) {
+        pyramid_base_kernel<<<(unsigned)ceil_div(n, 1024), 1024, 0, st>>>(
+            P.pts, n, pyr + 2 * offs[1], nlev >= 2 ? pyr + 2 * offs[2] : nullptr);
+        RTD_LAUNCH_CHECK();
+        for (int j = 3; j <= nlev; ++j) {
+            pyramid_level_kernel<<<grid_for(sizes[j] * 32, 256, 148 * 8), 256, 0, st>>>(
+                pyr + 2 * offs[j - 1], sizes[j - 1], pyr + 2 * offs[j], sizes[j]);
+            RTD_LAUNCH_CHECK();
+        }
+    }
     const int gi = grid_for(ni, BLOCK, 148 * 8);
     karras_kernel<K><<<gi, BLOCK, 0, st>>>(skeys, (int64_t)n, idx->leaf_size,
                                            idx->kleft.as<uint32_t>(), idx->kright.as<uint32_t>(),
                                            idx->kfirst.as<uint32_t>(), idx->klast.as<uint32_t>(),
                                            idx->kparent.as<uint32_t>(), idx->flags.as<uint32_t>());
     RTD_LAUNCH_CHECK();
-    RTD_TRY(exclusive_scan_u32_32(idx->flags.as<uint32_t>(), idx->cidx.as<uint32_t>(), ni,
-                                  &h->n_internal, idx->scan, d_err, st));
-    compact_kernel<<<gi, BLOCK, 0, st>>>(
-        (int64_t)n, idx->kleft.as<uint32_t>(), idx->kright.as<uint32_t>(),
-        idx->kfirst.as<uint32_t>(), idx->klast.as<uint32_t>(), idx->kparent.as<uint32_t>(),
-        idx->flags.as<uint32_t>(), idx->cidx.as<uint32_t>(), idx->nodes.as<BvhNode>(),
-        idx->cparent.as<uint32_t>(), idx->counter.as<uint32_t>());
-    RTD_LAUNCH_CHECK();
-    refit_kernel<<<gi, BLOCK, 0, st>>>((uint32_t)ni, h, idx->pts.as<float4>(),
-                                        idx->nodes.as<BvhNode>(), idx->cparent.as<uint32_t>(),
-                                        idx->counter.as<uint32_t>());
+    RTD_TRY(exclusive_scan_select_u32(idx->flags.as<uint32_t>(), idx->cidx.as<uint32_t>(),
+                                      idx->csel.as<uint32_t>(), ni, &h->n_internal, idx->scan,
+                                      d_err, st));
+    // kept nodes: at most (n - 1) / leaf_size of them have more than leaf_size points
+    const uint64_t kept_max = ni / idx->leaf_size + 1 < ni ? ni / idx->leaf_size + 1 : ni;
+    compact_kernel<<<grid_for(kept_max, BLOCK, 148 * 8), BLOCK, 0, st>>>(
+        (uint32_t)ni, h, idx->csel.as<uint32_t>(), idx->kleft.as<uint32_t>(),
+        idx->kright.as<uint32_t>(), idx->kfirst.as<uint32_t>(), idx->klast.as<uint32_t>(),
+        idx->flags.as<uint32_t>(), idx->cidx.as<uint32_t>(), P, idx->nodes.as<BvhNode>());
     RTD_LAUNCH_CHECK();
     return RTD_OK;
 }

@@ -209,12 +209,14 @@ constexpr uint64_t SC_AGG = 1ull << 62;
 constexpr uint64_t SC_INC = 2ull << 62;
 constexpr uint64_t SC_MASK = (1ull << 62) - 1;
 
+// With select != nullptr, also select[out[i]] = i for every i with in[i] != 0
+// (stream compaction of the indices of flagged entries).
 template <typename OutT>
 __global__ void __launch_bounds__(SC_BLOCK) scan_kernel(const uint32_t *__restrict__ in,
                                                         OutT *__restrict__ out, uint64_t n,
                                                         OutT *d_total, uint64_t *status,
                                                         uint32_t *counter, uint32_t ntiles,
-                                                        uint32_t *d_err) {
+                                                        uint32_t *d_err, uint32_t *select) {
     __shared__ uint64_t s_io[SC_TILE];
     __shared__ uint64_t s_warp[SC_BLOCK / 32 + 1];
     __shared__ uint64_t s_prefix;
@@ -303,6 +305,7 @@ __global__ void __launch_bounds__(SC_BLOCK) scan_kernel(const uint32_t *__restri
 #pragma unroll
     for (int i = 0; i < SC_ITEMS; ++i) {
         s_io[tid * SC_ITEMS + i] = run;
+        if (select && v[i]) select[run] = (uint32_t)(base + (uint64_t)tid * SC_ITEMS + i);
         run += v[i];
     }
     __syncthreads();
@@ -314,7 +317,7 @@ __global__ void __launch_bounds__(SC_BLOCK) scan_kernel(const uint32_t *__restri
 
 template <typename OutT>
 rtd_status scan_impl(const uint32_t *in, OutT *out, uint64_t n, OutT *d_total, ScanScratch &scr,
-                     uint32_t *d_err, cudaStream_t stream) {
+                     uint32_t *d_err, cudaStream_t stream, uint32_t *select = nullptr) {
     if (n == 0) {
         if (d_total) RTD_CUDA(cudaMemsetAsync(d_total, 0, sizeof(OutT), stream));
         return RTD_OK;
@@ -327,7 +330,7 @@ rtd_status scan_impl(const uint32_t *in, OutT *out, uint64_t n, OutT *d_total, S
     RTD_CUDA(cudaMemsetAsync(scr.counter.ptr, 0, sizeof(uint32_t), stream));
     scan_kernel<OutT><<<(unsigned)ntiles, SC_BLOCK, 0, stream>>>(
         in, out, n, d_total, scr.status.as<uint64_t>(), scr.counter.as<uint32_t>(),
-        (uint32_t)ntiles, d_err);
+        (uint32_t)ntiles, d_err, select);
     RTD_LAUNCH_CHECK();
     return RTD_OK;
 }
@@ -390,6 +393,11 @@ rtd_status exclusive_scan_u32(const uint32_t *in, uint64_t *out, uint64_t n, uin
 rtd_status exclusive_scan_u32_32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *d_total,
                                  ScanScratch &scr, uint32_t *d_err, cudaStream_t stream) {
     return scan_impl<uint32_t>(in, out, n, d_total, scr, d_err, stream);
+}
+rtd_status exclusive_scan_select_u32(const uint32_t *in, uint32_t *out, uint32_t *select,
+                                     uint64_t n, uint32_t *d_total, ScanScratch &scr,
+                                     uint32_t *d_err, cudaStream_t stream) {
+    return scan_impl<uint32_t>(in, out, n, d_total, scr, d_err, stream, select);
 }
 
 }  // namespace rtd

@@ -40,5 +40,10 @@ rtd_status exclusive_scan_u32(const uint32_t *in, uint64_t *out, uint64_t n, uin
 // Same, 32-bit output (caller guarantees the sum fits).
 rtd_status exclusive_scan_u32_32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *d_total,
                                  ScanScratch &scr, uint32_t *d_err, cudaStream_t stream);
+// Same for 0/1 flags, also writing select[out[i]] = i where in[i] != 0:
+// the indices of the flagged entries in order.
+rtd_status exclusive_scan_select_u32(const uint32_t *in, uint32_t *out, uint32_t *select,
+                                     uint64_t n, uint32_t *d_total, ScanScratch &scr,
+                                     uint32_t *d_err, cudaStream_t stream);
 
 }  // namespace rtd
