@@ -213,14 +213,15 @@ __device__ __forceinline__ void item_thread(const BatchArgs &a, const TreeRef &t
 
 template <int S>
 __device__ __forceinline__ void item_warp(const BatchArgs &a, const TreeRef &t, const RoundSpec &rs,
-                                          const CloudDesc &c, const WorkItem &w, uint2 *stk) {
+                                          const CloudDesc &c, const WorkItem &w, uint2 *stk,
+                                          uint2 *ls) {
     const int lane = threadIdx.x & 31;
     for (uint32_t j = 0; j < w.count; ++j) {
         const uint32_t qi = a.qperm[w.start + j];
         const float qx = a.q[3 * (uint64_t)qi], qy = a.q[3 * (uint64_t)qi + 1], qz = a.q[3 * (uint64_t)qi + 2];
         float lk[S];
         uint32_t li[S];
-        knn_query_warp<S>(t, rs, qx, qy, qz, c.k, stk, a.err, lk, li);
+        knn_query_warp<S>(t, rs, qx, qy, qz, c.k, stk, ls, a.err, lk, li);
         const uint64_t ob = c.out_off + (uint64_t)(qi - c.q_begin) * c.k;
 #pragma unroll
         for (int s = 0; s < S; ++s) {
@@ -245,6 +246,8 @@ __global__ void __launch_bounds__(SWARPS * 32) batch_knn_kernel(const BatchArgs 
     constexpr bool THREAD = CLS < 2;
     __shared__ uint2 s_stack[THREAD ? SHORT_STACK : 1][SWARPS * 32];
     __shared__ uint2 s_wstack[THREAD ? 1 : SWARPS][THREAD ? 1 : STACK_MAX];
+    constexpr int LIST = CLS == 2 ? 32 : CLS == 3 ? 64 : 256;
+    __shared__ uint2 s_list[THREAD ? 1 : SWARPS][THREAD ? 1 : LIST];
     uint2 l_stack[THREAD ? STACK_MAX - SHORT_STACK : 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t visit_cap = 2u * a.hdr->n_internal + 4u;
@@ -259,9 +262,9 @@ __global__ void __launch_bounds__(SWARPS * 32) batch_knn_kernel(const BatchArgs 
         const RoundSpec rs{c.r0sq, a.mult2, a.max_rounds};
         if constexpr (CLS == 0) item_thread<8>(a, t, rs, c, w, &s_stack[0][threadIdx.x], l_stack);
         else if constexpr (CLS == 1) item_thread<16>(a, t, rs, c, w, &s_stack[0][threadIdx.x], l_stack);
-        else if constexpr (CLS == 2) item_warp<1>(a, t, rs, c, w, s_wstack[warp]);
-        else if constexpr (CLS == 3) item_warp<2>(a, t, rs, c, w, s_wstack[warp]);
-        else item_warp<8>(a, t, rs, c, w, s_wstack[warp]);
+        else if constexpr (CLS == 2) item_warp<1>(a, t, rs, c, w, s_wstack[warp], s_list[warp]);
+        else if constexpr (CLS == 3) item_warp<2>(a, t, rs, c, w, s_wstack[warp], s_list[warp]);
+        else item_warp<8>(a, t, rs, c, w, s_wstack[warp], s_list[warp]);
         __syncwarp();
     }
 }

@@ -392,13 +392,12 @@ __global__ void __launch_bounds__(WARPS * 32) knn_packet_kernel(const KnnArgs p)
     }
 }
 
-// One warp per query.  The sorted list of S*32 slots is striped over the
-// lanes (slot j lives in lane j % 32, register j / 32); candidates from a
-// leaf are tested one per lane and inserted with ballots and shuffles.
+// One warp per query (knn_query_warp).
 template <int S, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) knn_warp_kernel(const KnnArgs p) {
     __shared__ BvhNode s_top[TOP_MAX];
     __shared__ uint2 s_stack[WARPS][STACK_MAX];
+    __shared__ uint2 s_list[WARPS][S * 32];
     const IndexHeader *h = p.ix.hdr;
     const uint32_t ntop = h->n_top;
     for (uint32_t i = threadIdx.x; i < ntop; i += WARPS * 32) s_top[i] = p.ix.top[i];
@@ -416,7 +415,7 @@ __global__ void __launch_bounds__(WARPS * 32) knn_warp_kernel(const KnnArgs p) {
         const float qx = p.q[3 * qi], qy = p.q[3 * qi + 1], qz = p.q[3 * qi + 2];
         float lk[S];
         uint32_t li[S];
-        knn_query_warp<S>(tree, rs, qx, qy, qz, kk, stk, p.err, lk, li);
+        knn_query_warp<S>(tree, rs, qx, qy, qz, kk, stk, s_list[warp], p.err, lk, li);
         const uint64_t ob = qi * (uint64_t)kk;
 #pragma unroll
         for (int s = 0; s < S; ++s) {

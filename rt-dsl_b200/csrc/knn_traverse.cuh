@@ -161,17 +161,83 @@ __device__ __forceinline__ void knn_query_thread(const TreeRef &t, const RoundSp
     }
 }
 
+// Merges the candidates of one batch (lane i holds (key, id) when acc) into
+// a sorted list of kk <= S*32 slots striped over the warp (slot j in lane
+// j % 32, register j / 32; slots >= kk stay empty).  For every accepted
+// candidate, broadcast in turn, a ballot per register counts the list
+// entries before it and each lane counts how many candidates precede its
+// own entries and its own candidate; every item then lands at its merged
+// position through the warp's shared scratch ls (S*32 entries), and items
+// past kk drop out.  (key, id) pairs are distinct, so the order is strict.
+template <int S>
+__device__ __forceinline__ void warp_list_merge(float (&lk)[S], uint32_t (&li)[S], uint32_t kk,
+                                                bool acc, float key, uint32_t id, uint2 *ls,
+                                                float &wk, uint32_t &wi) {
+    const int lane = threadIdx.x & 31;
+    uint32_t m = __ballot_sync(0xffffffffu, acc);
+    if (!m) return;
+    int before[S];                 // candidates ordered before each of my entries
+#pragma unroll
+    for (int s = 0; s < S; ++s) before[s] = 0;
+    int r_list = 0, r_cand = 0;    // for my candidate: entries / candidates before it
+    while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        const float ck = __shfl_sync(0xffffffffu, key, src);
+        const uint32_t ci = __shfl_sync(0xffffffffu, id, src);
+        int n_before = 0;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const bool in_list = (uint32_t)(s * 32 + lane) < kk;
+            const bool e_lt = in_list && key_less(lk[s], li[s], ck, ci);
+            n_before += __popc(__ballot_sync(0xffffffffu, e_lt));
+            before[s] += (in_list && !e_lt) ? 1 : 0;
+        }
+        if (lane == src) r_list = n_before;
+        if (acc && key_less(ck, ci, key, id)) ++r_cand;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const uint32_t j = (uint32_t)(s * 32 + lane);
+        const uint32_t pos = j + (uint32_t)before[s];
+        if (j < kk && pos < kk) ls[pos] = make_uint2(__float_as_uint(lk[s]), li[s]);
+    }
+    if (acc) {
+        const uint32_t pos = (uint32_t)(r_list + r_cand);
+        if (pos < kk) ls[pos] = make_uint2(__float_as_uint(key), id);
+    }
+    __syncwarp();
+    const int wslot = (int)((kk - 1) >> 5), wlane = (int)((kk - 1) & 31);
+    float nk = 0.f;
+    uint32_t ni = 0;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const uint32_t j = (uint32_t)(s * 32 + lane);
+        if (j < kk) {
+            const uint2 e = ls[j];
+            lk[s] = __uint_as_float(e.x);
+            li[s] = e.y;
+        }
+        if (s == wslot) { nk = lk[s]; ni = li[s]; }
+    }
+    __syncwarp();
+    wk = __shfl_sync(0xffffffffu, nk, wlane);
+    wi = __shfl_sync(0xffffffffu, ni, wlane);
+}
+
 // Warp per query: the sorted list of S*32 slots is striped over the lanes
-// (slot j in lane j % 32, register j / 32); candidates from a leaf are
-// tested one per lane and inserted with ballots and shuffles.  stk is the
-// warp's shared-memory stack (STACK_MAX entries).  All arguments must be
-// warp-uniform.
+// (slot j in lane j % 32, register j / 32); the candidates of a node's leaf
+// children are tested one per lane and the accepted ones merged into the
+// list in one batch (warp_list_merge).  stk is the warp's shared-memory
+// stack (STACK_MAX entries), ls its list scratch (S*32 entries).  All
+// arguments must be warp-uniform.
 template <int S>
 __device__ __forceinline__ void knn_query_warp(const TreeRef &t, const RoundSpec &rs, float qx,
                                                float qy, float qz, uint32_t kk, uint2 *stk,
-                                               uint32_t *err, float (&lk)[S], uint32_t (&li)[S]) {
+                                               uint2 *ls, uint32_t *err, float (&lk)[S],
+                                               uint32_t (&li)[S]) {
     const int lane = threadIdx.x & 31;
-    const int wslot = (int)((kk - 1) >> 5), wlane = (int)((kk - 1) & 31);
 #pragma unroll
     for (int s = 0; s < S; ++s) { lk[s] = INFINITY; li[s] = EMPTY_ID; }
     float wk = INFINITY;
@@ -214,53 +280,20 @@ __device__ __forceinline__ void knn_query_warp(const TreeRef &t, const RoundSpec
                 if (v0 && (d.x & CHILD_LEAF)) { lf_first[nleaf] = d.x & CHILD_INDEX; lf_cnt[nleaf] = d.z; ++nleaf; v0 = false; }
                 if (v1 && (d.y & CHILD_LEAF)) { lf_first[nleaf] = d.y & CHILD_INDEX; lf_cnt[nleaf] = d.w; ++nleaf; v1 = false; }
             }
-            for (int l = 0; l < nleaf; ++l) {
-                for (uint32_t j0 = 0; j0 < lf_cnt[l]; j0 += 32) {
+            if (nleaf) {   // both leaves' points, 32 per batch
+                const uint32_t c0 = lf_cnt[0], tot = c0 + (nleaf > 1 ? lf_cnt[1] : 0u);
+                for (uint32_t j0 = 0; j0 < tot; j0 += 32) {
+                    const uint32_t j = j0 + lane;
                     float key = INFINITY;
                     uint32_t id = EMPTY_ID;
                     bool acc = false;
-                    if (j0 + lane < lf_cnt[l]) {
-                        float4 pt = __ldg(&t.pts[lf_first[l] + j0 + lane]);
+                    if (j < tot) {
+                        const float4 pt = __ldg(&t.pts[j < c0 ? lf_first[0] + j : lf_first[1] + (j - c0)]);
                         key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
                         id = __float_as_uint(pt.w);
                         acc = key <= bound && key > prev && key_less(key, id, wk, wi);
                     }
-                    uint32_t m = __ballot_sync(0xffffffffu, acc);
-                    while (m) {
-                        int src = __ffs(m) - 1;
-                        m &= m - 1;
-                        float ck = __shfl_sync(0xffffffffu, key, src);
-                        uint32_t ci = __shfl_sync(0xffffffffu, id, src);
-                        if (!key_less(ck, ci, wk, wi)) continue;   // warp-uniform
-                        // position = number of slots ordered before the candidate
-                        int pos = 0;
-#pragma unroll
-                        for (int s = 0; s < S; ++s)
-                            pos += __popc(__ballot_sync(0xffffffffu, key_less(lk[s], li[s], ck, ci)));
-                        // shift slots >= pos up by one
-                        float carry_k = INFINITY;
-                        uint32_t carry_i = EMPTY_ID;
-#pragma unroll
-                        for (int s = 0; s < S; ++s) {
-                            float upk = __shfl_up_sync(0xffffffffu, lk[s], 1);
-                            uint32_t upi = __shfl_up_sync(0xffffffffu, li[s], 1);
-                            float topk = __shfl_sync(0xffffffffu, lk[s], 31);
-                            uint32_t topi = __shfl_sync(0xffffffffu, li[s], 31);
-                            if (lane == 0) { upk = carry_k; upi = carry_i; }
-                            int j = s * 32 + lane;
-                            if (j > pos) { lk[s] = upk; li[s] = upi; }
-                            else if (j == pos) { lk[s] = ck; li[s] = ci; }
-                            carry_k = topk;
-                            carry_i = topi;
-                        }
-                        float nk = 0.f;
-                        uint32_t ni = 0;
-#pragma unroll
-                        for (int s = 0; s < S; ++s)
-                            if (s == wslot) { nk = lk[s]; ni = li[s]; }
-                        wk = __shfl_sync(0xffffffffu, nk, wlane);
-                        wi = __shfl_sync(0xffffffffu, ni, wlane);
-                    }
+                    warp_list_merge<S>(lk, li, kk, acc, key, id, ls, wk, wi);
                 }
                 lim = fminf(bound, wk);
             }
