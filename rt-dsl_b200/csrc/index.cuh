@@ -73,6 +73,7 @@ struct rtd_index {
     rtd::DevBuf sample, seed;
     // search scratch
     rtd::DevBuf qkeys, qkeys_alt, qperm, qperm_alt;
+    const void *skeys = nullptr;   // the points' sorted Morton keys (in keys or keys_alt)
     rtd::DevBuf rcounts, roffsets, rcursor, rpairs_alt, rkeys, rkeys_alt;
     // What the last range count left behind for a fill of the same queries:
     // per-query exclusive offsets (roffsets), the total, and the query order.
@@ -107,6 +108,35 @@ enum : int { EV_BUILD0 = 0, EV_BUILD_SORTED, EV_BUILD1, EV_SEARCH0, EV_SEEDED, E
 }  // namespace rtd
 
 namespace rtd {
+
+// Normalisation of the Morton quantisation: the scene box (per axis) or its
+// cube (one extent, the largest).
+struct SceneNorm {
+    float lo[3], ext[3];
+};
+__device__ __forceinline__ SceneNorm scene_norm(const IndexHeader *h) {
+    SceneNorm s;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float lo = float_unflip(h->box[a]), hi = float_unflip(h->box[3 + a]);
+        s.lo[a] = lo;
+        // morton.rs:37-39: extent clamped to >= 1e-6
+        s.ext[a] = fmaxf(__fsub_rn(hi, lo), 1e-6f);
+    }
+    return s;
+}
+
+// One extent for all three axes (the largest): every Morton bit level then
+// halves the same length on each axis, so a flat or elongated cloud is split
+// along its long axes first.  With an extent per axis, the top levels of a
+// thin sheet's tree would split its thickness and give every node a box
+// spanning the whole sheet.
+__device__ __forceinline__ SceneNorm scene_norm_cubic(const IndexHeader *h) {
+    SceneNorm s = scene_norm(h);
+    const float e = fmaxf(s.ext[0], fmaxf(s.ext[1], s.ext[2]));
+    s.ext[0] = s.ext[1] = s.ext[2] = e;
+    return s;
+}
 
 // Arguments the search kernels need from an index.
 struct IndexView {

@@ -20,7 +20,57 @@ struct KnnArgs {
     uint32_t *ids;
     float *d2;
     uint32_t *err;
+    // Morton-window seed (RTD_RADIUS_MORTON_WINDOW): the points' sorted keys
+    // (u64 when key64, else u32) and the quantisation scale of the build
+    const void *skeys;
+    int key64;
+    float scale;
 };
+
+// Seeds a query's list with the 2k points around its position in the
+// points' Morton order (found by binary search over the sorted keys, with
+// the build's quantisation); returns that window [w0, w1) of sorted indices.
+template <int KC>
+__device__ __forceinline__ void morton_window_seed(const KnnArgs &p, float qx, float qy, float qz,
+                                                   int kk, float (&bk)[KC], uint32_t (&bi)[KC],
+                                                   uint32_t &w0, uint32_t &w1) {
+    const IndexHeader *h = p.ix.hdr;
+    const uint32_t n = (uint32_t)p.ix.n;
+    uint32_t lo = 0, hi = n;
+    if (p.key64) {
+        const SceneNorm s = scene_norm_cubic(h);
+        const uint64_t key = morton63(quantize(qx, s.lo[0], s.ext[0], p.scale),
+                                      quantize(qy, s.lo[1], s.ext[1], p.scale),
+                                      quantize(qz, s.lo[2], s.ext[2], p.scale));
+        const uint64_t *sk = static_cast<const uint64_t *>(p.skeys);
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(&sk[mid]) < key) lo = mid + 1;
+            else hi = mid;
+        }
+    } else {
+        const SceneNorm s = scene_norm(h);
+        const uint32_t key = morton30(quantize(qx, s.lo[0], s.ext[0], 1023.0f),
+                                      quantize(qy, s.lo[1], s.ext[1], 1023.0f),
+                                      quantize(qz, s.lo[2], s.ext[2], 1023.0f));
+        const uint32_t *sk = static_cast<const uint32_t *>(p.skeys);
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(&sk[mid]) < key) lo = mid + 1;
+            else hi = mid;
+        }
+    }
+    const uint32_t w = 2u * (uint32_t)kk < n ? 2u * (uint32_t)kk : n;
+    w0 = lo > (uint32_t)kk ? lo - (uint32_t)kk : 0u;
+    if (w0 + w > n) w0 = n - w;
+    w1 = w0 + w;
+    for (uint32_t j = w0; j < w1; ++j) {
+        const float4 pt = __ldg(&p.ix.pts[j]);
+        const float key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
+        const uint32_t id = __float_as_uint(pt.w);
+        if (key_less(key, id, bk[KC - 1], bi[KC - 1])) list_insert<KC>(bk, bi, key, id);
+    }
+}
 
 // One thread per query.
 template <int KC, int BLOCK>
@@ -44,8 +94,19 @@ __global__ void __launch_bounds__(BLOCK) knn_thread_kernel(const KnnArgs p) {
         const float qx = p.q[3 * qi], qy = p.q[3 * qi + 1], qz = p.q[3 * qi + 2];
         float bk[KC];
         uint32_t bi[KC];
-        knn_query_thread<KC>(tree, rs, qx, qy, qz, kk, &s_stack[0][threadIdx.x], BLOCK, l_stack,
-                             p.err, bk, bi);
+        if (p.skeys) {
+            // one unbounded round from a list seeded with the query's
+            // Morton neighbours
+            list_init<KC>(bk, bi, kk);
+            uint32_t w0 = 0, w1 = 0;
+            if (h->root != CHILD_NONE) morton_window_seed<KC>(p, qx, qy, qz, kk, bk, bi, w0, w1);
+            const RoundSpec one{rs.r0sq, rs.mult2, 1u};
+            knn_query_thread<KC, true>(tree, one, qx, qy, qz, kk, &s_stack[0][threadIdx.x], BLOCK,
+                                       l_stack, p.err, bk, bi, w0, w1);
+        } else {
+            knn_query_thread<KC>(tree, rs, qx, qy, qz, kk, &s_stack[0][threadIdx.x], BLOCK,
+                                 l_stack, p.err, bk, bi);
+        }
         const uint64_t ob = qi * (uint64_t)kk;
 #pragma unroll
         for (int j = 0; j < KC; ++j) {
@@ -579,7 +640,10 @@ rtd_status seed_radius(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k
         break;
     case RTD_RADIUS_FIXED:
     case RTD_RADIUS_SAMPLED_NN:
-        seed_set_kernel<<<1, 1, 0, st>>>(h, s.radius_heuristic, s.radius_param);
+    case RTD_RADIUS_MORTON_WINDOW:
+        seed_set_kernel<<<1, 1, 0, st>>>(
+            h, s.radius_heuristic == RTD_RADIUS_FIXED ? RTD_RADIUS_FIXED : RTD_RADIUS_SAMPLED_NN,
+            s.radius_param);
         break;
     default:
         return fail(RTD_ERR_INVALID_ARGUMENT, "unknown radius heuristic");
@@ -628,6 +692,9 @@ rtd_status knn_search_ex(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t
     a.ids = d_ids;
     a.d2 = d_d2;
     a.err = &idx->hdr.as<IndexHeader>()->err;
+    a.skeys = nullptr;
+    a.key64 = idx->morton_bits != 30;
+    a.scale = idx->morton_bits == 30 ? 1023.0f : (float)((1u << (idx->morton_bits / 3)) - 1u);
     uint32_t lanes = s.lanes_per_query;
     if (lanes == 0) lanes = k <= 16 ? 1 : 32;
     if (lanes == 1 && k > 32) lanes = 32;
@@ -657,6 +724,9 @@ rtd_status knn_search_ex(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t
         else if (k <= 16) r = launch_refill<16>(a, block, ctr, st);
         else r = launch_refill<32>(a, block, ctr, st);
     } else if (lanes == 1) {
+        // The Morton-window seed runs in the thread-per-query kernel; the
+        // other launch modes treat the heuristic as RTD_RADIUS_SAMPLED_NN.
+        if (s.radius_heuristic == RTD_RADIUS_MORTON_WINDOW && idx->n > 1) a.skeys = idx->skeys;
         if (k <= 1) r = launch_thread<1>(a, block, st);
         else if (k <= 2) r = launch_thread<2>(a, block, st);
         else if (k <= 4) r = launch_thread<4>(a, block, st);

@@ -64,21 +64,31 @@ __device__ __forceinline__ void list_insert(float (&bk)[KC], uint32_t (&bi)[KC],
     if (key_less(key, id, bk[0], bi[0])) { bk[0] = key; bi[0] = id; }
 }
 
-// Thread per query: the register list ends holding the k best (key, id)
-// pairs in slots KC-k .. KC-1.  The stack keeps SHORT_STACK entries in this
-// thread's shared-memory column (s_col[sp * s_stride]) and the rest in
-// l_stack (local memory).
+// Empty register list for k <= KC: slots before KC-k hold -inf and never
+// move; slot KC-1 is the k-th best.
 template <int KC>
-__device__ __forceinline__ void knn_query_thread(const TreeRef &t, const RoundSpec &rs, float qx,
-                                                 float qy, float qz, int kk, uint2 *s_col,
-                                                 int s_stride, uint2 *l_stack, uint32_t *err,
-                                                 float (&bk)[KC], uint32_t (&bi)[KC]) {
+__device__ __forceinline__ void list_init(float (&bk)[KC], uint32_t (&bi)[KC], int kk) {
 #pragma unroll
     for (int j = 0; j < KC; ++j) {
         bool pad = j < KC - kk;
         bk[j] = pad ? -INFINITY : INFINITY;
         bi[j] = pad ? 0u : EMPTY_ID;
     }
+}
+
+// Thread per query: the register list ends holding the k best (key, id)
+// pairs in slots KC-k .. KC-1.  The stack keeps SHORT_STACK entries in this
+// thread's shared-memory column (s_col[sp * s_stride]) and the rest in
+// l_stack (local memory).  SEEDED: the caller has already put the points
+// with sorted indices [skip_lo, skip_hi) through the list, so leaves skip
+// them; otherwise the list starts empty.
+template <int KC, bool SEEDED = false>
+__device__ __forceinline__ void knn_query_thread(const TreeRef &t, const RoundSpec &rs, float qx,
+                                                 float qy, float qz, int kk, uint2 *s_col,
+                                                 int s_stride, uint2 *l_stack, uint32_t *err,
+                                                 float (&bk)[KC], uint32_t (&bi)[KC],
+                                                 uint32_t skip_lo = 0, uint32_t skip_hi = 0) {
+    if (!SEEDED) list_init<KC>(bk, bi, kk);
     const bool valid = t.root != CHILD_NONE && !isnan(qx) && !isnan(qy) && !isnan(qz);
     float bound = rs.r0sq > 0.0f ? rs.r0sq : 1e-30f, prev = -1.0f;
     for (uint32_t round = 0; valid; ++round) {
@@ -119,6 +129,7 @@ __device__ __forceinline__ void knn_query_thread(const TreeRef &t, const RoundSp
             }
             for (int l = 0; l < nleaf; ++l) {
                 for (uint32_t j = 0; j < lf_cnt[l]; ++j) {
+                    if (SEEDED && lf_first[l] + j - skip_lo < skip_hi - skip_lo) continue;
                     float4 pt = __ldg(&t.pts[lf_first[l] + j]);
                     float key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
                     uint32_t id = __float_as_uint(pt.w);

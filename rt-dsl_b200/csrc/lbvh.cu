@@ -61,33 +61,6 @@ __global__ void __launch_bounds__(BLOCK) bbox_kernel(const float *__restrict__ x
     }
 }
 
-struct SceneNorm {
-    float lo[3], ext[3];
-};
-__device__ __forceinline__ SceneNorm scene_norm(const IndexHeader *h) {
-    SceneNorm s;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        float lo = float_unflip(h->box[a]), hi = float_unflip(h->box[3 + a]);
-        s.lo[a] = lo;
-        // morton.rs:37-39: extent clamped to >= 1e-6
-        s.ext[a] = fmaxf(__fsub_rn(hi, lo), 1e-6f);
-    }
-    return s;
-}
-
-// One extent for all three axes (the largest): every Morton bit level then
-// halves the same length on each axis, so a flat or elongated cloud is split
-// along its long axes first.  With an extent per axis, the top levels of a
-// thin sheet's tree would split its thickness and give every node a box
-// spanning the whole sheet.
-__device__ __forceinline__ SceneNorm scene_norm_cubic(const IndexHeader *h) {
-    SceneNorm s = scene_norm(h);
-    const float e = fmaxf(s.ext[0], fmaxf(s.ext[1], s.ext[2]));
-    s.ext[0] = s.ext[1] = s.ext[2] = e;
-    return s;
-}
-
 // 30-bit codes follow compute_morton_codes (gprt-core/src/morton.rs:19-48),
 // extent per axis; wider codes (B = bits / 3 per axis, scale = 2^B - 1,
 // B <= 21, interleaved in the low 3B bits of a u64) use one cubic extent.
@@ -563,6 +536,7 @@ rtd_status build_typed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStrea
                                 idx->vals_alt.as<uint32_t>(), true, n, 0, kbits, idx->sort, d_err,
                                 st, &in_alt));
     K *skeys = in_alt ? idx->keys_alt.as<K>() : idx->keys.as<K>();
+    idx->skeys = skeys;
     uint32_t *perm = in_alt ? idx->vals_alt.as<uint32_t>() : idx->vals.as<uint32_t>();
     gather_points_kernel<<<g, BLOCK, 0, st>>>(d_xyz, perm, n, idx->pts.as<float4>());
     RTD_LAUNCH_CHECK();
@@ -650,6 +624,7 @@ rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd
         return fail(RTD_ERR_INVALID_ARGUMENT, "morton_bits must be 30 or a multiple of 3 in [33, 63]");
     RTD_CUDA(cudaGetDevice(&idx->device));
     idx->rtoken.valid = false;
+    idx->skeys = nullptr;
     idx->n = n;
     idx->leaf_size = s->leaf_size;
     idx->morton_bits = mb;

@@ -5,7 +5,7 @@ of include/rtdsl.h); this package binds it with ctypes and mirrors the
 reference's k_nn! / range_query! / barnes_hut! interface.
 """
 from ._capi import (BH_LAW_PLUMMER, BH_LAW_REFERENCE, EMPTY_ID, RADIUS_FIXED,
-                    RADIUS_SAMPLED_MAX, RADIUS_SAMPLED_NN, RADIUS_SAMPLED_PERCENTILE, BhParams,
+                    RADIUS_MORTON_WINDOW, RADIUS_SAMPLED_MAX, RADIUS_SAMPLED_NN, RADIUS_SAMPLED_PERCENTILE, BhParams,
                     RtdError, Schedule, default_batch_schedule, default_bh_params,
                     default_schedule, load)
 from .api import (Context, Index, dbscan, k_nn, k_nn_array, knn_backward, range_query,
@@ -14,7 +14,8 @@ from .batch import Batch
 from .bh import BarnesHut, barnes_hut
 
 __all__ = [
-    "BH_LAW_PLUMMER", "BH_LAW_REFERENCE", "EMPTY_ID", "RADIUS_FIXED", "RADIUS_SAMPLED_MAX",
+    "BH_LAW_PLUMMER", "BH_LAW_REFERENCE", "EMPTY_ID", "RADIUS_FIXED", "RADIUS_MORTON_WINDOW",
+    "RADIUS_SAMPLED_MAX",
     "RADIUS_SAMPLED_NN", "RADIUS_SAMPLED_PERCENTILE", "BhParams", "RtdError", "Schedule",
     "default_batch_schedule", "default_bh_params", "default_schedule", "load", "Context", "Index", "k_nn", "k_nn_array",
     "knn_backward", "range_query", "spatial_join", "dbscan", "Batch", "BarnesHut", "barnes_hut",

@@ -25,6 +25,7 @@ RADIUS_SAMPLED_NN = 0
 RADIUS_SAMPLED_PERCENTILE = 1
 RADIUS_FIXED = 2
 RADIUS_SAMPLED_MAX = 3
+RADIUS_MORTON_WINDOW = 4
 
 EMPTY_ID = 0xFFFFFFFF
 

@@ -3,10 +3,10 @@
 The reference tunes its Schedule offline and stores it as gprt_wisdom.json
 (gprt-sandbox/src/main.rs:53-77; grid + subsample funnel in
 gprt-profiler/src/main.rs:40-126; hill-climb in gprt-macros/src/lib.rs:
-120-214).  Here the knobs are the LBVH leaf size, the initial-radius
-multiplier and growth factor of the in-kernel radius expansion, the block
-size, and the traversal mode (thread per query, 32-query packets, warp per
-query).  Because every candidate returns identical results (exact search),
+120-214).  Here the knobs are the LBVH leaf size and key width, the
+initial-radius heuristic (sampled 1-NN radius with its multiplier and growth
+factor, or the Morton-window seed), the block size, and the traversal mode
+(thread or warp per query).  Because every candidate returns identical results (exact search),
 the tuner only times them; it still checks each candidate's ids against the
 first candidate's and refuses one that differs.
 
@@ -26,11 +26,13 @@ from . import _capi
 WISDOM = os.path.join(os.path.dirname(os.path.abspath(__file__)), "wisdom.json")
 
 DEFAULT_GRID = {
-    "leaf_size": [1, 2, 4, 8],
+    "leaf_size": [2, 4, 5, 8],
+    "morton_bits": [39, 42, 48],
+    "radius_heuristic": [_capi.RADIUS_SAMPLED_NN, _capi.RADIUS_MORTON_WINDOW],
     "radius_param": [0.0625, 0.25, 0.5, 1.0],
     "radius_increment_mult": [2.0, 4.0],
-    "block_size": [64, 128, 256],
-    "mode": ["thread", "packet", "warp"],
+    "block_size": [128, 256],
+    "mode": ["thread", "warp"],
 }
 
 _MODES = {"thread": dict(lanes_per_query=1, packet_traversal=2, lane_refill=2),
@@ -99,13 +101,23 @@ def tune_knn(P, Q, k: int, tag: str, grid: dict | None = None, reps: int = 3,
     from .api import Index
     grid = grid or DEFAULT_GRID
     keys = list(grid)
-    cands = []
+    cands, seen = [], set()
     for combo in itertools.product(*(grid[k_] for k_ in keys)):
         kw = dict(zip(keys, combo))
         mode = kw.pop("mode", "thread")
         if mode != "warp" and k > 32:
             continue
+        if kw.get("radius_heuristic") == _capi.RADIUS_MORTON_WINDOW:
+            if mode != "thread":
+                continue   # the window seed runs in the thread-per-query kernel only
+            # one unbounded round: the radius knobs do not apply
+            kw["radius_param"] = grid.get("radius_param", [0.5])[0]
+            kw["radius_increment_mult"] = grid.get("radius_increment_mult", [2.0])[0]
         kw.update(_MODES[mode])
+        key = tuple(sorted(kw.items()))
+        if key in seen:
+            continue
+        seen.add(key)
         cands.append(kw)
     Qs = Q[:: max(1, subsample)].contiguous()
     ref_ids = None
@@ -243,9 +255,11 @@ def main():
     pts, q = workloads.clustered()
     P = torch.from_numpy(pts).cuda()
     Q = torch.from_numpy(q).cuda()
-    grid = {"leaf_size": [2, 4, 8], "radius_param": [0.25, 0.5, 1.0],
-            "radius_increment_mult": [2.0, 4.0], "block_size": [64, 128, 256],
-            "morton_bits": [42, 48, 63], "mode": ["thread", "warp"]}
+    grid = {"leaf_size": [2, 3, 4, 5, 6, 8], "radius_param": [0.25, 0.5, 1.0],
+            "radius_increment_mult": [2.0, 4.0], "block_size": [128, 256],
+            "morton_bits": [39, 42, 48],
+            "radius_heuristic": [_capi.RADIUS_SAMPLED_NN, _capi.RADIUS_MORTON_WINDOW],
+            "mode": ["thread", "warp"]}
     best, table = tune_knn(P, Q, 5, "clustered_1p8m_k5", grid=grid, log=log)
     log(f"clustered_1p8m_k5 best {table[0]}")
     cl = workloads.clouds()

@@ -64,7 +64,8 @@ def wisdom_from_schedule(s: Schedule) -> dict:
     elif s.radius_heuristic == RADIUS_FIXED:
         d["radius_heuristic"] = {"Fixed": float(s.radius_param)}
     else:
-        raise ValueError("the sampled-NN seed has no counterpart in the reference's Schedule")
+        raise ValueError("the sampled-NN and Morton-window seeds have no counterpart in the "
+                         "reference's Schedule")
     return d
 
 

@@ -82,12 +82,34 @@ def test_knn_leaf_and_key_width(rtd, orc, cuda, leaf, bits):
 
 
 @pytest.mark.parametrize("heur,param", [(0, 2 ** -4), (1, 0.10), (1, 0.02), (2, 1e-6),
-                                        (2, 100.0), (3, 0.0)])
+                                        (2, 100.0), (3, 0.0), (4, 0.5)])
 def test_knn_radius_heuristics_do_not_change_results(rtd, orc, cuda, heur, param):
     pts, q = clustered_small(n=20_000, nq=2_000, seed=14)
     ids, d2, _ = gpu_knn(rtd, pts, q, 8, radius_heuristic=heur, radius_param=param)
     oi, od = orc.knn(pts, q, 8)
     assert_same(oi, od, ids, d2)
+
+
+@pytest.mark.parametrize("k", [1, 5, 16, 40])
+@pytest.mark.parametrize("bits", [30, 42, 63])
+def test_knn_morton_window_seed(rtd, orc, cuda, k, bits):
+    """RTD_RADIUS_MORTON_WINDOW: lists seeded with each query's 2k Morton
+    neighbours, then one unbounded round that skips them; ids and keys equal
+    the oracle's for every key width, for duplicates, far queries and tiny
+    clouds (k = 40 takes the warp path, where the heuristic is the sampled
+    1-NN radius)."""
+    pts, q = clustered_small(n=20_000, nq=2_000, seed=19)
+    rng = np.random.default_rng(19)
+    pts = np.concatenate([pts, pts[:500]])                        # exact duplicates
+    q = np.concatenate([q, rng.uniform(-50.0, 60.0, size=(200, 3)).astype(np.float32)])
+    ids, d2, _ = gpu_knn(rtd, pts, q, k, radius_heuristic=4, radius_param=0.5, morton_bits=bits,
+                         leaf_size=8)
+    oi, od = orc.knn(pts, q, k)
+    assert_same(oi, od, ids, d2)
+    for n in (1, 3, 2 * k + 1):
+        ids, d2, _ = gpu_knn(rtd, pts[:n], q[:50], k, radius_heuristic=4, morton_bits=bits)
+        oi, od = orc.knn(pts[:n], q[:50], k)
+        assert_same(oi, od, ids, d2)
 
 
 @pytest.mark.parametrize("mult,rounds", [(2.0, 1), (2.0, 2), (1.05, 32), (3.0, 30), (64.0, 4)])
