@@ -144,6 +144,29 @@ def traffic_for(kernel: str, workload: str):
     return None if e is None else e.get("dram_bytes_per_launch")
 
 
+def copy_bandwidth(h_in, h_out, dev, reps: int = 10):
+    """Median pinned host-to-device and device-to-host bandwidth (GB/s) for
+    copies of h_in's and h_out's sizes, timed with CUDA events."""
+    import torch
+    hi = torch.from_numpy(h_in).view(-1)
+    ho = torch.from_numpy(h_out).view(-1)
+    di = torch.empty_like(hi, device=dev)
+    do = torch.empty_like(ho, device=dev)
+    out = []
+    for dst, src, nbytes in ((di, hi, hi.numel() * hi.element_size()),
+                             (ho, do, ho.numel() * ho.element_size())):
+        ts = []
+        for _ in range(reps):
+            e0, e1 = _events()
+            e0.record()
+            dst.copy_(src, non_blocking=True)
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        out.append(nbytes / (statistics.median(ts) / 1e3) / 1e9)
+    return out[0], out[1]
+
+
 # ------------------------------------------------------------- workloads
 def load_workload():
     from rtdsl import workloads
@@ -182,8 +205,7 @@ def run_ours(args, ws, rank, local):
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
 
     def step():
-        ix.build(P, s)
-        ix.knn(Q, K, s, out_ids=ids, out_d2=d2)
+        ix.k_nn(P, Q, K, s, out_ids=ids, out_d2=d2)
 
     for _ in range(max(args.warmup, 3)):
         step()
@@ -246,8 +268,13 @@ def run_ours(args, ws, rank, local):
             ctx.k_nn(hp, hq, K, s, out_ids=hids)
             e2e_t.append(time.perf_counter() - t0)
         e2e_s = max_over_ranks(statistics.mean(e2e_t), dist, dev)
+        # this host's pinned copy bandwidth for the same bytes (it differs
+        # between hosts and bounds the end-to-end number)
+        h2d_gbs, d2h_gbs = copy_bandwidth(hp, hids, dev)
         e2e = {"value": ws * nq / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(hp.nbytes + hq.nbytes),
                "d2h_bytes_per_step": int(hids.nbytes), "ms_per_step": e2e_s * 1e3,
+               "ms_min": min(e2e_t) * 1e3, "ms_median": statistics.median(e2e_t) * 1e3,
+               "host_h2d_gbs": h2d_gbs, "host_d2h_gbs": d2h_gbs,
                "api": "rtd_k_nn_host (k_nn! host buffers, pinned)"}
         ctx.close()
 
@@ -272,7 +299,7 @@ def run_ours(args, ws, rank, local):
         "scaling": "weak", "vs_baseline": value / PUBLISHED_QPS, "vs_baseline_ref": PUBLISHED_REF,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": "clustered_1p8m_k5: 1.8M clustered points, 400K queries, k=5, "
-                               "one step = LBVH build + in-kernel radius-expansion search",
+                               "one step = rtd_k_nn on resident inputs (LBVH build + exact search, queries Morton-ordered on a second stream during the build)",
                    "n_points": n, "n_queries": nq, "k": K, "parallelism": f"replica x{ws}",
                    "l2": "256 MiB buffer written between timed steps (outside step events)",
                    "schedule": s.as_dict()},
@@ -296,6 +323,8 @@ def bench_range(args, dev, flush, P, Q, s) -> dict:
     import rtdsl
     from rtdsl.api import radius_for_mean_count
 
+    from rtdsl import autotune
+    s = autotune.cached_schedule("clustered_1p8m_r50", s)   # range: its own tuned leaf / key width
     ix = rtdsl.Index().build(P, s)
     r = radius_for_mean_count(ix, Q, 50.0, schedule=s)
     counts = torch.empty((Q.shape[0],), dtype=torch.int32, device=dev)
@@ -332,7 +361,7 @@ def bench_range(args, dev, flush, P, Q, s) -> dict:
         "unit": "pairs/s",
         "config": {"workload": "clustered_1p8m_r50: the headline cloud, radius for a mean of 50 "
                                "neighbours per query, unsorted (query, id) u32 pairs",
-                   "radius": r, "pairs": int(total)},
+                   "radius": r, "pairs": int(total), "schedule": s.as_dict()},
         "ms": {"count_kernel": mc, "fill_kernel": mf, "step": m},
         "queries_per_s": nq / (m / 1e3),
         "roofline": {"kernel": "range_kernel<MODE_SEG> (fill)", "bound": "hbm",

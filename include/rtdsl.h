@@ -162,6 +162,15 @@ uint64_t rtd_launch_count(void);
 rtd_status rtd_knn(rtd_index *idx, const float *d_queries, uint64_t nq, uint32_t k,
                    const rtd_schedule *sched, uint32_t *d_ids, float *d_d2, rtd_stream stream);
 
+/* k_nn!(data, queries, k, out[, schedule]) on device buffers: builds the
+ * index over d_points (as rtd_index_build) and searches d_queries (as
+ * rtd_knn) in one call, the whole k_nn! macro of gprt-macros/src/lib.rs:
+ * 408-604.  The queries are Morton-ordered on a second stream owned by the
+ * index while the index builds on `stream`; the call does not synchronise. */
+rtd_status rtd_k_nn(rtd_index *idx, const float *d_points, uint64_t n, const float *d_queries,
+                    uint64_t nq, uint32_t k, const rtd_schedule *sched, uint32_t *d_ids,
+                    float *d_d2, rtd_stream stream);
+
 /* Host-buffer k_nn!(data, queries, k, out[, schedule]): copies in, builds
  * the index, searches, copies ids (and d2 if non-NULL) out, synchronises.
  * The context caches device buffers across calls. */

@@ -68,6 +68,9 @@ void DevBuf::release() {
 // Implemented in lbvh.cu / knn.cu / range.cu / knn_backward.cu.
 rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd_schedule *s,
                        cudaStream_t st);
+rtd_status k_nn_device(rtd_index *idx, const float *d_points, uint64_t n, const float *d_q,
+                       uint64_t nq, uint32_t k, const rtd_schedule *sched, uint32_t *d_ids,
+                       float *d_d2, cudaStream_t st);
 rtd_status knn_search(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k,
                       const rtd_schedule *sched, uint32_t *d_ids, float *d_d2, cudaStream_t st);
 rtd_status range_count(rtd_index *idx, const float *d_q, uint64_t nq, float r,
@@ -228,6 +231,12 @@ uint64_t rtd_launch_count(void) { return g_launches.load(std::memory_order_relax
 rtd_status rtd_knn(rtd_index *idx, const float *d_queries, uint64_t nq, uint32_t k,
                    const rtd_schedule *sched, uint32_t *d_ids, float *d_d2, rtd_stream stream) {
     return knn_search(idx, d_queries, nq, k, sched, d_ids, d_d2, (cudaStream_t)stream);
+}
+
+rtd_status rtd_k_nn(rtd_index *idx, const float *d_points, uint64_t n, const float *d_queries,
+                    uint64_t nq, uint32_t k, const rtd_schedule *sched, uint32_t *d_ids,
+                    float *d_d2, rtd_stream stream) {
+    return k_nn_device(idx, d_points, n, d_queries, nq, k, sched, d_ids, d_d2, (cudaStream_t)stream);
 }
 
 rtd_status rtd_context_create(rtd_context **out) {

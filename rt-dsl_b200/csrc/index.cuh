@@ -53,6 +53,17 @@ constexpr int SEED_PCT_QUERIES = 100;
 
 }  // namespace rtd
 
+namespace rtd {
+// The same order computed against the queries' own box with scratch of its
+// own, so that it can run on another stream while an index is being built.
+// Device errors land in the scratch header's err word.
+struct QueryOrderScratch {
+    DevBuf hdr;   // IndexHeader: the query box and err
+    DevBuf keys, keys_alt, perm, perm_alt;
+    SortScratch sort;
+};
+}  // namespace rtd
+
 struct rtd_index {
     uint64_t n = 0;
     uint32_t leaf_size = 4;
@@ -86,6 +97,10 @@ struct rtd_index {
         uint64_t total = 0;
         const uint32_t *perm = nullptr;
     } rtoken;
+    // rtd_k_nn: the queries are ordered on side_stream while the index builds
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    rtd::QueryOrderScratch qorder;
     // phase timers (rtd_index_profile_*)
     bool prof = false;
     cudaEvent_t ev[8] = {};
@@ -98,6 +113,9 @@ struct rtd_index {
     ~rtd_index() {
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (side_stream) cudaStreamDestroy(side_stream);
     }
 };
 
@@ -162,16 +180,12 @@ rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStr
 rtd_status order_queries(rtd_index *idx, const float *d_q, uint64_t nq, bool morton,
                          const uint32_t **perm, cudaStream_t stream);
 
-// The same order computed against the queries' own box with scratch of its
-// own, so that it can run on another stream while an index is being built.
-// Device errors land in the scratch header's err word.
-struct QueryOrderScratch {
-    DevBuf hdr;   // IndexHeader: the query box and err
-    DevBuf keys, keys_alt, perm, perm_alt;
-    SortScratch sort;
-};
 rtd_status order_queries_own(QueryOrderScratch &qs, const float *d_q, uint64_t nq,
                              const uint32_t **perm, cudaStream_t stream);
+
+// LBVH build over n device points (lbvh.cu).
+rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd_schedule *s,
+                       cudaStream_t st);
 
 // k-NN search (knn.cu); with have_perm the query order is given (perm, or
 // nullptr for caller order) instead of computed on the index.

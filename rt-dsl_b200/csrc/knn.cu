@@ -626,6 +626,14 @@ rtd_status launch_warp(const KnnArgs &a, uint32_t block, cudaStream_t st) {
     return RTD_OK;
 }
 
+// Moves the query-ordering error flags into the index's.
+__global__ void fold_errors_kernel(IndexHeader *into, IndexHeader *from) {
+    if (from->err) {
+        atomicOr(&into->err, from->err);
+        from->err = 0;
+    }
+}
+
 }  // namespace
 
 rtd_status seed_radius(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k,
@@ -744,6 +752,41 @@ rtd_status knn_search_ex(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t
     }
     idx->mark(EV_SEARCH1, st);
     return r;
+}
+
+// k_nn! on device buffers: build + search in one call.  The queries are
+// Morton-ordered on the index's side stream (against their own box, with
+// their own scratch) while the index builds on the caller's stream; the
+// search waits for both.
+rtd_status k_nn_device(rtd_index *idx, const float *d_points, uint64_t n, const float *d_q,
+                       uint64_t nq, uint32_t k, const rtd_schedule *sched, uint32_t *d_ids,
+                       float *d_d2, cudaStream_t st) {
+    if (!idx) return fail(RTD_ERR_INVALID_ARGUMENT, "index is NULL");
+    if (nq && (!d_q || !d_ids)) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL queries or ids");
+    rtd_schedule def;
+    rtd_schedule_default(&def);
+    const rtd_schedule &s = sched ? *sched : def;
+    if (!idx->side_stream) {
+        RTD_CUDA(cudaStreamCreateWithFlags(&idx->side_stream, cudaStreamNonBlocking));
+        RTD_CUDA(cudaEventCreateWithFlags(&idx->ev_fork, cudaEventDisableTiming));
+        RTD_CUDA(cudaEventCreateWithFlags(&idx->ev_join, cudaEventDisableTiming));
+    }
+    cudaStream_t side = idx->side_stream;
+    RTD_CUDA(cudaEventRecord(idx->ev_fork, st));   // the queries' producers come first
+    RTD_CUDA(cudaStreamWaitEvent(side, idx->ev_fork, 0));
+    const uint32_t *perm = nullptr;
+    rtd_status ord = RTD_OK;
+    if (s.use_morton_lbv && nq >= 2 && k > 0) ord = order_queries_own(idx->qorder, d_q, nq, &perm, side);
+    RTD_CUDA(cudaEventRecord(idx->ev_join, side));
+    rtd_status r = index_build(idx, d_points, n, &s, st);
+    RTD_CUDA(cudaStreamWaitEvent(st, idx->ev_join, 0));   // also on the error paths
+    RTD_TRY(ord);
+    RTD_TRY(r);
+    if (perm) {
+        fold_errors_kernel<<<1, 1, 0, st>>>(idx->hdr.as<IndexHeader>(), idx->qorder.hdr.as<IndexHeader>());
+        RTD_LAUNCH_CHECK();
+    }
+    return knn_search_ex(idx, d_q, nq, k, &s, d_ids, d_d2, st, true, perm);
 }
 
 }  // namespace rtd

@@ -187,6 +187,28 @@ class Index:
                                 _stream_handle(stream)))
         return ids, d2
 
+    def k_nn(self, points, queries, k: int, schedule: Schedule | None = None,
+             with_d2: bool = True, out_ids=None, out_d2=None, stream=None):
+        """k_nn! on CUDA tensors: builds this index over `points` and
+        searches `queries` in one call (the queries are ordered on a second
+        stream while the index builds).  Returns (ids, d2) as knn does."""
+        import torch
+        _check_points_tensor(points, "points")
+        _check_points_tensor(queries, "queries")
+        nq = queries.shape[0]
+        dev = queries.device
+        ids = out_ids if out_ids is not None else torch.empty((nq, k), dtype=torch.int32, device=dev)
+        d2 = out_d2 if out_d2 is not None else (
+            torch.empty((nq, k), dtype=torch.float32, device=dev) if with_d2 else None)
+        s = schedule if schedule is not None else default_schedule()
+        check(self._lib.rtd_k_nn(self._h, C.c_void_p(points.data_ptr()), points.shape[0],
+                                 C.c_void_p(queries.data_ptr()), nq, k, C.byref(s),
+                                 C.c_void_p(ids.data_ptr()),
+                                 C.c_void_p(d2.data_ptr()) if d2 is not None else None,
+                                 _stream_handle(stream)))
+        self.points = points
+        return ids, d2
+
     def range_count(self, queries, radius: float, schedule: Schedule | None = None,
                     out_counts=None, stream=None):
         import torch

@@ -224,6 +224,26 @@ def test_knn_host_context_overlap(rtd, orc, cuda, order):
         assert_same(oi, od, ids, d2)
 
 
+@pytest.mark.parametrize("sched", [dict(), dict(use_morton_lbv=0),
+                                   dict(radius_heuristic=4, leaf_size=5, morton_bits=39),
+                                   dict(lanes_per_query=32)])
+def test_knn_device_k_nn_one_call(rtd, orc, cuda, sched):
+    """rtd_k_nn builds and searches in one call, ordering the queries on a
+    second stream during the build: same ids and keys as the oracle, on
+    repeated calls over different clouds and query counts."""
+    ix = rtd.Index()
+    s = rtd.default_schedule(**sched)
+    for n, nq, seed, k in [(30_000, 3_000, 61, 5), (8_000, 9_000, 62, 16), (20_000, 1, 63, 8),
+                           (3, 100, 64, 5), (0, 10, 65, 5)]:
+        pts, q = clustered_small(n=max(n, 1), nq=max(nq, 1), seed=seed)
+        pts, q = pts[:n], q[:nq]
+        ids, d2 = ix.k_nn(torch.from_numpy(np.ascontiguousarray(pts).reshape(-1, 3)).cuda(),
+                          torch.from_numpy(np.ascontiguousarray(q)).cuda(), k, s)
+        torch.cuda.synchronize()
+        oi, od = orc.knn(pts.reshape(-1, 3), q, k)
+        assert_same(oi, od, ids.cpu().numpy().view(np.uint32), d2.cpu().numpy())
+
+
 def test_knn_deterministic_and_reusable_index(rtd, cuda):
     pts, q = clustered_small(n=20_000, nq=2_000, seed=18)
     s = rtd.default_schedule()
