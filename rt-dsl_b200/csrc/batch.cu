@@ -156,18 +156,22 @@ __global__ void __launch_bounds__(BLOCK) batch_gather_kernel(const float *__rest
     }
 }
 
-// The forest node whose range is exactly a cloud's points is that cloud's root.
+// The kept forest node whose range is exactly a cloud's points is that
+// cloud's root.
 __global__ void __launch_bounds__(BLOCK) batch_roots_kernel(
     const uint64_t *__restrict__ skeys, uint64_t n, int shift, const uint32_t *__restrict__ kfirst,
     const uint32_t *__restrict__ klast, const uint32_t *__restrict__ flags,
     const uint32_t *__restrict__ cidx, CloudDesc *cd) {
     for (uint64_t i = (uint64_t)blockIdx.x * BLOCK + threadIdx.x; i + 1 < n;
          i += (uint64_t)gridDim.x * BLOCK) {
+        // only kept nodes carry their range; a cloud of <= leaf_size points
+        // keeps the leaf root batch_reset_kernel gave it
+        if (!flags[i]) continue;
         const uint32_t f = kfirst[i], l = klast[i];
         const uint32_t c = (uint32_t)(skeys[f] >> shift);
         const CloudDesc d = cd[c];
         if (f == d.pt_begin && l + 1 == d.pt_begin + d.n_pts) {
-            cd[c].root = flags[i] ? cidx[i] : (CHILD_LEAF | f);
+            cd[c].root = cidx[i];
             cd[c].root_count = d.n_pts;
         }
     }

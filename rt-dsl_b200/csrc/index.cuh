@@ -75,7 +75,10 @@ struct rtd_index {
     rtd::DevBuf top;        // BvhNode * TOP_MAX
     // build scratch
     rtd::DevBuf keys, keys_alt, vals, vals_alt;
-    rtd::DevBuf kleft, kright, kfirst, klast, kparent, flags, cidx, csel;
+    // Karras nodes (split, first and last point; valid where flags is 1,
+    // i.e. the node keeps more than leaf_size points), compact indices and
+    // the list of kept nodes
+    rtd::DevBuf ksplit, kfirst, klast, flags, cidx, csel;
     rtd::DevBuf pyramid;    // run boxes over the sorted points (2 float4 per run)
     rtd::SortScratch sort;
     rtd::ScanScratch scan;

@@ -105,17 +105,28 @@ __device__ __forceinline__ int delta(const K *__restrict__ keys, int64_t n, int6
     return sizeof(K) == 8 ? __clzll((unsigned long long)(a ^ b)) : __clz((uint32_t)(a ^ b));
 }
 
+// Karras nodes.  Only nodes with more than leaf_size points are kept (the
+// rest collapse into leaves), and a node's point count exceeds leaf_size
+// exactly when the key leaf_size steps away in its direction still shares
+// more than the node's lower bound on the common prefix: the prefix length
+// of the (key, position) pairs, which are strictly increasing, cannot grow
+// with distance.  So a collapsed node costs that one test and writes only
+// its flag; the searches run for kept nodes alone.
 template <typename K>
 __global__ void __launch_bounds__(BLOCK) karras_kernel(const K *__restrict__ keys, int64_t n,
-                                                       uint32_t leaf_size, uint32_t *kleft,
-                                                       uint32_t *kright, uint32_t *kfirst,
-                                                       uint32_t *klast, uint32_t *kparent,
+                                                       uint32_t leaf_size, uint32_t *ksplit,
+                                                       uint32_t *kfirst, uint32_t *klast,
                                                        uint32_t *flags) {
     for (int64_t i = (int64_t)blockIdx.x * BLOCK + threadIdx.x; i < n - 1;
          i += (int64_t)gridDim.x * BLOCK) {
         int dir = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
         int dmin = delta(keys, n, i, i - dir);
+        if (!(delta(keys, n, i, i + (int64_t)leaf_size * dir) > dmin)) {
+            flags[i] = 0u;
+            continue;
+        }
         int64_t lmax = 2;
+        while (lmax <= (int64_t)leaf_size) lmax <<= 1;
         while (delta(keys, n, i, i + lmax * dir) > dmin) lmax <<= 1;
         int64_t l = 0;
         for (int64_t t = lmax >> 1; t >= 1; t >>= 1)
@@ -127,18 +138,11 @@ __global__ void __launch_bounds__(BLOCK) karras_kernel(const K *__restrict__ key
             t = (t + 1) >> 1;
             if (delta(keys, n, i, i + (s + t) * dir) > dnode) s += t;
         } while (t > 1);
-        int64_t gamma = i + s * dir + (dir < 0 ? -1 : 0);
-        int64_t first = i < j ? i : j, last = i < j ? j : i;
-        uint32_t left = (uint32_t)gamma, right = (uint32_t)(gamma + 1);
-        if (first == gamma) left |= CHILD_LEAF;
-        else kparent[gamma] = (uint32_t)i;
-        if (last == gamma + 1) right |= CHILD_LEAF;
-        else kparent[gamma + 1] = (uint32_t)i;
-        kleft[i] = left;
-        kright[i] = right;
-        kfirst[i] = (uint32_t)first;
-        klast[i] = (uint32_t)last;
-        flags[i] = (uint32_t)(last - first + 1) > leaf_size ? 1u : 0u;
+        const int64_t gamma = i + s * dir + (dir < 0 ? -1 : 0);
+        ksplit[i] = (uint32_t)gamma;
+        kfirst[i] = (uint32_t)(i < j ? i : j);
+        klast[i] = (uint32_t)(i < j ? j : i);
+        flags[i] = 1u;
     }
 }
 
@@ -316,30 +320,21 @@ __device__ __noinline__ Box range_box(const Pyramid &P, uint32_t first, uint32_t
 // computed independently, so no bottom-up pass over the tree follows.
 __global__ void __launch_bounds__(BLOCK) compact_kernel(
     uint32_t n_internal_max, const IndexHeader *h, const uint32_t *__restrict__ sel,
-    const uint32_t *__restrict__ kleft, const uint32_t *__restrict__ kright,
-    const uint32_t *__restrict__ kfirst, const uint32_t *__restrict__ klast,
-    const uint32_t *__restrict__ flags, const uint32_t *__restrict__ cidx, const Pyramid P,
-    BvhNode *nodes) {
+    const uint32_t *__restrict__ ksplit, const uint32_t *__restrict__ kfirst,
+    const uint32_t *__restrict__ klast, const uint32_t *__restrict__ cidx, uint32_t leaf_size,
+    const Pyramid P, BvhNode *nodes) {
     const uint32_t n_int = h->n_internal;
     for (uint32_t c = blockIdx.x * BLOCK + threadIdx.x; c < n_int && c < n_internal_max;
          c += gridDim.x * BLOCK) {
         const uint32_t i = sel[c];
-        const uint32_t ch[2] = {kleft[i], kright[i]};
+        // children [first, split] and [split + 1, last]: Karras nodes split
+        // and split + 1 when they keep more than leaf_size points, else leaves
+        const uint32_t f0 = kfirst[i], sp = ksplit[i];
         uint32_t word[2], cnt[2];
-        for (int s = 0; s < 2; ++s) {
-            const uint32_t w = ch[s];
-            if (w & CHILD_LEAF) {
-                word[s] = CHILD_LEAF | (w & CHILD_INDEX);
-                cnt[s] = 1;
-            } else if (flags[w]) {
-                word[s] = cidx[w];
-                cnt[s] = klast[w] - kfirst[w] + 1;
-            } else {
-                word[s] = CHILD_LEAF | kfirst[w];
-                cnt[s] = klast[w] - kfirst[w] + 1;
-            }
-        }
-        const uint32_t f0 = kfirst[i];
+        cnt[0] = sp - f0 + 1;
+        cnt[1] = klast[i] - sp;
+        word[0] = cnt[0] > leaf_size ? cidx[sp] : (CHILD_LEAF | f0);
+        word[1] = cnt[1] > leaf_size ? cidx[sp + 1] : (CHILD_LEAF | (sp + 1));
         const Box b0 = range_box(P, f0, cnt[0]);
         const Box b1 = range_box(P, f0 + cnt[0], cnt[1]);
         BvhNode nd;
@@ -554,8 +549,8 @@ rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStr
     uint32_t *d_err = &h->err;
     if (n < 2 || n <= idx->leaf_size) return RTD_OK;
     const uint64_t ni = n - 1;
-    for (rtd::DevBuf *b : {&idx->kleft, &idx->kright, &idx->kfirst, &idx->klast, &idx->kparent,
-                           &idx->flags, &idx->cidx, &idx->csel})
+    for (rtd::DevBuf *b : {&idx->ksplit, &idx->kfirst, &idx->klast, &idx->flags, &idx->cidx,
+                           &idx->csel})
         RTD_TRY(b->reserve(ni * sizeof(uint32_t)));
     // box pyramid over the sorted points (levels until one has <= 32 entries)
     Pyramid P;
@@ -584,9 +579,8 @@ rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStr
     }
     const int gi = grid_for(ni, BLOCK, 148 * 8);
     karras_kernel<K><<<gi, BLOCK, 0, st>>>(skeys, (int64_t)n, idx->leaf_size,
-                                           idx->kleft.as<uint32_t>(), idx->kright.as<uint32_t>(),
-                                           idx->kfirst.as<uint32_t>(), idx->klast.as<uint32_t>(),
-                                           idx->kparent.as<uint32_t>(), idx->flags.as<uint32_t>());
+                                           idx->ksplit.as<uint32_t>(), idx->kfirst.as<uint32_t>(),
+                                           idx->klast.as<uint32_t>(), idx->flags.as<uint32_t>());
     RTD_LAUNCH_CHECK();
     RTD_TRY(exclusive_scan_select_u32(idx->flags.as<uint32_t>(), idx->cidx.as<uint32_t>(),
                                       idx->csel.as<uint32_t>(), ni, &h->n_internal, idx->scan,
@@ -594,9 +588,9 @@ rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStr
     // kept nodes: at most (n - 1) / leaf_size of them have more than leaf_size points
     const uint64_t kept_max = ni / idx->leaf_size + 1 < ni ? ni / idx->leaf_size + 1 : ni;
     compact_kernel<<<grid_for(kept_max, BLOCK, 148 * 8), BLOCK, 0, st>>>(
-        (uint32_t)ni, h, idx->csel.as<uint32_t>(), idx->kleft.as<uint32_t>(),
-        idx->kright.as<uint32_t>(), idx->kfirst.as<uint32_t>(), idx->klast.as<uint32_t>(),
-        idx->flags.as<uint32_t>(), idx->cidx.as<uint32_t>(), P, idx->nodes.as<BvhNode>());
+        (uint32_t)ni, h, idx->csel.as<uint32_t>(), idx->ksplit.as<uint32_t>(),
+        idx->kfirst.as<uint32_t>(), idx->klast.as<uint32_t>(), idx->cidx.as<uint32_t>(),
+        idx->leaf_size, P, idx->nodes.as<BvhNode>());
     RTD_LAUNCH_CHECK();
     return RTD_OK;
 }
