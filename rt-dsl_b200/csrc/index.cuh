@@ -100,9 +100,11 @@ struct rtd_index {
         uint64_t total = 0;
         const uint32_t *perm = nullptr;
     } rtoken;
-    // rtd_k_nn: the queries are ordered on side_stream while the index builds
+    // Side stream for work that overlaps the build: the radius-seed sample
+    // (every build) and rtd_k_nn's query ordering
     cudaStream_t side_stream = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_seed_fork = nullptr,
+                ev_seed_join = nullptr;
     rtd::QueryOrderScratch qorder;
     // phase timers (rtd_index_profile_*)
     bool prof = false;
@@ -116,8 +118,8 @@ struct rtd_index {
     ~rtd_index() {
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
-        if (ev_fork) cudaEventDestroy(ev_fork);
-        if (ev_join) cudaEventDestroy(ev_join);
+        for (cudaEvent_t e : {ev_fork, ev_join, ev_seed_fork, ev_seed_join})
+            if (e) cudaEventDestroy(e);
         if (side_stream) cudaStreamDestroy(side_stream);
     }
 };
@@ -185,6 +187,9 @@ rtd_status order_queries(rtd_index *idx, const float *d_q, uint64_t nq, bool mor
 
 rtd_status order_queries_own(QueryOrderScratch &qs, const float *d_q, uint64_t nq,
                              const uint32_t **perm, cudaStream_t stream);
+
+// Creates the index's side stream and its events on first use.
+rtd_status ensure_side_stream(rtd_index *idx);
 
 // LBVH build over n device points (lbvh.cu).
 rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd_schedule *s,

@@ -766,11 +766,7 @@ rtd_status k_nn_device(rtd_index *idx, const float *d_points, uint64_t n, const 
     rtd_schedule def;
     rtd_schedule_default(&def);
     const rtd_schedule &s = sched ? *sched : def;
-    if (!idx->side_stream) {
-        RTD_CUDA(cudaStreamCreateWithFlags(&idx->side_stream, cudaStreamNonBlocking));
-        RTD_CUDA(cudaEventCreateWithFlags(&idx->ev_fork, cudaEventDisableTiming));
-        RTD_CUDA(cudaEventCreateWithFlags(&idx->ev_join, cudaEventDisableTiming));
-    }
+    RTD_TRY(ensure_side_stream(idx));
     cudaStream_t side = idx->side_stream;
     RTD_CUDA(cudaEventRecord(idx->ev_fork, st));   // the queries' producers come first
     RTD_CUDA(cudaStreamWaitEvent(side, idx->ev_fork, 0));

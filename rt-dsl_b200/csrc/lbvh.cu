@@ -84,17 +84,6 @@ __global__ void __launch_bounds__(BLOCK) morton_kernel(const float *__restrict__
     }
 }
 
-__global__ void __launch_bounds__(BLOCK) gather_points_kernel(const float *__restrict__ xyz,
-                                                              const uint32_t *__restrict__ perm,
-                                                              uint64_t n, float4 *__restrict__ pts) {
-    for (uint64_t i = (uint64_t)blockIdx.x * BLOCK + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x * BLOCK) {
-        uint32_t o = perm[i];
-        pts[i] = make_float4(xyz[3 * (uint64_t)o], xyz[3 * (uint64_t)o + 1],
-                             xyz[3 * (uint64_t)o + 2], __uint_as_float(o));
-    }
-}
-
 // Common-prefix length of sorted keys i and j, ties broken by index
 // (Karras 2012, "Maximizing parallelism in the construction of BVHs").
 template <typename K>
@@ -527,14 +516,12 @@ rtd_status build_typed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStrea
     morton_kernel<K><<<g, BLOCK, 0, st>>>(d_xyz, n, h, scale, idx->keys.as<K>());
     RTD_LAUNCH_CHECK();
     bool in_alt = false;
+    // the last pass gathers the points into idx->pts in key order
     RTD_TRY(radix_sort_pairs<K>(idx->keys.as<K>(), idx->keys_alt.as<K>(), idx->vals.as<uint32_t>(),
                                 idx->vals_alt.as<uint32_t>(), true, n, 0, kbits, idx->sort, d_err,
-                                st, &in_alt));
+                                st, &in_alt, d_xyz, idx->pts.as<float4>()));
     K *skeys = in_alt ? idx->keys_alt.as<K>() : idx->keys.as<K>();
     idx->skeys = skeys;
-    uint32_t *perm = in_alt ? idx->vals_alt.as<uint32_t>() : idx->vals.as<uint32_t>();
-    gather_points_kernel<<<g, BLOCK, 0, st>>>(d_xyz, perm, n, idx->pts.as<float4>());
-    RTD_LAUNCH_CHECK();
     idx->mark(EV_BUILD_SORTED, st);
     return build_tree_sorted<K>(idx, skeys, n, st);
 }
@@ -600,6 +587,14 @@ template rtd_status build_tree_sorted<uint32_t>(rtd_index *, const uint32_t *, u
 template rtd_status build_tree_sorted<uint64_t>(rtd_index *, const uint64_t *, uint64_t,
                                                 cudaStream_t);
 
+rtd_status ensure_side_stream(rtd_index *idx) {
+    if (idx->side_stream) return RTD_OK;
+    RTD_CUDA(cudaStreamCreateWithFlags(&idx->side_stream, cudaStreamNonBlocking));
+    for (cudaEvent_t *e : {&idx->ev_fork, &idx->ev_join, &idx->ev_seed_fork, &idx->ev_seed_join})
+        RTD_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    return RTD_OK;
+}
+
 rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd_schedule *s,
                        cudaStream_t st) {
     if (!idx) return fail(RTD_ERR_INVALID_ARGUMENT, "index is NULL");
@@ -634,9 +629,18 @@ rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd
     if (n > 0) {
         bbox_kernel<<<grid_for(n, BLOCK, 148 * 4), BLOCK, 0, st>>>(d_xyz, n, h);
         RTD_LAUNCH_CHECK();
-        RTD_TRY(build_seed(idx, d_xyz, n, st));
-        if (mb == 30) RTD_TRY(build_typed<uint32_t>(idx, d_xyz, n, st));
-        else RTD_TRY(build_typed<uint64_t>(idx, d_xyz, n, st));
+        // the radius-seed sample reads only the input points: it runs on the
+        // side stream while the keys are made and sorted
+        RTD_TRY(ensure_side_stream(idx));
+        RTD_CUDA(cudaEventRecord(idx->ev_seed_fork, st));
+        RTD_CUDA(cudaStreamWaitEvent(idx->side_stream, idx->ev_seed_fork, 0));
+        const rtd_status rs = build_seed(idx, d_xyz, n, idx->side_stream);
+        RTD_CUDA(cudaEventRecord(idx->ev_seed_join, idx->side_stream));
+        const rtd_status rb = mb == 30 ? build_typed<uint32_t>(idx, d_xyz, n, st)
+                                       : build_typed<uint64_t>(idx, d_xyz, n, st);
+        RTD_CUDA(cudaStreamWaitEvent(st, idx->ev_seed_join, 0));   // also on the error paths
+        RTD_TRY(rs);
+        RTD_TRY(rb);
     }
     stage_top_kernel<<<1, 32, 0, st>>>(h, idx->nodes.as<BvhNode>(), idx->top.as<BvhNode>(), n,
                                       idx->leaf_size);

@@ -84,7 +84,8 @@ template <typename K>
 __global__ void __launch_bounds__(RS_BLOCK) rs_pass_kernel(
     const K *__restrict__ kin, K *__restrict__ kout, const uint32_t *__restrict__ vin,
     uint32_t *__restrict__ vout, uint64_t n, int shift, const uint32_t *__restrict__ digit_off,
-    uint32_t *status, uint32_t *tile_counter, uint32_t *d_err) {
+    uint32_t *status, uint32_t *tile_counter, uint32_t *d_err, const float *__restrict__ gxyz,
+    float4 *__restrict__ gout) {
     extern __shared__ __align__(16) unsigned char rs_smem[];
     K *s_keys = reinterpret_cast<K *>(rs_smem);
     uint32_t *s_vals = reinterpret_cast<uint32_t *>(s_keys + RS_TILE);
@@ -193,7 +194,13 @@ __global__ void __launch_bounds__(RS_BLOCK) rs_pass_kernel(
         uint32_t dj = (uint32_t)(k >> shift) & 255u;
         uint32_t dst = s_base[dj] + j;
         kout[dst] = k;
-        vout[dst] = s_vals[j];
+        const uint32_t v = s_vals[j];
+        if (gout) {   // last pass with a gather: the point itself, its index in w
+            const uint64_t o = v;
+            gout[dst] = make_float4(gxyz[3 * o], gxyz[3 * o + 1], gxyz[3 * o + 2], __uint_as_float(v));
+        } else {
+            vout[dst] = v;
+        }
     }
 }
 
@@ -340,7 +347,8 @@ rtd_status scan_impl(const uint32_t *in, OutT *out, uint64_t n, OutT *d_total, S
 template <typename K>
 rtd_status radix_sort_pairs(K *keys, K *keys_alt, uint32_t *vals, uint32_t *vals_alt,
                             bool vals_iota, uint64_t n, int begin_bit, int end_bit,
-                            SortScratch &scr, uint32_t *d_err, cudaStream_t stream, bool *in_alt) {
+                            SortScratch &scr, uint32_t *d_err, cudaStream_t stream, bool *in_alt,
+                            const float *gather_xyz, float4 *gather_out) {
     *in_alt = false;
     if (n == 0) return RTD_OK;
     if (n >= (1ull << 30)) return fail(RTD_ERR_INVALID_ARGUMENT, "radix sort: n must be < 2^30");
@@ -370,7 +378,7 @@ rtd_status radix_sort_pairs(K *keys, K *keys_alt, uint32_t *vals, uint32_t *vals
             kin, kout, (p == 0 && vals_iota) ? nullptr : vin, vout, n, begin_bit + 8 * p,
             scr.hist.as<uint32_t>() + p * 256,
             scr.status.as<uint32_t>() + (size_t)p * ntiles * 256, scr.counters.as<uint32_t>() + p,
-            d_err);
+            d_err, gather_xyz, p == passes - 1 ? gather_out : nullptr);
         RTD_LAUNCH_CHECK();
         K *tk = kin; kin = kout; kout = tk;
         uint32_t *tv = vin; vin = vout; vout = tv;
@@ -381,10 +389,12 @@ rtd_status radix_sort_pairs(K *keys, K *keys_alt, uint32_t *vals, uint32_t *vals
 
 template rtd_status radix_sort_pairs<uint32_t>(uint32_t *, uint32_t *, uint32_t *, uint32_t *,
                                                bool, uint64_t, int, int, SortScratch &,
-                                               uint32_t *, cudaStream_t, bool *);
+                                               uint32_t *, cudaStream_t, bool *, const float *,
+                                               float4 *);
 template rtd_status radix_sort_pairs<uint64_t>(uint64_t *, uint64_t *, uint32_t *, uint32_t *,
                                                bool, uint64_t, int, int, SortScratch &,
-                                               uint32_t *, cudaStream_t, bool *);
+                                               uint32_t *, cudaStream_t, bool *, const float *,
+                                               float4 *);
 
 rtd_status exclusive_scan_u32(const uint32_t *in, uint64_t *out, uint64_t n, uint64_t *d_total,
                               ScanScratch &scr, uint32_t *d_err, cudaStream_t stream) {

@@ -24,11 +24,14 @@ struct SortScratch {
 // input; keys_alt/vals_alt are scratch of the same size (all four buffers
 // are required).  With vals_iota the input values are taken to be 0..n-1
 // and vals is not read.  On return *in_alt tells whether the sorted result
-// is in the *_alt buffers.  n must be < 2^30.
+// is in the *_alt buffers.  n must be < 2^30.  With gather_out, the last
+// pass writes gather_out[i] = (x, y, z, bits of v) of the i-th sorted value
+// v from the xyz triples gather_xyz instead of the sorted values.
 template <typename K>
 rtd_status radix_sort_pairs(K *keys, K *keys_alt, uint32_t *vals, uint32_t *vals_alt,
                             bool vals_iota, uint64_t n, int begin_bit, int end_bit,
-                            SortScratch &scr, uint32_t *d_err, cudaStream_t stream, bool *in_alt);
+                            SortScratch &scr, uint32_t *d_err, cudaStream_t stream, bool *in_alt,
+                            const float *gather_xyz = nullptr, float4 *gather_out = nullptr);
 
 // out[i] = sum(in[0..i)), out has n entries; *d_total (device) = sum(in).
 struct ScanScratch {
