@@ -116,7 +116,14 @@ __global__ void __launch_bounds__(RS_BLOCK) rs_pass_kernel(
     uint32_t *wh = s_wh + warp * 256;
 #pragma unroll
     for (int i = 0; i < RS_ITEMS; ++i) {
-        uint32_t peers = __match_any_sync(0xffffffffu, dig[i]);
+        // lanes holding the same digit: one ballot per digit bit
+        uint32_t peers = 0xffffffffu;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const bool bit = (dig[i] >> b) & 1u;
+            const uint32_t m = __ballot_sync(0xffffffffu, bit);
+            peers &= bit ? m : ~m;
+        }
         uint32_t before = __popc(peers & lt);
         uint32_t cnt = wh[dig[i]];
         rank[i] = cnt + before;
