@@ -294,7 +294,7 @@ rtd_status rtd_k_nn_host(rtd_context *ctx, const rtd_vec3 *data, uint64_t n,
     RTD_TRY(ord);
     RTD_TRY(r);
     RTD_TRY(knn_search_ex(&ctx->index, ctx->queries.as<float>(), nq, k, &s, ctx->ids.as<uint32_t>(),
-                          d2 ? ctx->d2.as<float>() : nullptr, st, true, perm));
+                          d2 ? ctx->d2.as<float>() : nullptr, st, true, perm, nullptr));
     if (nq) {
         RTD_CUDA(cudaMemcpyAsync(ids, ctx->ids.ptr, nq * (uint64_t)k * 4, cudaMemcpyDeviceToHost, st));
         if (d2) RTD_CUDA(cudaMemcpyAsync(d2, ctx->d2.ptr, nq * (uint64_t)k * 4, cudaMemcpyDeviceToHost, st));

@@ -104,7 +104,8 @@ struct rtd_index {
     // (every build) and rtd_k_nn's query ordering
     cudaStream_t side_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_seed_fork = nullptr,
-                ev_seed_join = nullptr;
+                ev_seed_join = nullptr, ev_sorted = nullptr;
+    rtd::DevBuf wpos;       // queries' Morton positions for the window seed
     rtd::QueryOrderScratch qorder;
     // phase timers (rtd_index_profile_*)
     bool prof = false;
@@ -118,7 +119,7 @@ struct rtd_index {
     ~rtd_index() {
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
-        for (cudaEvent_t e : {ev_fork, ev_join, ev_seed_fork, ev_seed_join})
+        for (cudaEvent_t e : {ev_fork, ev_join, ev_seed_fork, ev_seed_join, ev_sorted})
             if (e) cudaEventDestroy(e);
         if (side_stream) cudaStreamDestroy(side_stream);
     }
@@ -196,9 +197,12 @@ rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd
                        cudaStream_t st);
 
 // k-NN search (knn.cu); with have_perm the query order is given (perm, or
-// nullptr for caller order) instead of computed on the index.
+// nullptr for caller order) instead of computed on the index; wpos, when
+// not nullptr, holds the Morton-window positions of the queries in that
+// order.
 rtd_status knn_search_ex(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k,
                          const rtd_schedule *sched, uint32_t *d_ids, float *d_d2,
-                         cudaStream_t st, bool have_perm, const uint32_t *perm);
+                         cudaStream_t st, bool have_perm, const uint32_t *perm,
+                         const uint32_t *wpos);
 
 }  // namespace rtd

@@ -25,24 +25,21 @@ struct KnnArgs {
     const void *skeys;
     int key64;
     float scale;
+    const uint32_t *wpos;   // optional: each query's position, by processing order
 };
 
-// Seeds a query's list with the 2k points around its position in the
-// points' Morton order (found by binary search over the sorted keys, with
-// the build's quantisation); returns that window [w0, w1) of sorted indices.
-template <int KC>
-__device__ __forceinline__ void morton_window_seed(const KnnArgs &p, float qx, float qy, float qz,
-                                                   int kk, float (&bk)[KC], uint32_t (&bi)[KC],
-                                                   uint32_t &w0, uint32_t &w1) {
-    const IndexHeader *h = p.ix.hdr;
-    const uint32_t n = (uint32_t)p.ix.n;
+// Position of a query among the points' sorted Morton keys (lower bound),
+// with the build's quantisation.
+__device__ __forceinline__ uint32_t morton_position(const IndexHeader *h, const void *skeys,
+                                                    uint32_t n, int key64, float scale, float qx,
+                                                    float qy, float qz) {
     uint32_t lo = 0, hi = n;
-    if (p.key64) {
+    if (key64) {
         const SceneNorm s = scene_norm_cubic(h);
-        const uint64_t key = morton63(quantize(qx, s.lo[0], s.ext[0], p.scale),
-                                      quantize(qy, s.lo[1], s.ext[1], p.scale),
-                                      quantize(qz, s.lo[2], s.ext[2], p.scale));
-        const uint64_t *sk = static_cast<const uint64_t *>(p.skeys);
+        const uint64_t key = morton63(quantize(qx, s.lo[0], s.ext[0], scale),
+                                      quantize(qy, s.lo[1], s.ext[1], scale),
+                                      quantize(qz, s.lo[2], s.ext[2], scale));
+        const uint64_t *sk = static_cast<const uint64_t *>(skeys);
         while (lo < hi) {
             const uint32_t mid = (lo + hi) >> 1;
             if (__ldg(&sk[mid]) < key) lo = mid + 1;
@@ -53,13 +50,40 @@ __device__ __forceinline__ void morton_window_seed(const KnnArgs &p, float qx, f
         const uint32_t key = morton30(quantize(qx, s.lo[0], s.ext[0], 1023.0f),
                                       quantize(qy, s.lo[1], s.ext[1], 1023.0f),
                                       quantize(qz, s.lo[2], s.ext[2], 1023.0f));
-        const uint32_t *sk = static_cast<const uint32_t *>(p.skeys);
+        const uint32_t *sk = static_cast<const uint32_t *>(skeys);
         while (lo < hi) {
             const uint32_t mid = (lo + hi) >> 1;
             if (__ldg(&sk[mid]) < key) lo = mid + 1;
             else hi = mid;
         }
     }
+    return lo;
+}
+
+// Every query's position, in processing order, ahead of the search (so the
+// search's dependent loads do not include the binary search).
+__global__ void __launch_bounds__(256) window_pos_kernel(const IndexHeader *h, const void *skeys,
+                                                         uint32_t n, int key64, float scale,
+                                                         const float *__restrict__ q,
+                                                         const uint32_t *__restrict__ perm,
+                                                         uint64_t nq, uint32_t *__restrict__ pos) {
+    for (uint64_t t = (uint64_t)blockIdx.x * 256 + threadIdx.x; t < nq;
+         t += (uint64_t)gridDim.x * 256) {
+        const uint64_t qi = perm ? perm[t] : t;
+        pos[t] = morton_position(h, skeys, n, key64, scale, q[3 * qi], q[3 * qi + 1], q[3 * qi + 2]);
+    }
+}
+
+// Seeds a query's list with the 2k points around its position in the
+// points' Morton order (given in wpos, else found by binary search over the
+// sorted keys); returns that window [w0, w1) of sorted indices.
+template <int KC>
+__device__ __forceinline__ void morton_window_seed(const KnnArgs &p, uint64_t t, float qx, float qy,
+                                                   float qz, int kk, float (&bk)[KC],
+                                                   uint32_t (&bi)[KC], uint32_t &w0, uint32_t &w1) {
+    const uint32_t n = (uint32_t)p.ix.n;
+    const uint32_t lo = p.wpos ? p.wpos[t]
+                               : morton_position(p.ix.hdr, p.skeys, n, p.key64, p.scale, qx, qy, qz);
     const uint32_t w = 2u * (uint32_t)kk < n ? 2u * (uint32_t)kk : n;
     w0 = lo > (uint32_t)kk ? lo - (uint32_t)kk : 0u;
     if (w0 + w > n) w0 = n - w;
@@ -99,7 +123,7 @@ __global__ void __launch_bounds__(BLOCK) knn_thread_kernel(const KnnArgs p) {
             // Morton neighbours
             list_init<KC>(bk, bi, kk);
             uint32_t w0 = 0, w1 = 0;
-            if (h->root != CHILD_NONE) morton_window_seed<KC>(p, qx, qy, qz, kk, bk, bi, w0, w1);
+            if (h->root != CHILD_NONE) morton_window_seed<KC>(p, t, qx, qy, qz, kk, bk, bi, w0, w1);
             const RoundSpec one{rs.r0sq, rs.mult2, 1u};
             knn_query_thread<KC, true>(tree, one, qx, qy, qz, kk, &s_stack[0][threadIdx.x], BLOCK,
                                        l_stack, p.err, bk, bi, w0, w1);
@@ -662,12 +686,23 @@ rtd_status seed_radius(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k
 
 rtd_status knn_search(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k,
                       const rtd_schedule *sched, uint32_t *d_ids, float *d_d2, cudaStream_t st) {
-    return knn_search_ex(idx, d_q, nq, k, sched, d_ids, d_d2, st, false, nullptr);
+    return knn_search_ex(idx, d_q, nq, k, sched, d_ids, d_d2, st, false, nullptr, nullptr);
+}
+
+// Whether a search with this schedule runs the Morton-window seed (the
+// thread-per-query kernel with RTD_RADIUS_MORTON_WINDOW).
+static bool uses_window(const rtd_index *idx, const rtd_schedule &s, uint32_t k) {
+    uint32_t lanes = s.lanes_per_query;
+    if (lanes == 0) lanes = k <= 16 ? 1 : 32;
+    if (lanes == 1 && k > 32) lanes = 32;
+    return lanes == 1 && s.packet_traversal != RTD_PACKET_ON && s.lane_refill != RTD_REFILL_ON &&
+           s.radius_heuristic == RTD_RADIUS_MORTON_WINDOW && idx->n > 1 && idx->skeys != nullptr;
 }
 
 rtd_status knn_search_ex(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k,
                          const rtd_schedule *sched, uint32_t *d_ids, float *d_d2,
-                         cudaStream_t st, bool have_perm, const uint32_t *given_perm) {
+                         cudaStream_t st, bool have_perm, const uint32_t *given_perm,
+                         const uint32_t *wpos) {
     if (!idx || !idx->hdr.ptr) return fail(RTD_ERR_INVALID_ARGUMENT, "index not built");
     if (nq == 0) return RTD_OK;
     if (!d_q || !d_ids) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL queries or ids");
@@ -701,6 +736,7 @@ rtd_status knn_search_ex(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t
     a.d2 = d_d2;
     a.err = &idx->hdr.as<IndexHeader>()->err;
     a.skeys = nullptr;
+    a.wpos = wpos;
     a.key64 = idx->morton_bits != 30;
     a.scale = idx->morton_bits == 30 ? 1023.0f : (float)((1u << (idx->morton_bits / 3)) - 1u);
     uint32_t lanes = s.lanes_per_query;
@@ -734,7 +770,8 @@ rtd_status knn_search_ex(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t
     } else if (lanes == 1) {
         // The Morton-window seed runs in the thread-per-query kernel; the
         // other launch modes treat the heuristic as RTD_RADIUS_SAMPLED_NN.
-        if (s.radius_heuristic == RTD_RADIUS_MORTON_WINDOW && idx->n > 1) a.skeys = idx->skeys;
+        if (uses_window(idx, s, k)) a.skeys = idx->skeys;
+        else a.wpos = nullptr;
         if (k <= 1) r = launch_thread<1>(a, block, st);
         else if (k <= 2) r = launch_thread<2>(a, block, st);
         else if (k <= 4) r = launch_thread<4>(a, block, st);
@@ -775,6 +812,23 @@ rtd_status k_nn_device(rtd_index *idx, const float *d_points, uint64_t n, const 
     if (s.use_morton_lbv && nq >= 2 && k > 0) ord = order_queries_own(idx->qorder, d_q, nq, &perm, side);
     RTD_CUDA(cudaEventRecord(idx->ev_join, side));
     rtd_status r = index_build(idx, d_points, n, &s, st);
+    // With the Morton-window seed, the queries' positions among the sorted
+    // keys are found on the side stream as soon as the keys are sorted,
+    // while the tree is built.
+    const uint32_t *wpos = nullptr;
+    if (r == RTD_OK && ord == RTD_OK && nq && uses_window(idx, s, k)) {
+        r = idx->wpos.reserve(nq * sizeof(uint32_t));
+        if (r == RTD_OK) {
+            RTD_CUDA(cudaStreamWaitEvent(side, idx->ev_sorted, 0));
+            window_pos_kernel<<<grid_for(nq, 256, 148 * 8), 256, 0, side>>>(
+                idx->hdr.as<IndexHeader>(), idx->skeys, (uint32_t)idx->n, idx->morton_bits != 30,
+                idx->morton_bits == 30 ? 1023.0f : (float)((1u << (idx->morton_bits / 3)) - 1u),
+                d_q, perm, nq, idx->wpos.as<uint32_t>());
+            RTD_LAUNCH_CHECK();
+            RTD_CUDA(cudaEventRecord(idx->ev_join, side));
+            wpos = idx->wpos.as<uint32_t>();
+        }
+    }
     RTD_CUDA(cudaStreamWaitEvent(st, idx->ev_join, 0));   // also on the error paths
     RTD_TRY(ord);
     RTD_TRY(r);
@@ -782,7 +836,7 @@ rtd_status k_nn_device(rtd_index *idx, const float *d_points, uint64_t n, const 
         fold_errors_kernel<<<1, 1, 0, st>>>(idx->hdr.as<IndexHeader>(), idx->qorder.hdr.as<IndexHeader>());
         RTD_LAUNCH_CHECK();
     }
-    return knn_search_ex(idx, d_q, nq, k, &s, d_ids, d_d2, st, true, perm);
+    return knn_search_ex(idx, d_q, nq, k, &s, d_ids, d_d2, st, true, perm, wpos);
 }
 
 }  // namespace rtd

@@ -523,6 +523,8 @@ rtd_status build_typed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStrea
     K *skeys = in_alt ? idx->keys_alt.as<K>() : idx->keys.as<K>();
     idx->skeys = skeys;
     idx->mark(EV_BUILD_SORTED, st);
+    // the sorted keys are ready: side-stream work may wait on this
+    if (idx->ev_sorted) RTD_CUDA(cudaEventRecord(idx->ev_sorted, st));
     return build_tree_sorted<K>(idx, skeys, n, st);
 }
 
@@ -590,7 +592,8 @@ template rtd_status build_tree_sorted<uint64_t>(rtd_index *, const uint64_t *, u
 rtd_status ensure_side_stream(rtd_index *idx) {
     if (idx->side_stream) return RTD_OK;
     RTD_CUDA(cudaStreamCreateWithFlags(&idx->side_stream, cudaStreamNonBlocking));
-    for (cudaEvent_t *e : {&idx->ev_fork, &idx->ev_join, &idx->ev_seed_fork, &idx->ev_seed_join})
+    for (cudaEvent_t *e : {&idx->ev_fork, &idx->ev_join, &idx->ev_seed_fork, &idx->ev_seed_join,
+                           &idx->ev_sorted})
         RTD_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     return RTD_OK;
 }
