@@ -102,17 +102,11 @@ struct rtd_context {
     rtd_index index;
     DevBuf data, queries, ids, d2, pairs;
     cudaStream_t stream = nullptr;
-    // k_nn! overlap: the queries are copied and ordered on side_stream while
-    // the index is built on stream
-    cudaStream_t side_stream = nullptr;
-    cudaEvent_t ev_data = nullptr, ev_queries = nullptr;
-    QueryOrderScratch qorder;
+    cudaEvent_t ev_data = nullptr;  // the points are on the device (k_nn!)
     rtd_context_bh *bh = nullptr;   // created on the first barnes_hut! call
     ~rtd_context() {
         delete bh;
         if (ev_data) cudaEventDestroy(ev_data);
-        if (ev_queries) cudaEventDestroy(ev_queries);
-        if (side_stream) cudaStreamDestroy(side_stream);
     }
 };
 
@@ -244,7 +238,9 @@ rtd_status rtd_context_create(rtd_context **out) {
     rtd_context *c = new (std::nothrow) rtd_context();
     if (!c) return fail(RTD_ERR_OUT_OF_MEMORY, "host allocation failed");
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_data, cudaEventDisableTiming);
     if (e != cudaSuccess) {
+        if (c->stream) cudaStreamDestroy(c->stream);
         delete c;
         return cuda_fail(e, "cudaStreamCreateWithFlags");
     }
@@ -265,48 +261,29 @@ rtd_status rtd_k_nn_host(rtd_context *ctx, const rtd_vec3 *data, uint64_t n,
     if (!ctx) return fail(RTD_ERR_INVALID_ARGUMENT, "context is NULL");
     if ((n && !data) || (nq && (!queries || !ids)))
         return fail(RTD_ERR_INVALID_ARGUMENT, "NULL host buffer");
-    rtd_schedule def;
-    rtd_schedule_default(&def);
-    const rtd_schedule &s = sched ? *sched : def;
     cudaStream_t st = ctx->stream;
-    if (!ctx->side_stream) {
-        RTD_CUDA(cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking));
-        RTD_CUDA(cudaEventCreateWithFlags(&ctx->ev_data, cudaEventDisableTiming));
-        RTD_CUDA(cudaEventCreateWithFlags(&ctx->ev_queries, cudaEventDisableTiming));
-    }
-    cudaStream_t side = ctx->side_stream;
+    rtd_index *idx = &ctx->index;
+    RTD_TRY(ensure_side_stream(idx));
     RTD_TRY(ctx->data.reserve(n * sizeof(rtd_vec3)));
     RTD_TRY(ctx->queries.reserve(nq * sizeof(rtd_vec3)));
     RTD_TRY(ctx->ids.reserve(nq * (uint64_t)k * sizeof(uint32_t)));
     if (d2) RTD_TRY(ctx->d2.reserve(nq * (uint64_t)k * sizeof(float)));
     // The points go first at full copy bandwidth; the queries follow on the
-    // side stream and are ordered there while the index is built.
+    // index's side stream, where k_nn_device then orders them (and finds
+    // their Morton-window positions) while the index is built.
     if (n) RTD_CUDA(cudaMemcpyAsync(ctx->data.ptr, data, n * sizeof(rtd_vec3), cudaMemcpyHostToDevice, st));
     RTD_CUDA(cudaEventRecord(ctx->ev_data, st));
-    RTD_CUDA(cudaStreamWaitEvent(side, ctx->ev_data, 0));
-    if (nq) RTD_CUDA(cudaMemcpyAsync(ctx->queries.ptr, queries, nq * sizeof(rtd_vec3), cudaMemcpyHostToDevice, side));
-    const uint32_t *perm = nullptr;
-    rtd_status ord = RTD_OK;
-    if (s.use_morton_lbv) ord = order_queries_own(ctx->qorder, ctx->queries.as<float>(), nq, &perm, side);
-    RTD_CUDA(cudaEventRecord(ctx->ev_queries, side));
-    rtd_status r = index_build(&ctx->index, ctx->data.as<float>(), n, &s, st);
-    RTD_CUDA(cudaStreamWaitEvent(st, ctx->ev_queries, 0));   // also on the error paths
-    RTD_TRY(ord);
-    RTD_TRY(r);
-    RTD_TRY(knn_search_ex(&ctx->index, ctx->queries.as<float>(), nq, k, &s, ctx->ids.as<uint32_t>(),
-                          d2 ? ctx->d2.as<float>() : nullptr, st, true, perm, nullptr));
+    RTD_CUDA(cudaStreamWaitEvent(idx->side_stream, ctx->ev_data, 0));
+    if (nq)
+        RTD_CUDA(cudaMemcpyAsync(ctx->queries.ptr, queries, nq * sizeof(rtd_vec3),
+                                 cudaMemcpyHostToDevice, idx->side_stream));
+    RTD_TRY(k_nn_device(idx, ctx->data.as<float>(), n, ctx->queries.as<float>(), nq, k, sched,
+                        ctx->ids.as<uint32_t>(), d2 ? ctx->d2.as<float>() : nullptr, st));
     if (nq) {
         RTD_CUDA(cudaMemcpyAsync(ids, ctx->ids.ptr, nq * (uint64_t)k * 4, cudaMemcpyDeviceToHost, st));
         if (d2) RTD_CUDA(cudaMemcpyAsync(d2, ctx->d2.ptr, nq * (uint64_t)k * 4, cudaMemcpyDeviceToHost, st));
     }
-    uint32_t qerr = 0;   // device errors of the query ordering
-    if (ctx->qorder.hdr.ptr) {
-        IndexHeader *qh = ctx->qorder.hdr.as<IndexHeader>();
-        RTD_CUDA(cudaMemcpyAsync(&qerr, &qh->err, sizeof(qerr), cudaMemcpyDeviceToHost, st));
-    }
-    rtd_status r2 = check_index_errors(&ctx->index, st);   // synchronises
-    if (qerr) return status_from_deverr(qerr);   // the next ordering re-initialises the word
-    return r2;
+    return check_index_errors(idx, st);   // synchronises
 }
 
 rtd_status rtd_range_count(rtd_index *idx, const float *d_queries, uint64_t nq, float radius,
