@@ -48,7 +48,8 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the BH / batched sub-benchmarks")
-    ap.add_argument("--only", choices=["range", "bh", "batch"], default=None,
+    ap.add_argument("--only", choices=["range", "bh", "batch", "dbscan", "leapfrog", "io"],
+                    default=None,
                     help="run one sub-benchmark alone (one GPU) and print its JSON")
     return ap.parse_args()
 
@@ -283,6 +284,9 @@ def run_ours(args, ws, rank, local):
         extras["range"] = bench_range(args, dev, flush, P, Q, s)
         extras["barnes_hut"] = bench_bh(args, dev, flush)
         extras["batched"] = bench_batch(args, dev, flush)
+        extras["dbscan"] = bench_dbscan(args, dev, flush)
+        extras["leapfrog"] = bench_leapfrog(args, dev, flush)
+        extras["io"] = bench_io(args)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -604,6 +608,158 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------ DBSCAN / leapfrog / io
+def bench_dbscan(args, dev, flush) -> dict:
+    """DBSCAN over the range query (index build + neighbour count + pair fill
+    + union-find), eps for a mean of 20 neighbours, min_pts 10:
+    - on 200K clustered points, beside scikit-learn's DBSCAN on the same
+      points with all host cores (the route the oracle's DBSCAN is pinned
+      to), with cluster and noise counts compared;
+    - on the 1.8M-point headline cloud (GPU only)."""
+    import numpy as np
+    import torch
+    import rtdsl
+    from rtdsl import workloads
+    from rtdsl.api import radius_for_mean_count
+
+    def run(pts, eps, min_pts):
+        P = torch.from_numpy(pts).to(dev)
+        ix = rtdsl.Index()
+        s = rtdsl.default_schedule(leaf_size=12, morton_bits=42)
+
+        def step():
+            ix.build(P, s)
+            return rtdsl.dbscan(P, eps, min_pts, index=ix)
+
+        for _ in range(max(args.warmup, 3)):
+            labels, nc = step()
+        ms = []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = _events()
+            e0.record()
+            labels, nc = step()
+            e1.record()
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return statistics.mean(ms), labels.cpu().numpy(), nc
+
+    def eps_for(pts, mean):
+        P = torch.from_numpy(pts).to(dev)
+        ix = rtdsl.Index().build(P, rtdsl.default_schedule(leaf_size=12, morton_bits=42))
+        return radius_for_mean_count(ix, P, mean)
+
+    small, _ = workloads.clustered(n=200_000, nq=1, seed=3)
+    eps_s = eps_for(small, 20.0)
+    ms_s, labels_s, nc_s = run(small, eps_s, 10)
+    cpu = None
+    try:
+        import os as _os
+        from sklearn.cluster import DBSCAN
+        t0 = time.perf_counter()
+        sk = DBSCAN(eps=eps_s, min_samples=10, n_jobs=-1).fit(small.astype(np.float64))
+        cpu_s = time.perf_counter() - t0
+        sk_nc = int(sk.labels_.max()) + 1
+        cpu = {"value": len(small) / cpu_s, "unit": "points/s", "cores": _os.cpu_count(),
+               "kind": "scikit-learn DBSCAN (n_jobs=-1), the oracle's pinning route",
+               "sample": "the same 200K points", "seconds": cpu_s,
+               "clusters_equal": sk_nc == int(nc_s),
+               "noise_equal": int((sk.labels_ == -1).sum()) == int((labels_s == -1).sum())}
+    except Exception as e:   # noqa: BLE001
+        cpu = {"unavailable": str(e)[:200]}
+    big, _ = load_workload()
+    eps_b = eps_for(big, 20.0)
+    ms_b, _, nc_b = run(big, eps_b, 10)
+    return {
+        "metric": "DBSCAN points/s (index build + clustering)", "value": len(big) / (ms_b / 1e3),
+        "unit": "points/s",
+        "config": {"workload": "clustered_1p8m: the headline cloud, eps for a mean of 20 "
+                               "neighbours, min_pts 10", "eps": eps_b, "clusters": int(nc_b)},
+        "ms": ms_b,
+        "small": {"workload": "clustered_200k", "eps": eps_s, "ms": ms_s,
+                  "points_per_s": len(small) / (ms_s / 1e3), "clusters": int(nc_s)},
+        "cpu_baseline": cpu,
+    }
+
+
+def bench_leapfrog(args, dev, flush, steps_per_call: int = 4) -> dict:
+    """Barnes-Hut leapfrog time integration on the 1M-body Plummer sphere
+    (theta 0.5, eps 1e-3, quadrupole): each step rebuilds the tree from the
+    new positions and walks it; body-steps per second."""
+    import torch
+    import rtdsl
+    from rtdsl import workloads
+    from rtdsl._capi import BH_LAW_PLUMMER, default_bh_params
+
+    n = 1_000_000
+    pos, mass = workloads.plummer(n, seed=7)
+    p = default_bh_params(law=BH_LAW_PLUMMER, theta=0.5, eps=1e-3, G=1.0, quadrupole=1, bucket=32)
+    P = torch.from_numpy(pos).to(dev)
+    M = torch.from_numpy(mass).to(dev)
+    V = torch.zeros_like(P)
+    bh = rtdsl.BarnesHut()
+    dt = 1e-3
+    acc = None
+    for _ in range(max(args.warmup, 3)):
+        acc = bh.leapfrog(P, V, M, dt, steps_per_call, p, acc=acc)
+    ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = _events()
+        e0.record()
+        acc = bh.leapfrog(P, V, M, dt, steps_per_call, p, acc=acc)
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    m = statistics.mean(ms)
+    return {"metric": "BH leapfrog body-steps/s", "value": n * steps_per_call / (m / 1e3),
+            "unit": "body-steps/s",
+            "config": {"workload": "plummer_1m: 1M-body Plummer sphere, theta 0.5, eps 1e-3, "
+                                   "quadrupole, dt 1e-3; a step = tree rebuild + walk + kick/drift",
+                       "steps_per_call": steps_per_call},
+            "ms_per_step": m / steps_per_call,
+            "cpu_baseline": None,
+            "cpu_baseline_note": "none: the reference has no runnable Barnes-Hut integration"}
+
+
+def bench_io(args) -> dict:
+    """The reference point-file format ("x,y,z" lines, gprt-sandbox/src/io.rs):
+    the headline cloud written as text, then parsed by rtd_load_points_csv
+    (native, all host threads); pandas' C parser on the same file is timed
+    beside it for context."""
+    import numpy as np
+    import os as _os
+    import tempfile
+    from rtdsl import io as rio
+
+    pts, _ = load_workload()
+    with tempfile.TemporaryDirectory() as d:
+        path = _os.path.join(d, "points.csv")
+        np.savetxt(path, pts, fmt="%.7g", delimiter=",")
+        size = _os.path.getsize(path)
+        rio.load_points_csv(path)
+        ts = []
+        for _ in range(max(args.steps, 3)):
+            t0 = time.perf_counter()
+            got = rio.load_points_csv(path)
+            ts.append(time.perf_counter() - t0)
+        ok = got.shape == pts.shape and bool(np.allclose(got, pts, rtol=1e-6, atol=0.0))
+        ctx = None
+        try:
+            import pandas as pd
+            t0 = time.perf_counter()
+            pd.read_csv(path, header=None, dtype=np.float32, engine="c")
+            ctx = {"seconds": time.perf_counter() - t0, "what": "pandas read_csv, C engine"}
+        except Exception as e:   # noqa: BLE001
+            ctx = {"unavailable": str(e)[:200]}
+    t = statistics.median(ts)
+    return {"metric": "point-file parse MB/s", "value": size / t / 1e6, "unit": "MB/s",
+            "config": {"workload": "clustered_1p8m written as x,y,z text lines", "bytes": size,
+                       "points": int(len(pts))},
+            "points_per_s": len(pts) / t, "ms": t * 1e3, "matches_input": ok,
+            "host_threads": _os.cpu_count(), "context": ctx}
+
+
 def main():
     args = parse_args()
     ws, rank, local = dist_env()
@@ -621,6 +777,12 @@ def main():
                               torch.from_numpy(q).to(dev), tuned_schedule(rtdsl))
         elif args.only == "bh":
             out = bench_bh(args, dev, flush)
+        elif args.only == "dbscan":
+            out = bench_dbscan(args, dev, flush)
+        elif args.only == "leapfrog":
+            out = bench_leapfrog(args, dev, flush)
+        elif args.only == "io":
+            out = bench_io(args)
         else:
             out = bench_batch(args, dev, flush)
         print(json.dumps(out), flush=True)

@@ -137,7 +137,10 @@ extern "C" rtd_status rtd_dbscan(rtd_index *idx, const float *d_points, uint64_t
     if (n == 0) return RTD_OK;
     if (!d_points || !d_labels) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL device buffer");
     cudaStream_t st = (cudaStream_t)stream;
-    DevBuf counts, pairs, core, parent, flag, rank, ncbuf;
+    // scratch kept on the index and grown only, so repeated calls allocate nothing
+    DevBuf &counts = idx->db_counts, &pairs = idx->db_pairs, &core = idx->db_core,
+           &parent = idx->db_parent, &flag = idx->db_flag, &rank = idx->db_rank,
+           &ncbuf = idx->db_nc;
     RTD_TRY(counts.reserve(n * 4));
     uint64_t total = 0;
     RTD_TRY(range_count(idx, d_points, n, eps, nullptr, counts.as<uint32_t>(), &total, st));
@@ -162,7 +165,7 @@ extern "C" rtd_status rtd_dbscan(rtd_index *idx, const float *d_points, uint64_t
     dbscan_roots_kernel<<<g, BLOCK, 0, st>>>(n, core.as<uint8_t>(), parent.as<uint32_t>(),
                                              flag.as<uint32_t>(), err);
     RTD_LAUNCH_CHECK();
-    ScanScratch scan;
+    ScanScratch &scan = idx->db_scan;
     RTD_TRY(ncbuf.reserve(sizeof(uint32_t)));
     uint32_t *d_nc = ncbuf.as<uint32_t>();
     RTD_TRY(exclusive_scan_u32_32(flag.as<uint32_t>(), rank.as<uint32_t>(), n, d_nc, scan, err, st));

@@ -89,6 +89,9 @@ struct rtd_index {
     rtd::DevBuf qkeys, qkeys_alt, qperm, qperm_alt;
     const void *skeys = nullptr;   // the points' sorted Morton keys (in keys or keys_alt)
     rtd::DevBuf rcounts, roffsets, rcursor, rpairs_alt, rkeys, rkeys_alt;
+    // DBSCAN scratch (rtd_dbscan): counts, pairs, core flags, union-find
+    rtd::DevBuf db_counts, db_pairs, db_core, db_parent, db_flag, db_rank, db_nc;
+    rtd::ScanScratch db_scan;
     // What the last range count left behind for a fill of the same queries:
     // per-query exclusive offsets (roffsets), the total, and the query order.
     // Cleared by a build and by any other query ordering on this index.
