@@ -151,7 +151,7 @@ def tune_knn(P, Q, k: int, tag: str, grid: dict | None = None, reps: int = 3,
 
 
 BATCH_GRID = {
-    "leaf_size": [2, 4, 8],
+    "leaf_size": [8, 16, 32, 64],
     "radius_param": [0.5, 1.0, 2.0],
     "radius_increment_mult": [2.0, 4.0],
     "lanes_per_query": [0, 32],

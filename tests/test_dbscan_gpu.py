@@ -59,3 +59,18 @@ def test_spatial_join(rtd, orc, cuda):
                                   exclude_self=True).cpu().numpy().view(np.uint32)
     ref = orc.range_pairs(a, a, 0.03)
     np.testing.assert_array_equal(self_pairs, ref[ref[:, 0] != ref[:, 1]])
+
+
+def test_dbscan_reuses_index_scratch(rtd, orc, cuda):
+    """DBSCAN keeps its scratch on the index: calls on one index with more,
+    then fewer neighbour pairs (larger, then smaller eps) and on rebuilt
+    point sets of other sizes all match the oracle."""
+    ix = rtd.Index()
+    for n_noise, eps, mp in ((1500, 0.02, 10), (1500, 0.06, 5), (300, 0.01, 3), (4000, 0.03, 8)):
+        pts = blobs(11, n_noise=n_noise)
+        P = torch.from_numpy(pts).cuda()
+        ix.build(P)
+        labels, nc = rtd.dbscan(P, eps, mp, index=ix)
+        ref, ref_nc = orc.dbscan(pts, eps, mp)
+        np.testing.assert_array_equal(labels.cpu().numpy(), ref)
+        assert nc == ref_nc
