@@ -57,8 +57,10 @@ def _load() -> dict:
 
 
 def cached_schedule(tag: str, default: _capi.Schedule | None = None) -> _capi.Schedule:
-    """Schedule tuned for `tag` on this GPU type, else `default`."""
-    s = default if default is not None else _capi.default_schedule()
+    """Schedule tuned for `tag` on this GPU type, else a copy of `default`.
+    The caller's schedule is never modified."""
+    s = _capi.Schedule.from_buffer_copy(default) if default is not None \
+        else _capi.default_schedule()
     entry = _load().get(tag)
     if not entry:
         return s

@@ -43,6 +43,16 @@ def test_schedule_defaults(rtd):
     assert s.use_morton_lbv == 1 and s.leaf_size == 4 and s.max_rounds == 32
 
 
+def test_cached_schedule_leaves_default_alone(rtd):
+    from rtdsl import autotune
+    base = rtd.default_schedule()
+    before = base.as_dict()
+    for tag in ("clustered_1p8m_k5", "clustered_1p8m_r50", "clouds_256", "no_such_tag"):
+        s = autotune.cached_schedule(tag, base)
+        assert s is not base
+    assert base.as_dict() == before
+
+
 def test_status_strings(rtd):
     lib = rtd.load()
     assert lib.rtd_status_string(0) == b"RTD_OK"
