@@ -96,9 +96,10 @@ __device__ __forceinline__ void morton_window_seed(const KnnArgs &p, uint64_t t,
     }
 }
 
-// One thread per query.
+// One thread per query.  Lists of up to 5 slots keep 40 warps resident per
+// SM (48 registers a thread); longer lists take the registers they need.
 template <int KC, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) knn_thread_kernel(const KnnArgs p) {
+__global__ void __launch_bounds__(BLOCK, KC <= 5 ? 1280 / BLOCK : 0) knn_thread_kernel(const KnnArgs p) {
     __shared__ BvhNode s_top[TOP_MAX];
     __shared__ uint2 s_stack[SHORT_STACK][BLOCK];
     const IndexHeader *h = p.ix.hdr;
@@ -238,16 +239,14 @@ __global__ void __launch_bounds__(BLOCK) knn_refill_kernel(const KnnArgs p,
             atomicOr(p.err, DEVERR_STACK);
             done = true;
         } else {
-            uint32_t lf_first[2], lf_cnt[2];
-            int nleaf = 0;
+            uint32_t fa = 0, ca = 0, fb = 0, cb = 0;   // leaf ranges to test
             uint32_t next = CHILD_NONE;
             float k0 = 0.f, k1 = 0.f;
             bool v0 = false, v1 = false;
             uint4 d = make_uint4(0, 0, 0, 0);
             if (node & CHILD_LEAF) {
-                lf_first[0] = node & CHILD_INDEX;
-                lf_cnt[0] = root_count;
-                nleaf = 1;
+                fa = node & CHILD_INDEX;
+                ca = root_count;
             } else {
                 float4 a, b, c;
                 load_node(s_top, p.ix.nodes, node, a, b, c, d);
@@ -259,19 +258,18 @@ __global__ void __launch_bounds__(BLOCK) knn_refill_kernel(const KnnArgs p,
                     if (v0) v0 = !(box_max_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y) <= prev);
                     if (v1) v1 = !(box_max_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w) <= prev);
                 }
-                if (v0 && (d.x & CHILD_LEAF)) { lf_first[nleaf] = d.x & CHILD_INDEX; lf_cnt[nleaf] = d.z; ++nleaf; v0 = false; }
-                if (v1 && (d.y & CHILD_LEAF)) { lf_first[nleaf] = d.y & CHILD_INDEX; lf_cnt[nleaf] = d.w; ++nleaf; v1 = false; }
+                if (v0 && (d.x & CHILD_LEAF)) { fa = d.x & CHILD_INDEX; ca = d.z; v0 = false; }
+                if (v1 && (d.y & CHILD_LEAF)) { fb = d.y & CHILD_INDEX; cb = d.w; v1 = false; }
             }
-            for (int l = 0; l < nleaf; ++l) {
-                for (uint32_t j = 0; j < lf_cnt[l]; ++j) {
-                    const float4 pt = __ldg(&p.ix.pts[lf_first[l] + j]);
-                    const float key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
-                    const uint32_t id = __float_as_uint(pt.w);
-                    if (key <= bound && key > prev && key_less(key, id, bk[KC - 1], bi[KC - 1]))
-                        list_insert<KC>(bk, bi, key, id);
-                }
+            const uint32_t tot = ca + cb;
+            for (uint32_t j = 0; j < tot; ++j) {
+                const float4 pt = __ldg(&p.ix.pts[j < ca ? fa + j : fb + (j - ca)]);
+                const float key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
+                const uint32_t id = __float_as_uint(pt.w);
+                if (key <= bound && key > prev && key_less(key, id, bk[KC - 1], bi[KC - 1]))
+                    list_insert<KC>(bk, bi, key, id);
             }
-            if (nleaf) lim = fminf(bound, bk[KC - 1]);
+            if (tot) lim = fminf(bound, bk[KC - 1]);
             if (!(node & CHILD_LEAF)) {
                 v0 = v0 && !(k0 > lim);
                 v1 = v1 && !(k1 > lim);
@@ -381,18 +379,18 @@ __global__ void __launch_bounds__(WARPS * 32) knn_packet_kernel(const KnnArgs p)
                     if (lane == 0) atomicOr(p.err, DEVERR_STACK);
                     break;
                 }
-                uint32_t lf_first[2], lf_cnt[2];
-                bool lf_want[2];
-                int nleaf = 0;
+                // leaf ranges [fa, fa + ca) and [fb, fb + cb) (warp-uniform)
+                // and whether this lane wants each
+                uint32_t fa = 0, ca = 0, fb = 0, cb = 0;
+                bool wa = false, wb = false;
                 uint32_t next = CHILD_NONE;
                 float k0 = 0.f, k1 = 0.f;
                 bool w0 = false, w1 = false;
                 uint4 d = make_uint4(0, 0, 0, 0);
                 if (node & CHILD_LEAF) {
-                    lf_first[0] = node & CHILD_INDEX;
-                    lf_cnt[0] = root_count;
-                    lf_want[0] = active;
-                    nleaf = 1;
+                    fa = node & CHILD_INDEX;
+                    ca = root_count;
+                    wa = active;
                 } else {
                     float4 a, b, c;
                     load_node(s_top, gn, node, a, b, c, d);
@@ -405,25 +403,24 @@ __global__ void __launch_bounds__(WARPS * 32) knn_packet_kernel(const KnnArgs p)
                         if (w1) w1 = !(box_max_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w) <= prev);
                     }
                     if ((d.x & CHILD_LEAF) && __any_sync(0xffffffffu, w0)) {
-                        lf_first[nleaf] = d.x & CHILD_INDEX; lf_cnt[nleaf] = d.z; lf_want[nleaf] = w0; ++nleaf;
+                        fa = d.x & CHILD_INDEX; ca = d.z; wa = w0;
                     }
                     if ((d.y & CHILD_LEAF) && __any_sync(0xffffffffu, w1)) {
-                        lf_first[nleaf] = d.y & CHILD_INDEX; lf_cnt[nleaf] = d.w; lf_want[nleaf] = w1; ++nleaf;
+                        fb = d.y & CHILD_INDEX; cb = d.w; wb = w1;
                     }
                     if (d.x & CHILD_LEAF) w0 = false;
                     if (d.y & CHILD_LEAF) w1 = false;
                 }
-                for (int l = 0; l < nleaf; ++l) {
-                    const bool want = lf_want[l];
-                    for (uint32_t j = 0; j < lf_cnt[l]; ++j) {
-                        float4 pt = __ldg(&pts[lf_first[l] + j]);
-                        float key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
-                        uint32_t id = __float_as_uint(pt.w);
-                        if (want && key <= bound && key > prev && key_less(key, id, bk[KC - 1], bi[KC - 1]))
-                            list_insert<KC>(bk, bi, key, id);
-                    }
+                const uint32_t tot = ca + cb;
+                for (uint32_t j = 0; j < tot; ++j) {
+                    const bool want = j < ca ? wa : wb;
+                    float4 pt = __ldg(&pts[j < ca ? fa + j : fb + (j - ca)]);
+                    float key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
+                    uint32_t id = __float_as_uint(pt.w);
+                    if (want && key <= bound && key > prev && key_less(key, id, bk[KC - 1], bi[KC - 1]))
+                        list_insert<KC>(bk, bi, key, id);
                 }
-                if (nleaf) lim = active ? fminf(bound, bk[KC - 1]) : -1.0f;
+                if (tot) lim = active ? fminf(bound, bk[KC - 1]) : -1.0f;
                 if (!(node & CHILD_LEAF)) {
                     w0 = w0 && !(k0 > lim);
                     w1 = w1 && !(k1 > lim);

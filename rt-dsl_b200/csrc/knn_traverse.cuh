@@ -99,8 +99,10 @@ __device__ __forceinline__ void knn_query_thread(const TreeRef &t, const RoundSp
         int sp = 0;
         uint32_t visits = 0;
         while (true) {
-            uint32_t lf_first[2], lf_cnt[2];
-            int nleaf = 0;
+            // up to two leaf ranges to test, [fa, fa + ca) then [fb, fb + cb)
+            // (named scalars: an array indexed by a leaf count would live in
+            // local memory)
+            uint32_t fa = 0, ca = 0, fb = 0, cb = 0;
             uint32_t next = CHILD_NONE;
             if (++visits > t.visit_cap) {
                 atomicOr(err, DEVERR_STACK);
@@ -110,9 +112,8 @@ __device__ __forceinline__ void knn_query_thread(const TreeRef &t, const RoundSp
             bool v0 = false, v1 = false;
             uint4 d = make_uint4(0, 0, 0, 0);
             if (node & CHILD_LEAF) {
-                lf_first[0] = node & CHILD_INDEX;
-                lf_cnt[0] = t.root_count;
-                nleaf = 1;
+                fa = node & CHILD_INDEX;
+                ca = t.root_count;
             } else {
                 float4 a, b, c;
                 load_node(t.s_top, t.nodes, node, a, b, c, d);
@@ -124,20 +125,20 @@ __device__ __forceinline__ void knn_query_thread(const TreeRef &t, const RoundSp
                     if (v0) v0 = !(box_max_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y) <= prev);
                     if (v1) v1 = !(box_max_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w) <= prev);
                 }
-                if (v0 && (d.x & CHILD_LEAF)) { lf_first[nleaf] = d.x & CHILD_INDEX; lf_cnt[nleaf] = d.z; ++nleaf; v0 = false; }
-                if (v1 && (d.y & CHILD_LEAF)) { lf_first[nleaf] = d.y & CHILD_INDEX; lf_cnt[nleaf] = d.w; ++nleaf; v1 = false; }
+                if (v0 && (d.x & CHILD_LEAF)) { fa = d.x & CHILD_INDEX; ca = d.z; v0 = false; }
+                if (v1 && (d.y & CHILD_LEAF)) { fb = d.y & CHILD_INDEX; cb = d.w; v1 = false; }
             }
-            for (int l = 0; l < nleaf; ++l) {
-                for (uint32_t j = 0; j < lf_cnt[l]; ++j) {
-                    if (SEEDED && lf_first[l] + j - skip_lo < skip_hi - skip_lo) continue;
-                    float4 pt = __ldg(&t.pts[lf_first[l] + j]);
-                    float key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
-                    uint32_t id = __float_as_uint(pt.w);
-                    if (key <= bound && key > prev && key_less(key, id, bk[KC - 1], bi[KC - 1]))
-                        list_insert<KC>(bk, bi, key, id);
-                }
+            const uint32_t tot = ca + cb;
+            for (uint32_t j = 0; j < tot; ++j) {
+                const uint32_t pi = j < ca ? fa + j : fb + (j - ca);
+                if (SEEDED && pi - skip_lo < skip_hi - skip_lo) continue;
+                float4 pt = __ldg(&t.pts[pi]);
+                float key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
+                uint32_t id = __float_as_uint(pt.w);
+                if (key <= bound && key > prev && key_less(key, id, bk[KC - 1], bi[KC - 1]))
+                    list_insert<KC>(bk, bi, key, id);
             }
-            if (nleaf) lim = fminf(bound, bk[KC - 1]);
+            if (tot) lim = fminf(bound, bk[KC - 1]);
             if (!(node & CHILD_LEAF)) {
                 v0 = v0 && !(k0 > lim);
                 v1 = v1 && !(k1 > lim);
@@ -263,8 +264,7 @@ __device__ __forceinline__ void knn_query_warp(const TreeRef &t, const RoundSpec
         int sp = 0;
         uint32_t visits = 0;
         while (true) {
-            uint32_t lf_first[2], lf_cnt[2];
-            int nleaf = 0;
+            uint32_t fa = 0, ca = 0, fb = 0, cb = 0;   // leaf ranges, as in knn_query_thread
             uint32_t next = CHILD_NONE;
             float k0 = 0.f, k1 = 0.f;
             uint4 d = make_uint4(0, 0, 0, 0);
@@ -274,9 +274,8 @@ __device__ __forceinline__ void knn_query_warp(const TreeRef &t, const RoundSpec
                 break;
             }
             if (node & CHILD_LEAF) {
-                lf_first[0] = node & CHILD_INDEX;
-                lf_cnt[0] = t.root_count;
-                nleaf = 1;
+                fa = node & CHILD_INDEX;
+                ca = t.root_count;
             } else {
                 float4 a, b, c;
                 load_node(t.s_top, t.nodes, node, a, b, c, d);
@@ -288,18 +287,18 @@ __device__ __forceinline__ void knn_query_warp(const TreeRef &t, const RoundSpec
                     if (v0) v0 = !(box_max_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y) <= prev);
                     if (v1) v1 = !(box_max_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w) <= prev);
                 }
-                if (v0 && (d.x & CHILD_LEAF)) { lf_first[nleaf] = d.x & CHILD_INDEX; lf_cnt[nleaf] = d.z; ++nleaf; v0 = false; }
-                if (v1 && (d.y & CHILD_LEAF)) { lf_first[nleaf] = d.y & CHILD_INDEX; lf_cnt[nleaf] = d.w; ++nleaf; v1 = false; }
+                if (v0 && (d.x & CHILD_LEAF)) { fa = d.x & CHILD_INDEX; ca = d.z; v0 = false; }
+                if (v1 && (d.y & CHILD_LEAF)) { fb = d.y & CHILD_INDEX; cb = d.w; v1 = false; }
             }
-            if (nleaf) {   // both leaves' points, 32 per batch
-                const uint32_t c0 = lf_cnt[0], tot = c0 + (nleaf > 1 ? lf_cnt[1] : 0u);
+            const uint32_t tot = ca + cb;
+            if (tot) {   // both leaves' points, 32 per batch
                 for (uint32_t j0 = 0; j0 < tot; j0 += 32) {
                     const uint32_t j = j0 + lane;
                     float key = INFINITY;
                     uint32_t id = EMPTY_ID;
                     bool acc = false;
                     if (j < tot) {
-                        const float4 pt = __ldg(&t.pts[j < c0 ? lf_first[0] + j : lf_first[1] + (j - c0)]);
+                        const float4 pt = __ldg(&t.pts[j < ca ? fa + j : fb + (j - ca)]);
                         key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
                         id = __float_as_uint(pt.w);
                         acc = key <= bound && key > prev && key_less(key, id, wk, wi);
