@@ -137,15 +137,21 @@ __global__ void __launch_bounds__(BLOCK) karras_kernel(const K *__restrict__ key
 
 // ---------------------------------------------------- box pyramid
 // Boxes of aligned runs of the sorted points: level j entry e covers points
-// [e * 32^j, (e+1) * 32^j) as (lo.xyz, -) (hi.xyz, -).  A run holding a
+// [e * 8^j, (e+1) * 8^j) as (lo.xyz, -) (hi.xyz, -).  A run holding a
 // point with a NaN coordinate gets an unbounded box: such a point is never
 // a neighbour, but no finite box holds it, so no search may treat a
-// subtree containing it as lying wholly inside a ball.
-constexpr int PYR_MAX = 6;   // levels 1..6 cover 32^6 = 2^30 points
+// subtree containing it as lying wholly inside a ball.  Base 8 keeps the
+// walk of a range short: at most 7 entries per end and level.
+constexpr int PYR_SH = 3;                  // log2 of the base
+constexpr uint32_t PYR_B = 1u << PYR_SH;   // 8 entries of a level per entry of the next
+constexpr int PYR_MAX = 10;                // levels 1..10 cover 8^10 = 2^30 points
+// Levels 1..nlev lie back to back in pyr (2 float4 per entry), level j
+// holding ceil(n / 8^j) entries; nlev is the first level of <= 8 entries.
 struct Pyramid {
     const float4 *pts;
-    const float4 *lvl[PYR_MAX + 1];   // lvl[j]: 2 float4 per entry; lvl[0] unused
-    int nlev;                         // highest level built (its size is <= 32)
+    const float4 *pyr;
+    uint32_t n;
+    int nlev;
 };
 
 struct Box {
@@ -170,70 +176,65 @@ __device__ __forceinline__ void box_unbounded(Box &b) {
     for (int a = 0; a < 3; ++a) { b.lo[a] = -INFINITY; b.hi[a] = INFINITY; }
 }
 
-// Warp-wide min / max of one box per lane.
-__device__ __forceinline__ void warp_box_reduce(Box &b, bool &nan) {
-    for (int o = 16; o > 0; o >>= 1) {
-        for (int a = 0; a < 3; ++a) {
-            b.lo[a] = fminf(b.lo[a], __shfl_xor_sync(0xffffffffu, b.lo[a], o));
-            b.hi[a] = fmaxf(b.hi[a], __shfl_xor_sync(0xffffffffu, b.hi[a], o));
-        }
+// One step of a butterfly min / max over the lanes at xor distance o.
+__device__ __forceinline__ void box_xor(Box &b, int o) {
+    for (int a = 0; a < 3; ++a) {
+        b.lo[a] = fminf(b.lo[a], __shfl_xor_sync(0xffffffffu, b.lo[a], o));
+        b.hi[a] = fmaxf(b.hi[a], __shfl_xor_sync(0xffffffffu, b.hi[a], o));
     }
-    nan = __any_sync(0xffffffffu, nan);
 }
 
-// Levels 1 and 2 from the points: a 1024-thread block per 1024 points, a
-// warp per 32-point run, warp 0 folding the block's 32 runs.
-__global__ void __launch_bounds__(1024) pyramid_base_kernel(const float4 *__restrict__ pts,
-                                                            uint64_t n, float4 *l1, float4 *l2) {
-    __shared__ float4 s_lo[32], s_hi[32];
+__device__ __forceinline__ void box_store(float4 *out, uint64_t e, const Box &b) {
+    out[2 * e] = make_float4(b.lo[0], b.lo[1], b.lo[2], 0.f);
+    out[2 * e + 1] = make_float4(b.hi[0], b.hi[1], b.hi[2], 0.f);
+}
+
+// Three levels of the pyramid from `count` inputs (the sorted points when
+// PTS, else the boxes of the level below o1): a 512-thread block per 512
+// inputs, one input a thread.  Lanes fold 8 inputs into an o1 entry and a
+// warp's 32 into half an o2 entry; warp 0 folds the block's 16 warp boxes
+// into its 8 o2 entries and its o3 entry.  Inputs past count hold the empty
+// box; a null output is a level above the top and is not written.
+template <bool PTS>
+__global__ void __launch_bounds__(512) pyramid_fold_kernel(const float4 *__restrict__ in,
+                                                           uint64_t count, float4 *o1, float4 *o2,
+                                                           float4 *o3) {
+    __shared__ float4 s_lo[16], s_hi[16];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint64_t i = (uint64_t)blockIdx.x * 1024 + threadIdx.x;
+    const uint64_t i = (uint64_t)blockIdx.x * 512 + threadIdx.x;
     Box b;
     box_empty(b);
-    bool nan = false;
-    if (i < n) box_add_point(b, nan, pts[i]);
-    warp_box_reduce(b, nan);
-    if (nan) box_unbounded(b);
-    const uint64_t e1 = (uint64_t)blockIdx.x * 32 + warp;
-    const bool has1 = e1 * 32 < n;
+    if (i < count) {
+        if (PTS) {
+            bool nan = false;
+            box_add_point(b, nan, __ldg(&in[i]));
+            if (nan) box_unbounded(b);
+        } else {
+            box_add(b, __ldg(&in[2 * i]), __ldg(&in[2 * i + 1]));
+        }
+    }
+    box_xor(b, 1);
+    box_xor(b, 2);
+    box_xor(b, 4);
+    if ((lane & 7) == 0 && (i >> 3) * 8 < count) box_store(o1, i >> 3, b);
+    box_xor(b, 8);
+    box_xor(b, 16);
     if (lane == 0) {
-        const float4 lo = make_float4(b.lo[0], b.lo[1], b.lo[2], 0.f);
-        const float4 hi = make_float4(b.hi[0], b.hi[1], b.hi[2], 0.f);
-        if (has1) { l1[2 * e1] = lo; l1[2 * e1 + 1] = hi; }
-        s_lo[warp] = lo;
-        s_hi[warp] = hi;
+        s_lo[warp] = make_float4(b.lo[0], b.lo[1], b.lo[2], 0.f);
+        s_hi[warp] = make_float4(b.hi[0], b.hi[1], b.hi[2], 0.f);
     }
     __syncthreads();
-    if (warp == 0 && l2) {
+    if (warp == 0 && o2) {
         Box c;
         box_empty(c);
-        box_add(c, s_lo[lane], s_hi[lane]);   // empty runs past n hold the empty box
-        bool cn = false;
-        warp_box_reduce(c, cn);
-        if (lane == 0) {
-            l2[2 * blockIdx.x] = make_float4(c.lo[0], c.lo[1], c.lo[2], 0.f);
-            l2[2 * blockIdx.x + 1] = make_float4(c.hi[0], c.hi[1], c.hi[2], 0.f);
-        }
-    }
-}
-
-// Level j from level j-1 (count_prev entries): a warp per entry.
-__global__ void __launch_bounds__(256) pyramid_level_kernel(const float4 *__restrict__ prev,
-                                                            uint64_t count_prev, float4 *out,
-                                                            uint64_t count) {
-    const int lane = threadIdx.x & 31;
-    for (uint64_t e = ((uint64_t)blockIdx.x * 256 + threadIdx.x) >> 5; e < count;
-         e += ((uint64_t)gridDim.x * 256) >> 5) {
-        Box b;
-        box_empty(b);
-        const uint64_t src = e * 32 + lane;
-        if (src < count_prev) box_add(b, prev[2 * src], prev[2 * src + 1]);
-        bool nan = false;
-        warp_box_reduce(b, nan);
-        if (lane == 0) {
-            out[2 * e] = make_float4(b.lo[0], b.lo[1], b.lo[2], 0.f);
-            out[2 * e + 1] = make_float4(b.hi[0], b.hi[1], b.hi[2], 0.f);
-        }
+        if (lane < 16) box_add(c, s_lo[lane], s_hi[lane]);
+        box_xor(c, 1);   // lanes 2m, 2m + 1: the 64 inputs of o2 entry m
+        const uint64_t e2 = (uint64_t)blockIdx.x * 8 + (lane >> 1);
+        if (lane < 16 && (lane & 1) == 0 && e2 * 64 < count) box_store(o2, e2, c);
+        box_xor(c, 2);
+        box_xor(c, 4);
+        box_xor(c, 8);   // lane 0: the block's 512 inputs
+        if (lane == 0 && o3) box_store(o3, blockIdx.x, c);
     }
 }
 
@@ -268,33 +269,42 @@ __device__ __forceinline__ void add_run(Box &bx, bool &nan, const float4 *__rest
 
 // Box of the sorted points [first, first + count): partial runs at both
 // ends point by point, then whole runs from the pyramid level by level (at
-// most 31 entries per end and level); the highest level is taken whole.
-__device__ __noinline__ Box range_box(const Pyramid &P, uint32_t first, uint32_t count) {
+// most 7 entries per end and level); the highest level is taken whole.
+// The level offsets follow from n as the walk goes up, so the pyramid is
+// passed as scalars (a struct taken by reference would be copied to local
+// memory).
+__device__ __noinline__ Box range_box(const float4 *__restrict__ pts,
+                                      const float4 *__restrict__ pyr, uint32_t n, int nlev,
+                                      uint32_t first, uint32_t count) {
     Box b;
     box_empty(b);
     bool nan = false;
     uint32_t l = first, r = first + count;   // n < 2^30: no overflow
+    uint32_t size = n;                       // entries of the current level
+    const float4 *lvl = pyr;                 // level j >= 1 (2 float4 per entry)
 #pragma unroll 1
     for (int j = 0; j <= PYR_MAX; ++j) {
         if (l >= r) break;
-        if (j == P.nlev) {
-            if (j == 0) add_run<true>(b, nan, P.pts, l, r);
-            else add_run<false>(b, nan, P.lvl[j], l, r);
+        if (j == nlev) {
+            if (j == 0) add_run<true>(b, nan, pts, l, r);
+            else add_run<false>(b, nan, lvl, l, r);
             break;
         }
-        uint32_t head = (l + 31) & ~31u;
+        uint32_t head = (l + PYR_B - 1) & ~(PYR_B - 1);
         if (head > r) head = r;
-        uint32_t tail = r & ~31u;
+        uint32_t tail = r & ~(PYR_B - 1);
         if (tail < head) tail = head;
         if (j == 0) {
-            add_run<true>(b, nan, P.pts, l, head);
-            add_run<true>(b, nan, P.pts, tail, r);
+            add_run<true>(b, nan, pts, l, head);
+            add_run<true>(b, nan, pts, tail, r);
         } else {
-            add_run<false>(b, nan, P.lvl[j], l, head);
-            add_run<false>(b, nan, P.lvl[j], tail, r);
+            add_run<false>(b, nan, lvl, l, head);
+            add_run<false>(b, nan, lvl, tail, r);
+            lvl += 2 * (uint64_t)size;
         }
-        l = head >> 5;
-        r = tail >> 5;
+        l = head >> PYR_SH;
+        r = tail >> PYR_SH;
+        size = (size + PYR_B - 1) >> PYR_SH;
     }
     if (nan) box_unbounded(b);
     return b;
@@ -324,8 +334,8 @@ __global__ void __launch_bounds__(BLOCK) compact_kernel(
         cnt[1] = klast[i] - sp;
         word[0] = cnt[0] > leaf_size ? cidx[sp] : (CHILD_LEAF | f0);
         word[1] = cnt[1] > leaf_size ? cidx[sp + 1] : (CHILD_LEAF | (sp + 1));
-        const Box b0 = range_box(P, f0, cnt[0]);
-        const Box b1 = range_box(P, f0 + cnt[0], cnt[1]);
+        const Box b0 = range_box(P.pts, P.pyr, P.n, P.nlev, f0, cnt[0]);
+        const Box b1 = range_box(P.pts, P.pyr, P.n, P.nlev, f0 + cnt[0], cnt[1]);
         BvhNode nd;
         // layout: [lo.x0 lo.y0 lo.z0 hi.x0] [hi.y0 hi.z0 lo.x1 lo.y1] [lo.z1 hi.x1 hi.y1 hi.z1]
         nd.a = make_float4(b0.lo[0], b0.lo[1], b0.lo[2], b0.hi[0]);
@@ -541,30 +551,32 @@ rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStr
     for (rtd::DevBuf *b : {&idx->ksplit, &idx->kfirst, &idx->klast, &idx->flags, &idx->cidx,
                            &idx->csel})
         RTD_TRY(b->reserve(ni * sizeof(uint32_t)));
-    // box pyramid over the sorted points (levels until one has <= 32 entries)
+    // box pyramid over the sorted points (levels until one has <= 8 entries)
     Pyramid P;
     P.pts = idx->pts.as<float4>();
     uint64_t sizes[PYR_MAX + 1] = {n}, offs[PYR_MAX + 1] = {0}, total = 0;
     int nlev = 0;
-    while (sizes[nlev] > 32 && nlev < PYR_MAX) {
+    while (sizes[nlev] > PYR_B && nlev < PYR_MAX) {
         ++nlev;
-        sizes[nlev] = ceil_div(sizes[nlev - 1], 32);
+        sizes[nlev] = ceil_div(sizes[nlev - 1], PYR_B);
         offs[nlev] = total;
         total += sizes[nlev];
     }
     P.nlev = nlev;
+    P.n = (uint32_t)n;
     RTD_TRY(idx->pyramid.reserve((total ? total : 1) * 2 * sizeof(float4)));
     float4 *pyr = idx->pyramid.as<float4>();
-    for (int j = 0; j <= PYR_MAX; ++j) P.lvl[j] = j >= 1 && j <= nlev ? pyr + 2 * offs[j] : nullptr;
-    if (nlev >= 1) {
-        pyramid_base_kernel<<<(unsigned)ceil_div(n, 1024), 1024, 0, st>>>(
-            P.pts, n, pyr + 2 * offs[1], nlev >= 2 ? pyr + 2 * offs[2] : nullptr);
+    P.pyr = pyr;
+    float4 *lv[PYR_MAX + 1] = {};
+    for (int j = 1; j <= nlev; ++j) lv[j] = pyr + 2 * offs[j];
+    // three levels per launch: 1-3 from the points, 4-6 from level 3, ...
+    for (int j = 1; j <= nlev; j += 3) {
+        float4 *o2 = j + 1 <= nlev ? lv[j + 1] : nullptr;
+        float4 *o3 = j + 2 <= nlev ? lv[j + 2] : nullptr;
+        const unsigned g = (unsigned)ceil_div(sizes[j - 1], 512);
+        if (j == 1) pyramid_fold_kernel<true><<<g, 512, 0, st>>>(P.pts, n, lv[1], o2, o3);
+        else pyramid_fold_kernel<false><<<g, 512, 0, st>>>(lv[j - 1], sizes[j - 1], lv[j], o2, o3);
         RTD_LAUNCH_CHECK();
-        for (int j = 3; j <= nlev; ++j) {
-            pyramid_level_kernel<<<grid_for(sizes[j] * 32, 256, 148 * 8), 256, 0, st>>>(
-                pyr + 2 * offs[j - 1], sizes[j - 1], pyr + 2 * offs[j], sizes[j]);
-            RTD_LAUNCH_CHECK();
-        }
     }
     const int gi = grid_for(ni, BLOCK, 148 * 8);
     karras_kernel<K><<<gi, BLOCK, 0, st>>>(skeys, (int64_t)n, idx->leaf_size,
