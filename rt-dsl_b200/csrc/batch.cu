@@ -372,7 +372,7 @@ static rtd_status batch_pass(rtd_batch *b, const float *d_pts, const float *d_q,
         batch_gather_kernel<<<g, BLOCK, 0, st>>>(d_pts, perm, b->pcloud.as<uint32_t>(), cd, n,
                                                  f.pts.as<float4>());
         RTD_LAUNCH_CHECK();
-        RTD_TRY(build_tree_sorted<uint64_t>(&f, sk, n, st));
+        RTD_TRY(build_tree_sorted<uint64_t>(&f, sk, n, st, true));
         if (n >= 2 && n > f.leaf_size) {
             batch_roots_kernel<<<grid_for(n, BLOCK, 148 * 8), BLOCK, 0, st>>>(
                 sk, n, 3 * b->bpa, f.kfirst.as<uint32_t>(), f.klast.as<uint32_t>(),

@@ -75,10 +75,10 @@ struct rtd_index {
     rtd::DevBuf top;        // BvhNode * TOP_MAX
     // build scratch
     rtd::DevBuf keys, keys_alt, vals, vals_alt;
-    // Karras nodes (split, first and last point; valid where flags is 1,
-    // i.e. the node keeps more than leaf_size points), compact indices and
-    // the list of kept nodes
-    rtd::DevBuf ksplit, kfirst, klast, flags, cidx, csel;
+    // Karras node flags (1: the node keeps more than leaf_size points),
+    // compact indices, the list of kept nodes, and (forest builds) the kept
+    // nodes' first and last points by Karras index
+    rtd::DevBuf flags, cidx, csel, kfirst, klast;
     rtd::DevBuf pyramid;    // run boxes over the sorted points (2 float4 per run)
     rtd::SortScratch sort;
     rtd::ScanScratch scan;
@@ -179,9 +179,12 @@ inline IndexView view_of(const rtd_index *idx) {
 }
 
 // Karras tree, leaf collapse and child boxes over n keys already sorted
-// (idx->pts holds the points in key order; idx->leaf_size set).
+// (idx->pts holds the points in key order; idx->leaf_size set).  With
+// ranges, every kept Karras node i also leaves its point range in
+// kfirst[i], klast[i] (flags[i] says which nodes are kept).
 template <typename K>
-rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStream_t st);
+rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStream_t st,
+                             bool ranges = false);
 
 // Query ordering: Morton codes of the queries against the scene box, sorted;
 // perm[i] is the i-th query to process.  Returns perm (device) or nullptr

@@ -84,14 +84,24 @@ __global__ void __launch_bounds__(BLOCK) morton_kernel(const float *__restrict__
     }
 }
 
-// Common-prefix length of sorted keys i and j, ties broken by index
-// (Karras 2012, "Maximizing parallelism in the construction of BVHs").
+// Common-prefix length of sorted keys i and j (ki = keys[i]), ties broken
+// by index (Karras 2012, "Maximizing parallelism in the construction of
+// BVHs"); -1 when j is outside [0, n).
 template <typename K>
-__device__ __forceinline__ int delta(const K *__restrict__ keys, int64_t n, int64_t i, int64_t j) {
+__device__ __forceinline__ int delta(const K *__restrict__ keys, int64_t n, K ki, int64_t i,
+                                     int64_t j) {
     if (j < 0 || j >= n) return -1;
-    K a = keys[i], b = keys[j];
-    if (a == b) return (int)(8 * sizeof(K)) + __clz((uint32_t)(i ^ j));
-    return sizeof(K) == 8 ? __clzll((unsigned long long)(a ^ b)) : __clz((uint32_t)(a ^ b));
+    const K b = keys[j];
+    if (ki == b) return (int)(8 * sizeof(K)) + __clz((uint32_t)(i ^ j));
+    return sizeof(K) == 8 ? __clzll((unsigned long long)(ki ^ b)) : __clz((uint32_t)(ki ^ b));
+}
+
+// Direction of Karras node i and the lower bound on its common prefix.
+template <typename K>
+__device__ __forceinline__ void karras_dir(const K *__restrict__ keys, int64_t n, K ki, int64_t i,
+                                           int &dir, int &dmin) {
+    dir = (delta(keys, n, ki, i, i + 1) - delta(keys, n, ki, i, i - 1)) >= 0 ? 1 : -1;
+    dmin = delta(keys, n, ki, i, i - dir);
 }
 
 // Karras nodes.  Only nodes with more than leaf_size points are kept (the
@@ -99,40 +109,47 @@ __device__ __forceinline__ int delta(const K *__restrict__ keys, int64_t n, int6
 // exactly when the key leaf_size steps away in its direction still shares
 // more than the node's lower bound on the common prefix: the prefix length
 // of the (key, position) pairs, which are strictly increasing, cannot grow
-// with distance.  So a collapsed node costs that one test and writes only
-// its flag; the searches run for kept nodes alone.
+// with distance.  This kernel makes that one test per node; the range and
+// split searches run afterwards for the kept nodes alone, packed densely by
+// the scan of these flags (node_kernel), so no warp carries idle lanes of
+// collapsed nodes through them.
 template <typename K>
-__global__ void __launch_bounds__(BLOCK) karras_kernel(const K *__restrict__ keys, int64_t n,
-                                                       uint32_t leaf_size, uint32_t *ksplit,
-                                                       uint32_t *kfirst, uint32_t *klast,
-                                                       uint32_t *flags) {
+__global__ void __launch_bounds__(BLOCK) karras_flag_kernel(const K *__restrict__ keys, int64_t n,
+                                                            uint32_t leaf_size, uint32_t *flags) {
     for (int64_t i = (int64_t)blockIdx.x * BLOCK + threadIdx.x; i < n - 1;
          i += (int64_t)gridDim.x * BLOCK) {
-        int dir = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
-        int dmin = delta(keys, n, i, i - dir);
-        if (!(delta(keys, n, i, i + (int64_t)leaf_size * dir) > dmin)) {
-            flags[i] = 0u;
-            continue;
-        }
-        int64_t lmax = 2;
-        while (lmax <= (int64_t)leaf_size) lmax <<= 1;
-        while (delta(keys, n, i, i + lmax * dir) > dmin) lmax <<= 1;
-        int64_t l = 0;
-        for (int64_t t = lmax >> 1; t >= 1; t >>= 1)
-            if (delta(keys, n, i, i + (l + t) * dir) > dmin) l += t;
-        int64_t j = i + l * dir;
-        int dnode = delta(keys, n, i, j);
-        int64_t s = 0, t = l;
-        do {
-            t = (t + 1) >> 1;
-            if (delta(keys, n, i, i + (s + t) * dir) > dnode) s += t;
-        } while (t > 1);
-        const int64_t gamma = i + s * dir + (dir < 0 ? -1 : 0);
-        ksplit[i] = (uint32_t)gamma;
-        kfirst[i] = (uint32_t)(i < j ? i : j);
-        klast[i] = (uint32_t)(i < j ? j : i);
-        flags[i] = 1u;
+        const K ki = keys[i];
+        int dir, dmin;
+        karras_dir(keys, n, ki, i, dir, dmin);
+        flags[i] = delta(keys, n, ki, i, i + (int64_t)leaf_size * dir) > dmin ? 1u : 0u;
     }
+}
+
+// Point range [first, last] and split of kept Karras node i: the children
+// hold [first, split] and [split + 1, last].
+template <typename K>
+__device__ __forceinline__ void karras_range(const K *__restrict__ keys, int64_t n, int64_t i,
+                                             uint32_t leaf_size, uint32_t &first, uint32_t &last,
+                                             uint32_t &split) {
+    const K ki = keys[i];
+    int dir, dmin;
+    karras_dir(keys, n, ki, i, dir, dmin);
+    int64_t lmax = 2;
+    while (lmax <= (int64_t)leaf_size) lmax <<= 1;
+    while (delta(keys, n, ki, i, i + lmax * dir) > dmin) lmax <<= 1;
+    int64_t l = 0;
+    for (int64_t t = lmax >> 1; t >= 1; t >>= 1)
+        if (delta(keys, n, ki, i, i + (l + t) * dir) > dmin) l += t;
+    const int64_t j = i + l * dir;
+    const int dnode = delta(keys, n, ki, i, j);
+    int64_t s = 0, t = l;
+    do {
+        t = (t + 1) >> 1;
+        if (delta(keys, n, ki, i, i + (s + t) * dir) > dnode) s += t;
+    } while (t > 1);
+    split = (uint32_t)(i + s * dir + (dir < 0 ? -1 : 0));
+    first = (uint32_t)(i < j ? i : j);
+    last = (uint32_t)(i < j ? j : i);
 }
 
 // ---------------------------------------------------- box pyramid
@@ -311,27 +328,34 @@ __device__ __noinline__ Box range_box(const float4 *__restrict__ pts,
 }
 
 // Compact nodes: children become leaves when their subtree has <= leaf_size
-// points.  A thread per kept node (sel[c] = its Karras index).  Every child
-// carries the number of points below it (a subtree's points are contiguous
-// in sorted order, starting at the parent's first point for the left child
-// and after the left child's points for the right one), and its box: the
-// box of its contiguous points, from the pyramid.  Every node's boxes are
-// computed independently, so no bottom-up pass over the tree follows.
-__global__ void __launch_bounds__(BLOCK) compact_kernel(
-    uint32_t n_internal_max, const IndexHeader *h, const uint32_t *__restrict__ sel,
-    const uint32_t *__restrict__ ksplit, const uint32_t *__restrict__ kfirst,
-    const uint32_t *__restrict__ klast, const uint32_t *__restrict__ cidx, uint32_t leaf_size,
-    const Pyramid P, BvhNode *nodes) {
+// points.  A thread per kept node (sel[c] = its Karras index) finds the
+// node's range and split, then writes it.  Every child carries the number
+// of points below it (a subtree's points are contiguous in sorted order,
+// starting at the parent's first point for the left child and after the
+// left child's points for the right one), and its box: the box of its
+// contiguous points, from the pyramid.  Every node's boxes are computed
+// independently, so no bottom-up pass over the tree follows.  With kfirst
+// non-null the range is also stored by Karras index.
+template <typename K>
+__global__ void __launch_bounds__(BLOCK) node_kernel(
+    const K *__restrict__ keys, uint64_t n, const IndexHeader *h, const uint32_t *__restrict__ sel,
+    const uint32_t *__restrict__ cidx, uint32_t leaf_size, const Pyramid P, BvhNode *nodes,
+    uint32_t *kfirst, uint32_t *klast) {
     const uint32_t n_int = h->n_internal;
-    for (uint32_t c = blockIdx.x * BLOCK + threadIdx.x; c < n_int && c < n_internal_max;
+    for (uint32_t c = blockIdx.x * BLOCK + threadIdx.x; c < n_int && c + 1 < n;
          c += gridDim.x * BLOCK) {
         const uint32_t i = sel[c];
+        uint32_t f0, last, sp;
+        karras_range<K>(keys, (int64_t)n, i, leaf_size, f0, last, sp);
+        if (kfirst) {
+            kfirst[i] = f0;
+            klast[i] = last;
+        }
         // children [first, split] and [split + 1, last]: Karras nodes split
         // and split + 1 when they keep more than leaf_size points, else leaves
-        const uint32_t f0 = kfirst[i], sp = ksplit[i];
         uint32_t word[2], cnt[2];
         cnt[0] = sp - f0 + 1;
-        cnt[1] = klast[i] - sp;
+        cnt[1] = last - sp;
         word[0] = cnt[0] > leaf_size ? cidx[sp] : (CHILD_LEAF | f0);
         word[1] = cnt[1] > leaf_size ? cidx[sp + 1] : (CHILD_LEAF | (sp + 1));
         const Box b0 = range_box(P.pts, P.pyr, P.n, P.nlev, f0, cnt[0]);
@@ -507,9 +531,6 @@ rtd_status build_seed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStream
 
 }  // namespace
 
-template <typename K>
-rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStream_t st);
-
 namespace {
 
 template <typename K>
@@ -543,14 +564,16 @@ rtd_status build_typed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStrea
 // Karras tree, leaf collapse and child boxes over keys already sorted, with
 // idx->pts holding the points in key order.
 template <typename K>
-rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStream_t st) {
+rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStream_t st,
+                             bool ranges) {
     IndexHeader *h = idx->hdr.as<IndexHeader>();
     uint32_t *d_err = &h->err;
     if (n < 2 || n <= idx->leaf_size) return RTD_OK;
     const uint64_t ni = n - 1;
-    for (rtd::DevBuf *b : {&idx->ksplit, &idx->kfirst, &idx->klast, &idx->flags, &idx->cidx,
-                           &idx->csel})
+    for (rtd::DevBuf *b : {&idx->flags, &idx->cidx, &idx->csel})
         RTD_TRY(b->reserve(ni * sizeof(uint32_t)));
+    if (ranges)
+        for (rtd::DevBuf *b : {&idx->kfirst, &idx->klast}) RTD_TRY(b->reserve(ni * sizeof(uint32_t)));
     // box pyramid over the sorted points (levels until one has <= 8 entries)
     Pyramid P;
     P.pts = idx->pts.as<float4>();
@@ -579,27 +602,26 @@ rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStr
         RTD_LAUNCH_CHECK();
     }
     const int gi = grid_for(ni, BLOCK, 148 * 8);
-    karras_kernel<K><<<gi, BLOCK, 0, st>>>(skeys, (int64_t)n, idx->leaf_size,
-                                           idx->ksplit.as<uint32_t>(), idx->kfirst.as<uint32_t>(),
-                                           idx->klast.as<uint32_t>(), idx->flags.as<uint32_t>());
+    karras_flag_kernel<K><<<gi, BLOCK, 0, st>>>(skeys, (int64_t)n, idx->leaf_size,
+                                                idx->flags.as<uint32_t>());
     RTD_LAUNCH_CHECK();
     RTD_TRY(exclusive_scan_select_u32(idx->flags.as<uint32_t>(), idx->cidx.as<uint32_t>(),
                                       idx->csel.as<uint32_t>(), ni, &h->n_internal, idx->scan,
                                       d_err, st));
     // kept nodes: at most (n - 1) / leaf_size of them have more than leaf_size points
     const uint64_t kept_max = ni / idx->leaf_size + 1 < ni ? ni / idx->leaf_size + 1 : ni;
-    compact_kernel<<<grid_for(kept_max, BLOCK, 148 * 8), BLOCK, 0, st>>>(
-        (uint32_t)ni, h, idx->csel.as<uint32_t>(), idx->ksplit.as<uint32_t>(),
-        idx->kfirst.as<uint32_t>(), idx->klast.as<uint32_t>(), idx->cidx.as<uint32_t>(),
-        idx->leaf_size, P, idx->nodes.as<BvhNode>());
+    node_kernel<K><<<grid_for(kept_max, BLOCK, 148 * 8), BLOCK, 0, st>>>(
+        skeys, n, h, idx->csel.as<uint32_t>(), idx->cidx.as<uint32_t>(), idx->leaf_size, P,
+        idx->nodes.as<BvhNode>(), ranges ? idx->kfirst.as<uint32_t>() : nullptr,
+        ranges ? idx->klast.as<uint32_t>() : nullptr);
     RTD_LAUNCH_CHECK();
     return RTD_OK;
 }
 
 template rtd_status build_tree_sorted<uint32_t>(rtd_index *, const uint32_t *, uint64_t,
-                                                cudaStream_t);
+                                                cudaStream_t, bool);
 template rtd_status build_tree_sorted<uint64_t>(rtd_index *, const uint64_t *, uint64_t,
-                                                cudaStream_t);
+                                                cudaStream_t, bool);
 
 rtd_status ensure_side_stream(rtd_index *idx) {
     if (idx->side_stream) return RTD_OK;
