@@ -608,7 +608,9 @@ rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStr
     RTD_TRY(exclusive_scan_select_u32(idx->flags.as<uint32_t>(), idx->cidx.as<uint32_t>(),
                                       idx->csel.as<uint32_t>(), ni, &h->n_internal, idx->scan,
                                       d_err, st));
-    // kept nodes: at most (n - 1) / leaf_size of them have more than leaf_size points
+    // grid for about (n - 1) / leaf_size kept nodes, the count of a balanced
+    // tree; the kernel strides over however many there are (up to
+    // n - 1 - leaf_size in a chain-shaped tree)
     const uint64_t kept_max = ni / idx->leaf_size + 1 < ni ? ni / idx->leaf_size + 1 : ni;
     node_kernel<K><<<grid_for(kept_max, BLOCK, 148 * 8), BLOCK, 0, st>>>(
         skeys, n, h, idx->csel.as<uint32_t>(), idx->cidx.as<uint32_t>(), idx->leaf_size, P,

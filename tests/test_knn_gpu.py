@@ -257,6 +257,24 @@ def test_knn_deterministic_and_reusable_index(rtd, cuda):
 
 
 @pytest.mark.slow
+def test_knn_clustered_1p8m_window_headline(rtd, orc, cuda):
+    """The 1.8M-point / 400K-query workload with the headline schedule
+    (Morton-window seed, leaf 5, 39-bit keys) through rtd_k_nn: 2,000
+    queries against the oracle, every list sorted and in range."""
+    pts, q = workloads.clustered()
+    win = rtd.default_schedule(radius_heuristic=4, leaf_size=5, morton_bits=39)
+    ids, d2 = rtd.Index().k_nn(torch.from_numpy(pts).cuda(), torch.from_numpy(q).cuda(), 5, win)
+    torch.cuda.synchronize()
+    ids = ids.cpu().numpy().view(np.uint32)
+    d2 = d2.cpu().numpy()
+    sel = np.random.default_rng(1).choice(len(q), 2000, replace=False)
+    oi, od = orc.knn(pts, q[sel], 5)
+    assert_same(oi, od, ids[sel], d2[sel])
+    assert np.all(ids < len(pts))
+    assert np.all(np.diff(d2, axis=1) >= 0)
+
+
+@pytest.mark.slow
 def test_knn_clustered_1p8m_sampled(rtd, orc, cuda):
     """The 1.8M-point / 400K-query workload: all 400K queries on the GPU,
     2,000 of them against the oracle; every result sorted and in range."""
