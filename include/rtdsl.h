@@ -173,7 +173,10 @@ rtd_status rtd_k_nn(rtd_index *idx, const float *d_points, uint64_t n, const flo
 
 /* Host-buffer k_nn!(data, queries, k, out[, schedule]): copies in, builds
  * the index, searches, copies ids (and d2 if non-NULL) out, synchronises.
- * The context caches device buffers across calls. */
+ * The context caches device buffers and streams across calls.  With 65,536
+ * queries or more the search runs in eight chunks of the caller's query
+ * order on the context's streams, each chunk's rows copied out while the
+ * later chunks search; results are the same. */
 typedef struct rtd_context rtd_context;
 rtd_status rtd_context_create(rtd_context **out);
 rtd_status rtd_context_destroy(rtd_context *ctx);

@@ -70,7 +70,7 @@ rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd
                        cudaStream_t st);
 rtd_status k_nn_device(rtd_index *idx, const float *d_points, uint64_t n, const float *d_q,
                        uint64_t nq, uint32_t k, const rtd_schedule *sched, uint32_t *d_ids,
-                       float *d_d2, cudaStream_t st);
+                       float *d_d2, cudaStream_t st, const HostChunks *hc = nullptr);
 rtd_status knn_search(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k,
                       const rtd_schedule *sched, uint32_t *d_ids, float *d_d2, cudaStream_t st);
 rtd_status range_count(rtd_index *idx, const float *d_q, uint64_t nq, float r,
@@ -104,11 +104,32 @@ struct rtd_context {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_data = nullptr;  // the points are on the device (k_nn!)
     rtd_context_bh *bh = nullptr;   // created on the first barnes_hut! call
+    HostChunks chunks;              // k_nn! result chunks (streams made on first use)
     ~rtd_context() {
         delete bh;
         if (ev_data) cudaEventDestroy(ev_data);
+        if (chunks.fork) cudaEventDestroy(chunks.fork);
+        for (int c = 0; c < MAX_CHUNKS; ++c) {
+            if (chunks.done[c]) cudaEventDestroy(chunks.done[c]);
+            if (chunks.streams[c]) cudaStreamDestroy(chunks.streams[c]);
+        }
     }
 };
+
+// k_nn! returns results in this many chunks of the queries once there are
+// enough of them to fill the GPU several times over.
+constexpr uint64_t CHUNKED_MIN_QUERIES = 65536;
+
+static rtd_status ensure_chunk_streams(rtd_context *ctx) {
+    HostChunks &hc = ctx->chunks;
+    if (hc.fork) return RTD_OK;
+    for (int c = 0; c < MAX_CHUNKS; ++c) {
+        RTD_CUDA(cudaStreamCreateWithFlags(&hc.streams[c], cudaStreamNonBlocking));
+        RTD_CUDA(cudaEventCreateWithFlags(&hc.done[c], cudaEventDisableTiming));
+    }
+    RTD_CUDA(cudaEventCreateWithFlags(&hc.fork, cudaEventDisableTiming));
+    return RTD_OK;
+}
 
 
 
@@ -277,12 +298,16 @@ rtd_status rtd_k_nn_host(rtd_context *ctx, const rtd_vec3 *data, uint64_t n,
     if (nq)
         RTD_CUDA(cudaMemcpyAsync(ctx->queries.ptr, queries, nq * sizeof(rtd_vec3),
                                  cudaMemcpyHostToDevice, idx->side_stream));
+    // The results come back in chunks of the queries: each chunk's rows are
+    // copied to the host while the later chunks still search.
+    RTD_TRY(ensure_chunk_streams(ctx));
+    HostChunks hc = ctx->chunks;
+    hc.chunks = nq >= CHUNKED_MIN_QUERIES ? (uint32_t)MAX_CHUNKS : 1u;
+    hc.h_ids = ids;
+    hc.h_d2 = d2;
     RTD_TRY(k_nn_device(idx, ctx->data.as<float>(), n, ctx->queries.as<float>(), nq, k, sched,
-                        ctx->ids.as<uint32_t>(), d2 ? ctx->d2.as<float>() : nullptr, st));
-    if (nq) {
-        RTD_CUDA(cudaMemcpyAsync(ids, ctx->ids.ptr, nq * (uint64_t)k * 4, cudaMemcpyDeviceToHost, st));
-        if (d2) RTD_CUDA(cudaMemcpyAsync(d2, ctx->d2.ptr, nq * (uint64_t)k * 4, cudaMemcpyDeviceToHost, st));
-    }
+                        ctx->ids.as<uint32_t>(), d2 ? ctx->d2.as<float>() : nullptr, st,
+                        nq ? &hc : nullptr));
     return check_index_errors(idx, st);   // synchronises
 }
 

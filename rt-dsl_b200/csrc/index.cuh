@@ -192,8 +192,28 @@ rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStr
 rtd_status order_queries(rtd_index *idx, const float *d_q, uint64_t nq, bool morton,
                          const uint32_t **perm, cudaStream_t stream);
 
+// With chunks > 1 the order is by (chunk, Morton code), chunk c holding the
+// queries [ceil(c nq / chunks), ceil((c + 1) nq / chunks)) in caller order,
+// so each chunk's processing positions are the same range.
 rtd_status order_queries_own(QueryOrderScratch &qs, const float *d_q, uint64_t nq,
-                             const uint32_t **perm, cudaStream_t stream);
+                             const uint32_t **perm, cudaStream_t stream, uint32_t chunks = 1);
+
+// A search whose results go to host memory in chunks of the caller's query
+// order: chunk c searches on streams[c] (after `fork` on the caller's
+// stream) and copies its rows out as soon as it ends, while later chunks
+// search; the caller's stream then waits for every chunk (`done`).
+constexpr int MAX_CHUNKS = 8;
+struct HostChunks {
+    uint32_t chunks = 1;
+    cudaStream_t streams[MAX_CHUNKS] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t done[MAX_CHUNKS] = {};
+    uint32_t *h_ids = nullptr;
+    float *h_d2 = nullptr;
+};
+inline uint64_t chunk_begin(uint64_t nq, uint32_t chunks, uint32_t c) {
+    return (c * nq + chunks - 1) / chunks;
+}
 
 // Creates the index's side stream and its events on first use.
 rtd_status ensure_side_stream(rtd_index *idx);
@@ -209,6 +229,6 @@ rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd
 rtd_status knn_search_ex(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k,
                          const rtd_schedule *sched, uint32_t *d_ids, float *d_d2,
                          cudaStream_t st, bool have_perm, const uint32_t *perm,
-                         const uint32_t *wpos);
+                         const uint32_t *wpos, const HostChunks *hc = nullptr);
 
 }  // namespace rtd

@@ -696,46 +696,9 @@ static bool uses_window(const rtd_index *idx, const rtd_schedule &s, uint32_t k)
            s.radius_heuristic == RTD_RADIUS_MORTON_WINDOW && idx->n > 1 && idx->skeys != nullptr;
 }
 
-rtd_status knn_search_ex(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k,
-                         const rtd_schedule *sched, uint32_t *d_ids, float *d_d2,
-                         cudaStream_t st, bool have_perm, const uint32_t *given_perm,
-                         const uint32_t *wpos) {
-    if (!idx || !idx->hdr.ptr) return fail(RTD_ERR_INVALID_ARGUMENT, "index not built");
-    if (nq == 0) return RTD_OK;
-    if (!d_q || !d_ids) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL queries or ids");
-    if (k == 0) return fail(RTD_ERR_INVALID_ARGUMENT, "k must be >= 1");
-    if (k > 256) return fail(RTD_ERR_UNSUPPORTED, "k > 256 is not supported");
-    rtd_schedule def;
-    rtd_schedule_default(&def);
-    const rtd_schedule &s = sched ? *sched : def;
-    if (!(s.radius_increment_mult > 1.0f) || !(s.radius_increment_mult < INFINITY))
-        return fail(RTD_ERR_INVALID_ARGUMENT, "radius_increment_mult must be > 1");
-    if (s.max_rounds < 1) return fail(RTD_ERR_INVALID_ARGUMENT, "max_rounds must be >= 1");
-    if (s.radius_heuristic == RTD_RADIUS_FIXED && !(s.radius_param > 0.0f))
-        return fail(RTD_ERR_INVALID_ARGUMENT, "fixed radius must be > 0");
-    for (int e = EV_SEARCH0; e <= EV_SEARCH1; ++e) idx->ev_set[e] = false;
-    idx->mark(EV_SEARCH0, st);
-    RTD_TRY(seed_radius(idx, d_q, nq, k, s, st));
-    idx->mark(EV_SEEDED, st);
-    const uint32_t *perm = given_perm;
-    if (!have_perm) RTD_TRY(order_queries(idx, d_q, nq, s.use_morton_lbv != 0, &perm, st));
-    idx->mark(EV_ORDERED, st);
-    KnnArgs a;
-    a.ix = view_of(idx);
-    a.q = d_q;
-    a.nq = nq;
-    a.perm = perm;
-    a.k = k;
-    float m = s.radius_increment_mult;
-    a.mult2 = m * m;
-    a.max_rounds = s.max_rounds;
-    a.ids = d_ids;
-    a.d2 = d_d2;
-    a.err = &idx->hdr.as<IndexHeader>()->err;
-    a.skeys = nullptr;
-    a.wpos = wpos;
-    a.key64 = idx->morton_bits != 30;
-    a.scale = idx->morton_bits == 30 ? 1023.0f : (float)((1u << (idx->morton_bits / 3)) - 1u);
+// Launches the search kernel the schedule selects for the queries of a.
+static rtd_status launch_search(rtd_index *idx, const rtd_schedule &s, uint32_t k, KnnArgs a,
+                                cudaStream_t st) {
     uint32_t lanes = s.lanes_per_query;
     if (lanes == 0) lanes = k <= 16 ? 1 : 32;
     if (lanes == 1 && k > 32) lanes = 32;
@@ -784,6 +747,91 @@ rtd_status knn_search_ex(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t
     } else {
         return fail(RTD_ERR_INVALID_ARGUMENT, "lanes_per_query must be 0, 1 or 32");
     }
+    return r;
+}
+
+rtd_status knn_search_ex(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k,
+                         const rtd_schedule *sched, uint32_t *d_ids, float *d_d2,
+                         cudaStream_t st, bool have_perm, const uint32_t *given_perm,
+                         const uint32_t *wpos, const HostChunks *hc) {
+    if (!idx || !idx->hdr.ptr) return fail(RTD_ERR_INVALID_ARGUMENT, "index not built");
+    if (nq == 0) return RTD_OK;
+    if (!d_q || !d_ids) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL queries or ids");
+    if (k == 0) return fail(RTD_ERR_INVALID_ARGUMENT, "k must be >= 1");
+    if (k > 256) return fail(RTD_ERR_UNSUPPORTED, "k > 256 is not supported");
+    rtd_schedule def;
+    rtd_schedule_default(&def);
+    const rtd_schedule &s = sched ? *sched : def;
+    if (!(s.radius_increment_mult > 1.0f) || !(s.radius_increment_mult < INFINITY))
+        return fail(RTD_ERR_INVALID_ARGUMENT, "radius_increment_mult must be > 1");
+    if (s.max_rounds < 1) return fail(RTD_ERR_INVALID_ARGUMENT, "max_rounds must be >= 1");
+    if (s.radius_heuristic == RTD_RADIUS_FIXED && !(s.radius_param > 0.0f))
+        return fail(RTD_ERR_INVALID_ARGUMENT, "fixed radius must be > 0");
+    for (int e = EV_SEARCH0; e <= EV_SEARCH1; ++e) idx->ev_set[e] = false;
+    idx->mark(EV_SEARCH0, st);
+    RTD_TRY(seed_radius(idx, d_q, nq, k, s, st));
+    idx->mark(EV_SEEDED, st);
+    const uint32_t *perm = given_perm;
+    if (!have_perm) RTD_TRY(order_queries(idx, d_q, nq, s.use_morton_lbv != 0, &perm, st));
+    idx->mark(EV_ORDERED, st);
+    KnnArgs a;
+    a.ix = view_of(idx);
+    a.q = d_q;
+    a.nq = nq;
+    a.perm = perm;
+    a.k = k;
+    float m = s.radius_increment_mult;
+    a.mult2 = m * m;
+    a.max_rounds = s.max_rounds;
+    a.ids = d_ids;
+    a.d2 = d_d2;
+    a.err = &idx->hdr.as<IndexHeader>()->err;
+    a.skeys = nullptr;
+    a.wpos = wpos;
+    a.key64 = idx->morton_bits != 30;
+    a.scale = idx->morton_bits == 30 ? 1023.0f : (float)((1u << (idx->morton_bits / 3)) - 1u);
+    rtd_status r = RTD_OK;
+    if (!hc || hc->chunks <= 1) {
+        r = launch_search(idx, s, k, a, st);
+        if (r == RTD_OK && hc) {   // one chunk: copy every row out
+            RTD_CUDA(cudaMemcpyAsync(hc->h_ids, d_ids, nq * (uint64_t)k * 4, cudaMemcpyDeviceToHost, st));
+            if (d_d2 && hc->h_d2)
+                RTD_CUDA(cudaMemcpyAsync(hc->h_d2, d_d2, nq * (uint64_t)k * 4, cudaMemcpyDeviceToHost, st));
+        }
+    } else {
+        // Chunk c (caller rows [b, e), processing positions [b, e)) searches
+        // on its own stream and copies its rows out when it ends; the block
+        // scheduler takes the chunks' blocks in launch order, so the first
+        // chunks end (and copy) while the last ones still search.
+        RTD_CUDA(cudaEventRecord(hc->fork, st));
+        for (uint32_t c = 0; c < hc->chunks && r == RTD_OK; ++c) {
+            const uint64_t b = chunk_begin(nq, hc->chunks, c), e = chunk_begin(nq, hc->chunks, c + 1);
+            cudaStream_t cs = hc->streams[c];
+            RTD_CUDA(cudaStreamWaitEvent(cs, hc->fork, 0));
+            if (e > b) {
+                KnnArgs ac = a;
+                ac.nq = e - b;
+                if (a.perm) {
+                    ac.perm = a.perm + b;
+                } else {   // caller order: the chunk's queries and rows themselves
+                    ac.q = a.q + 3 * b;
+                    ac.ids = a.ids + b * k;
+                    if (a.d2) ac.d2 = a.d2 + b * k;
+                }
+                if (a.wpos) ac.wpos = a.wpos + b;
+                r = launch_search(idx, s, k, ac, cs);
+                if (r == RTD_OK) {
+                    RTD_CUDA(cudaMemcpyAsync(hc->h_ids + b * k, d_ids + b * k, (e - b) * k * 4,
+                                             cudaMemcpyDeviceToHost, cs));
+                    if (d_d2 && hc->h_d2)
+                        RTD_CUDA(cudaMemcpyAsync(hc->h_d2 + b * k, d_d2 + b * k, (e - b) * k * 4,
+                                                 cudaMemcpyDeviceToHost, cs));
+                }
+            }
+            RTD_CUDA(cudaEventRecord(hc->done[c], cs));
+            RTD_CUDA(cudaStreamWaitEvent(st, hc->done[c], 0));
+        }
+    }
     idx->mark(EV_SEARCH1, st);
     return r;
 }
@@ -794,19 +842,28 @@ rtd_status knn_search_ex(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t
 // search waits for both.
 rtd_status k_nn_device(rtd_index *idx, const float *d_points, uint64_t n, const float *d_q,
                        uint64_t nq, uint32_t k, const rtd_schedule *sched, uint32_t *d_ids,
-                       float *d_d2, cudaStream_t st) {
+                       float *d_d2, cudaStream_t st, const HostChunks *hc) {
     if (!idx) return fail(RTD_ERR_INVALID_ARGUMENT, "index is NULL");
     if (nq && (!d_q || !d_ids)) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL queries or ids");
     rtd_schedule def;
     rtd_schedule_default(&def);
     const rtd_schedule &s = sched ? *sched : def;
+    // the refilling kernel shares one work counter: it runs unchunked
+    HostChunks one;
+    if (hc && hc->chunks > 1 && s.lane_refill == RTD_REFILL_ON) {
+        one = *hc;
+        one.chunks = 1;
+        hc = &one;
+    }
+    const uint32_t chunks = hc ? hc->chunks : 1u;
     RTD_TRY(ensure_side_stream(idx));
     cudaStream_t side = idx->side_stream;
     RTD_CUDA(cudaEventRecord(idx->ev_fork, st));   // the queries' producers come first
     RTD_CUDA(cudaStreamWaitEvent(side, idx->ev_fork, 0));
     const uint32_t *perm = nullptr;
     rtd_status ord = RTD_OK;
-    if (s.use_morton_lbv && nq >= 2 && k > 0) ord = order_queries_own(idx->qorder, d_q, nq, &perm, side);
+    if (s.use_morton_lbv && nq >= 2 && k > 0)
+        ord = order_queries_own(idx->qorder, d_q, nq, &perm, side, chunks);
     RTD_CUDA(cudaEventRecord(idx->ev_join, side));
     rtd_status r = index_build(idx, d_points, n, &s, st);
     // With the Morton-window seed, the queries' positions among the sorted
@@ -833,7 +890,7 @@ rtd_status k_nn_device(rtd_index *idx, const float *d_points, uint64_t n, const 
         fold_errors_kernel<<<1, 1, 0, st>>>(idx->hdr.as<IndexHeader>(), idx->qorder.hdr.as<IndexHeader>());
         RTD_LAUNCH_CHECK();
     }
-    return knn_search_ex(idx, d_q, nq, k, &s, d_ids, d_d2, st, true, perm, wpos);
+    return knn_search_ex(idx, d_q, nq, k, &s, d_ids, d_d2, st, true, perm, wpos, hc);
 }
 
 }  // namespace rtd

@@ -690,15 +690,21 @@ rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd
 
 // ------------------------------------------------------- query ordering
 namespace {
+// Processing-order keys of the queries: 30-bit Morton codes; with chunks > 1
+// the query's chunk (i * chunks / nq) takes the top cbits bits of a 32-bit
+// key and the code loses its cbits - 2 lowest bits if it must.
 __global__ void __launch_bounds__(BLOCK) query_morton_kernel(const float *__restrict__ q,
                                                              uint64_t nq, const IndexHeader *h,
+                                                             uint32_t chunks, int cbits,
                                                              uint32_t *__restrict__ keys) {
     const SceneNorm s = scene_norm_cubic(h);   // processing order only
+    const int drop = cbits > 2 ? cbits - 2 : 0;
     for (uint64_t i = (uint64_t)blockIdx.x * BLOCK + threadIdx.x; i < nq;
          i += (uint64_t)gridDim.x * BLOCK) {
-        keys[i] = morton30(quantize(q[3 * i], s.lo[0], s.ext[0], 1023.0f),
-                           quantize(q[3 * i + 1], s.lo[1], s.ext[1], 1023.0f),
-                           quantize(q[3 * i + 2], s.lo[2], s.ext[2], 1023.0f));
+        const uint32_t code = morton30(quantize(q[3 * i], s.lo[0], s.ext[0], 1023.0f),
+                                       quantize(q[3 * i + 1], s.lo[1], s.ext[1], 1023.0f),
+                                       quantize(q[3 * i + 2], s.lo[2], s.ext[2], 1023.0f));
+        keys[i] = cbits ? ((uint32_t)(i * chunks / nq) << (32 - cbits)) | (code >> drop) : code;
     }
 }
 }  // namespace
@@ -714,7 +720,7 @@ rtd_status order_queries(rtd_index *idx, const float *d_q, uint64_t nq, bool mor
     RTD_TRY(idx->qperm.reserve(nq * 4));
     RTD_TRY(idx->qperm_alt.reserve(nq * 4));
     IndexHeader *h = idx->hdr.as<IndexHeader>();
-    query_morton_kernel<<<grid_for(nq, BLOCK, 148 * 8), BLOCK, 0, st>>>(d_q, nq, h,
+    query_morton_kernel<<<grid_for(nq, BLOCK, 148 * 8), BLOCK, 0, st>>>(d_q, nq, h, 1u, 0,
                                                                         idx->qkeys.as<uint32_t>());
     RTD_LAUNCH_CHECK();
     bool in_alt = false;
@@ -726,10 +732,11 @@ rtd_status order_queries(rtd_index *idx, const float *d_q, uint64_t nq, bool mor
 }
 
 rtd_status order_queries_own(QueryOrderScratch &qs, const float *d_q, uint64_t nq,
-                             const uint32_t **perm, cudaStream_t st) {
+                             const uint32_t **perm, cudaStream_t st, uint32_t chunks) {
     *perm = nullptr;
     if (nq < 2) return RTD_OK;
     if (nq >= (1ull << 30)) return fail(RTD_ERR_INVALID_ARGUMENT, "at most 2^30-1 queries");
+    if (chunks < 1 || chunks > (uint32_t)MAX_CHUNKS) return fail(RTD_ERR_INVALID_ARGUMENT, "bad chunk count");
     RTD_TRY(qs.hdr.reserve(sizeof(IndexHeader)));
     RTD_TRY(qs.keys.reserve(nq * 4));
     RTD_TRY(qs.keys_alt.reserve(nq * 4));
@@ -740,13 +747,15 @@ rtd_status order_queries_own(QueryOrderScratch &qs, const float *d_q, uint64_t n
     RTD_LAUNCH_CHECK();
     bbox_kernel<<<grid_for(nq, BLOCK, 148 * 4), BLOCK, 0, st>>>(d_q, nq, h);
     RTD_LAUNCH_CHECK();
-    query_morton_kernel<<<grid_for(nq, BLOCK, 148 * 8), BLOCK, 0, st>>>(d_q, nq, h,
+    int cbits = 0;
+    while ((1u << cbits) < chunks) ++cbits;
+    query_morton_kernel<<<grid_for(nq, BLOCK, 148 * 8), BLOCK, 0, st>>>(d_q, nq, h, chunks, cbits,
                                                                         qs.keys.as<uint32_t>());
     RTD_LAUNCH_CHECK();
     bool in_alt = false;
     RTD_TRY(radix_sort_pairs<uint32_t>(qs.keys.as<uint32_t>(), qs.keys_alt.as<uint32_t>(),
                                        qs.perm.as<uint32_t>(), qs.perm_alt.as<uint32_t>(), true,
-                                       nq, 0, 30, qs.sort, &h->err, st, &in_alt));
+                                       nq, 0, cbits ? 32 : 30, qs.sort, &h->err, st, &in_alt));
     *perm = in_alt ? qs.perm_alt.as<uint32_t>() : qs.perm.as<uint32_t>();
     return RTD_OK;
 }

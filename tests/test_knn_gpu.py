@@ -224,6 +224,28 @@ def test_knn_host_context_overlap(rtd, orc, cuda, order):
         assert_same(oi, od, ids, d2)
 
 
+@pytest.mark.parametrize("sched", [dict(radius_heuristic=4, leaf_size=5, morton_bits=39),
+                                   dict(use_morton_lbv=0), dict(lanes_per_query=32),
+                                   dict(lane_refill=1), dict(packet_traversal=1)])
+def test_knn_host_chunked_results(rtd, orc, cuda, sched):
+    """With 65,536 queries or more, rtd_k_nn_host searches the queries in
+    eight chunks of the caller's order (ordered by chunk, then Morton code),
+    each on its own stream, and copies each chunk's rows out while the later
+    chunks search.  Rows land in the caller's order, equal to the oracle's,
+    for uneven chunks, every launch mode (the refilling kernel runs
+    unchunked), and repeated calls on one context."""
+    ctx = rtd.Context()
+    s = rtd.default_schedule(**sched)
+    for n, nq, seed, k in [(30_000, 70_001, 81, 5), (12_000, 65_536, 82, 8), (30_000, 65_535, 83, 5)]:
+        pts, q = clustered_small(n=n, nq=nq, seed=seed)
+        ids, d2 = ctx.k_nn(pts, q, k, s, with_d2=True)
+        sel = np.random.default_rng(seed).choice(nq, 4_000, replace=False)
+        sel = np.concatenate([sel, np.arange(8) * nq // 8, np.arange(1, 9) * nq // 8 - 1])
+        oi, od = orc.knn(pts, q[sel], k)
+        assert_same(oi, od, ids[sel], d2[sel])
+        assert np.all(ids < n) and np.all(np.diff(d2, axis=1) >= 0)
+
+
 @pytest.mark.parametrize("sched", [dict(), dict(use_morton_lbv=0),
                                    dict(radius_heuristic=4, leaf_size=5, morton_bits=39),
                                    dict(lanes_per_query=32)])
