@@ -171,6 +171,24 @@ rtd_status rtd_k_nn(rtd_index *idx, const float *d_points, uint64_t n, const flo
                     uint64_t nq, uint32_t k, const rtd_schedule *sched, uint32_t *d_ids,
                     float *d_d2, rtd_stream stream);
 
+/* A captured k_nn! pipeline: rtd_k_nn over fixed device buffers, recorded
+ * once as a CUDA graph over an index of its own, then replayed -- the
+ * per-frame pattern of repeated builds and searches of same-sized inputs,
+ * without the per-kernel launch cost.  Every launch rebuilds the index from
+ * the points' current contents and searches the queries' current contents;
+ * nothing is cached between launches.  create runs the pipeline once
+ * (results valid on return) and synchronises; the buffers must stay
+ * allocated with their sizes until destroy.  launch does not synchronise;
+ * errors reports the device error flags of the last launch (synchronises). */
+typedef struct rtd_knn_graph rtd_knn_graph;
+rtd_status rtd_knn_graph_create(const float *d_points, uint64_t n, const float *d_queries,
+                                uint64_t nq, uint32_t k, const rtd_schedule *sched,
+                                uint32_t *d_ids, float *d_d2, rtd_stream stream,
+                                rtd_knn_graph **out);
+rtd_status rtd_knn_graph_launch(rtd_knn_graph *g, rtd_stream stream);
+rtd_status rtd_knn_graph_errors(rtd_knn_graph *g, rtd_stream stream);
+rtd_status rtd_knn_graph_destroy(rtd_knn_graph *g);
+
 /* Host-buffer k_nn!(data, queries, k, out[, schedule]): copies in, builds
  * the index, searches, copies ids (and d2 if non-NULL) out, synchronises.
  * The context caches device buffers and streams across calls.  With 65,536

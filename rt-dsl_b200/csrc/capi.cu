@@ -254,6 +254,89 @@ rtd_status rtd_k_nn(rtd_index *idx, const float *d_points, uint64_t n, const flo
     return k_nn_device(idx, d_points, n, d_queries, nq, k, sched, d_ids, d_d2, (cudaStream_t)stream);
 }
 
+}  // extern "C"
+
+struct rtd_knn_graph {
+    rtd_index index;
+    cudaStream_t cap = nullptr;   // capture stream (the NULL stream cannot capture)
+    cudaEvent_t ev = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t kernels = 0;         // kernel launches recorded in the graph
+    ~rtd_knn_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (ev) cudaEventDestroy(ev);
+        if (cap) cudaStreamDestroy(cap);
+    }
+};
+
+static rtd_status knn_graph_build(rtd_knn_graph *g, const float *d_points, uint64_t n,
+                                  const float *d_queries, uint64_t nq, uint32_t k,
+                                  const rtd_schedule *sched, uint32_t *d_ids, float *d_d2,
+                                  cudaStream_t st) {
+    RTD_CUDA(cudaStreamCreateWithFlags(&g->cap, cudaStreamNonBlocking));
+    RTD_CUDA(cudaEventCreateWithFlags(&g->ev, cudaEventDisableTiming));
+    // after the caller's work on its stream; an eager run sizes every
+    // buffer (nothing may be allocated while capturing) and checks the inputs
+    RTD_CUDA(cudaEventRecord(g->ev, st));
+    RTD_CUDA(cudaStreamWaitEvent(g->cap, g->ev, 0));
+    RTD_TRY(k_nn_device(&g->index, d_points, n, d_queries, nq, k, sched, d_ids, d_d2, g->cap));
+    RTD_TRY(check_index_errors(&g->index, g->cap));   // synchronises
+    RTD_CUDA(cudaStreamBeginCapture(g->cap, cudaStreamCaptureModeRelaxed));
+    const uint64_t before = g_launches.load(std::memory_order_relaxed);
+    const rtd_status r = k_nn_device(&g->index, d_points, n, d_queries, nq, k, sched, d_ids, d_d2,
+                                     g->cap);
+    // recorded, not run: each launch of the graph counts them instead
+    g->kernels = g_launches.load(std::memory_order_relaxed) - before;
+    g_launches.fetch_sub(g->kernels, std::memory_order_relaxed);
+    const cudaError_t e = cudaStreamEndCapture(g->cap, &g->graph);
+    RTD_TRY(r);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    RTD_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0));
+    return RTD_OK;
+}
+
+extern "C" {
+
+rtd_status rtd_knn_graph_create(const float *d_points, uint64_t n, const float *d_queries,
+                                uint64_t nq, uint32_t k, const rtd_schedule *sched,
+                                uint32_t *d_ids, float *d_d2, rtd_stream stream,
+                                rtd_knn_graph **out) {
+    if (!out) return fail(RTD_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    rtd_knn_graph *g = new (std::nothrow) rtd_knn_graph();
+    if (!g) return fail(RTD_ERR_OUT_OF_MEMORY, "graph handle");
+    const rtd_status r = knn_graph_build(g, d_points, n, d_queries, nq, k, sched, d_ids, d_d2,
+                                         (cudaStream_t)stream);
+    if (r != RTD_OK) {
+        delete g;
+        return r;
+    }
+    *out = g;
+    return RTD_OK;
+}
+
+rtd_status rtd_knn_graph_launch(rtd_knn_graph *g, rtd_stream stream) {
+    if (!g || !g->exec) return fail(RTD_ERR_INVALID_ARGUMENT, "graph is NULL");
+    RTD_CUDA(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+    g_launches.fetch_add(g->kernels, std::memory_order_relaxed);
+    return RTD_OK;
+}
+
+rtd_status rtd_knn_graph_errors(rtd_knn_graph *g, rtd_stream stream) {
+    if (!g) return fail(RTD_ERR_INVALID_ARGUMENT, "graph is NULL");
+    return check_index_errors(&g->index, (cudaStream_t)stream);
+}
+
+rtd_status rtd_knn_graph_destroy(rtd_knn_graph *g) {
+    if (g) {
+        cudaDeviceSynchronize();   // no launch may still use its buffers
+        delete g;
+    }
+    return RTD_OK;
+}
+
 rtd_status rtd_context_create(rtd_context **out) {
     if (!out) return fail(RTD_ERR_INVALID_ARGUMENT, "out is NULL");
     rtd_context *c = new (std::nothrow) rtd_context();

@@ -239,6 +239,54 @@ class Index:
         return pairs[: written.value]
 
 
+class KnnGraph:
+    """k_nn! over fixed CUDA tensors, captured once as a CUDA graph
+    (rtd_knn_graph_create) and replayed by launch(): each launch rebuilds
+    the index from the points' current contents and searches the queries'
+    current contents into out_ids / out_d2, without per-kernel launch cost.
+    The tensors must keep their storage until close()."""
+
+    def __init__(self, points, queries, k: int, schedule: Schedule | None = None,
+                 out_ids=None, out_d2=None, with_d2: bool = True, stream=None):
+        import torch
+        _check_points_tensor(points, "points")
+        _check_points_tensor(queries, "queries")
+        self._lib = load()
+        nq = queries.shape[0]
+        dev = queries.device
+        self.ids = out_ids if out_ids is not None else torch.empty((nq, k), dtype=torch.int32, device=dev)
+        self.d2 = out_d2 if out_d2 is not None else (
+            torch.empty((nq, k), dtype=torch.float32, device=dev) if with_d2 else None)
+        self.points, self.queries = points, queries   # keep the storage alive
+        s = schedule if schedule is not None else default_schedule()
+        h = C.c_void_p()
+        check(self._lib.rtd_knn_graph_create(
+            C.c_void_p(points.data_ptr()), points.shape[0], C.c_void_p(queries.data_ptr()), nq, k,
+            C.byref(s), C.c_void_p(self.ids.data_ptr()),
+            C.c_void_p(self.d2.data_ptr()) if self.d2 is not None else None,
+            _stream_handle(stream), C.byref(h)))
+        self._h = h
+
+    def launch(self, stream=None):
+        check(self._lib.rtd_knn_graph_launch(self._h, _stream_handle(stream)))
+        return self.ids, self.d2
+
+    def check(self, stream=None):
+        """Device error flags of the last launch (synchronises)."""
+        check(self._lib.rtd_knn_graph_errors(self._h, _stream_handle(stream)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.rtd_knn_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def radius_for_mean_count(index: "Index", queries, target_mean: float, sample: int = 20000,
                           iters: int = 30, schedule: Schedule | None = None) -> float:
     """Radius whose mean neighbour count over a query sample is target_mean,

@@ -266,6 +266,43 @@ def test_knn_device_k_nn_one_call(rtd, orc, cuda, sched):
         assert_same(oi, od, ids.cpu().numpy().view(np.uint32), d2.cpu().numpy())
 
 
+@pytest.mark.parametrize("sched", [dict(radius_heuristic=4, leaf_size=5, morton_bits=39), dict(),
+                                   dict(use_morton_lbv=0), dict(lanes_per_query=32)])
+def test_knn_graph_replays_whole_pipeline(rtd, orc, cuda, sched):
+    """rtd_knn_graph: k_nn! captured once over fixed tensors and replayed.
+    Results equal the oracle's after create and after every launch, also
+    when the points' and queries' contents change between launches (each
+    launch rebuilds and searches, nothing is cached); a launch counts the
+    graph's kernels."""
+    s = rtd.default_schedule(**sched)
+    k = 5 if sched.get("lanes_per_query", 1) == 1 else 40
+    pts, q = clustered_small(n=30_000, nq=4_000, seed=91)
+    P, Q = torch.from_numpy(pts).cuda(), torch.from_numpy(q).cuda()
+    g = rtd.KnnGraph(P, Q, k, s)
+    oi, od = orc.knn(pts, q, k)
+    assert_same(oi, od, g.ids.cpu().numpy().view(np.uint32), g.d2.cpu().numpy())
+    lib = rtd.load()
+    for seed in (92, 93):
+        pts2, q2 = clustered_small(n=30_000, nq=4_000, seed=seed)
+        P.copy_(torch.from_numpy(pts2))
+        Q.copy_(torch.from_numpy(q2))
+        before = lib.rtd_launch_count()
+        ids, d2 = g.launch()
+        assert lib.rtd_launch_count() - before > 10
+        g.check()
+        oi, od = orc.knn(pts2, q2, k)
+        assert_same(oi, od, ids.cpu().numpy().view(np.uint32), d2.cpu().numpy())
+    g.close()
+
+
+def test_knn_graph_rejects_bad_arguments(rtd, cuda):
+    P = torch.rand((100, 3), device="cuda")
+    with pytest.raises(rtd.RtdError):
+        rtd.KnnGraph(P, P, 0)
+    with pytest.raises(rtd.RtdError):
+        rtd.KnnGraph(P, P, 300)
+
+
 def test_knn_deterministic_and_reusable_index(rtd, cuda):
     pts, q = clustered_small(n=20_000, nq=2_000, seed=18)
     s = rtd.default_schedule()
