@@ -295,6 +295,26 @@ def test_knn_graph_replays_whole_pipeline(rtd, orc, cuda, sched):
     g.close()
 
 
+@pytest.mark.parametrize("n,nq,k", [(1, 7, 3), (4, 5, 8), (40, 1, 5), (3_000, 2, 16), (500, 0, 5)])
+def test_knn_graph_small_and_empty(rtd, orc, cuda, n, nq, k):
+    """Captured pipelines over clouds whose root is a leaf, k above the
+    point count, one query, and no queries: launches equal the oracle."""
+    s = rtd.default_schedule(radius_heuristic=4, leaf_size=5, morton_bits=39)
+    rng = np.random.default_rng(n + nq + k)
+    pts = rng.random((n, 3)).astype(np.float32)
+    q = rng.random((nq, 3)).astype(np.float32)
+    P = torch.from_numpy(pts).cuda()
+    Q = torch.from_numpy(q).cuda() if nq else torch.zeros((0, 3), device="cuda")
+    g = rtd.KnnGraph(P, Q, k, s)
+    for _ in range(2):
+        ids, d2 = g.launch()
+        g.check()
+        if nq:
+            oi, od = orc.knn(pts, q, k)
+            assert_same(oi, od, ids.cpu().numpy().view(np.uint32), d2.cpu().numpy())
+    g.close()
+
+
 def test_knn_graph_rejects_bad_arguments(rtd, cuda):
     P = torch.rand((100, 3), device="cuda")
     with pytest.raises(rtd.RtdError):
