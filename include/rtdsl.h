@@ -185,6 +185,15 @@ rtd_status rtd_knn_graph_create(const float *d_points, uint64_t n, const float *
                                 uint64_t nq, uint32_t k, const rtd_schedule *sched,
                                 uint32_t *d_ids, float *d_d2, rtd_stream stream,
                                 rtd_knn_graph **out);
+/* The host-buffer form (k_nn! with host buffers, as rtd_k_nn_host):
+ * copies the points and queries in, builds, searches and copies ids (and d2
+ * if non-NULL) out, results in chunks as rtd_k_nn_host does.  Every host
+ * buffer must be page-locked (cudaHostAlloc / cudaHostRegister); a launch
+ * followed by rtd_knn_graph_errors leaves the results in h_ids / h_d2. */
+rtd_status rtd_knn_graph_create_host(const rtd_vec3 *h_points, uint64_t n,
+                                     const rtd_vec3 *h_queries, uint64_t nq, uint32_t k,
+                                     const rtd_schedule *sched, uint32_t *h_ids, float *h_d2,
+                                     rtd_knn_graph **out);
 rtd_status rtd_knn_graph_launch(rtd_knn_graph *g, rtd_stream stream);
 rtd_status rtd_knn_graph_errors(rtd_knn_graph *g, rtd_stream stream);
 rtd_status rtd_knn_graph_destroy(rtd_knn_graph *g);

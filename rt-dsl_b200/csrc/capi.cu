@@ -97,6 +97,8 @@ rtd_status check_index_errors(rtd_index *idx, cudaStream_t st) {
 
 using namespace rtd;
 
+static void destroy_chunk_streams(HostChunks &hc);
+
 // Host-buffer context: an index plus device staging buffers and a stream.
 struct rtd_context {
     rtd_index index;
@@ -108,20 +110,24 @@ struct rtd_context {
     ~rtd_context() {
         delete bh;
         if (ev_data) cudaEventDestroy(ev_data);
-        if (chunks.fork) cudaEventDestroy(chunks.fork);
-        for (int c = 0; c < MAX_CHUNKS; ++c) {
-            if (chunks.done[c]) cudaEventDestroy(chunks.done[c]);
-            if (chunks.streams[c]) cudaStreamDestroy(chunks.streams[c]);
-        }
+        destroy_chunk_streams(chunks);
     }
 };
+
+static void destroy_chunk_streams(HostChunks &hc) {
+    if (hc.fork) cudaEventDestroy(hc.fork);
+    for (int c = 0; c < MAX_CHUNKS; ++c) {
+        if (hc.done[c]) cudaEventDestroy(hc.done[c]);
+        if (hc.streams[c]) cudaStreamDestroy(hc.streams[c]);
+    }
+    hc = HostChunks();
+}
 
 // k_nn! returns results in this many chunks of the queries once there are
 // enough of them to fill the GPU several times over.
 constexpr uint64_t CHUNKED_MIN_QUERIES = 65536;
 
-static rtd_status ensure_chunk_streams(rtd_context *ctx) {
-    HostChunks &hc = ctx->chunks;
+static rtd_status ensure_chunk_streams(HostChunks &hc) {
     if (hc.fork) return RTD_OK;
     for (int c = 0; c < MAX_CHUNKS; ++c) {
         RTD_CUDA(cudaStreamCreateWithFlags(&hc.streams[c], cudaStreamNonBlocking));
@@ -129,6 +135,43 @@ static rtd_status ensure_chunk_streams(rtd_context *ctx) {
     }
     RTD_CUDA(cudaEventCreateWithFlags(&hc.fork, cudaEventDisableTiming));
     return RTD_OK;
+}
+
+// Host-buffer k_nn! (rtd_k_nn_host and its captured form): copies the
+// points and queries in, builds, searches and copies the results out on
+// stream st, in chunks of the queries once there are enough of them.  Does
+// not synchronise.
+static rtd_status k_nn_host_run(rtd_index *idx, DevBuf &data, DevBuf &queries, DevBuf &ids,
+                                DevBuf &d2buf, cudaEvent_t ev_data, HostChunks &chunks,
+                                const rtd_vec3 *h_data, uint64_t n, const rtd_vec3 *h_queries,
+                                uint64_t nq, uint32_t k, const rtd_schedule *sched,
+                                uint32_t *h_ids, float *h_d2, cudaStream_t st) {
+    if ((n && !h_data) || (nq && (!h_queries || !h_ids)))
+        return fail(RTD_ERR_INVALID_ARGUMENT, "NULL host buffer");
+    RTD_TRY(ensure_side_stream(idx));
+    RTD_TRY(data.reserve(n * sizeof(rtd_vec3)));
+    RTD_TRY(queries.reserve(nq * sizeof(rtd_vec3)));
+    RTD_TRY(ids.reserve(nq * (uint64_t)k * sizeof(uint32_t)));
+    if (h_d2) RTD_TRY(d2buf.reserve(nq * (uint64_t)k * sizeof(float)));
+    // The points go first at full copy bandwidth; the queries follow on the
+    // index's side stream, where k_nn_device then orders them (and finds
+    // their Morton-window positions) while the index is built.
+    if (n) RTD_CUDA(cudaMemcpyAsync(data.ptr, h_data, n * sizeof(rtd_vec3), cudaMemcpyHostToDevice, st));
+    RTD_CUDA(cudaEventRecord(ev_data, st));
+    RTD_CUDA(cudaStreamWaitEvent(idx->side_stream, ev_data, 0));
+    if (nq)
+        RTD_CUDA(cudaMemcpyAsync(queries.ptr, h_queries, nq * sizeof(rtd_vec3),
+                                 cudaMemcpyHostToDevice, idx->side_stream));
+    // The results come back in chunks of the queries: each chunk's rows are
+    // copied to the host while the later chunks still search.
+    RTD_TRY(ensure_chunk_streams(chunks));
+    HostChunks hc = chunks;
+    hc.chunks = nq >= CHUNKED_MIN_QUERIES ? (uint32_t)MAX_CHUNKS : 1u;
+    hc.h_ids = h_ids;
+    hc.h_d2 = h_d2;
+    return k_nn_device(idx, data.as<float>(), n, queries.as<float>(), nq, k, sched,
+                       ids.as<uint32_t>(), h_d2 ? d2buf.as<float>() : nullptr, st,
+                       nq ? &hc : nullptr);
 }
 
 
@@ -263,13 +306,38 @@ struct rtd_knn_graph {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint64_t kernels = 0;         // kernel launches recorded in the graph
+    // host-buffer form: device staging and the result-chunk streams
+    DevBuf data, queries, ids, d2;
+    cudaEvent_t ev_data = nullptr;
+    HostChunks chunks;
     ~rtd_knn_graph() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (ev) cudaEventDestroy(ev);
+        if (ev_data) cudaEventDestroy(ev_data);
+        destroy_chunk_streams(chunks);
         if (cap) cudaStreamDestroy(cap);
     }
 };
+
+// Records `run` on the graph's capture stream after an eager run of it
+// (which sizes every buffer: nothing may be allocated while capturing).
+template <typename Run>
+static rtd_status knn_graph_capture(rtd_knn_graph *g, Run run) {
+    RTD_TRY(run());
+    RTD_TRY(check_index_errors(&g->index, g->cap));   // synchronises
+    RTD_CUDA(cudaStreamBeginCapture(g->cap, cudaStreamCaptureModeRelaxed));
+    const uint64_t before = g_launches.load(std::memory_order_relaxed);
+    const rtd_status r = run();
+    // recorded, not run: each launch of the graph counts them instead
+    g->kernels = g_launches.load(std::memory_order_relaxed) - before;
+    g_launches.fetch_sub(g->kernels, std::memory_order_relaxed);
+    const cudaError_t e = cudaStreamEndCapture(g->cap, &g->graph);
+    RTD_TRY(r);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    RTD_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0));
+    return RTD_OK;
+}
 
 static rtd_status knn_graph_build(rtd_knn_graph *g, const float *d_points, uint64_t n,
                                   const float *d_queries, uint64_t nq, uint32_t k,
@@ -281,20 +349,35 @@ static rtd_status knn_graph_build(rtd_knn_graph *g, const float *d_points, uint6
     // buffer (nothing may be allocated while capturing) and checks the inputs
     RTD_CUDA(cudaEventRecord(g->ev, st));
     RTD_CUDA(cudaStreamWaitEvent(g->cap, g->ev, 0));
-    RTD_TRY(k_nn_device(&g->index, d_points, n, d_queries, nq, k, sched, d_ids, d_d2, g->cap));
-    RTD_TRY(check_index_errors(&g->index, g->cap));   // synchronises
-    RTD_CUDA(cudaStreamBeginCapture(g->cap, cudaStreamCaptureModeRelaxed));
-    const uint64_t before = g_launches.load(std::memory_order_relaxed);
-    const rtd_status r = k_nn_device(&g->index, d_points, n, d_queries, nq, k, sched, d_ids, d_d2,
-                                     g->cap);
-    // recorded, not run: each launch of the graph counts them instead
-    g->kernels = g_launches.load(std::memory_order_relaxed) - before;
-    g_launches.fetch_sub(g->kernels, std::memory_order_relaxed);
-    const cudaError_t e = cudaStreamEndCapture(g->cap, &g->graph);
-    RTD_TRY(r);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
-    RTD_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0));
-    return RTD_OK;
+    return knn_graph_capture(g, [&] {
+        return k_nn_device(&g->index, d_points, n, d_queries, nq, k, sched, d_ids, d_d2, g->cap);
+    });
+}
+
+// Page-locked host memory (or NULL): what a captured copy may use.
+static bool host_pinned(const void *p) {
+    if (!p) return true;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+static rtd_status knn_graph_build_host(rtd_knn_graph *g, const rtd_vec3 *h_points, uint64_t n,
+                                       const rtd_vec3 *h_queries, uint64_t nq, uint32_t k,
+                                       const rtd_schedule *sched, uint32_t *h_ids, float *h_d2) {
+    if (!host_pinned(h_points) || !host_pinned(h_queries) || !host_pinned(h_ids) ||
+        !host_pinned(h_d2))
+        return fail(RTD_ERR_INVALID_ARGUMENT, "host buffers of a captured pipeline must be page-locked");
+    RTD_CUDA(cudaStreamCreateWithFlags(&g->cap, cudaStreamNonBlocking));
+    RTD_CUDA(cudaEventCreateWithFlags(&g->ev, cudaEventDisableTiming));
+    RTD_CUDA(cudaEventCreateWithFlags(&g->ev_data, cudaEventDisableTiming));
+    return knn_graph_capture(g, [&] {
+        return k_nn_host_run(&g->index, g->data, g->queries, g->ids, g->d2, g->ev_data, g->chunks,
+                             h_points, n, h_queries, nq, k, sched, h_ids, h_d2, g->cap);
+    });
 }
 
 extern "C" {
@@ -309,6 +392,23 @@ rtd_status rtd_knn_graph_create(const float *d_points, uint64_t n, const float *
     if (!g) return fail(RTD_ERR_OUT_OF_MEMORY, "graph handle");
     const rtd_status r = knn_graph_build(g, d_points, n, d_queries, nq, k, sched, d_ids, d_d2,
                                          (cudaStream_t)stream);
+    if (r != RTD_OK) {
+        delete g;
+        return r;
+    }
+    *out = g;
+    return RTD_OK;
+}
+
+rtd_status rtd_knn_graph_create_host(const rtd_vec3 *h_points, uint64_t n,
+                                     const rtd_vec3 *h_queries, uint64_t nq, uint32_t k,
+                                     const rtd_schedule *sched, uint32_t *h_ids, float *h_d2,
+                                     rtd_knn_graph **out) {
+    if (!out) return fail(RTD_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    rtd_knn_graph *g = new (std::nothrow) rtd_knn_graph();
+    if (!g) return fail(RTD_ERR_OUT_OF_MEMORY, "graph handle");
+    const rtd_status r = knn_graph_build_host(g, h_points, n, h_queries, nq, k, sched, h_ids, h_d2);
     if (r != RTD_OK) {
         delete g;
         return r;
@@ -363,35 +463,9 @@ rtd_status rtd_k_nn_host(rtd_context *ctx, const rtd_vec3 *data, uint64_t n,
                          const rtd_vec3 *queries, uint64_t nq, uint32_t k,
                          const rtd_schedule *sched, uint32_t *ids, float *d2) {
     if (!ctx) return fail(RTD_ERR_INVALID_ARGUMENT, "context is NULL");
-    if ((n && !data) || (nq && (!queries || !ids)))
-        return fail(RTD_ERR_INVALID_ARGUMENT, "NULL host buffer");
-    cudaStream_t st = ctx->stream;
-    rtd_index *idx = &ctx->index;
-    RTD_TRY(ensure_side_stream(idx));
-    RTD_TRY(ctx->data.reserve(n * sizeof(rtd_vec3)));
-    RTD_TRY(ctx->queries.reserve(nq * sizeof(rtd_vec3)));
-    RTD_TRY(ctx->ids.reserve(nq * (uint64_t)k * sizeof(uint32_t)));
-    if (d2) RTD_TRY(ctx->d2.reserve(nq * (uint64_t)k * sizeof(float)));
-    // The points go first at full copy bandwidth; the queries follow on the
-    // index's side stream, where k_nn_device then orders them (and finds
-    // their Morton-window positions) while the index is built.
-    if (n) RTD_CUDA(cudaMemcpyAsync(ctx->data.ptr, data, n * sizeof(rtd_vec3), cudaMemcpyHostToDevice, st));
-    RTD_CUDA(cudaEventRecord(ctx->ev_data, st));
-    RTD_CUDA(cudaStreamWaitEvent(idx->side_stream, ctx->ev_data, 0));
-    if (nq)
-        RTD_CUDA(cudaMemcpyAsync(ctx->queries.ptr, queries, nq * sizeof(rtd_vec3),
-                                 cudaMemcpyHostToDevice, idx->side_stream));
-    // The results come back in chunks of the queries: each chunk's rows are
-    // copied to the host while the later chunks still search.
-    RTD_TRY(ensure_chunk_streams(ctx));
-    HostChunks hc = ctx->chunks;
-    hc.chunks = nq >= CHUNKED_MIN_QUERIES ? (uint32_t)MAX_CHUNKS : 1u;
-    hc.h_ids = ids;
-    hc.h_d2 = d2;
-    RTD_TRY(k_nn_device(idx, ctx->data.as<float>(), n, ctx->queries.as<float>(), nq, k, sched,
-                        ctx->ids.as<uint32_t>(), d2 ? ctx->d2.as<float>() : nullptr, st,
-                        nq ? &hc : nullptr));
-    return check_index_errors(idx, st);   // synchronises
+    RTD_TRY(k_nn_host_run(&ctx->index, ctx->data, ctx->queries, ctx->ids, ctx->d2, ctx->ev_data,
+                          ctx->chunks, data, n, queries, nq, k, sched, ids, d2, ctx->stream));
+    return check_index_errors(&ctx->index, ctx->stream);   // synchronises
 }
 
 rtd_status rtd_range_count(rtd_index *idx, const float *d_queries, uint64_t nq, float radius,

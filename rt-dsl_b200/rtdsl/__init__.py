@@ -8,7 +8,7 @@ from ._capi import (BH_LAW_PLUMMER, BH_LAW_REFERENCE, EMPTY_ID, RADIUS_FIXED,
                     RADIUS_MORTON_WINDOW, RADIUS_SAMPLED_MAX, RADIUS_SAMPLED_NN, RADIUS_SAMPLED_PERCENTILE, BhParams,
                     RtdError, Schedule, default_batch_schedule, default_bh_params,
                     default_schedule, load)
-from .api import (Context, Index, KnnGraph, dbscan, k_nn, k_nn_array, knn_backward, range_query,
+from .api import (Context, Index, KnnGraph, KnnHostGraph, dbscan, k_nn, k_nn_array, knn_backward, range_query,
                   spatial_join)
 from .batch import Batch
 from .bh import BarnesHut, barnes_hut
@@ -17,6 +17,6 @@ __all__ = [
     "BH_LAW_PLUMMER", "BH_LAW_REFERENCE", "EMPTY_ID", "RADIUS_FIXED", "RADIUS_MORTON_WINDOW",
     "RADIUS_SAMPLED_MAX",
     "RADIUS_SAMPLED_NN", "RADIUS_SAMPLED_PERCENTILE", "BhParams", "RtdError", "Schedule",
-    "default_batch_schedule", "default_bh_params", "default_schedule", "load", "Context", "Index", "KnnGraph", "k_nn", "k_nn_array",
+    "default_batch_schedule", "default_bh_params", "default_schedule", "load", "Context", "Index", "KnnGraph", "KnnHostGraph", "k_nn", "k_nn_array",
     "knn_backward", "range_query", "spatial_join", "dbscan", "Batch", "BarnesHut", "barnes_hut",
 ]

@@ -88,6 +88,8 @@ _SIGNATURES = {
     "rtd_k_nn": (_I, [_P, _P, _U64, _P, _U64, _U32, C.POINTER(Schedule), _P, _P, _P]),
     "rtd_knn_graph_create": (_I, [_P, _U64, _P, _U64, _U32, C.POINTER(Schedule), _P, _P, _P,
                                   C.POINTER(_P)]),
+    "rtd_knn_graph_create_host": (_I, [_P, _U64, _P, _U64, _U32, C.POINTER(Schedule), _P, _P,
+                                       C.POINTER(_P)]),
     "rtd_knn_graph_launch": (_I, [_P, _P]),
     "rtd_knn_graph_errors": (_I, [_P, _P]),
     "rtd_knn_graph_destroy": (_I, [_P]),

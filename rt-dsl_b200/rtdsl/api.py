@@ -287,6 +287,50 @@ class KnnGraph:
             pass
 
 
+class KnnHostGraph:
+    """k_nn! with host buffers (as Context.k_nn), captured once as a CUDA
+    graph over fixed page-locked numpy arrays (rtd_knn_graph_create_host):
+    each launch() copies the points' and queries' current contents in,
+    rebuilds, searches and copies the results out (ids, and d2 with
+    with_d2), then synchronises.  The arrays must be page-locked, e.g.
+    torch.empty(...).pin_memory().numpy(), and outlive close()."""
+
+    def __init__(self, data: np.ndarray, queries: np.ndarray, k: int,
+                 schedule: Schedule | None = None, out_ids: np.ndarray | None = None,
+                 out_d2: np.ndarray | None = None, with_d2: bool = False):
+        for a, name in ((data, "data"), (queries, "queries")):
+            if a.dtype != np.float32 or a.ndim != 2 or a.shape[1] != 3 or not a.flags.c_contiguous:
+                raise ValueError(f"{name} must be a contiguous float32 (N, 3) array")
+        self._lib = load()
+        nq = queries.shape[0]
+        self.ids = out_ids if out_ids is not None else np.empty((nq, k), dtype=np.uint32)
+        self.d2 = out_d2 if out_d2 is not None else (np.empty((nq, k), dtype=np.float32)
+                                                    if with_d2 else None)
+        self.data, self.queries = data, queries
+        s = schedule if schedule is not None else default_schedule()
+        h = C.c_void_p()
+        check(self._lib.rtd_knn_graph_create_host(
+            _ptr(data), data.shape[0], _ptr(queries), nq, k, C.byref(s), _ptr(self.ids),
+            _ptr(self.d2) if self.d2 is not None else None, C.byref(h)))
+        self._h = h
+
+    def launch(self):
+        check(self._lib.rtd_knn_graph_launch(self._h, None))
+        check(self._lib.rtd_knn_graph_errors(self._h, None))   # synchronises
+        return (self.ids, self.d2) if self.d2 is not None else self.ids
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.rtd_knn_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def radius_for_mean_count(index: "Index", queries, target_mean: float, sample: int = 20000,
                           iters: int = 30, schedule: Schedule | None = None) -> float:
     """Radius whose mean neighbour count over a query sample is target_mean,

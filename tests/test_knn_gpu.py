@@ -315,6 +315,42 @@ def test_knn_graph_small_and_empty(rtd, orc, cuda, n, nq, k):
     g.close()
 
 
+def _pinned(a):
+    t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    return t, t.numpy()
+
+
+@pytest.mark.parametrize("nq,k", [(3_000, 5), (70_001, 5), (65_536, 8)])
+def test_knn_host_graph(rtd, orc, cuda, nq, k):
+    """The captured host-buffer pipeline (rtd_knn_graph_create_host) copies
+    in, builds, searches and copies out on every launch -- in chunks from
+    65,536 queries -- and its rows equal the oracle's after the points and
+    queries change in place between launches."""
+    s = rtd.default_schedule(radius_heuristic=4, leaf_size=5, morton_bits=39)
+    pts, q = clustered_small(n=30_000, nq=nq, seed=95)
+    tp, hp = _pinned(pts)
+    tq, hq = _pinned(q)
+    ti = torch.empty((nq, k), dtype=torch.int32).pin_memory()
+    td = torch.empty((nq, k), dtype=torch.float32).pin_memory()
+    g = rtd.KnnHostGraph(hp, hq, k, s, out_ids=ti.numpy().view(np.uint32), out_d2=td.numpy())
+    for seed in (96, 97):
+        pts, q = clustered_small(n=30_000, nq=nq, seed=seed)
+        hp[:] = pts
+        hq[:] = q
+        ids, d2 = g.launch()
+        sel = np.random.default_rng(seed).choice(nq, min(nq, 3_000), replace=False)
+        sel = np.concatenate([sel, [0, nq - 1]])
+        oi, od = orc.knn(pts, q[sel], k)
+        assert_same(oi, od, ids[sel], d2[sel])
+    g.close()
+
+
+def test_knn_host_graph_needs_page_locked_buffers(rtd, cuda):
+    pts = np.random.default_rng(0).random((100, 3)).astype(np.float32)
+    with pytest.raises(rtd.RtdError):
+        rtd.KnnHostGraph(pts, pts, 4)
+
+
 def test_knn_graph_rejects_bad_arguments(rtd, cuda):
     P = torch.rand((100, 3), device="cuda")
     with pytest.raises(rtd.RtdError):
