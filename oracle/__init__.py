@@ -90,6 +90,19 @@ def lib() -> C.CDLL:
             L.orc_bh_plummer_eval.restype = C.c_double
             L.orc_direct_plummer_f64.argtypes = [P, P, I64, C.c_double, C.c_double, P, P, P, P]
             L.orc_direct_plummer_f64.restype = C.c_double
+            L.orc_kd_build.argtypes = [P, I64]
+            L.orc_kd_build.restype = P
+            L.orc_kd_free.argtypes = [P]
+            L.orc_kd_size.argtypes = [P]
+            L.orc_kd_size.restype = I64
+            L.orc_kd_knn.argtypes = [P, P, I64, C.c_int, P, P]
+            L.orc_kd_range_count.argtypes = [P, P, I64, F, P]
+            L.orc_kd_range_count.restype = I64
+            L.orc_kd_range_pairs.argtypes = [P, P, I64, F, P, P]
+            L.orc_cpu_bvh_range.argtypes = [P, I64, P, I64, F, P]
+            L.orc_cpu_bvh_range.restype = I64
+            L.orc_direct_plummer_at_f64.argtypes = [P, P, I64, C.c_double, C.c_double, P, I64, P, P]
+            L.orc_bh_ref_forces_at.argtypes = [P, P, I64, P, I64, P, F, F, P, I64, P]
             _lib = L
     return _lib
 
@@ -199,6 +212,16 @@ def cpu_bvh_knn(pts, q, k: int, radius0: float, mult: float, use_morton: bool = 
     return ids, d2, int(rounds)
 
 
+def cpu_bvh_range(pts, q, r: float):
+    """The reference's CPU range search (Scene::build + one Scene::traverse
+    per query at radius r, hits pushed per query).  Returns (counts, total)."""
+    pts = _f32(pts)
+    q = _f32(q)
+    counts = np.empty(len(q), dtype=np.uint32)
+    total = lib().orc_cpu_bvh_range(_p(pts), len(pts), _p(q), len(q), C.c_float(r), _p(counts))
+    return counts, int(total)
+
+
 def bh_build(pos, mass, bucket: int = 128, min_width: float = 1e-5):
     """Reference Barnes-Hut tree: (nodes structured array, flat body order,
     root box [min xyz, max xyz, width])."""
@@ -221,6 +244,20 @@ def bh_ref_forces(pos, mass, nodes, order, theta: float, G: float = 6.674e-11) -
     out = np.empty((len(pos), 3), dtype=np.float32)
     lib().orc_bh_ref_forces(_p(pos), _p(mass), len(pos), _p(nodes), len(nodes), _p(order),
                             C.c_float(theta), C.c_float(G), _p(out))
+    return out
+
+
+def bh_ref_forces_at(pos, mass, nodes, order, targets, theta: float,
+                     G: float = 6.674e-11) -> np.ndarray:
+    """bh_ref_forces for the caller bodies listed in targets only."""
+    pos = _f32(pos)
+    mass = _f32(mass)
+    nodes = np.ascontiguousarray(nodes, dtype=FLAT_NODE_DTYPE)
+    order = np.ascontiguousarray(order, dtype=np.uint32)
+    t = np.ascontiguousarray(targets, dtype=np.int64)
+    out = np.empty((len(t), 3), dtype=np.float32)
+    lib().orc_bh_ref_forces_at(_p(pos), _p(mass), len(pos), _p(nodes), len(nodes), _p(order),
+                               C.c_float(theta), C.c_float(G), _p(t), len(t), _p(out))
     return out
 
 
@@ -263,6 +300,18 @@ class PlummerFrozen:
         return float(L), out_phi, out_acc
 
 
+def direct_plummer_at_f64(pos, mass, targets, eps: float, G: float):
+    """FP64 direct-sum (phi [T], acc [T,3]) at the listed bodies only."""
+    pos = _f32(pos)
+    mass = _f32(mass)
+    t = np.ascontiguousarray(targets, dtype=np.int64)
+    phi = np.empty(len(t))
+    acc = np.empty((len(t), 3))
+    lib().orc_direct_plummer_at_f64(_p(pos), _p(mass), len(pos), eps, G, _p(t), len(t), _p(phi),
+                                    _p(acc))
+    return phi, acc
+
+
 def direct_plummer_f64(pos, mass, eps: float, G: float, grad: bool = False):
     """FP64 direct sum: (L, phi, acc[, g_pos, g_mass]) for L = sum phi + 0.5 sum |a|^2."""
     p = np.ascontiguousarray(np.asarray(pos, dtype=np.float64))
@@ -274,3 +323,54 @@ def direct_plummer_f64(pos, mass, eps: float, G: float, grad: bool = False):
     gm = np.empty(n) if grad else None
     L = lib().orc_direct_plummer_f64(_p(p), _p(m), n, eps, G, _p(phi), _p(acc), _p(gp), _p(gm))
     return (float(L), phi, acc, gp, gm) if grad else (float(L), phi, acc)
+
+
+class KdTree:
+    """Exact k-NN / range checker for large clouds (orc_kd_*): the same
+    results as knn() / range_count() / range_pairs(), in O(log n) per query.
+    Subtrees are pruned only when the FP32 key of their box's nearest point
+    is strictly above the k-th key (or RN(r*r)), a lower bound of every key
+    inside, so no tolerance is involved."""
+
+    def __init__(self, pts):
+        self._pts = _f32(pts)
+        self._L = lib()
+        self._h = self._L.orc_kd_build(_p(self._pts), len(self._pts))
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            self._L.orc_kd_free(h)
+
+    def __len__(self):
+        return int(self._L.orc_kd_size(self._h))
+
+    def knn(self, q, k: int):
+        q = _f32(q).reshape(-1, 3)
+        ids = np.empty((len(q), k), dtype=np.uint32)
+        d2 = np.empty((len(q), k), dtype=np.float32)
+        if len(q) and k > 0:
+            self._L.orc_kd_knn(self._h, _p(q), len(q), k, _p(ids), _p(d2))
+        return ids, d2
+
+    def range_count(self, q, r: float):
+        q = _f32(q).reshape(-1, 3)
+        counts = np.empty(len(q), dtype=np.uint32)
+        total = self._L.orc_kd_range_count(self._h, _p(q), len(q), C.c_float(r), _p(counts))
+        return counts, int(total)
+
+    def range_pairs(self, q, r: float) -> np.ndarray:
+        """(query, id) pairs sorted by query then id; query = row of q."""
+        q = _f32(q).reshape(-1, 3)
+        counts, total = self.range_count(q, r)
+        off = np.zeros(len(q), dtype=np.uint64)
+        if len(q) > 1:
+            off[1:] = np.cumsum(counts[:-1].astype(np.uint64))
+        pairs = np.empty((max(total, 1), 2), dtype=np.uint32)
+        self._L.orc_kd_range_pairs(self._h, _p(q), len(q), C.c_float(r), _p(off), _p(pairs))
+        return pairs[:total]
+
+
+def knn_exact(pts, q, k: int):
+    """knn() through a k-d tree: for clouds too large for brute force."""
+    return KdTree(pts).knn(q, k)

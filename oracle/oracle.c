@@ -410,20 +410,78 @@ static int orc_ray_box(const orc_bvh_node *nd, float r, const float *o, float tm
     return tmax >= tmin && tmax > 0.0f;
 }
 
+/* Scene::build over n points (midpoint split, leaf <= 2). */
+static void orc_scene_build(orc_scene *s, const float *pts, int64_t n) {
+    memset(s, 0, sizeof *s);
+    s->pts = pts;
+    if (n <= 0) return;
+    s->idx = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)n);
+    for (int64_t i = 0; i < n; ++i) s->idx[i] = (uint32_t)i;
+    orc_scene_push(s, 0, (uint32_t)n);
+    orc_scene_bounds(s, 0);
+    orc_scene_subdivide(s, 0);
+}
+
+/* The reference's fixed-radius search on its CPU BVH: Scene::build, then
+ * one Scene::traverse per query at radius r (the global-push programs'
+ * single launch, gprt-macros/src/lib.rs:276-295, where each hit with
+ * dist_sq <= r*r is pushed to the query's buffer).  Every hit id is stored
+ * (per-thread buffer, like the push slab); counts[q] = hits of query q.
+ * Returns the total.  Timed CPU baseline of the range query ("port"). */
+int64_t orc_cpu_bvh_range(const float *pts, int64_t n, const float *q, int64_t nq, float r,
+                          uint32_t *counts) {
+    orc_scene s;
+    orc_scene_build(&s, pts, n);
+    const float r2 = r * r;
+    int64_t total = 0;
+#pragma omp parallel reduction(+ : total)
+    {
+        int64_t scap = 256, bcap = 4096, nb = 0;
+        int64_t *stack = (int64_t *)malloc(sizeof(int64_t) * (size_t)scap);
+        uint32_t *buf = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)bcap);
+#pragma omp for schedule(dynamic, 64)
+        for (int64_t qi = 0; qi < nq; ++qi) {
+            const float *o = q + 3 * qi;
+            uint32_t hits = 0;
+            int64_t sp = 0;
+            nb = 0;
+            if (s.nn) stack[sp++] = 0;
+            while (sp) {
+                const orc_bvh_node *nd = &s.nodes[stack[--sp]];
+                if (!orc_ray_box(nd, r, o, r)) continue;
+                if (nd->count > 0) {
+                    for (uint32_t i = 0; i < nd->count; ++i) {
+                        uint32_t pid = s.idx[nd->left_first + i];
+                        if (!(orc_key(o, pts + 3 * (size_t)pid) <= r2)) continue;
+                        if (nb == bcap) {
+                            bcap *= 2;
+                            buf = (uint32_t *)realloc(buf, sizeof(uint32_t) * (size_t)bcap);
+                        }
+                        buf[nb++] = pid;
+                        ++hits;
+                    }
+                } else {
+                    if (sp + 2 > scap) { scap *= 2; stack = (int64_t *)realloc(stack, sizeof(int64_t) * (size_t)scap); }
+                    stack[sp++] = nd->left_first;
+                    stack[sp++] = nd->left_first + 1;
+                }
+            }
+            counts[qi] = hits;
+            total += hits;
+        }
+        free(stack); free(buf);
+    }
+    free(s.nodes); free(s.idx);
+    return total;
+}
+
 /* Returns the number of rounds run.  ids/d2 are nq*k, (key, id)-ascending,
  * ORC_EMPTY/+inf where a query ended with fewer than k hits. */
 int orc_cpu_bvh_knn(const float *pts, int64_t n, const float *q, int64_t nq, int k,
                     float radius0, float mult, int use_morton, uint32_t *ids, float *d2) {
-    orc_scene s; memset(&s, 0, sizeof s);
-    s.pts = pts;
+    orc_scene s;
+    orc_scene_build(&s, pts, n);
     int rounds = 0;
-    if (n > 0) {
-        s.idx = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)n);
-        for (int64_t i = 0; i < n; ++i) s.idx[i] = (uint32_t)i;
-        orc_scene_push(&s, 0, (uint32_t)n);
-        orc_scene_bounds(&s, 0);
-        orc_scene_subdivide(&s, 0);
-    }
     int64_t *active = (int64_t *)malloc(sizeof(int64_t) * (size_t)(nq > 0 ? nq : 1));
     int64_t na = nq;
     if (use_morton && nq > 0) {
@@ -691,52 +749,77 @@ static inline float orc_dot3(float x, float y, float z) {
  * fixes lib.rs:829 indexing the unsorted array).  Accepted internal nodes:
  * monopole.  Law: G*m_i*m_j*delta / (r2*sqrt(r2+1e-6)), skipped when
  * r2 <= 1e-10.  Forces are returned in original body order. */
-void orc_bh_ref_forces(const float *pos, const float *mass, int64_t n, const orc_flat_node *nodes,
-                       int64_t nn, const uint32_t *order, float theta, float G, float *force) {
+/* One body of the walk: force on caller body i (fb = bodies in flat order
+ * as (x, y, z, m)). */
+static void orc_bh_ref_body(const float *pos, const float *mass, int64_t i,
+                            const orc_flat_node *nodes, int64_t nn, const float *fb, float theta,
+                            float G, float *out) {
+    const float px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
+    const float gm = G * mass[i];
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+    uint32_t p = 0;
+    while ((int64_t)p < nn) {
+        const orc_flat_node *nd = &nodes[p];
+        float dx = nd->com[0] - px, dy = nd->com[1] - py, dz = nd->com[2] - pz;
+        float dist_sq = orc_dot3(dx, dy, dz);
+        float d = sqrtf(dist_sq);
+        float tmax = fmaxf(1e-6f, theta * d) + 1e-5f;
+        int hit = nd->width < tmax;
+        if (nd->is_leaf) {
+            for (uint32_t j = 0; j < nd->num_particles; ++j) {
+                const float *b = fb + 4 * (size_t)(nd->bucket_start + j);
+                float ex = b[0] - px, ey = b[1] - py, ez = b[2] - pz;
+                float d2 = orc_dot3(ex, ey, ez);
+                if (d2 > 1e-10f) {
+                    float denom = d2 * sqrtf(d2 + 1e-6f);
+                    float fm = (gm * b[3]) / denom;
+                    sx = sx + ex * fm; sy = sy + ey * fm; sz = sz + ez * fm;
+                }
+            }
+            p = hit ? nd->autorope : nd->next_idx;
+        } else if (hit) {
+            if (dist_sq > 1e-10f) {
+                float denom = dist_sq * sqrtf(dist_sq + 1e-6f);
+                float fm = (gm * nd->mass) / denom;
+                sx = sx + dx * fm; sy = sy + dy * fm; sz = sz + dz * fm;
+            }
+            p = nd->autorope;
+        } else {
+            p = nd->next_idx;
+        }
+    }
+    out[0] = sx; out[1] = sy; out[2] = sz;
+}
+
+static float *orc_bh_flat_bodies(const float *pos, const float *mass, int64_t n,
+                                 const uint32_t *order) {
     float *fb = (float *)malloc(sizeof(float) * 4 * (size_t)(n > 0 ? n : 1));
     for (int64_t i = 0; i < n; ++i) {
         uint32_t o = order[i];
         fb[4 * i] = pos[3 * o]; fb[4 * i + 1] = pos[3 * o + 1]; fb[4 * i + 2] = pos[3 * o + 2];
         fb[4 * i + 3] = mass[o];
     }
+    return fb;
+}
+
+void orc_bh_ref_forces(const float *pos, const float *mass, int64_t n, const orc_flat_node *nodes,
+                       int64_t nn, const uint32_t *order, float theta, float G, float *force) {
+    float *fb = orc_bh_flat_bodies(pos, mass, n, order);
 #pragma omp parallel for schedule(dynamic, 64)
-    for (int64_t i = 0; i < n; ++i) {
-        const float px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
-        const float gm = G * mass[i];
-        float sx = 0.0f, sy = 0.0f, sz = 0.0f;
-        uint32_t p = 0;
-        while ((int64_t)p < nn) {
-            const orc_flat_node *nd = &nodes[p];
-            float dx = nd->com[0] - px, dy = nd->com[1] - py, dz = nd->com[2] - pz;
-            float dist_sq = orc_dot3(dx, dy, dz);
-            float d = sqrtf(dist_sq);
-            float tmax = fmaxf(1e-6f, theta * d) + 1e-5f;
-            int hit = nd->width < tmax;
-            if (nd->is_leaf) {
-                for (uint32_t j = 0; j < nd->num_particles; ++j) {
-                    const float *b = fb + 4 * (size_t)(nd->bucket_start + j);
-                    float ex = b[0] - px, ey = b[1] - py, ez = b[2] - pz;
-                    float d2 = orc_dot3(ex, ey, ez);
-                    if (d2 > 1e-10f) {
-                        float denom = d2 * sqrtf(d2 + 1e-6f);
-                        float fm = (gm * b[3]) / denom;
-                        sx = sx + ex * fm; sy = sy + ey * fm; sz = sz + ez * fm;
-                    }
-                }
-                p = hit ? nd->autorope : nd->next_idx;
-            } else if (hit) {
-                if (dist_sq > 1e-10f) {
-                    float denom = dist_sq * sqrtf(dist_sq + 1e-6f);
-                    float fm = (gm * nd->mass) / denom;
-                    sx = sx + dx * fm; sy = sy + dy * fm; sz = sz + dz * fm;
-                }
-                p = nd->autorope;
-            } else {
-                p = nd->next_idx;
-            }
-        }
-        force[3 * i] = sx; force[3 * i + 1] = sy; force[3 * i + 2] = sz;
-    }
+    for (int64_t i = 0; i < n; ++i)
+        orc_bh_ref_body(pos, mass, i, nodes, nn, fb, theta, G, force + 3 * i);
+    free(fb);
+}
+
+/* The same walk for the listed caller bodies only (force[3*t] for
+ * targets[t]): the check of a large tree on a sample of its bodies. */
+void orc_bh_ref_forces_at(const float *pos, const float *mass, int64_t n,
+                          const orc_flat_node *nodes, int64_t nn, const uint32_t *order,
+                          float theta, float G, const int64_t *targets, int64_t nt, float *force) {
+    float *fb = orc_bh_flat_bodies(pos, mass, n, order);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t t = 0; t < nt; ++t)
+        orc_bh_ref_body(pos, mass, targets[t], nodes, nn, fb, theta, G, force + 3 * t);
     free(fb);
 }
 
@@ -937,6 +1020,32 @@ double orc_direct_plummer_f64(const double *pos, const double *mass, int64_t n, 
     return L;
 }
 
+/* FP64 direct sum of the Plummer potential and acceleration (as
+ * orc_direct_plummer_f64) at the listed targets only, from FP32 inputs:
+ * the BH-vs-direct error of a large run on a subsample of its bodies. */
+void orc_direct_plummer_at_f64(const float *pos, const float *mass, int64_t n, double eps,
+                               double G, const int64_t *targets, int64_t nt, double *phi,
+                               double *acc) {
+    const double e2 = eps * eps;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t t = 0; t < nt; ++t) {
+        const int64_t i = targets[t];
+        const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
+        double ph = 0, ax = 0, ay = 0, az = 0;
+        for (int64_t j = 0; j < n; ++j) {
+            if (j == i) continue;
+            double rx = px - pos[3 * j], ry = py - pos[3 * j + 1], rz = pz - pos[3 * j + 2];
+            double s2 = rx * rx + ry * ry + rz * rz + e2;
+            double i1 = 1.0 / sqrt(s2), i3 = i1 * i1 * i1;
+            double m = mass[j];
+            ph -= m * i1;
+            ax -= m * rx * i3; ay -= m * ry * i3; az -= m * rz * i3;
+        }
+        phi[t] = G * ph;
+        acc[3 * t] = G * ax; acc[3 * t + 1] = G * ay; acc[3 * t + 2] = G * az;
+    }
+}
+
 /* ------------------------------------------------------------------------
  * DBSCAN over the range-query membership (FP32 key <= RN(eps*eps), the
  * point itself included).  The reference advertises DBSCAN on top of its
@@ -988,4 +1097,340 @@ int64_t orc_dbscan(const float *pts, int64_t n, float eps, uint32_t min_pts, int
     free(core);
     free(stack);
     return next;
+}
+
+/* ------------------------------------------------------------------------
+ * Exact k-NN and range membership at full size: a k-d tree over the points
+ * that returns exactly what the brute-force orc_knn / orc_range_* return
+ * (the k smallest (FP32 key, id) pairs; every id with key <= RN(r*r)), in
+ * O(log n) per query, so the large configurations can be checked on every
+ * query rather than a sample.
+ *
+ * Pruning is exact, with no tolerance.  For a box [lo, hi] and a query q,
+ * the box key is the FP32 key of the clamped point c = clamp(q, lo, hi),
+ * computed with the same rounded operations as orc_key.  For any point p in
+ * the box, |q_a - p_a| >= |q_a - c_a| on each axis, and round-to-nearest is
+ * monotone, so |RN(q_a - p_a)| >= |RN(q_a - c_a)|; squaring and the two
+ * rounded additions are monotone in non-negative operands, so
+ * key(q, p) >= key(q, c).  A subtree is skipped only when its box key is
+ * strictly greater than the current k-th key (an equal key with a lower id
+ * could still enter) or than RN(r*r).  NaN anywhere makes a comparison
+ * false, so such a box is never skipped.
+ *
+ * Layout: balanced tree in heap order (node i has children 2i+1, 2i+2),
+ * median split along the widest axis, leaves of <= ORC_KD_LEAF points.
+ * Points with a NaN coordinate are left out: their key is NaN for every
+ * query and neither brute-force routine selects them.
+ * ---------------------------------------------------------------------- */
+#define ORC_KD_LEAF 16
+
+typedef struct { float lo[3], hi[3]; uint32_t begin, end; } orc_kd_node;
+
+typedef struct orc_kdtree {
+    int64_t n;            /* points in the tree (NaN points excluded) */
+    int depth;            /* leaves sit at this depth (root = 0) */
+    int64_t n_nodes;
+    orc_kd_node *nodes;
+    float *xyz;           /* points in tree order */
+    uint32_t *ids;        /* original index of each tree-order point */
+} orc_kdtree;
+
+static void orc_kd_select(float *xyz, uint32_t *ids, int64_t lo, int64_t hi, int64_t kth,
+                          int axis) {
+    /* quickselect on [lo, hi): element kth in place, smaller (or equal)
+     * coordinates before it, larger (or equal) after */
+    while (hi - lo > 1) {
+        const int64_t m = lo + (hi - lo) / 2;
+        float a = xyz[3 * lo + axis], b = xyz[3 * m + axis], c = xyz[3 * (hi - 1) + axis];
+        float pivot = (a < b) ? ((b < c) ? b : (a < c ? c : a)) : ((a < c) ? a : (b < c ? c : b));
+        int64_t i = lo, j = hi - 1;
+        while (i <= j) {
+            while (xyz[3 * i + axis] < pivot) ++i;
+            while (xyz[3 * j + axis] > pivot) --j;
+            if (i <= j) {
+                for (int t = 0; t < 3; ++t) {
+                    float v = xyz[3 * i + t]; xyz[3 * i + t] = xyz[3 * j + t]; xyz[3 * j + t] = v;
+                }
+                uint32_t u = ids[i]; ids[i] = ids[j]; ids[j] = u;
+                ++i; --j;
+            }
+        }
+        if (kth <= j) hi = j + 1;
+        else if (kth >= i) lo = i;
+        else return;
+    }
+}
+
+static void orc_kd_build_node(orc_kdtree *t, int64_t ni, int d, int64_t b, int64_t e) {
+    orc_kd_node *nd = &t->nodes[ni];
+    nd->begin = (uint32_t)b; nd->end = (uint32_t)e;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t i = b; i < e; ++i)
+        for (int a = 0; a < 3; ++a) {
+            float v = t->xyz[3 * i + a];
+            if (v < lo[a]) lo[a] = v;
+            if (v > hi[a]) hi[a] = v;
+        }
+    memcpy(nd->lo, lo, sizeof lo); memcpy(nd->hi, hi, sizeof hi);
+    if (d == t->depth) return;
+    int axis = 0;
+    float ext0 = hi[0] - lo[0], ext1 = hi[1] - lo[1], ext2 = hi[2] - lo[2];
+    if (ext1 > ext0) axis = 1;
+    if (ext2 > ext0 && ext2 > ext1) axis = 2;
+    const int64_t mid = b + (e - b) / 2;
+    orc_kd_select(t->xyz, t->ids, b, e, mid, axis);
+    if (e - b > 65536) {
+#pragma omp task
+        orc_kd_build_node(t, 2 * ni + 1, d + 1, b, mid);
+#pragma omp task
+        orc_kd_build_node(t, 2 * ni + 2, d + 1, mid, e);
+#pragma omp taskwait
+    } else {
+        orc_kd_build_node(t, 2 * ni + 1, d + 1, b, mid);
+        orc_kd_build_node(t, 2 * ni + 2, d + 1, mid, e);
+    }
+}
+
+orc_kdtree *orc_kd_build(const float *pts, int64_t n) {
+    orc_kdtree *t = (orc_kdtree *)calloc(1, sizeof(orc_kdtree));
+    t->xyz = (float *)malloc(sizeof(float) * 3 * (size_t)(n > 0 ? n : 1));
+    t->ids = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
+    int64_t m = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        const float *p = pts + 3 * i;
+        if (isnan(p[0]) || isnan(p[1]) || isnan(p[2])) continue;
+        t->xyz[3 * m] = p[0]; t->xyz[3 * m + 1] = p[1]; t->xyz[3 * m + 2] = p[2];
+        t->ids[m] = (uint32_t)i;
+        ++m;
+    }
+    t->n = m;
+    if (m == 0) return t;
+    int depth = 0;
+    while ((m + ((int64_t)1 << depth) - 1) >> depth > ORC_KD_LEAF) ++depth;
+    t->depth = depth;
+    t->n_nodes = ((int64_t)2 << depth) - 1;
+    t->nodes = (orc_kd_node *)malloc(sizeof(orc_kd_node) * (size_t)t->n_nodes);
+#pragma omp parallel
+#pragma omp single
+    orc_kd_build_node(t, 0, 0, 0, m);
+    return t;
+}
+
+void orc_kd_free(orc_kdtree *t) {
+    if (!t) return;
+    free(t->nodes); free(t->xyz); free(t->ids); free(t);
+}
+
+int64_t orc_kd_size(const orc_kdtree *t) { return t ? t->n : 0; }
+
+/* FP32 key of the box point nearest to q (a lower bound of every key in
+ * the box, see above). */
+static inline float orc_kd_box_key(const orc_kd_node *nd, const float *q) {
+    float c[3];
+    for (int a = 0; a < 3; ++a) {
+        float v = q[a];
+        if (v < nd->lo[a]) v = nd->lo[a];
+        if (v > nd->hi[a]) v = nd->hi[a];
+        c[a] = v;
+    }
+    return orc_key(q, c);
+}
+
+/* Max-heap on (key, id) for k above ORC_KD_LIST (the root is the k-th). */
+#define ORC_KD_LIST 64
+static void orc_heap_sift_down(float *hk, uint32_t *hi, int64_t n, int64_t i) {
+    while (1) {
+        int64_t l = 2 * i + 1, r = l + 1, m = i;
+        if (l < n && orc_less(hk[m], hi[m], hk[l], hi[l])) m = l;
+        if (r < n && orc_less(hk[m], hi[m], hk[r], hi[r])) m = r;
+        if (m == i) return;
+        float tk = hk[i]; hk[i] = hk[m]; hk[m] = tk;
+        uint32_t ti = hi[i]; hi[i] = hi[m]; hi[m] = ti;
+        i = m;
+    }
+}
+
+typedef struct { float *bk; uint32_t *bi; int64_t cnt; int k; } orc_klist;
+
+static inline float orc_klist_worst(const orc_klist *L, uint32_t *wid) {
+    if (L->cnt < L->k) { *wid = ORC_EMPTY; return INFINITY; }
+    if (L->k <= ORC_KD_LIST) { *wid = L->bi[L->k - 1]; return L->bk[L->k - 1]; }
+    *wid = L->bi[0]; return L->bk[0];
+}
+
+static inline void orc_klist_add(orc_klist *L, float key, uint32_t id) {
+    const int k = L->k;
+    if (k <= ORC_KD_LIST) {
+        /* sorted array, unused slots hold (+inf, EMPTY) */
+        if (!orc_less(key, id, L->bk[k - 1], L->bi[k - 1])) return;
+        int j = k - 1;
+        while (j > 0 && orc_less(key, id, L->bk[j - 1], L->bi[j - 1])) {
+            L->bk[j] = L->bk[j - 1]; L->bi[j] = L->bi[j - 1]; --j;
+        }
+        L->bk[j] = key; L->bi[j] = id;
+        if (L->cnt < k) ++L->cnt;
+        return;
+    }
+    if (L->cnt < k) {   /* heap insert (sift up) */
+        int64_t i = L->cnt++;
+        L->bk[i] = key; L->bi[i] = id;
+        while (i > 0) {
+            int64_t p = (i - 1) / 2;
+            if (!orc_less(L->bk[p], L->bi[p], L->bk[i], L->bi[i])) break;
+            float tk = L->bk[i]; L->bk[i] = L->bk[p]; L->bk[p] = tk;
+            uint32_t ti = L->bi[i]; L->bi[i] = L->bi[p]; L->bi[p] = ti;
+            i = p;
+        }
+        return;
+    }
+    if (!orc_less(key, id, L->bk[0], L->bi[0])) return;
+    L->bk[0] = key; L->bi[0] = id;
+    orc_heap_sift_down(L->bk, L->bi, k, 0);
+}
+
+/* Writes the list ascending into ids/d2 (k slots, EMPTY / +inf padded). */
+static void orc_klist_out(orc_klist *L, uint32_t *ids, float *d2) {
+    const int k = L->k;
+    if (k > ORC_KD_LIST) {   /* heap sort in place: pop the max to the end */
+        int64_t n = L->cnt;
+        while (n > 1) {
+            float tk = L->bk[0]; L->bk[0] = L->bk[n - 1]; L->bk[n - 1] = tk;
+            uint32_t ti = L->bi[0]; L->bi[0] = L->bi[n - 1]; L->bi[n - 1] = ti;
+            --n;
+            orc_heap_sift_down(L->bk, L->bi, n, 0);
+        }
+        for (int64_t j = L->cnt; j < k; ++j) { L->bk[j] = INFINITY; L->bi[j] = ORC_EMPTY; }
+    }
+    for (int j = 0; j < k; ++j) {
+        ids[j] = L->bi[j];
+        if (d2) d2[j] = L->bk[j];
+    }
+}
+
+static void orc_kd_knn_one(const orc_kdtree *t, const float *q, orc_klist *L, int64_t *stack) {
+    const int k = L->k;
+    L->cnt = 0;
+    for (int j = 0; j < (k <= ORC_KD_LIST ? k : 0); ++j) { L->bk[j] = INFINITY; L->bi[j] = ORC_EMPTY; }
+    if (t->n == 0 || isnan(q[0]) || isnan(q[1]) || isnan(q[2])) return;
+    int64_t sp = 0;
+    stack[sp++] = 0;
+    const int64_t first_leaf = ((int64_t)1 << t->depth) - 1;
+    while (sp) {
+        const int64_t ni = stack[--sp];
+        const orc_kd_node *nd = &t->nodes[ni];
+        uint32_t wid;
+        const float worst = orc_klist_worst(L, &wid);
+        if (orc_kd_box_key(nd, q) > worst) continue;
+        if (ni >= first_leaf) {
+            for (uint32_t i = nd->begin; i < nd->end; ++i) {
+                const float key = orc_key(q, t->xyz + 3 * (size_t)i);
+                if (!(key <= INFINITY)) continue;   /* NaN */
+                orc_klist_add(L, key, t->ids[i]);
+            }
+            continue;
+        }
+        const int64_t l = 2 * ni + 1, r = l + 1;
+        const float kl = orc_kd_box_key(&t->nodes[l], q), kr = orc_kd_box_key(&t->nodes[r], q);
+        /* near child on top of the stack */
+        if (kl <= kr) { stack[sp++] = r; stack[sp++] = l; }
+        else { stack[sp++] = l; stack[sp++] = r; }
+    }
+}
+
+/* Exact k-NN of nq queries: identical to orc_knn's output. */
+void orc_kd_knn(const orc_kdtree *t, const float *q, int64_t nq, int k, uint32_t *ids, float *d2) {
+    if (k <= 0) return;
+#pragma omp parallel
+    {
+        orc_klist L;
+        L.k = k;
+        L.bk = (float *)malloc(sizeof(float) * (size_t)k);
+        L.bi = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)k);
+        int64_t *stack = (int64_t *)malloc(sizeof(int64_t) * (size_t)(2 * t->depth + 4));
+#pragma omp for schedule(dynamic, 64)
+        for (int64_t qi = 0; qi < nq; ++qi) {
+            orc_kd_knn_one(t, q + 3 * qi, &L, stack);
+            orc_klist_out(&L, ids + qi * (int64_t)k, d2 ? d2 + qi * (int64_t)k : NULL);
+        }
+        free(L.bk); free(L.bi); free(stack);
+    }
+}
+
+/* Visits every tree point with key <= r2 for query q; returns the count and,
+ * when out != NULL, writes their ids (unsorted). */
+static int64_t orc_kd_range_one(const orc_kdtree *t, const float *q, float r2, uint32_t *out,
+                                int64_t *stack) {
+    if (t->n == 0) return 0;
+    int64_t sp = 0, c = 0;
+    stack[sp++] = 0;
+    const int64_t first_leaf = ((int64_t)1 << t->depth) - 1;
+    while (sp) {
+        const int64_t ni = stack[--sp];
+        const orc_kd_node *nd = &t->nodes[ni];
+        if (orc_kd_box_key(nd, q) > r2) continue;
+        if (ni >= first_leaf) {
+            for (uint32_t i = nd->begin; i < nd->end; ++i)
+                if (orc_key(q, t->xyz + 3 * (size_t)i) <= r2) {
+                    if (out) out[c] = t->ids[i];
+                    ++c;
+                }
+            continue;
+        }
+        stack[sp++] = 2 * ni + 2;
+        stack[sp++] = 2 * ni + 1;
+    }
+    return c;
+}
+
+static int orc_cmp_u32(const void *a, const void *b) {
+    uint32_t x = *(const uint32_t *)a, y = *(const uint32_t *)b;
+    return (x > y) - (x < y);
+}
+
+/* Range counts (membership key <= RN(r*r), as orc_range_count). */
+int64_t orc_kd_range_count(const orc_kdtree *t, const float *q, int64_t nq, float r,
+                           uint32_t *counts) {
+    const float r2 = r * r;
+    int64_t total = 0;
+#pragma omp parallel reduction(+ : total)
+    {
+        int64_t *stack = (int64_t *)malloc(sizeof(int64_t) * (size_t)(2 * t->depth + 4));
+#pragma omp for schedule(dynamic, 64)
+        for (int64_t qi = 0; qi < nq; ++qi) {
+            const int64_t c = orc_kd_range_one(t, q + 3 * qi, r2, NULL, stack);
+            counts[qi] = (uint32_t)c;
+            total += c;
+        }
+        free(stack);
+    }
+    return total;
+}
+
+/* (query, id) pairs sorted by (query, id) at the exclusive offsets of the
+ * counts, as orc_range_pairs. */
+void orc_kd_range_pairs(const orc_kdtree *t, const float *q, int64_t nq, float r,
+                        const uint64_t *offsets, uint32_t *pairs) {
+    const float r2 = r * r;
+#pragma omp parallel
+    {
+        int64_t *stack = (int64_t *)malloc(sizeof(int64_t) * (size_t)(2 * t->depth + 4));
+        int64_t cap = 1024;
+        uint32_t *buf = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)cap);
+#pragma omp for schedule(dynamic, 64)
+        for (int64_t qi = 0; qi < nq; ++qi) {
+            int64_t c = orc_kd_range_one(t, q + 3 * qi, r2, NULL, stack);
+            if (c > cap) {
+                cap = c;
+                buf = (uint32_t *)realloc(buf, sizeof(uint32_t) * (size_t)cap);
+            }
+            orc_kd_range_one(t, q + 3 * qi, r2, buf, stack);
+            qsort(buf, (size_t)c, sizeof(uint32_t), orc_cmp_u32);
+            uint64_t o = offsets[qi];
+            for (int64_t j = 0; j < c; ++j) {
+                pairs[2 * (o + j)] = (uint32_t)qi;
+                pairs[2 * (o + j) + 1] = buf[j];
+            }
+        }
+        free(stack); free(buf);
+    }
 }
