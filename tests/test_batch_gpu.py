@@ -29,13 +29,15 @@ def check_against_oracle(orc, batch, cl, ids, d2):
 
 
 def mixed_clouds(seed=5):
-    """Clouds of 0 .. 20,000 points, k from 1 to 200 (every k class of the
-    search), duplicates, k above the cloud size and a cloud without queries."""
+    """Clouds of 0 .. 20,000 points, k from 1 to 3,000 (every k class of the
+    search, the memory list above 256 included), duplicates, k above the
+    cloud size and a cloud without queries."""
     rng = np.random.default_rng(seed)
     cl = []
     for c, (n, k) in enumerate([(20_000, 5), (1, 1), (3, 8), (1500, 16), (0, 4), (700, 32),
                                 (4000, 64), (900, 200), (12_000, 1), (50, 64), (2, 2),
-                                (5000, 12), (6000, 40), (8, 16)]):
+                                (5000, 12), (6000, 40), (8, 16), (3000, 300), (8000, 1000),
+                                (150, 400), (5000, 3000)]):
         if c % 3 == 0:
             p = rng.random((n, 3)) * (1 + c)
         elif c % 3 == 1:
@@ -52,13 +54,18 @@ def mixed_clouds(seed=5):
     return cl
 
 
-def test_batched_mixed_clouds_eager(rtd, orc, cuda):
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_batched_mixed_clouds(rtd, orc, cuda, use_graph):
     cl = mixed_clouds()
     pts, q, sizes = packed(cl)
     b = rtd.Batch(sizes)
-    ids, d2 = b.knn(torch.from_numpy(pts).cuda(), torch.from_numpy(q).cuda())
-    torch.cuda.synchronize()
-    check_against_oracle(orc, b, cl, ids, d2)
+    st = torch.cuda.Stream()
+    with torch.cuda.stream(st):
+        P, Q = torch.from_numpy(pts).cuda(), torch.from_numpy(q).cuda()
+        for _ in range(2 if use_graph else 1):   # capture, then replay
+            ids, d2 = b.knn(P, Q, use_graph=use_graph, stream=st)
+            st.synchronize()
+            check_against_oracle(orc, b, cl, ids, d2)
 
 
 @pytest.mark.parametrize("leaf", [1, 4, 16])
@@ -71,6 +78,31 @@ def test_batched_workload_clouds(rtd, orc, cuda, leaf):
     ids, d2 = b.knn(torch.from_numpy(pts).cuda(), torch.from_numpy(q).cuda())
     torch.cuda.synchronize()
     check_against_oracle(orc, b, cl, ids, d2)
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("tuned", [False, True])
+def test_batched_full_256_clouds(rtd, orc, cuda, tuned):
+    """The full many-cloud workload (256 clouds, 1,000-200,000 points each,
+    k in {1, 5, 16, 64}) in one batched pass with the default and the tuned
+    schedule: every query of every cloud against the oracle's exact k-NN of
+    that cloud (k-d tree), ids and FP32 keys bit for bit."""
+    from rtdsl import autotune
+    cl = workloads.clouds()
+    assert len(cl) == 256
+    pts, q, sizes = packed(cl)
+    s = autotune.schedule_for(autotune.batch_key(len(pts), len(q), len(cl)),
+                              rtd.default_batch_schedule()) if tuned else None
+    b = rtd.Batch(sizes, s)
+    ids, d2 = b.knn(torch.from_numpy(pts).cuda(), torch.from_numpy(q).cuda(), use_graph=tuned)
+    torch.cuda.synchronize()
+    ids = ids.cpu().numpy().view(np.uint32)
+    d2 = d2.cpu().numpy()
+    for c, (ci, cd) in enumerate(zip(b.split(ids), b.split(d2))):
+        oi, od = orc.KdTree(cl[c]["points"]).knn(cl[c]["queries"], cl[c]["k"])
+        bad = np.nonzero(np.any(oi != ci, axis=1))[0]
+        assert len(bad) == 0, f"cloud {c} (k={cl[c]['k']}): {len(bad)} queries differ"
+        np.testing.assert_array_equal(od.view(np.uint32), cd.view(np.uint32))
 
 
 def test_batched_fixed_radius_schedule(rtd, orc, cuda):

@@ -42,23 +42,20 @@ def test_plain_knn_small_config(rtd, orc, cuda):
 
 
 @pytest.mark.parametrize("k", [1, 2, 5, 8, 16, 32])
-@pytest.mark.parametrize("mode", ["packet", "thread", "refill", "warp"])
+@pytest.mark.parametrize("mode", ["thread", "warp"])
 def test_knn_k_and_traversal(rtd, orc, cuda, k, mode):
     pts, q = clustered_small()
-    kw = {"packet": dict(lanes_per_query=1, packet_traversal=1),
-          "thread": dict(lanes_per_query=1, packet_traversal=2, lane_refill=2),
-          "refill": dict(lanes_per_query=1, packet_traversal=2, lane_refill=1),
-          "warp": dict(lanes_per_query=32)}[mode]
+    kw = {"thread": dict(lanes_per_query=1), "warp": dict(lanes_per_query=32)}[mode]
     ids, d2, _ = gpu_knn(rtd, pts, q, k, **kw)
     oi, od = orc.knn(pts, q, k)
     assert_same(oi, od, ids, d2)
 
 
-@pytest.mark.parametrize("packet", [1, 2])
+@pytest.mark.parametrize("lanes", [1, 32])
 @pytest.mark.parametrize("block", [64, 128, 256])
-def test_knn_block_sizes(rtd, orc, cuda, packet, block):
+def test_knn_block_sizes(rtd, orc, cuda, lanes, block):
     pts, q = clustered_small(n=15_000, nq=1_500, seed=19)
-    ids, d2, _ = gpu_knn(rtd, pts, q, 5, packet_traversal=packet, block_size=block)
+    ids, d2, _ = gpu_knn(rtd, pts, q, 5, lanes_per_query=lanes, block_size=block)
     oi, od = orc.knn(pts, q, 5)
     assert_same(oi, od, ids, d2)
 
@@ -133,10 +130,10 @@ def test_knn_duplicates_and_ties(rtd, orc, cuda):
     pts = np.concatenate([base, base, base[:100]])
     q = np.concatenate([base[:200], rng.integers(0, 8, size=(200, 3)).astype(np.float32) + 0.5])
     for k in (1, 5, 16, 40):
-        for lanes, packet in ((1, 1), (1, 2), (32, 0)):
+        for lanes in (1, 32):
             if lanes == 1 and k > 32:
                 continue
-            ids, d2, _ = gpu_knn(rtd, pts, q, k, lanes_per_query=lanes, packet_traversal=packet)
+            ids, d2, _ = gpu_knn(rtd, pts, q, k, lanes_per_query=lanes)
             oi, od = orc.knn(pts, q, k)
             assert_same(oi, od, ids, d2)
 
@@ -225,15 +222,14 @@ def test_knn_host_context_overlap(rtd, orc, cuda, order):
 
 
 @pytest.mark.parametrize("sched", [dict(radius_heuristic=4, leaf_size=5, morton_bits=39),
-                                   dict(use_morton_lbv=0), dict(lanes_per_query=32),
-                                   dict(lane_refill=1), dict(packet_traversal=1)])
+                                   dict(use_morton_lbv=0), dict(lanes_per_query=32)])
 def test_knn_host_chunked_results(rtd, orc, cuda, sched):
     """With 65,536 queries or more, rtd_k_nn_host searches the queries in
     eight chunks of the caller's order (ordered by chunk, then Morton code),
     each on its own stream, and copies each chunk's rows out while the later
     chunks search.  Rows land in the caller's order, equal to the oracle's,
-    for uneven chunks, every launch mode (the refilling kernel runs
-    unchunked), and repeated calls on one context."""
+    for uneven chunks, every launch mode, and repeated calls on one
+    context."""
     ctx = rtd.Context()
     s = rtd.default_schedule(**sched)
     for n, nq, seed, k in [(30_000, 70_001, 81, 5), (12_000, 65_536, 82, 8), (30_000, 65_535, 83, 5)]:
@@ -356,7 +352,60 @@ def test_knn_graph_rejects_bad_arguments(rtd, cuda):
     with pytest.raises(rtd.RtdError):
         rtd.KnnGraph(P, P, 0)
     with pytest.raises(rtd.RtdError):
-        rtd.KnnGraph(P, P, 300)
+        rtd.KnnGraph(P, P, 4, rtd.default_schedule(radius_increment_mult=1.0))
+
+
+@pytest.mark.parametrize("k", [257, 300, 1000, 2048, 2049, 5000])
+def test_knn_large_k_uniform(rtd, orc, cuda, k):
+    """k above the register lists (the reference's slab takes any k): the
+    warp's sorted list in shared memory up to 2,048 entries, in the index's
+    device slab above that.  100,000 uniform points, the plain workload's
+    jittered queries (a 1,500-query slice), against the oracle."""
+    pts, q = workloads.plain_knn_small()
+    q = q[:1500]
+    ids, d2, _ = gpu_knn(rtd, pts, q, k)
+    oi, od = orc.KdTree(pts).knn(q, k)
+    assert_same(oi, od, ids, d2)
+
+
+@pytest.mark.parametrize("k", [300, 1000, 3000])
+def test_knn_large_k_clustered(rtd, orc, cuda, k):
+    """Clustered points with duplicates and far queries, k above 256."""
+    pts, q = clustered_small(n=20_000, nq=800, seed=61)
+    pts[::9] = pts[::9][::-1]          # shuffled duplicates
+    pts[1::50] = pts[0]
+    q[-20:] = q[-20:] * 5.0            # queries far outside the cloud
+    ids, d2, _ = gpu_knn(rtd, pts, q, k, max_rounds=6)
+    oi, od = orc.KdTree(pts).knn(q, k)
+    assert_same(oi, od, ids, d2)
+
+
+def test_knn_large_k_above_point_count(rtd, orc, cuda):
+    """k above the number of points: every point in order, then empty slots."""
+    rng = np.random.default_rng(62)
+    pts = rng.random((700, 3)).astype(np.float32)
+    q = rng.random((300, 3)).astype(np.float32)
+    for k in (700, 701, 4000):
+        ids, d2, _ = gpu_knn(rtd, pts, q, k)
+        oi, od = orc.knn(pts, q, k)
+        assert_same(oi, od, ids, d2)
+        assert np.all(ids[:, 700:] == 0xFFFFFFFF) and np.all(np.isinf(d2[:, 700:]))
+
+
+def test_knn_large_k_graph(rtd, orc, cuda):
+    """The captured pipeline with k = 600 (shared-memory list) and 2,500
+    (device slab): both replays exact."""
+    pts, q = clustered_small(n=30_000, nq=1_000, seed=63)
+    P, Q = torch.from_numpy(pts).cuda(), torch.from_numpy(q).cuda()
+    tree = orc.KdTree(pts)
+    for k in (600, 2500):
+        g = rtd.KnnGraph(P, Q, k)
+        for _ in range(2):
+            ids, d2 = g.launch()
+            g.check()
+            oi, od = tree.knn(q, k)
+            assert_same(oi, od, ids.cpu().numpy().view(np.uint32), d2.cpu().numpy())
+        g.close()
 
 
 def test_knn_deterministic_and_reusable_index(rtd, cuda):
@@ -374,29 +423,40 @@ def test_knn_deterministic_and_reusable_index(rtd, cuda):
 @pytest.mark.slow
 def test_knn_clustered_1p8m_window_headline(rtd, orc, cuda):
     """The 1.8M-point / 400K-query workload with the headline schedule
-    (Morton-window seed, leaf 5, 39-bit keys) through rtd_k_nn: 2,000
-    queries against the oracle, every list sorted and in range."""
+    (Morton-window seed, leaf 5, 39-bit keys) through rtd_k_nn: every one
+    of the 400K queries against the oracle (exact k-d tree), ids and FP32
+    keys bit for bit."""
     pts, q = workloads.clustered()
     win = rtd.default_schedule(radius_heuristic=4, leaf_size=5, morton_bits=39)
     ids, d2 = rtd.Index().k_nn(torch.from_numpy(pts).cuda(), torch.from_numpy(q).cuda(), 5, win)
     torch.cuda.synchronize()
     ids = ids.cpu().numpy().view(np.uint32)
     d2 = d2.cpu().numpy()
-    sel = np.random.default_rng(1).choice(len(q), 2000, replace=False)
-    oi, od = orc.knn(pts, q[sel], 5)
-    assert_same(oi, od, ids[sel], d2[sel])
-    assert np.all(ids < len(pts))
-    assert np.all(np.diff(d2, axis=1) >= 0)
+    oi, od = orc.KdTree(pts).knn(q, 5)
+    assert_same(oi, od, ids, d2)
 
 
 @pytest.mark.slow
-def test_knn_clustered_1p8m_sampled(rtd, orc, cuda):
-    """The 1.8M-point / 400K-query workload: all 400K queries on the GPU,
-    2,000 of them against the oracle; every result sorted and in range."""
+def test_knn_clustered_1p8m_graph_all_queries(rtd, orc, cuda):
+    """The same workload through the captured pipeline (rtd_knn_graph), the
+    bench's timed path, replayed twice: every query against the oracle."""
+    pts, q = workloads.clustered()
+    win = rtd.default_schedule(radius_heuristic=4, leaf_size=5, morton_bits=39)
+    P, Q = torch.from_numpy(pts).cuda(), torch.from_numpy(q).cuda()
+    g = rtd.KnnGraph(P, Q, 5, win)
+    g.launch()
+    ids, d2 = g.launch()
+    g.check()
+    oi, od = orc.KdTree(pts).knn(q, 5)
+    assert_same(oi, od, ids.cpu().numpy().view(np.uint32), d2.cpu().numpy())
+    g.close()
+
+
+@pytest.mark.slow
+def test_knn_clustered_1p8m_all_queries(rtd, orc, cuda):
+    """The 1.8M-point / 400K-query workload with the default schedule
+    (sampled radius, radius rounds): every query against the oracle."""
     pts, q = workloads.clustered()
     ids, d2, _ = gpu_knn(rtd, pts, q, 5)
-    sel = np.random.default_rng(0).choice(len(q), 2000, replace=False)
-    oi, od = orc.knn(pts, q[sel], 5)
-    assert_same(oi, od, ids[sel], d2[sel])
-    assert np.all(ids < len(pts))
-    assert np.all(np.diff(d2, axis=1) >= 0)
+    oi, od = orc.KdTree(pts).knn(q, 5)
+    assert_same(oi, od, ids, d2)

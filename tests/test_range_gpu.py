@@ -81,7 +81,8 @@ def test_range_host_api(rtd, orc, cuda):
 def test_range_large_property(rtd, orc, cuda):
     """400K queries on 1.8M points: the count pass and the fill agree
     (sum of counts = pairs written, per-query histogram of the pairs equals
-    the counts), and a query sample matches the oracle exactly."""
+    the counts), and every count and every pair equals the oracle's (exact
+    k-d tree)."""
     from rtdsl.api import radius_for_mean_count
     pts, q = workloads.clustered()
     s = rtd.default_schedule()
@@ -93,9 +94,14 @@ def test_range_large_property(rtd, orc, cuda):
     assert counts.sum() == total == len(pairs)
     np.testing.assert_array_equal(np.bincount(pairs[:, 0], minlength=len(q)), counts)
     assert np.all(np.diff(pairs[:, 0].astype(np.int64)) >= 0)
-    sel = np.arange(0, len(q), 997)[:300]
-    oc, _ = orc.range_count(pts, q[sel], r)
-    np.testing.assert_array_equal(counts[sel], oc)
+    tree = orc.KdTree(pts)
+    oc, ot = tree.range_count(q, r)
+    np.testing.assert_array_equal(counts, oc)
+    # every (query, id) pair of every query equals the oracle's
+    ref = tree.range_pairs(q, r)
+    assert ot == len(ref) == len(pairs)
+    key = lambda a: np.sort(a[:, 0].astype(np.uint64) << np.uint64(32) | a[:, 1].astype(np.uint64))
+    np.testing.assert_array_equal(key(pairs), key(ref))
 
 
 @pytest.mark.parametrize("r", [0.05, 0.3, 2.0])

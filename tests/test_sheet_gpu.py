@@ -3,9 +3,9 @@ sheet (z ~ N(0, 1e-4)) drawn from 2,000 Zipf-weighted Gaussian hotspots
 (sigma 1e-3 .. 1e-1 in [0,10]^2), 1M queries from the same distribution.
 k in {5, 16, 64} (k = 64 runs the warp-striped list) and a range query
 at the radius of 200 mean neighbours (a heavy-tailed, exactly sized
-output).  All queries run on the GPU; a sample is checked against the
-oracle bit for bit and the rest through properties (sorted, in range,
-count pass = fill)."""
+output).  Checked against the oracle (exact k-d tree) bit for bit: the
+k-NN ids and FP32 keys and the range count of every query, and the range
+pairs of a 20,000-query sample."""
 import numpy as np
 import pytest
 import torch
@@ -22,13 +22,18 @@ def sheet(cuda):
 
 
 @pytest.fixture(scope="module")
+def sheet_tree(orc, sheet):
+    return orc.KdTree(sheet[0])
+
+
+@pytest.fixture(scope="module")
 def sheet_index(rtd, sheet):
     s = rtd.default_schedule()
     return rtd.Index().build(sheet[2], s), s
 
 
 @pytest.mark.parametrize("k", [5, 16, 64])
-def test_sheet_knn(rtd, orc, sheet, sheet_index, k):
+def test_sheet_knn(rtd, orc, sheet, sheet_index, sheet_tree, k):
     pts, q, P, Q = sheet
     ix, s = sheet_index
     ids, d2 = ix.knn(Q, k, s)
@@ -39,13 +44,13 @@ def test_sheet_knn(rtd, orc, sheet, sheet_index, k):
     d2 = d2.cpu().numpy()
     assert np.all(ids < len(pts))
     assert np.all(np.diff(d2, axis=1) >= 0)
-    sel = np.random.default_rng(k).choice(len(q), 300, replace=False)
-    oi, od = orc.knn(pts, q[sel], k)
-    np.testing.assert_array_equal(ids[sel], oi)
-    np.testing.assert_array_equal(d2[sel].view(np.uint32), od.view(np.uint32))
+    oi, od = sheet_tree.knn(q, k)
+    bad = np.nonzero(np.any(ids != oi, axis=1))[0]
+    assert len(bad) == 0, f"{len(bad)} of {len(q)} queries differ, first {bad[:5]}"
+    np.testing.assert_array_equal(d2.view(np.uint32), od.view(np.uint32))
 
 
-def test_sheet_range_mean_200(rtd, orc, sheet, sheet_index):
+def test_sheet_range_mean_200(rtd, orc, sheet, sheet_index, sheet_tree):
     from rtdsl.api import radius_for_mean_count
     pts, q, P, Q = sheet
     ix, s = sheet_index
@@ -59,13 +64,13 @@ def test_sheet_range_mean_200(rtd, orc, sheet, sheet_index):
     assert c.max() > 10 * 200          # heavy tail in the dense hotspots
     per_q = torch.bincount(pairs[:, 0].long(), minlength=len(q)).cpu().numpy()
     np.testing.assert_array_equal(per_q, c)
-    sel = np.random.default_rng(1).choice(len(q), 200, replace=False)
-    oc, _ = orc.range_count(pts, q[sel], r)
-    np.testing.assert_array_equal(c[sel], oc)
-    # the pairs of the sampled queries are exactly the oracle's
+    oc, ot = sheet_tree.range_count(q, r)
+    np.testing.assert_array_equal(c, oc)
+    # every pair of a 20,000-query sample equals the oracle's
+    sel = np.sort(np.random.default_rng(1).choice(len(q), 20_000, replace=False))
     p = pairs.cpu().numpy().view(np.uint32)
     mine = p[np.isin(p[:, 0], sel)]
-    ref = orc.range_pairs(pts, q[sel], r)
+    ref = sheet_tree.range_pairs(q[sel], r)
     ref[:, 0] = sel[ref[:, 0]]
     key = lambda a: np.sort(a[:, 0].astype(np.uint64) << np.uint64(32) | a[:, 1].astype(np.uint64))
     np.testing.assert_array_equal(key(mine), key(ref))
