@@ -47,8 +47,12 @@ def test_cached_schedule_leaves_default_alone(rtd):
     from rtdsl import autotune
     base = rtd.default_schedule()
     before = base.as_dict()
-    for tag in ("clustered_1p8m_k5", "clustered_1p8m_r50", "clouds_256", "no_such_tag"):
-        s = autotune.cached_schedule(tag, base)
+    g = "NVIDIA B200"
+    for key in (autotune.knn_key(1_800_000, 400_000, 5, "clustered", g),
+                autotune.range_key(1_800_000, 400_000, 50, "clustered", g),
+                autotune.batch_key(8_961_867, 2_240_466, 256, g),
+                autotune.knn_key(10, 10, 5, "sheet", "no such GPU")):
+        s = autotune.schedule_for(key, base)
         assert s is not base
     assert base.as_dict() == before
 
