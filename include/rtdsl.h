@@ -72,7 +72,8 @@ typedef enum rtd_radius_heuristic {
  * picks. */
 typedef struct rtd_schedule {
     float radius_increment_mult;  /* M > 1: radius *= M per round (k_nn! lib.rs:592) */
-    uint32_t max_rounds;          /* the last round is unbounded, so results stay exact */
+    uint32_t max_rounds;          /* the last round is unbounded, so results stay exact
+                                     (unless partial_results) */
     int32_t radius_heuristic;     /* rtd_radius_heuristic */
     float radius_param;           /* see rtd_radius_heuristic */
     uint32_t use_morton_lbv;      /* process queries in Morton order (k_nn! lib.rs:456-460) */
@@ -81,24 +82,14 @@ typedef struct rtd_schedule {
     uint32_t lanes_per_query;     /* 1 = thread per query, 32 = warp per query (0 = auto) */
     uint32_t morton_bits;         /* 30 (u32 keys, the reference layout) or 33..63 in steps
                                      of 3 (u64 keys, bits/3 per axis); 0 = auto */
-    uint32_t packet_traversal;    /* thread-per-query kernels: 32 Morton-adjacent queries
-                                     share one traversal (rtd_packet_mode) */
-    uint32_t lane_refill;         /* thread-per-query kernels: persistent warps whose lanes
-                                     take the next query as soon as theirs ends
-                                     (rtd_refill_mode) */
+    uint32_t partial_results;     /* 0 (default): exact; the last allowed round is unbounded.
+                                     1: the reference's round cap (k_nn! gprt-macros/src/lib.rs:
+                                     466, 528-530): every round stays bounded, a query short of
+                                     k hits after max_rounds keeps the hits it has (remaining
+                                     slots 0xFFFFFFFF / +inf) and the call's device flags report
+                                     RTD_ERR_NOT_CONVERGED */
+    uint32_t reserved;            /* must be 0 */
 } rtd_schedule;
-
-typedef enum rtd_refill_mode {
-    RTD_REFILL_AUTO = 0,   /* currently: off (measured 2x slower on clustered data) */
-    RTD_REFILL_ON = 1,
-    RTD_REFILL_OFF = 2     /* one query per thread, the warp ends with its slowest lane */
-} rtd_refill_mode;
-
-typedef enum rtd_packet_mode {
-    RTD_PACKET_AUTO = 0,   /* currently: off (per-thread traversal measured faster) */
-    RTD_PACKET_ON = 1,
-    RTD_PACKET_OFF = 2
-} rtd_packet_mode;
 
 /* Defaults: M = 2, 32 rounds, sampled-NN seed x 2^-4, Morton query order,
  * leaf 4, auto launch shape, auto key width. */
@@ -121,8 +112,10 @@ typedef struct rtd_index rtd_index;
 rtd_status rtd_index_create(rtd_index **out);
 rtd_status rtd_index_destroy(rtd_index *idx);
 /* d_xyz: n points, x,y,z float triples (Vec3 layout) in device memory.
- * Morton codes -> onesweep radix sort -> Karras radix tree -> bottom-up
- * refit; subtrees of <= leaf_size points become leaves. */
+ * Morton codes -> onesweep radix sort -> Karras radix tree; subtrees of
+ * <= leaf_size points become leaves, and every child box is taken from a
+ * pyramid of boxes over runs of 8, 64, 512 ... sorted points (no bottom-up
+ * refit pass). */
 rtd_status rtd_index_build(rtd_index *idx, const float *d_xyz, uint64_t n,
                            const rtd_schedule *sched, rtd_stream stream);
 typedef struct rtd_index_info {
@@ -141,7 +134,7 @@ rtd_status rtd_index_info_get(rtd_index *idx, rtd_index_info *info, rtd_stream s
  * on the caller's stream; rtd_index_profile_get waits for them. */
 typedef struct rtd_profile {
     float build_sort_ms;   /* scene box + Morton codes + radix sort + point gather */
-    float build_tree_ms;   /* Karras tree + leaf collapse + refit + top staging */
+    float build_tree_ms;   /* Karras tree + leaf collapse + child boxes + top staging */
     float seed_ms;         /* initial-radius seed */
     float order_ms;        /* query Morton ordering */
     float search_ms;       /* the search kernel (kNN or range count + fill) */
@@ -151,6 +144,29 @@ rtd_status rtd_index_profile_get(rtd_index *idx, rtd_profile *out);
 /* Kernels this library has launched in this process (all handles). */
 uint64_t rtd_launch_count(void);
 
+/* Diagnostic of the bounded device waits (no reference counterpart: the
+ * reference exits on any error).  Every device wait on another block's
+ * progress (the look-back of the radix sort and of the scans) gives up after
+ * a retry limit and reports RTD_ERR_TIMEOUT instead of hanging the GPU.
+ * This call runs that same wait on a device flag: never set (flag_set = 0),
+ * the wait gives up after spin_limit retries and the call returns
+ * RTD_ERR_TIMEOUT with the context still usable; set (flag_set = 1), it
+ * returns RTD_OK.  Synchronises. */
+rtd_status rtd_wait_selftest(uint32_t spin_limit, int flag_set, rtd_stream stream);
+
+/* Process-wide bounds of bounded device loops.  0 keeps a field's default.
+ * bh_stack_entries: traversal stack entries each warp of the Plummer-law
+ * Barnes-Hut walks may use (default and maximum 8192, minimum 8); a walk
+ * that needs more refuses the push and its tree reports RTD_ERR_OVERFLOW,
+ * so lowering it exercises that failure path.  Takes effect at the next
+ * launch. */
+typedef struct rtd_limits {
+    uint32_t bh_stack_entries;
+    uint32_t reserved[7];
+} rtd_limits;
+rtd_status rtd_limits_set(const rtd_limits *l);
+void rtd_limits_get(rtd_limits *l);
+
 /* ---------------------------------------------------------------------
  * Exact k-NN.  Replaces the k_nn! round loop (gprt-macros/src/lib.rs:
  * 408-604) and its per-round gprt_execute + gprt_retrieve_array_* calls
@@ -158,6 +174,11 @@ uint64_t rtd_launch_count(void);
  * Output per query: the k smallest (FP32 squared distance, point id)
  * pairs, ascending, ties to the lower id; ids[q*k+j] (and d2[q*k+j] when
  * d2 != NULL).  Slots beyond the number of points hold 0xFFFFFFFF / +inf.
+ * Any k >= 1, as the reference's 2K-slot per-query slab
+ * (gprt-macros/src/lib.rs:300-310): k <= 16 keeps a thread's list in
+ * registers, k <= 256 a warp's list striped over its registers, and larger
+ * k a warp's sorted list in shared memory (min(k, n) <= 2048) or in a
+ * device slab the index keeps (grown on demand, at most 1 GiB).
  * ------------------------------------------------------------------- */
 rtd_status rtd_knn(rtd_index *idx, const float *d_queries, uint64_t nq, uint32_t k,
                    const rtd_schedule *sched, uint32_t *d_ids, float *d_d2, rtd_stream stream);
@@ -279,9 +300,10 @@ rtd_status rtd_knn_backward(const float *d_queries, uint64_t nq, const float *d_
  * Batched k-NN over many independent point clouds, each with its own
  * queries and k (no reference counterpart: the reference searches one scene
  * per k_nn! call).  One pass builds every cloud's LBVH as one forest (a
- * single sort over (cloud, Morton) keys) and searches every query in one
- * persistent launch fed from a device work queue; with use_graph the pass is
- * captured once as a CUDA graph and replayed.
+ * single sort over (cloud, Morton) keys) and searches every query of every
+ * cloud, whatever its k, in one persistent launch fed from one device work
+ * queue; with use_graph the pass is captured once as a CUDA graph and
+ * replayed.
  * ------------------------------------------------------------------- */
 typedef struct rtd_cloud {
     uint64_t point_offset;  /* first point of the cloud in the packed point array */
@@ -289,7 +311,7 @@ typedef struct rtd_cloud {
     uint64_t out_offset;    /* results of the cloud's query j at out_offset + j*k */
     uint32_t n_points;
     uint32_t n_queries;
-    uint32_t k;             /* 1 .. 256 */
+    uint32_t k;             /* >= 1, any size (k above 256 keeps its list in a device slab) */
     uint32_t pad;
 } rtd_cloud;
 
@@ -360,7 +382,9 @@ rtd_status rtd_bh_destroy(rtd_bh *b);
  * holds its own copy of the bodies in flat (leaf) order. */
 rtd_status rtd_bh_build(rtd_bh *b, const float *d_pos, const float *d_mass, uint64_t n,
                         const rtd_bh_params *p, rtd_stream stream);
-/* Frees the tree (keeps the handle); a backward then needs a new build. */
+/* Frees the tree and every device buffer the handle holds (build scratch,
+ * walk structures and stacks, adjoint scratch), except its 256-byte header;
+ * the handle stays valid and the next walk or backward needs a new build. */
 rtd_status rtd_bh_release(rtd_bh *b);
 /* Walk over the built tree.  Reference law: d_out = forces, d_phi unused.
  * Plummer law: d_out = accelerations, d_phi = potentials (may be NULL).
@@ -373,16 +397,19 @@ rtd_status rtd_bh_forward(rtd_bh *b, const rtd_bh_params *p, float *d_out, float
  * the device memory, and step loops that must not stall on the device-wide
  * synchronisation cudaMalloc / cudaFree can cause.  The walk's per-warp
  * traversal stack, which rtd_bh_forward reserves on first use, comes here
- * from a fixed 37 MiB array (592 warp stacks) that each device loading the
- * library holds until the process exits.  The array limits how many warps
- * walk at once, not the number of bodies, so no tree is refused for its
- * size; a traversal deeper than a warp's stack is reported as
- * RTD_ERR_OVERFLOW like rtd_bh_forward.  The first call on a device looks up
- * the array's device address (with that device current); make that first
- * call before any stream capture.  Every call shares the array: calls that
- * overlap on the GPU (other streams, other threads) race and must be
- * serialised by the caller.  Results equal rtd_bh_forward's bit for bit.
- * RTD_BH_LAW_REFERENCE is refused with RTD_ERR_UNSUPPORTED. */
+ * from a fixed 37 MiB array (592 warp stacks).  The CUDA module loader
+ * places that array on a device the first time a call runs there (in that
+ * context), and it stays until the process exits: make the first call
+ * during set-up, while the device still has 37 MiB free, and before any
+ * stream capture.  Later calls take no device memory.  Each call looks up
+ * the array's address in the current context, so a call after
+ * cudaDeviceReset or under another context finds the array there.  The
+ * array limits how many warps walk at once, not the number of bodies, so no
+ * tree is refused for its size; a traversal deeper than a warp's stack is
+ * reported as RTD_ERR_OVERFLOW like rtd_bh_forward.  Every call shares the
+ * array: calls that overlap on the GPU (other streams, other threads) race
+ * and must be serialised by the caller.  Results equal rtd_bh_forward's bit
+ * for bit.  RTD_BH_LAW_REFERENCE is refused with RTD_ERR_UNSUPPORTED. */
 rtd_status rtd_bh_forward_noalloc(rtd_bh *b, const rtd_bh_params *p, float *d_out, float *d_phi,
                                   rtd_stream stream);
 /* Adjoint of the Plummer-law walk (same tree, same decisions): given
@@ -405,6 +432,8 @@ typedef struct rtd_bh_info {
     uint64_t n_bodies, n_nodes, n_leaves;
     uint32_t depth;          /* deepest level (root = 0) */
     float root_min[3], root_max[3];
+    uint32_t max_stack;      /* deepest per-warp traversal stack of the Plummer walks on
+                                this tree since its build */
 } rtd_bh_info;
 rtd_status rtd_bh_info_get(rtd_bh *b, rtd_bh_info *info, rtd_stream stream);
 /* Interaction counts of the Plummer-law walk at opening angle theta, for

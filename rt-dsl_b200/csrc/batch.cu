@@ -5,12 +5,15 @@
 // cloud's points together in Morton order, and one Karras tree over the
 // whole key array is a forest whose node covering a cloud's key range is
 // that cloud's LBVH (keys sharing the cloud prefix form a subtree of a
-// binary radix tree).  Search: work items of <= 32 Morton-ordered queries of
-// one cloud are taken from a device counter by persistent warps; each item
-// runs the thread-per-query register list (k <= 16) or the warp-per-query
-// shuffle list (k <= 256) of knn_traverse.cuh against its cloud's root.
-// The whole pass is launch-only (no host synchronisation), so it can be
-// captured as one CUDA graph and replayed.
+// binary radix tree).  Search: one persistent launch.  Work items of <= 32
+// Morton-ordered queries of one cloud, each carrying its k class, are taken
+// from one device counter by every warp of the grid; an item runs the
+// thread-per-query register list (k <= 16), the warp-per-query striped
+// register list (k <= 256) or the warp-per-query memory list (any larger k)
+// of knn_traverse.cuh against its cloud's root.  Items are queued heaviest
+// class first, so the long warp-per-query items start early and the short
+// ones fill the tail.  The whole pass is launch-only (no host
+// synchronisation), so it can be captured as one CUDA graph and replayed.
 #include <new>
 #include <vector>
 
@@ -32,7 +35,7 @@ struct CloudDesc {
 };
 
 struct WorkItem {
-    uint32_t cloud, start, count, pad;
+    uint32_t cloud, start, count, cls;   // cls: k class (k_class), the search it runs
 };
 
 __global__ void batch_reset_kernel(CloudDesc *cd, uint32_t n_clouds) {
@@ -191,7 +194,10 @@ struct BatchArgs {
     float *d2;
     float mult2;
     uint32_t max_rounds;
+    uint32_t partial;   // the reference's round cap (rtd_schedule.partial_results)
     uint32_t *err;
+    uint2 *wide;        // per-warp list slabs of the k > 256 class
+    uint32_t wide_kk;   // entries per slab: the largest min(k, points) of that class
 };
 
 template <int KC>
@@ -205,7 +211,7 @@ __device__ __forceinline__ void item_thread(const BatchArgs &a, const TreeRef &t
     const int kk = (int)c.k;
     float bk[KC];
     uint32_t bi[KC];
-    knn_query_thread<KC>(t, rs, qx, qy, qz, kk, s_col, SWARPS * 32, l_stack, a.err, bk, bi);
+    knn_query_thread<KC>(t, rs, qx, qy, qz, kk, s_col, 32, l_stack, a.err, bk, bi);
     const uint64_t ob = c.out_off + (uint64_t)(qi - c.q_begin) * kk;
 #pragma unroll
     for (int j = 0; j < KC; ++j)
@@ -238,22 +244,46 @@ __device__ __forceinline__ void item_warp(const BatchArgs &a, const TreeRef &t, 
     }
 }
 
-// k classes of the search: register list of 8 or 16 slots (thread per
-// query), warp list of 32, 64 or 256 slots (warp per query).
-constexpr int N_CLASSES = 5;
-__host__ __device__ constexpr int k_class(uint32_t k) {
-    return k <= 8 ? 0 : k <= 16 ? 1 : k <= 32 ? 2 : k <= 64 ? 3 : 4;
+__device__ __forceinline__ void item_wide(const BatchArgs &a, const TreeRef &t, const RoundSpec &rs,
+                                          const CloudDesc &c, const WorkItem &w, uint2 *stk,
+                                          uint32_t *s_r, uint2 *slab) {
+    WideList list;
+    list.L = slab;
+    list.s_r = s_r;
+    list.kk = c.k < c.n_pts ? c.k : (c.n_pts ? c.n_pts : 1u);
+    for (uint32_t j = 0; j < w.count; ++j) {
+        const uint32_t qi = a.qperm[w.start + j];
+        const float qx = a.q[3 * (uint64_t)qi], qy = a.q[3 * (uint64_t)qi + 1], qz = a.q[3 * (uint64_t)qi + 2];
+        knn_query_warp_list(t, rs, qx, qy, qz, stk, a.err, list);
+        const uint64_t ob = c.out_off + (uint64_t)(qi - c.q_begin) * c.k;
+        wide_list_store(list, c.k, a.ids + ob, a.d2 ? a.d2 + ob : nullptr);
+        __syncwarp();
+    }
 }
 
-template <int CLS>
+// k classes of the search: register list of 8 or 16 slots (thread per
+// query), warp list of 32, 64 or 256 slots (warp per query), memory list
+// (warp per query, k > 256).
+constexpr int N_CLASSES = 6;
+__host__ __device__ constexpr int k_class(uint32_t k) {
+    return k <= 8 ? 0 : k <= 16 ? 1 : k <= 32 ? 2 : k <= 64 ? 3 : k <= 256 ? 4 : 5;
+}
+
+// Shared memory of one warp, reused by whichever class its current item
+// has: the thread classes' short stacks (SHORT_STACK x 32 entries, one
+// column per lane) or the warp classes' stack, list scratch and rank words.
+constexpr int WARP_SMEM = SHORT_STACK * 32;   // uint2 entries (4 KB)
+static_assert(STACK_MAX + 256 + 16 <= WARP_SMEM, "warp classes fit the thread stacks' space");
+
 __global__ void __launch_bounds__(SWARPS * 32) batch_knn_kernel(const BatchArgs a) {
-    constexpr bool THREAD = CLS < 2;
-    __shared__ uint2 s_stack[THREAD ? SHORT_STACK : 1][SWARPS * 32];
-    __shared__ uint2 s_wstack[THREAD ? 1 : SWARPS][THREAD ? 1 : STACK_MAX];
-    constexpr int LIST = CLS == 2 ? 32 : CLS == 3 ? 64 : 256;
-    __shared__ uint2 s_list[THREAD ? 1 : SWARPS][THREAD ? 1 : LIST];
-    uint2 l_stack[THREAD ? STACK_MAX - SHORT_STACK : 1];
+    __shared__ uint2 s_warp[SWARPS][WARP_SMEM];
+    uint2 l_stack[STACK_MAX - SHORT_STACK];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint2 *const sw = s_warp[warp];
+    uint2 *const stk = sw;                       // warp classes: STACK_MAX entries
+    uint2 *const ls = sw + STACK_MAX;            // list scratch (256 entries)
+    uint32_t *const s_r = reinterpret_cast<uint32_t *>(sw + STACK_MAX + 256);   // 32 words
+    uint2 *const slab = a.wide ? a.wide + ((size_t)blockIdx.x * SWARPS + warp) * a.wide_kk : nullptr;
     const uint32_t visit_cap = 2u * a.hdr->n_internal + 4u;
     while (true) {
         uint32_t it = 0;
@@ -263,12 +293,15 @@ __global__ void __launch_bounds__(SWARPS * 32) batch_knn_kernel(const BatchArgs 
         const WorkItem w = a.items[it];
         const CloudDesc c = a.cd[w.cloud];
         const TreeRef t{a.pts, a.nodes, nullptr, c.root, c.root_count, visit_cap};
-        const RoundSpec rs{c.r0sq, a.mult2, a.max_rounds};
-        if constexpr (CLS == 0) item_thread<8>(a, t, rs, c, w, &s_stack[0][threadIdx.x], l_stack);
-        else if constexpr (CLS == 1) item_thread<16>(a, t, rs, c, w, &s_stack[0][threadIdx.x], l_stack);
-        else if constexpr (CLS == 2) item_warp<1>(a, t, rs, c, w, s_wstack[warp], s_list[warp]);
-        else if constexpr (CLS == 3) item_warp<2>(a, t, rs, c, w, s_wstack[warp], s_list[warp]);
-        else item_warp<8>(a, t, rs, c, w, s_wstack[warp], s_list[warp]);
+        const RoundSpec rs{c.r0sq, a.mult2, a.max_rounds, a.partial};
+        switch (w.cls) {
+        case 0: item_thread<8>(a, t, rs, c, w, sw + lane, l_stack); break;
+        case 1: item_thread<16>(a, t, rs, c, w, sw + lane, l_stack); break;
+        case 2: item_warp<1>(a, t, rs, c, w, stk, ls); break;
+        case 3: item_warp<2>(a, t, rs, c, w, stk, ls); break;
+        case 4: item_warp<8>(a, t, rs, c, w, stk, ls); break;
+        default: item_wide(a, t, rs, c, w, stk, s_r, slab); break;
+        }
         __syncwarp();
     }
 }
@@ -310,13 +343,13 @@ using namespace rtd;
 struct rtd_batch {
     std::vector<rtd_cloud> clouds;
     uint32_t n_clouds = 0, n_items = 0;
-    uint32_t class_begin[rtd::N_CLASSES + 1] = {};   // work items sorted by k class
-    int class_blocks[rtd::N_CLASSES] = {};
+    int blocks = 0;             // grid of the persistent search
+    uint32_t wide_kk = 0;       // list slab entries per warp (0: no k > 256 cloud)
     uint64_t n_points = 0, n_queries = 0;
     int cbits = 0, bpa = 21;
     rtd_schedule sched;
     rtd_index forest;
-    DevBuf cd, items, pcloud, qcloud, qkeys, qkeys_alt, qvals, qvals_alt, counter;
+    DevBuf cd, items, pcloud, qcloud, qkeys, qkeys_alt, qvals, qvals_alt, counter, wide;
     // captured graph and the pointers it was captured with
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -343,7 +376,7 @@ static rtd_status batch_pass(rtd_batch *b, const float *d_pts, const float *d_q,
     CloudDesc *cd = b->cd.as<CloudDesc>();
     IndexHeader *h = f.hdr.as<IndexHeader>();
     RTD_CUDA(cudaMemsetAsync(h, 0, sizeof(IndexHeader), st));
-    RTD_CUDA(cudaMemsetAsync(b->counter.ptr, 0, N_CLASSES * sizeof(uint32_t), st));
+    RTD_CUDA(cudaMemsetAsync(b->counter.ptr, 0, sizeof(uint32_t), st));
     batch_reset_kernel<<<grid_for(b->n_clouds, 128, 1024), 128, 0, st>>>(cd, b->n_clouds);
     RTD_LAUNCH_CHECK();
     batch_cloud_of_kernel<<<b->n_clouds, 256, 0, st>>>(cd, b->pcloud.as<uint32_t>(),
@@ -403,21 +436,15 @@ static rtd_status batch_pass(rtd_batch *b, const float *d_pts, const float *d_q,
         const float m = b->sched.radius_increment_mult;
         a.mult2 = m * m;
         a.max_rounds = b->sched.max_rounds;
+        a.partial = b->sched.partial_results ? 1u : 0u;
         a.err = &h->err;
-        for (int cls = 0; cls < N_CLASSES; ++cls) {
-            const uint32_t i0 = b->class_begin[cls], i1 = b->class_begin[cls + 1];
-            if (i1 == i0) continue;
-            a.items = b->items.as<WorkItem>() + i0;
-            a.n_items = i1 - i0;
-            a.counter = b->counter.as<uint32_t>() + cls;
-            const int g = b->class_blocks[cls];
-            switch (cls) {
-            case 0: batch_knn_kernel<0><<<g, SWARPS * 32, 0, st>>>(a); break;
-            case 1: batch_knn_kernel<1><<<g, SWARPS * 32, 0, st>>>(a); break;
-            case 2: batch_knn_kernel<2><<<g, SWARPS * 32, 0, st>>>(a); break;
-            case 3: batch_knn_kernel<3><<<g, SWARPS * 32, 0, st>>>(a); break;
-            default: batch_knn_kernel<4><<<g, SWARPS * 32, 0, st>>>(a); break;
-            }
+        a.items = b->items.as<WorkItem>();
+        a.n_items = b->n_items;
+        a.counter = b->counter.as<uint32_t>();
+        a.wide = b->wide_kk ? b->wide.as<uint2>() : nullptr;
+        a.wide_kk = b->wide_kk;
+        if (b->n_items) {
+            batch_knn_kernel<<<b->blocks, SWARPS * 32, 0, st>>>(a);
             RTD_LAUNCH_CHECK();
         }
     }
@@ -457,36 +484,39 @@ rtd_status rtd_batch_plan(rtd_batch *b, const rtd_cloud *clouds, uint32_t n_clou
     if (s.max_rounds < 1) return fail(RTD_ERR_INVALID_ARGUMENT, "max_rounds must be >= 1");
     if (s.leaf_size < 1 || s.leaf_size > 64) return fail(RTD_ERR_INVALID_ARGUMENT, "leaf_size must be in [1, 64]");
     uint64_t np = 0, nq = 0;
+    uint32_t wide_kk = 0;
     std::vector<CloudDesc> cd(n_clouds);
     std::vector<WorkItem> cls_items[N_CLASSES];
     for (uint32_t c = 0; c < n_clouds; ++c) {
         const rtd_cloud &x = clouds[c];
         if (x.point_offset != np || x.query_offset != nq)
             return fail(RTD_ERR_INVALID_ARGUMENT, "clouds must be packed in order");
-        if (x.k < 1 || x.k > 256) return fail(RTD_ERR_INVALID_ARGUMENT, "k must be in [1, 256]");
+        if (x.k < 1) return fail(RTD_ERR_INVALID_ARGUMENT, "k must be >= 1");
         cd[c] = CloudDesc{(uint32_t)np, x.n_points, (uint32_t)nq, x.n_queries, x.k, 0u, 0u, {}, 0.f,
                           x.out_offset};
+        const int cls = s.lanes_per_query == 32 && x.k <= 32 ? 2 : k_class(x.k);
+        if (cls == 5 && x.n_queries) {
+            const uint32_t kk = x.k < x.n_points ? x.k : (x.n_points ? x.n_points : 1u);
+            if (kk > wide_kk) wide_kk = kk;
+        }
         for (uint32_t s0 = 0; s0 < x.n_queries; s0 += 32)
-            cls_items[s.lanes_per_query == 32 && x.k <= 32 ? 2 : k_class(x.k)].push_back(
-                WorkItem{c, (uint32_t)nq + s0, x.n_queries - s0 < 32u ? x.n_queries - s0 : 32u, 0u});
+            cls_items[cls].push_back(WorkItem{c, (uint32_t)nq + s0,
+                                              x.n_queries - s0 < 32u ? x.n_queries - s0 : 32u,
+                                              (uint32_t)cls});
         np += x.n_points;
         nq += x.n_queries;
     }
     if (np >= (1ull << 30) - 1 || nq >= (1ull << 30)) return fail(RTD_ERR_INVALID_ARGUMENT, "batch too large");
+    // one queue, heaviest class first
     std::vector<WorkItem> items;
-    uint32_t class_begin[N_CLASSES + 1];
-    for (int c = 0; c < N_CLASSES; ++c) {
-        class_begin[c] = (uint32_t)items.size();
-        items.insert(items.end(), cls_items[c].begin(), cls_items[c].end());
-    }
-    class_begin[N_CLASSES] = (uint32_t)items.size();
+    for (int c = N_CLASSES - 1; c >= 0; --c) items.insert(items.end(), cls_items[c].begin(), cls_items[c].end());
     b->drop_graph();
     b->clouds.assign(clouds, clouds + n_clouds);
     b->n_clouds = n_clouds;
     b->n_points = np;
     b->n_queries = nq;
     b->n_items = (uint32_t)items.size();
-    for (int c = 0; c <= N_CLASSES; ++c) b->class_begin[c] = class_begin[c];
+    b->wide_kk = wide_kk;
     b->sched = s;
     int cb = 0;
     while (cb < 32 && (1ull << cb) < n_clouds) ++cb;
@@ -516,26 +546,28 @@ rtd_status rtd_batch_plan(rtd_batch *b, const rtd_cloud *clouds, uint32_t n_clou
     RTD_TRY(b->qkeys_alt.reserve(nq * 8 + 8));
     RTD_TRY(b->qvals.reserve(nq * 4 + 4));
     RTD_TRY(b->qvals_alt.reserve(nq * 4 + 4));
-    RTD_TRY(b->counter.reserve(N_CLASSES * sizeof(uint32_t)));
+    RTD_TRY(b->counter.reserve(sizeof(uint32_t)));
     if (n_clouds)
         RTD_CUDA(cudaMemcpy(b->cd.ptr, cd.data(), n_clouds * sizeof(CloudDesc), cudaMemcpyHostToDevice));
     if (!items.empty())
         RTD_CUDA(cudaMemcpy(b->items.ptr, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice));
     int sms = 148;
     RTD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, f.device));
-    const void *kern[N_CLASSES] = {(const void *)batch_knn_kernel<0>, (const void *)batch_knn_kernel<1>,
-                                   (const void *)batch_knn_kernel<2>, (const void *)batch_knn_kernel<3>,
-                                   (const void *)batch_knn_kernel<4>};
-    for (int c = 0; c < N_CLASSES; ++c) {
-        const uint32_t n_it = class_begin[c + 1] - class_begin[c];
-        b->class_blocks[c] = 0;
-        if (!n_it) continue;
-        int per_sm = 1;
-        RTD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern[c], SWARPS * 32, 0));
-        if (per_sm < 1) per_sm = 1;
-        const uint64_t full = (uint64_t)sms * per_sm, need = (n_it + SWARPS - 1) / SWARPS;
-        b->class_blocks[c] = (int)(full < need ? full : need);
+    // persistent grid: every resident warp, no more blocks than items need,
+    // and (with k > 256 clouds) at most 1 GiB of list slabs
+    int per_sm = 1;
+    RTD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_knn_kernel, SWARPS * 32, 0));
+    if (per_sm < 1) per_sm = 1;
+    uint64_t blocks = (uint64_t)sms * per_sm;
+    const uint64_t need = ((uint64_t)items.size() + SWARPS - 1) / SWARPS;
+    if (blocks > need) blocks = need ? need : 1;
+    if (wide_kk) {
+        const uint64_t per_block = (uint64_t)SWARPS * wide_kk * sizeof(uint2);
+        const uint64_t cap = (1ull << 30) / per_block;
+        if (blocks > cap) blocks = cap ? cap : 1;
+        RTD_TRY(b->wide.reserve(blocks * per_block));
     }
+    b->blocks = (int)blocks;
     return RTD_OK;
 }
 

@@ -35,7 +35,12 @@ struct BhHeader {
     uint32_t group_counter;   // work queue of the walks (next group to take)
 };
 
-constexpr int BH_STACK_CAP = 8192;          // traversal stack entries per walking warp
+// Traversal stack entries per walking warp: the slice each warp owns in a
+// stack buffer.  The walks push within stack_entries <= BH_STACK_CAP_MAX
+// (rtd_limits_set lowers it; a push beyond it is refused and reported as
+// DEVERR_STACK).
+constexpr uint32_t BH_STACK_CAP_MAX = 8192;
+uint32_t bh_stack_entries();   // the current per-warp limit (capi.cu)
 
 }  // namespace rtd
 

@@ -82,9 +82,13 @@ rtd_status rtd_bh_release(rtd_bh *b) {
                       &b->pvals, &b->pvals_alt, &b->lcp, &b->wmin, &b->lam, &b->nn, &b->base,
                       &b->heads, &b->leaf_head, &b->leaf_of, &b->fkeys, &b->fkeys_alt, &b->fvals,
                       &b->fvals_alt, &b->node_start, &b->node_level, &b->level_nodes, &b->order,
-                      &b->fbody, &b->node_a, &b->node_b, &b->node_q, &b->cell_grad, &b->prefix,
-                      &b->gpos_flat, &b->gmass_flat})
+                      &b->fbody, &b->node_a, &b->node_b, &b->node_q, &b->child8, &b->leaf_node,
+                      &b->groups, &b->stack, &b->cell_grad, &b->prefix, &b->gpos_flat,
+                      &b->gmass_flat})
         d->release();
+    b->stack_warps = 0;
+    b->plummer_ready = false;
+    b->has_quad = false;
     b->sort.hist.release();
     b->sort.status.release();
     b->sort.counters.release();
@@ -122,6 +126,7 @@ rtd_status rtd_bh_info_get(rtd_bh *b, rtd_bh_info *info, rtd_stream stream) {
         info->root_min[a] = h.root_min[a];
         info->root_max[a] = h.root_max[a];
     }
+    info->max_stack = h.max_stack;
     return check_bh_errors(b, st);
 }
 

@@ -10,8 +10,6 @@
 // runs the same walk kernel on a stack that lives in the fixed array below,
 // which the CUDA module loader places on each device that loads this
 // library's code and keeps there until the process exits.
-#include <mutex>
-
 #include <rtdsl.h>
 
 #include "bh.cuh"
@@ -23,32 +21,26 @@ rtd_status bh_forward_on_stack(rtd_bh *b, const rtd_bh_params *p, float *d_out, 
 
 using namespace rtd;
 
-// 592 warp stacks (148 SMs x one block of 4 warps) of BH_STACK_CAP = 8192
+// 592 warp stacks (148 SMs x one block of 4 warps) of BH_STACK_CAP_MAX = 8192
 // entries of 8 bytes: 37 MiB per device.
 static constexpr uint64_t NOALLOC_WARPS = 592;
-static __device__ __align__(256) uint2 g_noalloc_walk_stack[NOALLOC_WARPS * BH_STACK_CAP];
+static __device__ __align__(256) uint2 g_noalloc_walk_stack[NOALLOC_WARPS * BH_STACK_CAP_MAX];
 
 namespace {
-constexpr int MAX_DEVICES = 64;
-std::mutex g_setup_mutex;
-uint2 *g_stack_addr[MAX_DEVICES] = {};   // device address of the array, per device
-
-// Device address of the stack array on the current device.  The host symbol
-// g_noalloc_walk_stack is only a stand-in for it; the address is looked up
-// once per device, with that device current.
+// Device address of the stack array in the current context.  The host
+// symbol g_noalloc_walk_stack is only a stand-in for it.  The address is
+// looked up on every call, with the caller's device current: a table
+// lookup in the CUDA runtime once the module is loaded, and always the
+// address in the context the walk will run in (a cached address would go
+// stale after cudaDeviceReset, or under another context of the same device).
+// The first lookup in a context loads this file's module, which places the
+// 37 MiB array on the device: that is the one time the entry point takes
+// device memory, through the module loader rather than cudaMalloc.
 rtd_status stack_address(uint2 **out) {
-    int dev = 0;
-    RTD_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= MAX_DEVICES)
-        return fail(RTD_ERR_UNSUPPORTED, "device ordinal above 63");
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_stack_addr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_walk_stack);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress");
-        g_stack_addr[dev] = static_cast<uint2 *>(p);
-    }
-    *out = g_stack_addr[dev];
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_walk_stack);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress");
+    *out = static_cast<uint2 *>(p);
     return RTD_OK;
 }
 }  // namespace

@@ -160,12 +160,12 @@ __global__ void __launch_bounds__(WW * 32, ADJ ? 6 : 0) bh_walk_kernel(
     const BhView v, float theta2, float eps2, float G, const float *__restrict__ g_acc,
     const float *__restrict__ g_phi, float *__restrict__ acc_out, float *__restrict__ phi_out,
     float4 *__restrict__ cell_grad, float4 *__restrict__ body_grad, uint2 *__restrict__ stack,
-    BhHeader *hm) {
+    uint32_t stack_entries, BhHeader *hm) {
     __shared__ WarpTile tiles[WW];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     WarpTile &T = tiles[warp];
     const uint64_t gw = (uint64_t)blockIdx.x * WW + warp;
-    uint2 *stk = stack + gw * BH_STACK_CAP;
+    uint2 *stk = stack + gw * BH_STACK_CAP_MAX;   // this warp's slice
     const uint32_t ngroups = v.hdr->n_groups, n_nodes = v.hdr->n_nodes;
     const uint32_t lt = lane_lt();
     const uint32_t *child = reinterpret_cast<const uint32_t *>(v.child8);
@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(WW * 32, ADJ ? 6 : 0) bh_walk_kernel(
                     const uint32_t c = lane < 8 ? __ldg(&child[8 * (uint64_t)nk + lane]) : 0xFFFFFFFFu;
                     const uint32_t pm = __ballot_sync(0xffffffffu, c != 0xFFFFFFFFu);
                     const int np = __popc(pm);
-                    if (sp + np <= BH_STACK_CAP) {
+                    if ((uint32_t)(sp + np) <= stack_entries) {
                         if (c != 0xFFFFFFFFu) stk[sp + __popc(pm & lt)] = make_uint2(c, R);
                         sp += np;
                     } else if (lane == 0) {
@@ -476,7 +476,7 @@ rtd_status launch_walk(rtd_bh *b, const rtd_bh_params *p, const float *g_acc, co
     if (blocks < 1) blocks = 1;
     const uint64_t warps = blocks * WW;
     if (b->stack_warps < warps) {
-        RTD_TRY(b->stack.reserve(warps * BH_STACK_CAP * sizeof(uint2)));
+        RTD_TRY(b->stack.reserve(warps * BH_STACK_CAP_MAX * sizeof(uint2)));
         b->stack_warps = warps;
     }
     BhHeader *h = b->hdr.as<BhHeader>();
@@ -484,7 +484,8 @@ rtd_status launch_walk(rtd_bh *b, const rtd_bh_params *p, const float *g_acc, co
     const BhView v = bh_view(b);
     bh_walk_kernel<QUAD, ADJ><<<(unsigned)blocks, WW * 32, 0, st>>>(
         v, p->theta * p->theta, p->eps * p->eps, p->G, g_acc, g_phi, acc, phi,
-        b->cell_grad.as<float4>(), b->gpos_flat.as<float4>(), b->stack.as<uint2>(), h);
+        b->cell_grad.as<float4>(), b->gpos_flat.as<float4>(), b->stack.as<uint2>(),
+        bh_stack_entries(), h);
     RTD_LAUNCH_CHECK();
     return RTD_OK;
 }
@@ -546,7 +547,7 @@ rtd_status bh_backward(rtd_bh *b, const rtd_bh_params *p, const float *g_acc, co
 namespace {
 
 // Forward walk on a traversal stack supplied by the caller: `stack` holds
-// max_warps slices of BH_STACK_CAP entries and the launch is capped to that
+// max_warps slices of BH_STACK_CAP_MAX entries and the launch is capped to that
 // many warps.  Nothing is allocated.
 template <bool QUAD>
 rtd_status launch_walk_on_stack(rtd_bh *b, const rtd_bh_params *p, float *acc, float *phi,
@@ -567,7 +568,7 @@ rtd_status launch_walk_on_stack(rtd_bh *b, const rtd_bh_params *p, float *acc, f
     const BhView v = bh_view(b);
     bh_walk_kernel<QUAD, false><<<(unsigned)blocks, WW * 32, 0, st>>>(
         v, p->theta * p->theta, p->eps * p->eps, p->G, nullptr, nullptr, acc, phi, nullptr,
-        nullptr, stack, h);
+        nullptr, stack, bh_stack_entries(), h);
     RTD_LAUNCH_CHECK();
     return RTD_OK;
 }
@@ -575,7 +576,7 @@ rtd_status launch_walk_on_stack(rtd_bh *b, const rtd_bh_params *p, float *acc, f
 }  // namespace
 
 // Plummer-law forward walk with the traversal stack given by the caller
-// (max_warps slices of BH_STACK_CAP uint2 entries); same checks and results
+// (max_warps slices of BH_STACK_CAP_MAX uint2 entries); same checks and results
 // as bh_forward for the Plummer law.
 rtd_status bh_forward_on_stack(rtd_bh *b, const rtd_bh_params *p, float *d_out, float *d_phi,
                                uint2 *stack, uint64_t max_warps, cudaStream_t st) {

@@ -36,6 +36,7 @@ __global__ void bh_hdr_init_kernel(BhHeader *h) {
         h->box[3 + a] = 0u;
     }
     h->err = 0;
+    h->max_stack = 0;
     h->n_nodes = 0;
     h->n_leaves = 0;
     for (int l = 0; l < BH_MAX_LEVEL + 2; ++l) h->level_count[l] = 0;

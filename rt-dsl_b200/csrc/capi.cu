@@ -183,7 +183,56 @@ rtd_context_bh *context_bh(rtd_context *ctx) {
 
 cudaStream_t context_stream(rtd_context *ctx) { return ctx->stream; }
 
+namespace {
+// The look-backs' bounded wait (spin_more) on one flag: waits for
+// *flag != 0; when `limit` retries run out it sets DEVERR_TIMEOUT in *err
+// and returns.
+__global__ void wait_flag_kernel(const volatile uint32_t *flag, uint32_t limit, uint32_t *err) {
+    uint32_t spins = 0;
+    while (*flag == 0) {
+        if (!spin_more(spins, limit)) {
+            atomicOr(err, DEVERR_TIMEOUT);
+            return;
+        }
+    }
+}
+
+std::atomic<uint32_t> g_bh_stack_entries{BH_STACK_CAP_MAX};
+}  // namespace
+
+uint32_t rtd::bh_stack_entries() { return g_bh_stack_entries.load(std::memory_order_relaxed); }
+
 extern "C" {
+
+rtd_status rtd_wait_selftest(uint32_t spin_limit, int flag_set, rtd_stream stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    DevBuf words;   // flag, err
+    RTD_TRY(words.reserve(2 * sizeof(uint32_t)));
+    uint32_t *w = words.as<uint32_t>();
+    RTD_CUDA(cudaMemsetAsync(w, 0, 2 * sizeof(uint32_t), st));
+    if (flag_set) RTD_CUDA(cudaMemsetAsync(w, 0xFF, sizeof(uint32_t), st));
+    wait_flag_kernel<<<1, 1, 0, st>>>(w, spin_limit, w + 1);
+    RTD_LAUNCH_CHECK();
+    uint32_t err = 0;
+    RTD_CUDA(cudaMemcpyAsync(&err, w + 1, sizeof(err), cudaMemcpyDeviceToHost, st));
+    RTD_CUDA(cudaStreamSynchronize(st));
+    return status_from_deverr(err);
+}
+
+rtd_status rtd_limits_set(const rtd_limits *l) {
+    if (!l) return fail(RTD_ERR_INVALID_ARGUMENT, "limits is NULL");
+    const uint32_t e = l->bh_stack_entries ? l->bh_stack_entries : BH_STACK_CAP_MAX;
+    if (e < 8 || e > BH_STACK_CAP_MAX)
+        return fail(RTD_ERR_INVALID_ARGUMENT, "bh_stack_entries must be 0 or in [8, 8192]");
+    g_bh_stack_entries.store(e, std::memory_order_relaxed);
+    return RTD_OK;
+}
+
+void rtd_limits_get(rtd_limits *l) {
+    if (!l) return;
+    memset(l, 0, sizeof(*l));
+    l->bh_stack_entries = bh_stack_entries();
+}
 
 void rtd_schedule_default(rtd_schedule *s) {
     if (!s) return;
@@ -196,8 +245,8 @@ void rtd_schedule_default(rtd_schedule *s) {
     s->block_size = 0;
     s->lanes_per_query = 0;
     s->morton_bits = 0;
-    s->packet_traversal = RTD_PACKET_AUTO;
-    s->lane_refill = RTD_REFILL_AUTO;
+    s->partial_results = 0;
+    s->reserved = 0;
 }
 
 const char *rtd_status_string(rtd_status s) {

@@ -44,7 +44,6 @@ struct IndexHeader {
     uint64_t total;       // last range-count total
     float nn95_key;       // p95 of the squared 1-NN distance within a 4096-point sample
     uint32_t n_sample;    // points in the radius-seed sample (<= 1000)
-    unsigned long long qcounter;   // work counter of the refilling search kernels
 };
 
 constexpr int SEED_NN_SAMPLE = 4096;
@@ -109,6 +108,7 @@ struct rtd_index {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_seed_fork = nullptr,
                 ev_seed_join = nullptr, ev_sorted = nullptr;
     rtd::DevBuf wpos;       // queries' Morton positions for the window seed
+    rtd::DevBuf wide;       // per-warp list slabs of the k > 2048 search
     rtd::QueryOrderScratch qorder;
     // phase timers (rtd_index_profile_*)
     bool prof = false;

@@ -4,6 +4,8 @@
 // reference relaunches per round, copies a Q x 2k slab back to the host and
 // filters there, every query here runs all its rounds inside one launch
 // (knn_traverse.cuh).
+#include <atomic>
+
 #include "knn_traverse.cuh"
 
 namespace rtd {
@@ -17,6 +19,7 @@ struct KnnArgs {
     uint32_t k;
     float mult2;
     uint32_t max_rounds;
+    uint32_t partial;       // the reference's round cap (rtd_schedule.partial_results)
     uint32_t *ids;
     float *d2;
     uint32_t *err;
@@ -109,7 +112,7 @@ __global__ void __launch_bounds__(BLOCK, KC <= 5 ? 1280 / BLOCK : 0) knn_thread_
     // a round visits each internal node at most once; more means a broken tree
     const TreeRef tree{p.ix.pts, p.ix.nodes, s_top, h->root, h->root_count,
                        2u * h->n_internal + 4u};
-    const RoundSpec rs{h->r0sq, p.mult2, p.max_rounds};
+    const RoundSpec rs{h->r0sq, p.mult2, p.max_rounds, p.partial};
     const int kk = (int)p.k;
     uint2 l_stack[STACK_MAX - SHORT_STACK];
 
@@ -125,7 +128,7 @@ __global__ void __launch_bounds__(BLOCK, KC <= 5 ? 1280 / BLOCK : 0) knn_thread_
             list_init<KC>(bk, bi, kk);
             uint32_t w0 = 0, w1 = 0;
             if (h->root != CHILD_NONE) morton_window_seed<KC>(p, t, qx, qy, qz, kk, bk, bi, w0, w1);
-            const RoundSpec one{rs.r0sq, rs.mult2, 1u};
+            const RoundSpec one{rs.r0sq, rs.mult2, 1u, 0u};
             knn_query_thread<KC, true>(tree, one, qx, qy, qz, kk, &s_stack[0][threadIdx.x], BLOCK,
                                        l_stack, p.err, bk, bi, w0, w1);
         } else {
@@ -143,337 +146,6 @@ __global__ void __launch_bounds__(BLOCK, KC <= 5 ? 1280 / BLOCK : 0) knn_thread_
     }
 }
 
-// One thread per query with lane refill: persistent warps whose lanes take
-// the next query as soon as their own one finishes, so a warp does not idle
-// until its slowest query ends.  A warp takes chunks of REFILL_CHUNK
-// consecutive (Morton-ordered) queries from a global counter and hands them
-// to its idle lanes; every lane runs the same per-query algorithm as
-// knn_query_thread, one node per loop trip.
-constexpr uint32_t REFILL_CHUNK = 64;
-
-template <int KC, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) knn_refill_kernel(const KnnArgs p,
-                                                           unsigned long long *counter) {
-    __shared__ BvhNode s_top[TOP_MAX];
-    __shared__ uint2 s_stack[SHORT_STACK][BLOCK];
-    const IndexHeader *h = p.ix.hdr;
-    const uint32_t ntop = h->n_top;
-    for (uint32_t i = threadIdx.x; i < ntop; i += BLOCK) s_top[i] = p.ix.top[i];
-    __syncthreads();
-    const uint32_t root = h->root, root_count = h->root_count;
-    const uint32_t visit_cap = 2u * h->n_internal + 4u;
-    float r0sq = h->r0sq;
-    if (!(r0sq > 0.0f)) r0sq = 1e-30f;
-    const int kk = (int)p.k;
-    const int lane = threadIdx.x & 31;
-    uint32_t lt;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
-    uint2 *s_col = &s_stack[0][threadIdx.x];
-    uint2 l_stack[STACK_MAX - SHORT_STACK];
-
-    unsigned long long c_next = 0, c_end = 0;   // the warp's chunk (warp-uniform)
-    bool exhausted = false;                      // warp-uniform
-    bool active = false;
-    uint64_t qi = 0;
-    float qx = 0.f, qy = 0.f, qz = 0.f;
-    float bk[KC];
-    uint32_t bi[KC];
-    float bound = 0.f, prev = -1.f, lim = 0.f;
-    uint32_t node = 0, visits = 0, round = 0;
-    int sp = 0;
-    bool last = false;
-
-    while (true) {
-        // hand queries of the warp's chunk to idle lanes
-        uint32_t idle = __ballot_sync(0xffffffffu, !active);
-        while (idle && !exhausted) {
-            if (c_next == c_end) {
-                unsigned long long base = 0;
-                if (lane == 0) base = atomicAdd(counter, (unsigned long long)REFILL_CHUNK);
-                base = __shfl_sync(0xffffffffu, base, 0);
-                if (base >= p.nq) {
-                    exhausted = true;
-                    break;
-                }
-                c_next = base;
-                c_end = base + REFILL_CHUNK < p.nq ? base + REFILL_CHUNK : p.nq;
-            }
-            const uint32_t avail = (uint32_t)(c_end - c_next);
-            const uint32_t rank = __popc(idle & lt);
-            const bool mine = !active && rank < avail;
-            if (mine) {
-                const uint64_t t = c_next + rank;
-                qi = p.perm ? p.perm[t] : t;
-                qx = p.q[3 * qi];
-                qy = p.q[3 * qi + 1];
-                qz = p.q[3 * qi + 2];
-#pragma unroll
-                for (int j = 0; j < KC; ++j) {
-                    const bool pad = j < KC - kk;
-                    bk[j] = pad ? -INFINITY : INFINITY;
-                    bi[j] = pad ? 0u : EMPTY_ID;
-                }
-                bound = r0sq;
-                prev = -1.0f;
-                round = 0;
-                last = 1u >= p.max_rounds || !(bound < INFINITY);
-                if (last) bound = INFINITY;
-                lim = fminf(bound, bk[KC - 1]);
-                node = root;
-                sp = 0;
-                visits = 0;
-                active = true;
-            }
-            const uint32_t took = min(avail, (uint32_t)__popc(idle));
-            c_next += took;
-            idle = __ballot_sync(0xffffffffu, !active);
-        }
-        if (!__any_sync(0xffffffffu, active)) break;
-        if (!active) continue;
-
-        // one node of this lane's traversal
-        bool done = false;
-        if (root == CHILD_NONE || isnan(qx) || isnan(qy) || isnan(qz)) {
-            done = true;
-        } else if (++visits > visit_cap) {
-            atomicOr(p.err, DEVERR_STACK);
-            done = true;
-        } else {
-            uint32_t fa = 0, ca = 0, fb = 0, cb = 0;   // leaf ranges to test
-            uint32_t next = CHILD_NONE;
-            float k0 = 0.f, k1 = 0.f;
-            bool v0 = false, v1 = false;
-            uint4 d = make_uint4(0, 0, 0, 0);
-            if (node & CHILD_LEAF) {
-                fa = node & CHILD_INDEX;
-                ca = root_count;
-            } else {
-                float4 a, b, c;
-                load_node(s_top, p.ix.nodes, node, a, b, c, d);
-                k0 = box_min_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y);
-                k1 = box_min_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w);
-                v0 = !(k0 > lim);
-                v1 = !(k1 > lim);
-                if (prev >= 0.0f) {
-                    if (v0) v0 = !(box_max_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y) <= prev);
-                    if (v1) v1 = !(box_max_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w) <= prev);
-                }
-                if (v0 && (d.x & CHILD_LEAF)) { fa = d.x & CHILD_INDEX; ca = d.z; v0 = false; }
-                if (v1 && (d.y & CHILD_LEAF)) { fb = d.y & CHILD_INDEX; cb = d.w; v1 = false; }
-            }
-            const uint32_t tot = ca + cb;
-            for (uint32_t j = 0; j < tot; ++j) {
-                const float4 pt = __ldg(&p.ix.pts[j < ca ? fa + j : fb + (j - ca)]);
-                const float key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
-                const uint32_t id = __float_as_uint(pt.w);
-                if (key <= bound && key > prev && key_less(key, id, bk[KC - 1], bi[KC - 1]))
-                    list_insert<KC>(bk, bi, key, id);
-            }
-            if (tot) lim = fminf(bound, bk[KC - 1]);
-            if (!(node & CHILD_LEAF)) {
-                v0 = v0 && !(k0 > lim);
-                v1 = v1 && !(k1 > lim);
-                if (v0 && v1) {
-                    const bool near0 = k0 <= k1;
-                    const uint2 far = near0 ? make_uint2(d.y, __float_as_uint(k1))
-                                            : make_uint2(d.x, __float_as_uint(k0));
-                    next = near0 ? d.x : d.y;
-                    if (sp < SHORT_STACK) s_col[sp * BLOCK] = far;
-                    else if (sp < STACK_MAX) l_stack[sp - SHORT_STACK] = far;
-                    else atomicOr(p.err, DEVERR_STACK);
-                    if (sp < STACK_MAX) ++sp;
-                } else if (v0) {
-                    next = d.x;
-                } else if (v1) {
-                    next = d.y;
-                }
-            }
-            if (next == CHILD_NONE) {
-                while (sp > 0) {
-                    --sp;
-                    const uint2 e = sp < SHORT_STACK ? s_col[sp * BLOCK] : l_stack[sp - SHORT_STACK];
-                    if (!(__uint_as_float(e.y) > lim)) { next = e.x; break; }
-                }
-            }
-            if (next != CHILD_NONE) {
-                node = next;
-            } else if (bi[KC - 1] != EMPTY_ID || last) {
-                done = true;
-            } else {   // next round: grow the radius, restart at the root
-                prev = bound;
-                bound = __fmul_rn(bound, p.mult2);
-                ++round;
-                last = round + 1 >= p.max_rounds || !(bound < INFINITY);
-                if (last) bound = INFINITY;
-                lim = fminf(bound, bk[KC - 1]);
-                node = root;
-                sp = 0;
-                visits = 0;
-            }
-        }
-        if (done) {
-            const uint64_t ob = qi * (uint64_t)kk;
-#pragma unroll
-            for (int j = 0; j < KC; ++j) {
-                if (j >= KC - kk) {
-                    p.ids[ob + j - (KC - kk)] = bi[j];
-                    if (p.d2) p.d2[ob + j - (KC - kk)] = bk[j];
-                }
-            }
-            active = false;
-        }
-    }
-}
-
-// Packet traversal: a warp walks the tree once for 32 consecutive
-// (Morton-ordered) queries.  A child is visited when any lane's query wants
-// it; node loads are warp-uniform (broadcast) and the node stack is shared,
-// while every lane keeps its own register list, bound test and stacked box
-// key.  Rounds are warp-uniform because the radius schedule is global;
-// lanes whose list is full drop out.
-template <int KC, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) knn_packet_kernel(const KnnArgs p) {
-    __shared__ BvhNode s_top[TOP_MAX];
-    __shared__ uint32_t s_stack[WARPS][STACK_MAX];
-    const IndexHeader *h = p.ix.hdr;
-    const uint32_t ntop = h->n_top;
-    for (uint32_t i = threadIdx.x; i < ntop; i += WARPS * 32) s_top[i] = p.ix.top[i];
-    __syncthreads();
-    const uint32_t root = h->root, root_count = h->root_count;
-    float r0sq = h->r0sq;
-    if (!(r0sq > 0.0f)) r0sq = 1e-30f;
-    const float4 *__restrict__ pts = p.ix.pts;
-    const BvhNode *__restrict__ gn = p.ix.nodes;
-    const int kk = (int)p.k;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t visit_cap = 2u * h->n_internal + 4u;
-    uint32_t *stk = s_stack[warp];
-    float l_key[STACK_MAX];
-
-    for (uint64_t tb = ((uint64_t)blockIdx.x * WARPS + warp) * 32; tb < p.nq;
-         tb += (uint64_t)gridDim.x * WARPS * 32) {
-        const uint64_t t = tb + lane;
-        const bool have = t < p.nq;
-        const uint64_t qi = have ? (p.perm ? p.perm[t] : t) : 0;
-        float qx = 0.f, qy = 0.f, qz = 0.f;
-        if (have) { qx = p.q[3 * qi]; qy = p.q[3 * qi + 1]; qz = p.q[3 * qi + 2]; }
-        float bk[KC];
-        uint32_t bi[KC];
-#pragma unroll
-        for (int j = 0; j < KC; ++j) {
-            bool pad = j < KC - kk;
-            bk[j] = pad ? -INFINITY : INFINITY;
-            bi[j] = pad ? 0u : EMPTY_ID;
-        }
-        bool active = have && root != CHILD_NONE && !isnan(qx) && !isnan(qy) && !isnan(qz);
-        float bound = r0sq, prev = -1.0f;
-        for (uint32_t round = 0; __any_sync(0xffffffffu, active); ++round) {
-            const bool last = round + 1 >= p.max_rounds || !(bound < INFINITY);
-            if (last) bound = INFINITY;
-            float lim = active ? fminf(bound, bk[KC - 1]) : -1.0f;
-            uint32_t node = root;
-            int sp = 0;
-            uint32_t visits = 0;
-            while (true) {
-                if (++visits > visit_cap) {   // warp-uniform
-                    if (lane == 0) atomicOr(p.err, DEVERR_STACK);
-                    break;
-                }
-                // leaf ranges [fa, fa + ca) and [fb, fb + cb) (warp-uniform)
-                // and whether this lane wants each
-                uint32_t fa = 0, ca = 0, fb = 0, cb = 0;
-                bool wa = false, wb = false;
-                uint32_t next = CHILD_NONE;
-                float k0 = 0.f, k1 = 0.f;
-                bool w0 = false, w1 = false;
-                uint4 d = make_uint4(0, 0, 0, 0);
-                if (node & CHILD_LEAF) {
-                    fa = node & CHILD_INDEX;
-                    ca = root_count;
-                    wa = active;
-                } else {
-                    float4 a, b, c;
-                    load_node(s_top, gn, node, a, b, c, d);
-                    k0 = box_min_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y);
-                    k1 = box_min_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w);
-                    w0 = !(k0 > lim);
-                    w1 = !(k1 > lim);
-                    if (prev >= 0.0f) {
-                        if (w0) w0 = !(box_max_key(qx, qy, qz, a.x, a.y, a.z, a.w, b.x, b.y) <= prev);
-                        if (w1) w1 = !(box_max_key(qx, qy, qz, b.z, b.w, c.x, c.y, c.z, c.w) <= prev);
-                    }
-                    if ((d.x & CHILD_LEAF) && __any_sync(0xffffffffu, w0)) {
-                        fa = d.x & CHILD_INDEX; ca = d.z; wa = w0;
-                    }
-                    if ((d.y & CHILD_LEAF) && __any_sync(0xffffffffu, w1)) {
-                        fb = d.y & CHILD_INDEX; cb = d.w; wb = w1;
-                    }
-                    if (d.x & CHILD_LEAF) w0 = false;
-                    if (d.y & CHILD_LEAF) w1 = false;
-                }
-                const uint32_t tot = ca + cb;
-                for (uint32_t j = 0; j < tot; ++j) {
-                    const bool want = j < ca ? wa : wb;
-                    float4 pt = __ldg(&pts[j < ca ? fa + j : fb + (j - ca)]);
-                    float key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
-                    uint32_t id = __float_as_uint(pt.w);
-                    if (want && key <= bound && key > prev && key_less(key, id, bk[KC - 1], bi[KC - 1]))
-                        list_insert<KC>(bk, bi, key, id);
-                }
-                if (tot) lim = active ? fminf(bound, bk[KC - 1]) : -1.0f;
-                if (!(node & CHILD_LEAF)) {
-                    w0 = w0 && !(k0 > lim);
-                    w1 = w1 && !(k1 > lim);
-                    const uint32_t m0 = __ballot_sync(0xffffffffu, w0);
-                    const uint32_t m1 = __ballot_sync(0xffffffffu, w1);
-                    if (m0 && m1) {
-                        const uint32_t pref0 = __ballot_sync(0xffffffffu, w0 && (!w1 || k0 <= k1));
-                        const bool near0 = __popc(pref0) * 2 >= __popc(m0 | m1);
-                        next = near0 ? d.x : d.y;
-                        if (sp < STACK_MAX) {
-                            if (lane == 0) stk[sp] = near0 ? d.y : d.x;
-                            // -1 marks "this lane does not want it" (keys are >= 0 or NaN)
-                            l_key[sp] = near0 ? (w1 ? k1 : -1.0f) : (w0 ? k0 : -1.0f);
-                            ++sp;
-                        } else if (lane == 0) {
-                            atomicOr(p.err, DEVERR_STACK);
-                        }
-                    } else if (m0) {
-                        next = d.x;
-                    } else if (m1) {
-                        next = d.y;
-                    }
-                }
-                __syncwarp();
-                if (next == CHILD_NONE) {
-                    while (sp > 0) {
-                        --sp;
-                        const float lk = l_key[sp];
-                        if (__any_sync(0xffffffffu, lk != -1.0f && !(lk > lim))) { next = stk[sp]; break; }
-                    }
-                    if (next == CHILD_NONE) break;
-                }
-                __syncwarp();
-                node = next;
-            }
-            if (active && (bi[KC - 1] != EMPTY_ID || last)) active = false;
-            if (last) active = false;
-            prev = bound;
-            bound = __fmul_rn(bound, p.mult2);
-        }
-        if (have) {
-            const uint64_t ob = qi * (uint64_t)kk;
-#pragma unroll
-            for (int j = 0; j < KC; ++j) {
-                if (j >= KC - kk) {
-                    p.ids[ob + j - (KC - kk)] = bi[j];
-                    if (p.d2) p.d2[ob + j - (KC - kk)] = bk[j];
-                }
-            }
-        }
-    }
-}
-
 // One warp per query (knn_query_warp).
 template <int S, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) knn_warp_kernel(const KnnArgs p) {
@@ -486,7 +158,7 @@ __global__ void __launch_bounds__(WARPS * 32) knn_warp_kernel(const KnnArgs p) {
     __syncthreads();
     const TreeRef tree{p.ix.pts, p.ix.nodes, s_top, h->root, h->root_count,
                        2u * h->n_internal + 4u};
-    const RoundSpec rs{h->r0sq, p.mult2, p.max_rounds};
+    const RoundSpec rs{h->r0sq, p.mult2, p.max_rounds, p.partial};
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t kk = p.k;
     uint2 *stk = s_stack[warp];
@@ -507,6 +179,45 @@ __global__ void __launch_bounds__(WARPS * 32) knn_warp_kernel(const KnnArgs p) {
                 if (p.d2) p.d2[ob + j] = lk[s];
             }
         }
+    }
+}
+
+// One warp per query for k above the register lists (k > 256): the sorted
+// list (WideList) lives in dynamic shared memory (kk entries per warp) when
+// smem_list, else in the warp's own slab of `slab` (kk entries per warp of
+// the grid; the grid then covers the queries with a grid-stride loop).  kk
+// = min(k, points): no list ever holds more entries than the index has
+// points.
+constexpr int WIDE_WARPS = 4;
+constexpr uint32_t WIDE_SMEM_MAX_K = 2048;   // 4 warps x 2048 x 8 B = 64 KB per block
+
+__global__ void __launch_bounds__(WIDE_WARPS * 32) knn_wide_kernel(const KnnArgs p, uint2 *slab,
+                                                                   uint32_t kk, int smem_list) {
+    extern __shared__ uint2 s_dyn[];
+    __shared__ BvhNode s_top[TOP_MAX];
+    __shared__ uint2 s_stack[WIDE_WARPS][STACK_MAX];
+    __shared__ uint32_t s_rank[WIDE_WARPS][32];
+    const IndexHeader *h = p.ix.hdr;
+    const uint32_t ntop = h->n_top;
+    for (uint32_t i = threadIdx.x; i < ntop; i += WIDE_WARPS * 32) s_top[i] = p.ix.top[i];
+    __syncthreads();
+    const TreeRef tree{p.ix.pts, p.ix.nodes, s_top, h->root, h->root_count,
+                       2u * h->n_internal + 4u};
+    const RoundSpec rs{h->r0sq, p.mult2, p.max_rounds, p.partial};
+    const int warp = threadIdx.x >> 5;
+    WideList list;
+    list.L = smem_list ? s_dyn + (size_t)warp * kk
+                       : slab + ((size_t)blockIdx.x * WIDE_WARPS + warp) * kk;
+    list.s_r = s_rank[warp];
+    list.kk = kk;
+    for (uint64_t t = (uint64_t)blockIdx.x * WIDE_WARPS + warp; t < p.nq;
+         t += (uint64_t)gridDim.x * WIDE_WARPS) {
+        const uint64_t qi = p.perm ? p.perm[t] : t;
+        const float qx = p.q[3 * qi], qy = p.q[3 * qi + 1], qz = p.q[3 * qi + 2];
+        knn_query_warp_list(tree, rs, qx, qy, qz, s_stack[warp], p.err, list);
+        const uint64_t ob = qi * (uint64_t)p.k;
+        wide_list_store(list, p.k, p.ids + ob, p.d2 ? p.d2 + ob : nullptr);
+        __syncwarp();
     }
 }
 
@@ -596,45 +307,6 @@ rtd_status launch_thread(const KnnArgs &a, uint32_t block, cudaStream_t st) {
     return RTD_OK;
 }
 
-template <int KC, int BLOCK>
-rtd_status launch_refill_b(const KnnArgs &a, unsigned long long *counter, cudaStream_t st) {
-    int dev = 0, sms = 148, per_sm = 1;
-    RTD_CUDA(cudaGetDevice(&dev));
-    RTD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    RTD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, knn_refill_kernel<KC, BLOCK>,
-                                                           BLOCK, 0));
-    if (per_sm < 1) per_sm = 1;
-    uint64_t blocks = (uint64_t)sms * (uint64_t)per_sm;
-    const uint64_t need = (a.nq + BLOCK - 1) / BLOCK;
-    if (blocks > need) blocks = need;
-    RTD_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
-    knn_refill_kernel<KC, BLOCK><<<(unsigned)blocks, BLOCK, 0, st>>>(a, counter);
-    RTD_LAUNCH_CHECK();
-    return RTD_OK;
-}
-
-template <int KC>
-rtd_status launch_refill(const KnnArgs &a, uint32_t block, unsigned long long *counter,
-                         cudaStream_t st) {
-    if (block == 256) return launch_refill_b<KC, 256>(a, counter, st);
-    if (block == 64) return launch_refill_b<KC, 64>(a, counter, st);
-    return launch_refill_b<KC, 128>(a, counter, st);
-}
-
-template <int KC>
-rtd_status launch_packet(const KnnArgs &a, uint32_t block, cudaStream_t st) {
-    const uint64_t warps = (a.nq + 31) / 32;
-    if (block == 256) {
-        knn_packet_kernel<KC, 8><<<grid_for(warps, 8, 1 << 20), 256, 0, st>>>(a);
-    } else if (block == 64) {
-        knn_packet_kernel<KC, 2><<<grid_for(warps, 2, 1 << 20), 64, 0, st>>>(a);
-    } else {
-        knn_packet_kernel<KC, 4><<<grid_for(warps, 4, 1 << 20), 128, 0, st>>>(a);
-    }
-    RTD_LAUNCH_CHECK();
-    return RTD_OK;
-}
-
 template <int S>
 rtd_status launch_warp(const KnnArgs &a, uint32_t block, cudaStream_t st) {
     uint64_t warps = a.nq;
@@ -642,6 +314,38 @@ rtd_status launch_warp(const KnnArgs &a, uint32_t block, cudaStream_t st) {
         knn_warp_kernel<S, 8><<<grid_for(warps, 8, 1 << 20), 256, 0, st>>>(a);
     } else {
         knn_warp_kernel<S, 4><<<grid_for(warps, 4, 1 << 20), 128, 0, st>>>(a);
+    }
+    RTD_LAUNCH_CHECK();
+    return RTD_OK;
+}
+
+// k > 256: the wide-list kernel, lists in shared memory up to
+// WIDE_SMEM_MAX_K entries, else in a global slab on the index (one list per
+// warp of a grid of at most 148 x 8 blocks, and at most 1 GiB of slab).
+rtd_status launch_wide(rtd_index *idx, const KnnArgs &a, cudaStream_t st) {
+    const uint64_t kk64 = a.k < a.ix.n ? a.k : a.ix.n;
+    const uint32_t kk = kk64 ? (uint32_t)kk64 : 1u;
+    const uint64_t warps = a.nq;
+    if (kk <= WIDE_SMEM_MAX_K) {
+        const size_t smem = (size_t)WIDE_WARPS * kk * sizeof(uint2);
+        // the opt-in above 48 KB is per device, set once on each (an eager
+        // search always comes before a captured one)
+        static std::atomic<uint64_t> opted{0};
+        if (smem > 48 * 1024 && (idx->device >= 64 || !(opted.load() >> idx->device & 1u))) {
+            RTD_CUDA(cudaFuncSetAttribute(knn_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)(WIDE_WARPS * WIDE_SMEM_MAX_K * sizeof(uint2))));
+            if (idx->device < 64) opted.fetch_or(1ull << idx->device);
+        }
+        knn_wide_kernel<<<grid_for(warps, WIDE_WARPS, 1 << 20), WIDE_WARPS * 32, smem, st>>>(
+            a, nullptr, kk, 1);
+    } else {
+        uint64_t blocks = (warps + WIDE_WARPS - 1) / WIDE_WARPS;
+        if (blocks > 148u * 8u) blocks = 148u * 8u;
+        const uint64_t per_block = (uint64_t)WIDE_WARPS * kk * sizeof(uint2);
+        const uint64_t cap = (1ull << 30) / per_block;
+        if (blocks > cap) blocks = cap > 0 ? cap : 1;
+        RTD_TRY(idx->wide.reserve(blocks * per_block));
+        knn_wide_kernel<<<(unsigned)blocks, WIDE_WARPS * 32, 0, st>>>(a, idx->wide.as<uint2>(), kk, 0);
     }
     RTD_LAUNCH_CHECK();
     return RTD_OK;
@@ -692,8 +396,8 @@ static bool uses_window(const rtd_index *idx, const rtd_schedule &s, uint32_t k)
     uint32_t lanes = s.lanes_per_query;
     if (lanes == 0) lanes = k <= 16 ? 1 : 32;
     if (lanes == 1 && k > 32) lanes = 32;
-    return lanes == 1 && s.packet_traversal != RTD_PACKET_ON && s.lane_refill != RTD_REFILL_ON &&
-           s.radius_heuristic == RTD_RADIUS_MORTON_WINDOW && idx->n > 1 && idx->skeys != nullptr;
+    return lanes == 1 && !s.partial_results && s.radius_heuristic == RTD_RADIUS_MORTON_WINDOW &&
+           idx->n > 1 && idx->skeys != nullptr;
 }
 
 // Launches the search kernel the schedule selects for the queries of a.
@@ -702,32 +406,9 @@ static rtd_status launch_search(rtd_index *idx, const rtd_schedule &s, uint32_t 
     uint32_t lanes = s.lanes_per_query;
     if (lanes == 0) lanes = k <= 16 ? 1 : 32;
     if (lanes == 1 && k > 32) lanes = 32;
-    // Packet traversal measured ~3x slower than per-thread traversal on the
-    // clustered and uniform workloads, so AUTO means off.
-    const bool packet = lanes == 1 && s.packet_traversal == RTD_PACKET_ON;
     const uint32_t block = s.block_size;
     rtd_status r;
-    if (packet) {
-        if (k <= 1) r = launch_packet<1>(a, block, st);
-        else if (k <= 2) r = launch_packet<2>(a, block, st);
-        else if (k <= 4) r = launch_packet<4>(a, block, st);
-        else if (k == 5) r = launch_packet<5>(a, block, st);
-        else if (k <= 8) r = launch_packet<8>(a, block, st);
-        else if (k <= 16) r = launch_packet<16>(a, block, st);
-        else r = launch_packet<32>(a, block, st);
-    } else if (lanes == 1 && s.lane_refill == RTD_REFILL_ON) {
-        // Lane refill measured 2x slower than one query per thread on the
-        // clustered workload (lanes of a warp drift apart in the tree), so
-        // AUTO means off.
-        unsigned long long *ctr = &idx->hdr.as<IndexHeader>()->qcounter;
-        if (k <= 1) r = launch_refill<1>(a, block, ctr, st);
-        else if (k <= 2) r = launch_refill<2>(a, block, ctr, st);
-        else if (k <= 4) r = launch_refill<4>(a, block, ctr, st);
-        else if (k == 5) r = launch_refill<5>(a, block, ctr, st);
-        else if (k <= 8) r = launch_refill<8>(a, block, ctr, st);
-        else if (k <= 16) r = launch_refill<16>(a, block, ctr, st);
-        else r = launch_refill<32>(a, block, ctr, st);
-    } else if (lanes == 1) {
+    if (lanes == 1) {
         // The Morton-window seed runs in the thread-per-query kernel; the
         // other launch modes treat the heuristic as RTD_RADIUS_SAMPLED_NN.
         if (uses_window(idx, s, k)) a.skeys = idx->skeys;
@@ -739,6 +420,8 @@ static rtd_status launch_search(rtd_index *idx, const rtd_schedule &s, uint32_t 
         else if (k <= 8) r = launch_thread<8>(a, block, st);
         else if (k <= 16) r = launch_thread<16>(a, block, st);
         else r = launch_thread<32>(a, block, st);
+    } else if (k > 256) {
+        r = launch_wide(idx, a, st);
     } else if (lanes == 32) {
         if (k <= 32) r = launch_warp<1>(a, block, st);
         else if (k <= 64) r = launch_warp<2>(a, block, st);
@@ -758,13 +441,13 @@ rtd_status knn_search_ex(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t
     if (nq == 0) return RTD_OK;
     if (!d_q || !d_ids) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL queries or ids");
     if (k == 0) return fail(RTD_ERR_INVALID_ARGUMENT, "k must be >= 1");
-    if (k > 256) return fail(RTD_ERR_UNSUPPORTED, "k > 256 is not supported");
     rtd_schedule def;
     rtd_schedule_default(&def);
     const rtd_schedule &s = sched ? *sched : def;
     if (!(s.radius_increment_mult > 1.0f) || !(s.radius_increment_mult < INFINITY))
         return fail(RTD_ERR_INVALID_ARGUMENT, "radius_increment_mult must be > 1");
     if (s.max_rounds < 1) return fail(RTD_ERR_INVALID_ARGUMENT, "max_rounds must be >= 1");
+    if (s.reserved != 0) return fail(RTD_ERR_INVALID_ARGUMENT, "schedule.reserved must be 0");
     if (s.radius_heuristic == RTD_RADIUS_FIXED && !(s.radius_param > 0.0f))
         return fail(RTD_ERR_INVALID_ARGUMENT, "fixed radius must be > 0");
     for (int e = EV_SEARCH0; e <= EV_SEARCH1; ++e) idx->ev_set[e] = false;
@@ -783,6 +466,7 @@ rtd_status knn_search_ex(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t
     float m = s.radius_increment_mult;
     a.mult2 = m * m;
     a.max_rounds = s.max_rounds;
+    a.partial = s.partial_results ? 1u : 0u;
     a.ids = d_ids;
     a.d2 = d_d2;
     a.err = &idx->hdr.as<IndexHeader>()->err;
@@ -848,13 +532,6 @@ rtd_status k_nn_device(rtd_index *idx, const float *d_points, uint64_t n, const 
     rtd_schedule def;
     rtd_schedule_default(&def);
     const rtd_schedule &s = sched ? *sched : def;
-    // the refilling kernel shares one work counter: it runs unchunked
-    HostChunks one;
-    if (hc && hc->chunks > 1 && s.lane_refill == RTD_REFILL_ON) {
-        one = *hc;
-        one.chunks = 1;
-        hc = &one;
-    }
     const uint32_t chunks = hc ? hc->chunks : 1u;
     RTD_TRY(ensure_side_stream(idx));
     cudaStream_t side = idx->side_stream;

@@ -32,7 +32,10 @@ struct TreeRef {
 struct RoundSpec {
     float r0sq;              // squared radius of round 0
     float mult2;             // growth of the squared radius per round
-    uint32_t max_rounds;     // the last round is unbounded
+    uint32_t max_rounds;     // the last round is unbounded, unless partial
+    uint32_t partial;        // the reference's round cap: every round bounded; a query
+                             // short of k hits after max_rounds keeps its partial list
+                             // and raises DEVERR_NOT_CONVERGED
 };
 
 __device__ __forceinline__ void load_node(const BvhNode *__restrict__ s_top,
@@ -93,7 +96,7 @@ __device__ __forceinline__ void knn_query_thread(const TreeRef &t, const RoundSp
     float bound = rs.r0sq > 0.0f ? rs.r0sq : 1e-30f, prev = -1.0f;
     for (uint32_t round = 0; valid; ++round) {
         const bool last = round + 1 >= rs.max_rounds || !(bound < INFINITY);
-        if (last) bound = INFINITY;
+        if (last && !rs.partial) bound = INFINITY;
         float lim = fminf(bound, bk[KC - 1]);
         uint32_t node = t.root;
         int sp = 0;
@@ -167,7 +170,11 @@ __device__ __forceinline__ void knn_query_thread(const TreeRef &t, const RoundSp
             }
             node = next;
         }
-        if (bi[KC - 1] != EMPTY_ID || last) break;
+        if (bi[KC - 1] != EMPTY_ID) break;
+        if (last) {
+            if (rs.partial) atomicOr(err, DEVERR_NOT_CONVERGED);
+            break;
+        }
         prev = bound;
         bound = __fmul_rn(bound, rs.mult2);
     }
@@ -238,28 +245,133 @@ __device__ __forceinline__ void warp_list_merge(float (&lk)[S], uint32_t (&li)[S
     wi = __shfl_sync(0xffffffffu, ni, wlane);
 }
 
-// Warp per query: the sorted list of S*32 slots is striped over the lanes
-// (slot j in lane j % 32, register j / 32); the candidates of a node's leaf
-// children are tested one per lane and the accepted ones merged into the
-// list in one batch (warp_list_merge).  stk is the warp's shared-memory
-// stack (STACK_MAX entries), ls its list scratch (S*32 entries).  All
-// arguments must be warp-uniform.
+// The warp-striped register list of S*32 slots (k <= S*32) as a list type
+// of knn_query_warp_list: slot j in lane j % 32, register j / 32; ls is the
+// warp's shared merge scratch (S*32 entries).  wk / wi: the k-th entry.
 template <int S>
-__device__ __forceinline__ void knn_query_warp(const TreeRef &t, const RoundSpec &rs, float qx,
-                                               float qy, float qz, uint32_t kk, uint2 *stk,
-                                               uint2 *ls, uint32_t *err, float (&lk)[S],
-                                               uint32_t (&li)[S]) {
-    const int lane = threadIdx.x & 31;
+struct RegList {
+    float lk[S];
+    uint32_t li[S];
+    uint2 *ls;
+    uint32_t kk;
+    float wk;
+    uint32_t wi;
+    __device__ __forceinline__ void reset() {
 #pragma unroll
-    for (int s = 0; s < S; ++s) { lk[s] = INFINITY; li[s] = EMPTY_ID; }
-    float wk = INFINITY;
-    uint32_t wi = EMPTY_ID;
+        for (int s = 0; s < S; ++s) { lk[s] = INFINITY; li[s] = EMPTY_ID; }
+        wk = INFINITY;
+        wi = EMPTY_ID;
+    }
+    __device__ __forceinline__ void merge(bool acc, float key, uint32_t id) {
+        warp_list_merge<S>(lk, li, kk, acc, key, id, ls, wk, wi);
+    }
+};
+
+// A sorted list of kk (key, id) entries in memory, owned by one warp, for k
+// above what registers hold: L[0 .. cnt) ascending, in shared memory or in
+// a global-memory slab of the warp's own.  s_r is 32 words of the warp's
+// shared scratch.  A merge of up to 32 candidates (one per lane) works in
+// place, top down:
+//   - each candidate c finds r_c = #entries before it (binary search) and
+//     its rank j_c among the candidates; it lands at r_c + j_c;
+//   - entry t moves up by s(t) = #candidates with r_c <= t, the candidates'
+//     ranks sorted in s_r and counted by binary search;
+//   - entries move in chunks of 32 from the top, each chunk read before it
+//     is written; a destination is never below its source, so no chunk
+//     overwrites an entry that a later (lower) chunk still has to read;
+//   - destinations at or past kk drop out.
+// (key, id) pairs are distinct, so every position is unique.
+struct WideList {
+    uint2 *L;
+    uint32_t *s_r;
+    uint32_t kk;
+    uint32_t cnt;
+    float wk;
+    uint32_t wi;
+    __device__ __forceinline__ void reset() {
+        cnt = 0;
+        wk = INFINITY;
+        wi = EMPTY_ID;
+    }
+    __device__ __forceinline__ void merge(bool acc, float key, uint32_t id) {
+        const int lane = threadIdx.x & 31;
+        const uint32_t m = __ballot_sync(0xffffffffu, acc);
+        if (!m) return;
+        const uint32_t nc = __popc(m);
+        // rank among the candidates
+        uint32_t jc = 0;
+        for (uint32_t mm = m; mm;) {
+            const int src = __ffs(mm) - 1;
+            mm &= mm - 1;
+            const float ck = __shfl_sync(0xffffffffu, key, src);
+            const uint32_t ci = __shfl_sync(0xffffffffu, id, src);
+            if (acc && key_less(ck, ci, key, id)) ++jc;
+        }
+        // entries before the candidate (lower bound over L[0 .. cnt))
+        uint32_t rc = 0;
+        if (acc) {
+            uint32_t lo = 0, hi = cnt;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                const uint2 e = L[mid];
+                if (key_less(__uint_as_float(e.x), e.y, key, id)) lo = mid + 1;
+                else hi = mid;
+            }
+            rc = lo;
+            s_r[jc] = rc;   // ranks in candidate order are non-decreasing
+        }
+        uint32_t rmin = acc ? rc : 0xFFFFFFFFu;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) rmin = min(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
+        __syncwarp();
+        // move entries [rmin, cnt) up, top chunk first
+        const uint32_t top = cnt < kk ? cnt : kk;
+        for (int64_t hi = (int64_t)top - 1; hi >= (int64_t)rmin; hi -= 32) {
+            const int64_t t = hi - lane;
+            uint2 v = make_uint2(0, 0);
+            uint32_t dst = 0xFFFFFFFFu;
+            if (t >= (int64_t)rmin) {
+                v = L[t];
+                // s(t) = #candidates with r_c <= t (s_r ascending)
+                uint32_t lo = 0, hi2 = nc;
+                while (lo < hi2) {
+                    const uint32_t mid = (lo + hi2) >> 1;
+                    if (s_r[mid] <= (uint32_t)t) lo = mid + 1;
+                    else hi2 = mid;
+                }
+                dst = (uint32_t)t + lo;
+            }
+            __syncwarp();
+            if (dst < kk) L[dst] = v;
+            __syncwarp();
+        }
+        if (acc && rc + jc < kk) L[rc + jc] = make_uint2(__float_as_uint(key), id);
+        cnt = cnt + nc < kk ? cnt + nc : kk;
+        __syncwarp();
+        if (cnt == kk) {
+            const uint2 e = L[kk - 1];
+            wk = __uint_as_float(e.x);
+            wi = e.y;
+        }
+    }
+};
+
+// Warp per query over any list type (RegList, WideList): the candidates of
+// a node's leaf children are tested one per lane and the accepted ones
+// merged into the list in one batch.  stk is the warp's shared-memory stack
+// (STACK_MAX entries).  All arguments must be warp-uniform.
+template <class List>
+__device__ __forceinline__ void knn_query_warp_list(const TreeRef &t, const RoundSpec &rs,
+                                                    float qx, float qy, float qz, uint2 *stk,
+                                                    uint32_t *err, List &list) {
+    const int lane = threadIdx.x & 31;
+    list.reset();
     const bool valid = t.root != CHILD_NONE && !isnan(qx) && !isnan(qy) && !isnan(qz);
     float bound = rs.r0sq > 0.0f ? rs.r0sq : 1e-30f, prev = -1.0f;
     for (uint32_t round = 0; valid; ++round) {
         const bool last = round + 1 >= rs.max_rounds || !(bound < INFINITY);
-        if (last) bound = INFINITY;
-        float lim = fminf(bound, wk);
+        if (last && !rs.partial) bound = INFINITY;
+        float lim = fminf(bound, list.wk);
         uint32_t node = t.root;
         int sp = 0;
         uint32_t visits = 0;
@@ -301,11 +413,11 @@ __device__ __forceinline__ void knn_query_warp(const TreeRef &t, const RoundSpec
                         const float4 pt = __ldg(&t.pts[j < ca ? fa + j : fb + (j - ca)]);
                         key = exact_key(qx, qy, qz, pt.x, pt.y, pt.z);
                         id = __float_as_uint(pt.w);
-                        acc = key <= bound && key > prev && key_less(key, id, wk, wi);
+                        acc = key <= bound && key > prev && key_less(key, id, list.wk, list.wi);
                     }
-                    warp_list_merge<S>(lk, li, kk, acc, key, id, ls, wk, wi);
+                    list.merge(acc, key, id);
                 }
-                lim = fminf(bound, wk);
+                lim = fminf(bound, list.wk);
             }
             if (!(node & CHILD_LEAF)) {
                 v0 = v0 && !(k0 > lim);
@@ -339,9 +451,40 @@ __device__ __forceinline__ void knn_query_warp(const TreeRef &t, const RoundSpec
             __syncwarp();
             node = next;
         }
-        if (wi != EMPTY_ID || last) break;
+        if (list.wi != EMPTY_ID) break;
+        if (last) {
+            if (rs.partial && lane == 0) atomicOr(err, DEVERR_NOT_CONVERGED);
+            break;
+        }
         prev = bound;
         bound = __fmul_rn(bound, rs.mult2);
+    }
+}
+
+// Warp per query with the warp-striped register list (k <= S*32); ls is
+// the warp's list scratch (S*32 entries).
+template <int S>
+__device__ __forceinline__ void knn_query_warp(const TreeRef &t, const RoundSpec &rs, float qx,
+                                               float qy, float qz, uint32_t kk, uint2 *stk,
+                                               uint2 *ls, uint32_t *err, float (&lk)[S],
+                                               uint32_t (&li)[S]) {
+    RegList<S> list;
+    list.ls = ls;
+    list.kk = kk;
+    knn_query_warp_list(t, rs, qx, qy, qz, stk, err, list);
+#pragma unroll
+    for (int s = 0; s < S; ++s) { lk[s] = list.lk[s]; li[s] = list.li[s]; }
+}
+
+// Writes a WideList to the k slots of an ids / d2 row (EMPTY_ID / +inf
+// past cnt; k may exceed the list's kk, which is at most the tree's points).
+__device__ __forceinline__ void wide_list_store(const WideList &l, uint32_t k, uint32_t *ids,
+                                                float *d2) {
+    const int lane = threadIdx.x & 31;
+    for (uint32_t j = lane; j < k; j += 32) {
+        const uint2 e = j < l.cnt ? l.L[j] : make_uint2(__float_as_uint(INFINITY), EMPTY_ID);
+        ids[j] = e.y;
+        if (d2) d2[j] = __uint_as_float(e.x);
     }
 }
 

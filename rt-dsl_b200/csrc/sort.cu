@@ -174,12 +174,9 @@ __global__ void __launch_bounds__(RS_BLOCK) rs_pass_kernel(
             }
             if (done) break;
             t -= used;
-            if (used < 8) {
-                if (++spins > SPIN_LIMIT) {
-                    atomicOr(d_err, DEVERR_TIMEOUT);
-                    break;
-                }
-                __nanosleep(20);
+            if (used < 8 && !spin_more(spins, SPIN_LIMIT)) {
+                atomicOr(d_err, DEVERR_TIMEOUT);
+                break;
             }
         }
         st[(uint64_t)tile * 256 + d] = FLAG_INC | ((prev + tile_cnt) & VALUE_MASK);
@@ -290,8 +287,7 @@ __global__ void __launch_bounds__(SC_BLOCK) scan_kernel(const uint32_t *__restri
                 const int64_t ti = t - lane;
                 uint64_t w = ti >= 0 ? (uint64_t)st[ti] : (2ull << 62);
                 while (__any_sync(0xffffffffu, (w & ~SC_MASK) == 0)) {
-                    if (++spins > SPIN_LIMIT) break;
-                    __nanosleep(20);
+                    if (!spin_more(spins, SPIN_LIMIT)) break;
                     if ((w & ~SC_MASK) == 0) w = st[ti];
                 }
                 if (spins > SPIN_LIMIT) {

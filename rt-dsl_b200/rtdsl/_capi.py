@@ -50,7 +50,7 @@ class Schedule(C.Structure):
         ("block_size", C.c_uint32),
         ("lanes_per_query", C.c_uint32),
         ("morton_bits", C.c_uint32),
-        ("packet_traversal", C.c_uint32), ("lane_refill", C.c_uint32),
+        ("partial_results", C.c_uint32), ("reserved", C.c_uint32),
     ]
 
     def as_dict(self) -> dict:
@@ -106,6 +106,9 @@ _SIGNATURES = {
     "rtd_index_profile_enable": (_I, [_P, _I]),
     "rtd_index_profile_get": (_I, [_P, _P]),
     "rtd_launch_count": (_U64, []),
+    "rtd_wait_selftest": (_I, [_U32, _I, _P]),
+    "rtd_limits_set": (_I, [_P]),
+    "rtd_limits_get": (None, [_P]),
     "rtd_bh_params_default": (None, [_P]),
     "rtd_bh_create": (_I, [C.POINTER(_P)]),
     "rtd_bh_destroy": (_I, [_P]),
@@ -150,7 +153,13 @@ class BhParams(C.Structure):
 
 class BhInfo(C.Structure):
     _fields_ = [("n_bodies", C.c_uint64), ("n_nodes", C.c_uint64), ("n_leaves", C.c_uint64),
-                ("depth", C.c_uint32), ("root_min", C.c_float * 3), ("root_max", C.c_float * 3)]
+                ("depth", C.c_uint32), ("root_min", C.c_float * 3), ("root_max", C.c_float * 3),
+                ("max_stack", C.c_uint32)]
+
+
+class Limits(C.Structure):
+    """rtd_limits: process-wide bounds of bounded device loops."""
+    _fields_ = [("bh_stack_entries", C.c_uint32), ("reserved", C.c_uint32 * 7)]
 
 
 def default_bh_params(**overrides) -> BhParams:
