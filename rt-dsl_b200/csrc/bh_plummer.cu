@@ -34,6 +34,11 @@ namespace {
 
 constexpr int WW = 4;   // warps per block
 
+// Adjoint: source-side derivatives of RED_CELLS cells (3 float4 each) or
+// RED_BODIES bodies (1 float4 each) per chunk, one row per lane.
+constexpr int RED_CELLS = 3;
+constexpr int RED_BODIES = 9;
+
 struct WarpTile {
     float4 cell[32][3];   // (com, M), (Qxx Qyy Qzz Qxy), (Qxz Qyz 0 0)
     uint32_t cmask_t[32];
@@ -42,9 +47,13 @@ struct WarpTile {
     uint32_t bmask_t[32];
     uint32_t clist[32], cmask[32];
     uint32_t blist[64], bmask[64];
-    float4 gpos[32];      // group bodies (adjoint source-side pass)
-    float4 gv[32];        // (dL/da, dL/dphi)
 };
+
+// The adjoint's per-chunk table: red[j][lane] = lane's share of source j.
+struct WarpRed {
+    float4 red[RED_CELLS * 3][32];
+};
+static_assert(RED_BODIES <= RED_CELLS * 3, "body chunk fits the cell chunk's table");
 
 __device__ __forceinline__ float dot3_rn(float x, float y, float z) {
     float s = __fmul_rn(x, x);
@@ -162,8 +171,10 @@ __global__ void __launch_bounds__(WW * 32, ADJ ? 6 : 0) bh_walk_kernel(
     float4 *__restrict__ cell_grad, float4 *__restrict__ body_grad, uint2 *__restrict__ stack,
     uint32_t stack_entries, BhHeader *hm) {
     __shared__ WarpTile tiles[WW];
+    __shared__ WarpRed reds[ADJ ? WW : 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     WarpTile &T = tiles[warp];
+    WarpRed &R = reds[ADJ ? warp : 0];
     const uint64_t gw = (uint64_t)blockIdx.x * WW + warp;
     uint2 *stk = stack + gw * BH_STACK_CAP_MAX;   // this warp's slice
     const uint32_t ngroups = v.hdr->n_groups, n_nodes = v.hdr->n_nodes;
@@ -190,8 +201,6 @@ __global__ void __launch_bounds__(WW * 32, ADJ ? 6 : 0) bh_walk_kernel(
                 vz = g_acc[3 * (uint64_t)o + 2];
                 u = g_phi ? g_phi[o] : 0.f;
             }
-            T.gpos[lane] = me;
-            T.gv[lane] = make_float4(vx, vy, vz, u);
         }
         int cn = 0, bn = 0, sp = 0;
         const uint32_t all = __ballot_sync(0xffffffffu, valid);
@@ -215,37 +224,56 @@ __global__ void __launch_bounds__(WW * 32, ADJ ? 6 : 0) bh_walk_kernel(
             }
             __syncwarp();
             const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-            for (int k = 0; k < cnt; ++k) {   // lane = body
-                if (!((T.cmask_t[k] >> lane) & 1u)) continue;
-                const float4 c = T.cell[k][0];
-                const float4 q0 = QUAD ? T.cell[k][1] : z4, q1 = QUAD ? T.cell[k][2] : z4;
-                if (!ADJ) {
+            if (!ADJ) {
+                for (int k = 0; k < cnt; ++k) {   // lane = body
+                    if (!((T.cmask_t[k] >> lane) & 1u)) continue;
+                    const float4 c = T.cell[k][0];
+                    const float4 q0 = QUAD ? T.cell[k][1] : z4, q1 = QUAD ? T.cell[k][2] : z4;
                     cell_fwd<QUAD>(me.x - c.x, me.y - c.y, me.z - c.z, c, q0, q1, eps2, ax, ay, az, phi);
-                } else {
-                    float grx, gry, grz, gM, gq[6];
-                    cell_adj<QUAD>(me.x - c.x, me.y - c.y, me.z - c.z, c, q0, q1, eps2, u, vx, vy,
-                                   vz, grx, gry, grz, gM, gq);
-                    ax += grx; ay += gry; az += grz;
                 }
-            }
-            if (ADJ && lane < cnt) {          // lane = cell, over the group's bodies
-                const float4 c = T.cell[lane][0];
-                const float4 q0 = QUAD ? T.cell[lane][1] : z4, q1 = QUAD ? T.cell[lane][2] : z4;
-                float sx = 0.f, sy = 0.f, sz = 0.f, sM = 0.f, sq[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                for (uint32_t m = cm; m; m &= m - 1) {
-                    const int bb = __ffs(m) - 1;
-                    const float4 p = T.gpos[bb], w = T.gv[bb];
-                    float grx, gry, grz, gM, gq[6];
-                    cell_adj<QUAD>(p.x - c.x, p.y - c.y, p.z - c.z, c, q0, q1, eps2, w.w, w.x, w.y,
-                                   w.z, grx, gry, grz, gM, gq);
-                    sx -= grx; sy -= gry; sz -= grz; sM += gM;
-                    if (QUAD)
-                        for (int t = 0; t < 6; ++t) sq[t] += gq[t];
-                }
-                atomicAdd(&cell_grad[3 * nid], make_float4(G * sx, G * sy, G * sz, G * sM));
-                if (QUAD) {
-                    atomicAdd(&cell_grad[3 * nid + 1], make_float4(G * sq[0], G * sq[1], G * sq[2], G * sq[3]));
-                    atomicAdd(&cell_grad[3 * nid + 2], make_float4(G * sq[4], G * sq[5], 0.f, 0.f));
+            } else {
+                // One evaluation per (body, cell) pair, lane = body: the
+                // body's derivative stays in its registers, the cell's (COM,
+                // mass, quadrupole; d/dc = -d/dx) goes to the chunk table, one
+                // row per (cell, part), and each row is summed over the lanes
+                // by one lane (reads rotated by lane: no bank conflicts).
+                constexpr int PARTS = QUAD ? 3 : 1;
+                for (int k0 = 0; k0 < cnt; k0 += RED_CELLS) {
+                    const int kn = cnt - k0 < RED_CELLS ? cnt - k0 : RED_CELLS;
+                    for (int kk = 0; kk < kn; ++kk) {
+                        const int k = k0 + kk;
+                        float4 r0 = z4, r1 = z4, r2 = z4;
+                        if ((T.cmask_t[k] >> lane) & 1u) {
+                            const float4 c = T.cell[k][0];
+                            const float4 q0 = QUAD ? T.cell[k][1] : z4, q1 = QUAD ? T.cell[k][2] : z4;
+                            float grx, gry, grz, gM, gq[6];
+                            cell_adj<QUAD>(me.x - c.x, me.y - c.y, me.z - c.z, c, q0, q1, eps2, u,
+                                           vx, vy, vz, grx, gry, grz, gM, gq);
+                            ax += grx; ay += gry; az += grz;
+                            r0 = make_float4(-grx, -gry, -grz, gM);
+                            if (QUAD) {
+                                r1 = make_float4(gq[0], gq[1], gq[2], gq[3]);
+                                r2 = make_float4(gq[4], gq[5], 0.f, 0.f);
+                            }
+                        }
+                        R.red[PARTS * kk][lane] = r0;
+                        if (QUAD) {
+                            R.red[PARTS * kk + 1][lane] = r1;
+                            R.red[PARTS * kk + 2][lane] = r2;
+                        }
+                    }
+                    __syncwarp();
+                    if (lane < kn * PARTS) {
+                        float4 t = z4;
+                        for (int j = 0; j < 32; ++j) {
+                            const float4 e = R.red[lane][(j + lane) & 31];
+                            t.x += e.x; t.y += e.y; t.z += e.z; t.w += e.w;
+                        }
+                        const int kk = lane / PARTS, part = lane - kk * PARTS;
+                        const uint32_t cid = T.clist[k0 + kk];
+                        atomicAdd(&cell_grad[3 * cid + part], make_float4(G * t.x, G * t.y, G * t.z, G * t.w));
+                    }
+                    __syncwarp();
                 }
             }
             __syncwarp();
@@ -260,10 +288,10 @@ __global__ void __launch_bounds__(WW * 32, ADJ ? 6 : 0) bh_walk_kernel(
                 T.bmask_t[lane] = bm;
             }
             __syncwarp();
-            for (int k = 0; k < cnt; ++k) {   // lane = target
-                if (!((T.bmask_t[k] >> lane) & 1u) || T.bid[k] == i) continue;
-                const float4 o = T.body[k];
-                if (!ADJ) {
+            if (!ADJ) {
+                for (int k = 0; k < cnt; ++k) {   // lane = target
+                    if (!((T.bmask_t[k] >> lane) & 1u) || T.bid[k] == i) continue;
+                    const float4 o = T.body[k];
                     const float rx = me.x - o.x, ry = me.y - o.y, rz = me.z - o.z;
                     const float s = rx * rx + ry * ry + rz * rz + eps2;
                     const float i1 = rsqrtf(s), i3 = i1 * i1 * i1;
@@ -271,24 +299,37 @@ __global__ void __launch_bounds__(WW * 32, ADJ ? 6 : 0) bh_walk_kernel(
                     ax -= o.w * rx * i3;
                     ay -= o.w * ry * i3;
                     az -= o.w * rz * i3;
-                } else {
-                    float grx, gry, grz, gm;
-                    body_adj(me.x - o.x, me.y - o.y, me.z - o.z, o.w, eps2, u, vx, vy, vz, grx, gry, grz, gm);
-                    ax += grx; ay += gry; az += grz;
                 }
-            }
-            if (ADJ && lane < cnt) {          // lane = source, over the group's bodies
-                const float4 o = T.body[lane];
-                float sx = 0.f, sy = 0.f, sz = 0.f, sm = 0.f;
-                for (uint32_t m = bm; m; m &= m - 1) {
-                    const int bb = __ffs(m) - 1;
-                    if (gs + bb == bid) continue;
-                    const float4 p = T.gpos[bb], w = T.gv[bb];
-                    float grx, gry, grz, gm;
-                    body_adj(p.x - o.x, p.y - o.y, p.z - o.z, o.w, eps2, w.w, w.x, w.y, w.z, grx, gry, grz, gm);
-                    sx -= grx; sy -= gry; sz -= grz; sm += gm;
+            } else {
+                // as for cells: one evaluation per (target, source) pair,
+                // the source's derivative summed over the lanes
+                const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+                for (int k0 = 0; k0 < cnt; k0 += RED_BODIES) {
+                    const int kn = cnt - k0 < RED_BODIES ? cnt - k0 : RED_BODIES;
+                    for (int kk = 0; kk < kn; ++kk) {
+                        const int k = k0 + kk;
+                        float4 r = z4;
+                        if (((T.bmask_t[k] >> lane) & 1u) && T.bid[k] != i) {
+                            const float4 o = T.body[k];
+                            float grx, gry, grz, gm;
+                            body_adj(me.x - o.x, me.y - o.y, me.z - o.z, o.w, eps2, u, vx, vy, vz,
+                                     grx, gry, grz, gm);
+                            ax += grx; ay += gry; az += grz;
+                            r = make_float4(-grx, -gry, -grz, gm);
+                        }
+                        R.red[kk][lane] = r;
+                    }
+                    __syncwarp();
+                    if (lane < kn) {
+                        float4 t = z4;
+                        for (int j = 0; j < 32; ++j) {
+                            const float4 e = R.red[lane][(j + lane) & 31];
+                            t.x += e.x; t.y += e.y; t.z += e.z; t.w += e.w;
+                        }
+                        atomicAdd(&body_grad[T.bid[k0 + lane]], make_float4(G * t.x, G * t.y, G * t.z, G * t.w));
+                    }
+                    __syncwarp();
                 }
-                atomicAdd(&body_grad[bid], make_float4(G * sx, G * sy, G * sz, G * sm));
             }
             __syncwarp();
         };

@@ -73,6 +73,26 @@ def test_reference_tree_and_forces_bitwise(orc, cuda, case):
         np.testing.assert_array_equal(f.cpu().numpy().view(np.uint32), of.view(np.uint32))
 
 
+@pytest.mark.slow
+@pytest.mark.parametrize("bucket", [128, 32])
+def test_reference_tree_and_forces_1m_bitwise(orc, cuda, bucket):
+    """The 1M-body Plummer sphere (the Barnes-Hut workload's bodies) with the
+    reference law: the GPU tree node for node against the restated
+    BarnesHutTree::build, and the forces of 4,096 sampled bodies bit for bit
+    against the restated reference walk at theta 0.5."""
+    pos, mass = workloads.plummer(1_000_000, seed=7)
+    on, oo, _ = orc.bh_build(pos, mass, bucket=bucket)
+    bh, p = gpu_tree(pos, mass, bucket=bucket)
+    nodes, order = bh.export()
+    assert_tree_equal(on, oo, nodes, order)
+    p.theta = 0.5
+    f, _ = bh.forward(p)
+    f = f.cpu().numpy()
+    sel = np.sort(np.random.default_rng(bucket).choice(len(pos), 4096, replace=False))
+    of = orc.bh_ref_forces_at(pos, mass, on, oo, sel, 0.5)
+    np.testing.assert_array_equal(f[sel].view(np.uint32), of.view(np.uint32))
+
+
 def test_host_barnes_hut_physics_check(orc, cuda):
     """barnes_hut!(bodies, 0.5, G, out) on verify_physics.py's data: the sum
     of force magnitudes within 2% of the FP64 direct sum (verify_physics.py:45)
