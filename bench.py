@@ -48,7 +48,8 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the BH / batched sub-benchmarks")
-    ap.add_argument("--only", choices=["range", "bh", "batch", "dbscan", "leapfrog", "io"],
+    ap.add_argument("--only", choices=["range", "bh", "batch", "dbscan", "leapfrog", "io",
+                                       "large_k"],
                     default=None,
                     help="run one sub-benchmark alone (one GPU) and print its JSON")
     return ap.parse_args()
@@ -328,6 +329,7 @@ def run_ours(args, ws, rank, local):
         extras["range"] = bench_range(args, dev, flush, P, Q, s)
         extras["barnes_hut"] = bench_bh(args, dev, flush)
         extras["batched"] = bench_batch(args, dev, flush)
+        extras["large_k"] = bench_large_k(args, dev, flush, P, Q)
         extras["dbscan"] = bench_dbscan(args, dev, flush)
         extras["leapfrog"] = bench_leapfrog(args, dev, flush)
         extras["io"] = bench_io(args)
@@ -806,6 +808,52 @@ def cpu_baseline_batch(clouds, stride: int = 16) -> dict:
                        f"{nq_s} of their queries in {t:.2f} s, extrapolated to {nq} queries")}
 
 
+# ----------------------------------------------------- large-k sub-bench
+def bench_large_k(args, dev, flush, P, Q, ks=(300, 1000), stride: int = 10) -> dict:
+    """k above the register lists on the headline cloud: every 10th query
+    (40,000), k = 300 and 1,000 (the warp's sorted list in shared memory),
+    search only on a built index; every result against the oracle."""
+    import numpy as np
+    import torch
+    import rtdsl
+    import oracle
+    s = rtdsl.default_schedule()
+    ix = rtdsl.Index().build(P, s)
+    q = Q[::stride].contiguous()
+    nq = q.shape[0]
+    tree = oracle.KdTree(P.cpu().numpy())
+    out = {"metric": "exact kNN queries/s at large k (search on a built index)",
+           "unit": "queries/s",
+           "config": {"workload": f"clustered_1p8m: the headline cloud, every {stride}th query "
+                                  f"({nq}), k in {list(ks)}", "schedule": s.as_dict()},
+           "by_k": {}}
+    for k in ks:
+        ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
+        d2 = torch.empty((nq, k), dtype=torch.float32, device=dev)
+        for _ in range(max(args.warmup, 3)):
+            ix.knn(q, k, s, out_ids=ids, out_d2=d2)
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(max(3, args.steps // 3)):
+            flush.zero_()
+            e0, e1 = _events()
+            e0.record()
+            ix.knn(q, k, s, out_ids=ids, out_d2=d2)
+            e1.record()
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        m = statistics.mean(ms)
+        oi, od = tree.knn(q.cpu().numpy(), k)
+        gi = ids.cpu().numpy().view(np.uint32)
+        gd = d2.cpu().numpy()
+        out["by_k"][str(k)] = {
+            "ms": m, "queries_per_s": nq / (m / 1e3),
+            "id_agreement_vs_oracle": float((gi == oi).all(axis=1).mean()),
+            "key_agreement_vs_oracle": float((gd.view(np.uint32) == od.view(np.uint32)).all(axis=1).mean())}
+    out["value"] = out["by_k"][str(ks[-1])]["queries_per_s"]
+    return out
+
+
 # ---------------------------------------------------------- CPU baseline
 def cpu_baseline(pts, q, sample_q: int = 8000):
     """The reference's own CPU search (gprt-core Scene::build + traverse in
@@ -1041,6 +1089,10 @@ def main():
             out = bench_leapfrog(args, dev, flush)
         elif args.only == "io":
             out = bench_io(args)
+        elif args.only == "large_k":
+            pts, q = load_workload()
+            out = bench_large_k(args, dev, flush, torch.from_numpy(pts).to(dev),
+                                torch.from_numpy(q).to(dev))
         else:
             out = bench_batch(args, dev, flush)
         print(json.dumps(out), flush=True)

@@ -44,6 +44,7 @@ struct IndexHeader {
     uint64_t total;       // last range-count total
     float nn95_key;       // p95 of the squared 1-NN distance within a 4096-point sample
     uint32_t n_sample;    // points in the radius-seed sample (<= 1000)
+    unsigned long long qfp[2];   // query fingerprints of the last range count / fill
 };
 
 constexpr int SEED_NN_SAMPLE = 4096;
@@ -88,6 +89,11 @@ struct rtd_index {
     rtd::DevBuf qkeys, qkeys_alt, qperm, qperm_alt;
     const void *skeys = nullptr;   // the points' sorted Morton keys (in keys or keys_alt)
     rtd::DevBuf rcounts, roffsets, rcursor, rpairs_alt, rkeys, rkeys_alt;
+    // the count pass's own (query, id) pairs, kept when a buffer from an
+    // earlier count is large enough (rspec_cap pairs), and the fill's
+    // per-query cursors
+    rtd::DevBuf rspec, rqcur;
+    uint64_t rspec_cap = 0;
     // DBSCAN scratch (rtd_dbscan): counts, pairs, core flags, union-find
     rtd::DevBuf db_counts, db_pairs, db_core, db_parent, db_flag, db_rank, db_nc;
     rtd::ScanScratch db_scan;
@@ -101,6 +107,7 @@ struct rtd_index {
         float radius = 0.f;
         uint64_t total = 0;
         const uint32_t *perm = nullptr;
+        bool spec = false;   // rspec holds every pair of that count
     } rtoken;
     // Side stream for work that overlaps the build: the radius-seed sample
     // (every build) and rtd_k_nn's query ordering

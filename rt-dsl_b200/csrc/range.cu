@@ -24,8 +24,9 @@ constexpr int WBUF = 256;        // staged pairs per warp (2 KB)
 constexpr uint32_t BIG_SUB = 32;  // contained subtrees of this size or more: copied by the warp
 
 // Kernel modes: count hits, push pairs through warp staging and a global
-// cursor, or write pairs into per-query segments at known offsets.
-enum : int { MODE_COUNT = 0, MODE_PUSH = 1, MODE_SEG = 2 };
+// cursor, write pairs into per-query segments at known offsets, or count
+// hits and push them at once (a count whose pairs the next fill scatters).
+enum : int { MODE_COUNT = 0, MODE_PUSH = 1, MODE_SEG = 2, MODE_CPUSH = 3 };
 
 struct RangeArgs {
     IndexView ix;
@@ -39,6 +40,8 @@ struct RangeArgs {
     unsigned long long *cursor;
     const uint64_t *offsets;   // MODE_SEG: exclusive offsets of the count pass
     uint64_t total;            // MODE_SEG: end of the last segment
+    int skip_if_same;          // MODE_SEG: do nothing when the header's two query
+                               // fingerprints agree (the scatter fills instead)
     uint32_t *err;
 };
 
@@ -87,10 +90,12 @@ constexpr int F_COUNT_ONLY = F_DONE + 1;
 // pushes with one global atomic per flush.
 template <int MODE>
 __global__ void __launch_bounds__(RBLOCK, MODE == MODE_COUNT ? 10 : 8) range_kernel(const RangeArgs p) {
-    constexpr bool PUSH = MODE == MODE_PUSH;
+    constexpr bool PUSH = MODE == MODE_PUSH || MODE == MODE_CPUSH;   // through warp staging
     constexpr bool SEG = MODE == MODE_SEG;
     constexpr bool FILL = PUSH || SEG;
+    constexpr bool COUNTS = MODE == MODE_COUNT || MODE == MODE_CPUSH;
     constexpr int NF = FILL ? F_COUNT_ALL : F_COUNT_ONLY;
+    if (SEG && p.skip_if_same && p.ix.hdr->qfp[0] == p.ix.hdr->qfp[1]) return;
     __shared__ BvhNode s_top[TOP_MAX];
     __shared__ uint2 s_stack[SHORT_DEPTH][RBLOCK];
     __shared__ uint2 s_buf[PUSH ? RWARPS : 1][PUSH ? WBUF : 1];
@@ -123,7 +128,10 @@ __global__ void __launch_bounds__(RBLOCK, MODE == MODE_COUNT ? 10 : 8) range_ker
             const uint64_t dst = base + j;
             if (dst < p.capacity) p.pairs[dst] = buf[j];
         }
-        if (lane == 0 && base + fill > p.capacity) atomicOr(p.err, DEVERR_OVERFLOW);
+        // (the count's own pushes are speculative: a short buffer only
+        // means the fill runs its own traversal)
+        if (MODE == MODE_PUSH && lane == 0 && base + fill > p.capacity)
+            atomicOr(p.err, DEVERR_OVERFLOW);
         __syncwarp();
         fill = 0;
     };
@@ -226,6 +234,7 @@ __global__ void __launch_bounds__(RBLOCK, MODE == MODE_COUNT ? 10 : 8) range_ker
                 // contained subtrees of BIG_SUB points or more: the whole
                 // warp copies each one's contiguous ids, one pair per lane
                 const uint32_t b0 = n0 >= BIG_SUB ? n0 : 0u, b1 = n1 >= BIG_SUB ? n1 : 0u;
+                if (MODE == MODE_CPUSH) cnt += b0 + b1;
                 if (b0) n0 = 0;
                 if (b1) n1 = 0;
                 uint32_t m = __ballot_sync(0xffffffffu, (b0 | b1) != 0);
@@ -342,6 +351,7 @@ __global__ void __launch_bounds__(RBLOCK, MODE == MODE_COUNT ? 10 : 8) range_ker
                         fill += __popc(hm);
                         if (fill > WBUF - 32) flush();
                     }
+                    if (MODE == MODE_CPUSH && valid && lane == re) W[F_DONE][o] += run_hits;
                 } else {
                     if (valid && lane == re) W[F_DONE][o] += run_hits;
                 }
@@ -349,12 +359,57 @@ __global__ void __launch_bounds__(RBLOCK, MODE == MODE_COUNT ? 10 : 8) range_ker
             }
         }
         __syncwarp();
-        if (MODE == MODE_COUNT && have) p.counts[qi] = cnt + W[F_DONE][lane];
+        if (COUNTS && have) p.counts[qi] = cnt + W[F_DONE][lane];
         // a segment left short or overrun: the queries changed since the count
         if (SEG && (seg_bad || (have && W[F_DONE][lane] != W[F_WLEN][lane])))
             atomicOr(p.err, DEVERR_MISMATCH);
     }
     flush();
+}
+
+// Order-free 64-bit fingerprint of a query array (wrapping sum of mixed
+// per-query words, splitmix64 finalizer), added into *out.
+__device__ __forceinline__ uint64_t mix64(uint64_t x) {
+    x ^= x >> 30;
+    x *= 0xbf58476d1ce4e5b9ull;
+    x ^= x >> 27;
+    x *= 0x94d049bb133111ebull;
+    x ^= x >> 31;
+    return x;
+}
+
+__global__ void __launch_bounds__(256) query_fingerprint_kernel(const float *__restrict__ q,
+                                                                uint64_t nq,
+                                                                unsigned long long *out) {
+    uint64_t acc = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * 256 + threadIdx.x; i < nq;
+         i += (uint64_t)gridDim.x * 256) {
+        const uint64_t xy = (uint64_t)__float_as_uint(q[3 * i]) |
+                            ((uint64_t)__float_as_uint(q[3 * i + 1]) << 32);
+        const uint64_t z = __float_as_uint(q[3 * i + 2]);
+        acc += mix64(xy ^ mix64(z + (i + 1) * 0x9e3779b97f4a7c15ull));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, (unsigned long long)acc);
+}
+
+// The count's pairs into their queries' segments (order within a segment
+// unspecified), unless the queries changed since the count (fingerprints
+// differ), in which case the segment fill that follows runs instead.
+__global__ void __launch_bounds__(256) range_scatter_kernel(const uint2 *__restrict__ spec,
+                                                            uint64_t n_pairs,
+                                                            const uint64_t *__restrict__ offsets,
+                                                            uint32_t *__restrict__ qcur,
+                                                            uint2 *__restrict__ out,
+                                                            const IndexHeader *h) {
+    if (h->qfp[0] != h->qfp[1]) return;
+    for (uint64_t t = (uint64_t)blockIdx.x * 256 + threadIdx.x; t < n_pairs;
+         t += (uint64_t)gridDim.x * 256) {
+        const uint2 pr = spec[t];
+        const uint32_t slot = atomicAdd(&qcur[pr.x], 1u);
+        out[offsets[pr.x] + slot] = pr;
+    }
 }
 
 __global__ void pairs_from_keys_kernel(const uint64_t *__restrict__ keys, uint64_t n,
@@ -401,7 +456,19 @@ rtd_status range_args(rtd_index *idx, const float *d_q, uint64_t nq, float r,
     a.cursor = nullptr;
     a.offsets = nullptr;
     a.total = 0;
+    a.skip_if_same = 0;
     a.err = &idx->hdr.as<IndexHeader>()->err;
+    return RTD_OK;
+}
+
+// Largest buffer kept for the count's own pairs (2^28 pairs, 2 GiB).
+constexpr uint64_t RSPEC_MAX = 1ull << 28;
+
+rtd_status query_fingerprint(const float *d_q, uint64_t nq, unsigned long long *out,
+                             cudaStream_t st) {
+    RTD_CUDA(cudaMemsetAsync(out, 0, sizeof(unsigned long long), st));
+    query_fingerprint_kernel<<<grid_for(nq, 256, 148 * 4), 256, 0, st>>>(d_q, nq, out);
+    RTD_LAUNCH_CHECK();
     return RTD_OK;
 }
 
@@ -424,8 +491,22 @@ rtd_status range_count(rtd_index *idx, const float *d_q, uint64_t nq, float r,
     RTD_TRY(range_args(idx, d_q, nq, r, s, a, st));
     a.counts = d_counts;
     IndexHeader *h = idx->hdr.as<IndexHeader>();
+    // With a buffer left by an earlier count, this count also pushes its
+    // pairs there (and fingerprints the queries), so that a fill of the same
+    // queries only scatters them into their segments.
+    const bool spec = nq > 0 && idx->rspec_cap > 0;
     if (nq) {
-        RTD_TRY(launch_range<MODE_COUNT>(a, st));
+        if (spec) {
+            RTD_TRY(idx->rcursor.reserve(sizeof(unsigned long long)));
+            RTD_CUDA(cudaMemsetAsync(idx->rcursor.ptr, 0, sizeof(unsigned long long), st));
+            a.pairs = idx->rspec.as<uint2>();
+            a.capacity = idx->rspec_cap;
+            a.cursor = idx->rcursor.as<unsigned long long>();
+            RTD_TRY(query_fingerprint(d_q, nq, &h->qfp[0], st));
+            RTD_TRY(launch_range<MODE_CPUSH>(a, st));
+        } else {
+            RTD_TRY(launch_range<MODE_COUNT>(a, st));
+        }
         idx->mark(EV_SEARCH1, st);
         RTD_TRY(idx->roffsets.reserve(nq * sizeof(uint64_t)));
         RTD_TRY(exclusive_scan_u32(d_counts, idx->roffsets.as<uint64_t>(), nq, &h->total,
@@ -434,9 +515,22 @@ rtd_status range_count(rtd_index *idx, const float *d_q, uint64_t nq, float r,
         RTD_CUDA(cudaMemsetAsync(&h->total, 0, sizeof(uint64_t), st));
     }
     uint64_t total = 0;
+    unsigned long long pushed = 0;
     RTD_CUDA(cudaMemcpyAsync(&total, &h->total, sizeof(total), cudaMemcpyDeviceToHost, st));
+    if (spec)
+        RTD_CUDA(cudaMemcpyAsync(&pushed, idx->rcursor.ptr, sizeof(pushed), cudaMemcpyDeviceToHost, st));
     RTD_TRY(check_index_errors(idx, st));   // synchronises
     if (h_total) *h_total = total;
+    const bool spec_ok = spec && pushed == total && total <= idx->rspec_cap;
+    if (!spec_ok && total > 0 && total < RSPEC_MAX) {
+        // room for the next count's pairs (grown only)
+        uint64_t want = total + total / 8 + 4096;
+        if (want > RSPEC_MAX) want = RSPEC_MAX;
+        if (want > idx->rspec_cap) {
+            RTD_TRY(idx->rspec.reserve(want * sizeof(uint2)));
+            idx->rspec_cap = want;
+        }
+    }
     // a fill of the same queries can write straight into per-query segments
     idx->rtoken.valid = true;
     idx->rtoken.q = d_q;
@@ -444,6 +538,7 @@ rtd_status range_count(rtd_index *idx, const float *d_q, uint64_t nq, float r,
     idx->rtoken.radius = r;
     idx->rtoken.total = total;
     idx->rtoken.perm = a.perm;
+    idx->rtoken.spec = spec_ok;
     return RTD_OK;
 }
 
@@ -471,8 +566,9 @@ rtd_status range_fill(rtd_index *idx, const float *d_q, uint64_t nq, float r,
         a.r2 = r * r;
         a.counts = nullptr;
         a.cursor = nullptr;
-            a.offsets = idx->roffsets.as<uint64_t>();
+        a.offsets = idx->roffsets.as<uint64_t>();
         a.total = tk.total;
+        a.skip_if_same = 0;
         a.err = &idx->hdr.as<IndexHeader>()->err;
     } else {
         RTD_TRY(range_args(idx, d_q, nq, r, s, a, st));
@@ -482,7 +578,22 @@ rtd_status range_fill(rtd_index *idx, const float *d_q, uint64_t nq, float r,
     }
     a.pairs = reinterpret_cast<uint2 *>(d_pairs);
     a.capacity = capacity;
-    if (seg) {
+    if (seg && tk.spec) {
+        // the count's own pairs, scattered into the segments; the segment
+        // fill runs only if the queries changed since the count
+        IndexHeader *h = idx->hdr.as<IndexHeader>();
+        RTD_TRY(query_fingerprint(d_q, nq, &h->qfp[1], st));
+        RTD_TRY(idx->rqcur.reserve(nq * sizeof(uint32_t)));
+        RTD_CUDA(cudaMemsetAsync(idx->rqcur.ptr, 0, nq * sizeof(uint32_t), st));
+        if (tk.total) {
+            range_scatter_kernel<<<grid_for(tk.total, 256, 148 * 16), 256, 0, st>>>(
+                idx->rspec.as<uint2>(), tk.total, a.offsets, idx->rqcur.as<uint32_t>(), a.pairs, h);
+            RTD_LAUNCH_CHECK();
+        }
+        a.skip_if_same = 1;
+        RTD_TRY(launch_range<MODE_SEG>(a, st));
+        idx->mark(EV_SEARCH1, st);
+    } else if (seg) {
         RTD_TRY(launch_range<MODE_SEG>(a, st));
         idx->mark(EV_SEARCH1, st);
     } else if (nq) {

@@ -202,3 +202,46 @@ def test_range_fill_detects_queries_changed_after_count(rtd, orc, cuda):
     _, total2 = ix.range_count(qt, 0.2, s)
     got = ix.range_fill(qt, 0.2, total2, sort_pairs=True, schedule=s).cpu().numpy().view(np.uint32)
     np.testing.assert_array_equal(got, orc.range_pairs(pts, q[::-1].copy(), 0.2))
+
+
+def test_range_repeated_count_fill_scatters_the_counts_pairs(rtd, orc, cuda):
+    """Once a count has sized the index's pair buffer, later counts also push
+    their pairs there and a fill of the same queries only scatters them into
+    the segments: the pairs stay grouped by query with the count's counts
+    and equal the oracle's.  A count whose pairs overflow that buffer (a
+    larger radius) falls back to the segment fill's own traversal."""
+    pts, q = workloads.clustered(n=30_000, nq=3_000, seed=44, n_clusters=10, box=10.0)
+    s = rtd.default_schedule()
+    ix = rtd.Index().build(torch.from_numpy(pts).cuda(), s)
+    qt = torch.from_numpy(q).cuda()
+    tree = orc.KdTree(pts)
+    for r in (0.15, 0.15, 0.1, 0.3, 0.3):       # 0.3: more pairs than the buffer first
+        counts, total = ix.range_count(qt, r, s)
+        pairs = ix.range_fill(qt, r, total, sort_pairs=False, schedule=s)
+        c = counts.cpu().numpy().view(np.uint32)
+        p = pairs.cpu().numpy().view(np.uint32)
+        oc, ot = tree.range_count(q, r)
+        np.testing.assert_array_equal(c, oc)
+        assert total == ot == len(p)
+        assert np.all(np.diff(p[:, 0].astype(np.int64)) >= 0)
+        np.testing.assert_array_equal(_pair_keys(p), _pair_keys(tree.range_pairs(q, r)))
+        sp = ix.range_fill(qt, r, total, sort_pairs=True, schedule=s)   # the same count, again
+        np.testing.assert_array_equal(sp.cpu().numpy().view(np.uint32), tree.range_pairs(q, r))
+
+
+def test_range_changed_queries_detected_after_a_pushing_count(rtd, orc, cuda):
+    """The same change as above, after a count that kept its pairs: the
+    fill notices the queries differ from the count's (fingerprint), runs the
+    segment fill, and reports the mismatch."""
+    pts, q = workloads.clustered(n=20_000, nq=1_000, seed=45, n_clusters=6, box=5.0)
+    s = rtd.default_schedule()
+    ix = rtd.Index().build(torch.from_numpy(pts).cuda(), s)
+    qt = torch.from_numpy(q).cuda()
+    _, total = ix.range_count(qt, 0.2, s)          # sizes the pair buffer
+    _, total = ix.range_count(qt, 0.2, s)          # pushes its pairs
+    qt.copy_(torch.from_numpy(np.ascontiguousarray(q[::-1])).cuda())
+    pairs = torch.zeros((total + 1024, 2), dtype=torch.int32, device="cuda")
+    with pytest.raises(rtd.RtdError) as e:
+        ix.range_fill(qt, 0.2, total, schedule=s, out_pairs=pairs)
+    assert e.value.status == 1
+    assert torch.all(pairs[total:] == 0)
