@@ -243,11 +243,16 @@ rtd_status rtd_k_nn_host(rtd_context *ctx, const rtd_vec3 *data, uint64_t n,
  * same d_queries / nq / radius (and no build, k-NN search or other count
  * came between) and capacity >= its total, every query's pairs go into its
  * own segment at the count's offsets: grouped by query in the caller's
- * order, and RTD_ERR_INVALID_ARGUMENT if the hit counts no longer match
- * (queries changed in place).  Otherwise they are pushed by warp-aggregated
- * atomics in unspecified order.  sort_pairs != 0 sorts by (query, id).  If
- * capacity < total, nothing past capacity is written, *h_written = total
- * and RTD_ERR_OVERFLOW is returned.
+ * order (order within a query unspecified), and RTD_ERR_INVALID_ARGUMENT if
+ * the hit counts no longer match (queries changed in place).  Once an
+ * earlier count has sized it, the index keeps a buffer for the count's own
+ * pairs (grown only, at most 2^28 pairs, 2 GiB): such a count pushes its
+ * hits there while counting, and the fill of the same queries only
+ * scatters them into the segments (the queries are fingerprinted at both
+ * calls; changed queries make the fill traverse again).  Otherwise the fill
+ * pushes by warp-aggregated atomics in unspecified order.  sort_pairs != 0
+ * sorts by (query, id).  If capacity < total, nothing past capacity is
+ * written, *h_written = total and RTD_ERR_OVERFLOW is returned.
  * ------------------------------------------------------------------- */
 rtd_status rtd_range_count(rtd_index *idx, const float *d_queries, uint64_t nq, float radius,
                            const rtd_schedule *sched, uint32_t *d_counts, uint64_t *h_total,

@@ -55,6 +55,42 @@ struct WarpRed {
 };
 static_assert(RED_BODIES <= RED_CELLS * 3, "body chunk fits the cell chunk's table");
 
+// Sum of each of `rows` table rows over its 32 entries, L lanes per row:
+// lane l takes row l / L and the entries seg, seg + L, seg + 2L, ... of
+// it (seg = l % L), rotated by the row so that the lanes of one load phase
+// read different banks; the row's lanes then add up by shuffles.  On
+// return `owner` marks the row's first lane, which holds the sum.
+template <int L>
+__device__ __forceinline__ float4 table_row_sum(const WarpRed &R, int rows, int lane, int &row,
+                                                bool &owner) {
+    constexpr int T = (32 + L - 1) / L;
+    row = lane / L;
+    const int seg = lane - row * L;
+    float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (row < rows) {
+#pragma unroll
+        for (int i = 0; i < T; ++i) {
+            int ii = i + row;
+            if (ii >= T) ii -= T;
+            const int j = seg + L * ii;
+            if (j < 32) {
+                const float4 e = R.red[row][j];
+                t.x += e.x; t.y += e.y; t.z += e.z; t.w += e.w;
+            }
+        }
+    }
+    const float4 t0 = t;
+#pragma unroll
+    for (int d = 1; d < L; ++d) {
+        t.x += __shfl_down_sync(0xffffffffu, t0.x, d);
+        t.y += __shfl_down_sync(0xffffffffu, t0.y, d);
+        t.z += __shfl_down_sync(0xffffffffu, t0.z, d);
+        t.w += __shfl_down_sync(0xffffffffu, t0.w, d);
+    }
+    owner = row < rows && seg == 0;
+    return t;
+}
+
 __device__ __forceinline__ float dot3_rn(float x, float y, float z) {
     float s = __fmul_rn(x, x);
     s = __fadd_rn(s, __fmul_rn(y, y));
@@ -236,7 +272,7 @@ __global__ void __launch_bounds__(WW * 32, ADJ ? 6 : 0) bh_walk_kernel(
                 // body's derivative stays in its registers, the cell's (COM,
                 // mass, quadrupole; d/dc = -d/dx) goes to the chunk table, one
                 // row per (cell, part), and each row is summed over the lanes
-                // by one lane (reads rotated by lane: no bank conflicts).
+                // by a few lanes each (table_row_sum).
                 constexpr int PARTS = QUAD ? 3 : 1;
                 for (int k0 = 0; k0 < cnt; k0 += RED_CELLS) {
                     const int kn = cnt - k0 < RED_CELLS ? cnt - k0 : RED_CELLS;
@@ -263,13 +299,12 @@ __global__ void __launch_bounds__(WW * 32, ADJ ? 6 : 0) bh_walk_kernel(
                         }
                     }
                     __syncwarp();
-                    if (lane < kn * PARTS) {
-                        float4 t = z4;
-                        for (int j = 0; j < 32; ++j) {
-                            const float4 e = R.red[lane][(j + lane) & 31];
-                            t.x += e.x; t.y += e.y; t.z += e.z; t.w += e.w;
-                        }
-                        const int kk = lane / PARTS, part = lane - kk * PARTS;
+                    int row;
+                    bool owner;
+                    const float4 t = table_row_sum<32 / (RED_CELLS * PARTS)>(R, kn * PARTS, lane,
+                                                                             row, owner);
+                    if (owner) {
+                        const int kk = row / PARTS, part = row - kk * PARTS;
                         const uint32_t cid = T.clist[k0 + kk];
                         atomicAdd(&cell_grad[3 * cid + part], make_float4(G * t.x, G * t.y, G * t.z, G * t.w));
                     }
@@ -320,14 +355,11 @@ __global__ void __launch_bounds__(WW * 32, ADJ ? 6 : 0) bh_walk_kernel(
                         R.red[kk][lane] = r;
                     }
                     __syncwarp();
-                    if (lane < kn) {
-                        float4 t = z4;
-                        for (int j = 0; j < 32; ++j) {
-                            const float4 e = R.red[lane][(j + lane) & 31];
-                            t.x += e.x; t.y += e.y; t.z += e.z; t.w += e.w;
-                        }
-                        atomicAdd(&body_grad[T.bid[k0 + lane]], make_float4(G * t.x, G * t.y, G * t.z, G * t.w));
-                    }
+                    int row;
+                    bool owner;
+                    const float4 t = table_row_sum<32 / RED_BODIES>(R, kn, lane, row, owner);
+                    if (owner)
+                        atomicAdd(&body_grad[T.bid[k0 + row]], make_float4(G * t.x, G * t.y, G * t.z, G * t.w));
                     __syncwarp();
                 }
             }
