@@ -419,7 +419,14 @@ rtd_status rtd_bh_forward_noalloc(rtd_bh *b, const rtd_bh_params *p, float *d_ou
                                   rtd_stream stream);
 /* Adjoint of the Plummer-law walk (same tree, same decisions): given
  * dL/da (n*3) and dL/dphi (n, may be NULL = 0), writes dL/dpos (n*3) and
- * dL/dmass (n).  No reference counterpart (the reference has no gradients). */
+ * dL/dmass (n).  No reference counterpart (the reference has no gradients).
+ * Once a backward has run on a handle, each later rtd_bh_forward also
+ * records its interaction tiles (which cells and bodies each warp group
+ * evaluated, about 1.5 GB at 1M bodies, theta 0.5) in a pool the handle
+ * keeps, sized from the previous forward's need; a backward on the same
+ * tree with the same theta and quadrupole setting then replays them
+ * instead of walking the tree again (same decisions, same results).  A
+ * build or rtd_bh_release drops the log. */
 rtd_status rtd_bh_backward(rtd_bh *b, const rtd_bh_params *p, const float *d_g_acc,
                            const float *d_g_phi, float *d_g_pos, float *d_g_mass,
                            rtd_stream stream);
@@ -439,6 +446,8 @@ typedef struct rtd_bh_info {
     float root_min[3], root_max[3];
     uint32_t max_stack;      /* deepest per-warp traversal stack of the Plummer walks on
                                 this tree since its build */
+    uint32_t log_pages;      /* interaction-log pages (16 tiles of up to 32 interactions)
+                                the last Plummer forward recorded for the adjoint; 0 = none */
 } rtd_bh_info;
 rtd_status rtd_bh_info_get(rtd_bh *b, rtd_bh_info *info, rtd_stream stream);
 /* Interaction counts of the Plummer-law walk at opening angle theta, for

@@ -33,6 +33,24 @@ struct BhHeader {
     uint32_t n_groups;        // warp groups of the Plummer walks
     uint32_t max_stack;       // deepest traversal stack seen by a walk
     uint32_t group_counter;   // work queue of the walks (next group to take)
+    uint32_t ilog_used;       // interaction-log pages taken by the last logging forward
+    uint32_t ilog_need;       // pages its groups needed (pool size for the next one)
+};
+
+// Interaction log of a Plummer forward walk: every tile of interactions a
+// warp group evaluated (up to 32 (cell or body id, lane mask) entries),
+// in evaluation order, in pages of ILOG_PAGE tiles chained per group, so
+// that the adjoint replays the same decisions instead of walking the tree
+// again.  group[g] = (first page, tiles), tiles = ILOG_NONE when the pool ran
+// out before the group ended (that group walks).
+constexpr uint32_t ILOG_PAGE = 16;
+constexpr uint32_t ILOG_NONE = 0xFFFFFFFFu;
+struct IlogView {
+    uint2 *entries;     // pages * ILOG_PAGE * 32
+    uint8_t *counts;    // pages * ILOG_PAGE: entries | 0x80 for a body tile
+    uint32_t *next;     // pages: the group's next page
+    uint2 *group;       // per warp group; nullptr = no log (forward) / walk (adjoint)
+    uint32_t pages;     // pool capacity
 };
 
 // Traversal stack entries per walking warp: the slice each warp owns in a
@@ -69,6 +87,18 @@ struct rtd_bh {
     uint64_t stack_warps = 0;
     // adjoint scratch
     rtd::DevBuf cell_grad, prefix, gpos_flat, gmass_flat;
+    // interaction log (Plummer forward -> adjoint), kept once a backward has
+    // followed a forward on this handle; its pool is sized from the last
+    // logging forward's need (a pinned copy read when it has landed)
+    rtd::DevBuf ilog_entries, ilog_counts, ilog_next, ilog_group;
+    uint32_t ilog_pages = 0;
+    bool ilog_valid = false;      // the log holds the last forward's decisions
+    float ilog_theta = 0.f;
+    int ilog_quad = -1;
+    bool backward_seen = false;
+    uint32_t *ilog_hint = nullptr;   // pinned: pages the last logging forward needed
+    cudaEvent_t ilog_ev = nullptr;
+    ~rtd_bh();
 };
 
 // Device buffers a host-buffer context keeps for barnes_hut! calls.

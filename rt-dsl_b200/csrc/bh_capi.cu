@@ -46,6 +46,11 @@ using namespace rtd;
 rtd_context_bh *context_bh(rtd_context *ctx);
 cudaStream_t context_stream(rtd_context *ctx);
 
+rtd_bh::~rtd_bh() {
+    if (ilog_hint) cudaFreeHost(ilog_hint);
+    if (ilog_ev) cudaEventDestroy(ilog_ev);
+}
+
 extern "C" {
 
 void rtd_bh_params_default(rtd_bh_params *p) {
@@ -86,9 +91,13 @@ rtd_status rtd_bh_release(rtd_bh *b) {
                       &b->groups, &b->stack, &b->cell_grad, &b->prefix, &b->gpos_flat,
                       &b->gmass_flat})
         d->release();
+    for (DevBuf *d : {&b->ilog_entries, &b->ilog_counts, &b->ilog_next, &b->ilog_group})
+        d->release();
     b->stack_warps = 0;
     b->plummer_ready = false;
     b->has_quad = false;
+    b->ilog_pages = 0;
+    b->ilog_valid = false;
     b->sort.hist.release();
     b->sort.status.release();
     b->sort.counters.release();
@@ -127,6 +136,7 @@ rtd_status rtd_bh_info_get(rtd_bh *b, rtd_bh_info *info, rtd_stream stream) {
         info->root_max[a] = h.root_max[a];
     }
     info->max_stack = h.max_stack;
+    info->log_pages = b->ilog_valid ? (h.ilog_used < b->ilog_pages ? h.ilog_used : b->ilog_pages) : 0;
     return check_bh_errors(b, st);
 }
 

@@ -36,6 +36,7 @@ constexpr int WW = 4;   // warps per block
 
 // Adjoint: source-side derivatives of RED_CELLS cells (3 float4 each) or
 // RED_BODIES bodies (1 float4 each) per chunk, one row per lane.
+
 constexpr int RED_CELLS = 3;
 constexpr int RED_BODIES = 9;
 
@@ -205,7 +206,7 @@ __global__ void __launch_bounds__(WW * 32, ADJ ? 6 : 0) bh_walk_kernel(
     const BhView v, float theta2, float eps2, float G, const float *__restrict__ g_acc,
     const float *__restrict__ g_phi, float *__restrict__ acc_out, float *__restrict__ phi_out,
     float4 *__restrict__ cell_grad, float4 *__restrict__ body_grad, uint2 *__restrict__ stack,
-    uint32_t stack_entries, BhHeader *hm) {
+    uint32_t stack_entries, const IlogView lg, BhHeader *hm) {
     __shared__ WarpTile tiles[WW];
     __shared__ WarpRed reds[ADJ ? WW : 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -240,13 +241,47 @@ __global__ void __launch_bounds__(WW * 32, ADJ ? 6 : 0) bh_walk_kernel(
         }
         int cn = 0, bn = 0, sp = 0;
         const uint32_t all = __ballot_sync(0xffffffffu, valid);
-        if (n_nodes > 0) {
+        // The adjoint replays the group's tiles from the forward's log when
+        // the log holds them all; otherwise it walks the tree.
+        const uint2 lgg = (ADJ && lg.group) ? lg.group[g] : make_uint2(ILOG_NONE, ILOG_NONE);
+        const uint32_t logged = lgg.y;
+        if (n_nodes > 0 && logged == ILOG_NONE) {
             if (lane == 0) stk[0] = make_uint2(0u, all);
             sp = 1;
         }
         __syncwarp();
+        // forward: every evaluated tile (cnt entries of clist/cmask or
+        // blist/bmask) appended to the group's chain of log pages, while the
+        // pool has pages (all warp-uniform)
+        uint32_t nt = 0, page = ILOG_NONE, first = ILOG_NONE;
+        bool lok = !ADJ && lg.group != nullptr;
+        auto log_tile = [&](int cnt, bool bodies) {
+            if (ADJ || !lg.group) return;
+            const uint32_t pos = nt % ILOG_PAGE;
+            if (pos == 0 && lok) {
+                uint32_t pg = 0;
+                if (lane == 0) pg = atomicAdd(&hm->ilog_used, 1u);
+                pg = __shfl_sync(0xffffffffu, pg, 0);
+                if (pg >= lg.pages) {
+                    lok = false;
+                } else {
+                    if (page == ILOG_NONE) first = pg;
+                    else if (lane == 0) lg.next[page] = pg;
+                    page = pg;
+                }
+            }
+            if (lok) {
+                const uint64_t slot = (uint64_t)page * ILOG_PAGE + pos;
+                if (lane < cnt)
+                    lg.entries[slot * 32 + lane] = bodies ? make_uint2(T.blist[lane], T.bmask[lane])
+                                                          : make_uint2(T.clist[lane], T.cmask[lane]);
+                if (lane == 0) lg.counts[slot] = (uint8_t)(cnt | (bodies ? 0x80 : 0));
+            }
+            ++nt;
+        };
 
         auto eval_cells = [&](int cnt) {
+            log_tile(cnt, false);
             uint32_t nid = 0, cm = 0;
             if (lane < cnt) {
                 nid = T.clist[lane];
@@ -314,6 +349,7 @@ __global__ void __launch_bounds__(WW * 32, ADJ ? 6 : 0) bh_walk_kernel(
             __syncwarp();
         };
         auto eval_bodies = [&](int cnt) {
+            log_tile(cnt, true);
             uint32_t bid = 0, bm = 0;
             if (lane < cnt) {
                 bid = T.blist[lane];
@@ -366,6 +402,26 @@ __global__ void __launch_bounds__(WW * 32, ADJ ? 6 : 0) bh_walk_kernel(
             __syncwarp();
         };
 
+        if (logged != ILOG_NONE) {
+            // replay: each logged tile back into the lists, evaluated as
+            // the walk evaluated it (same tiles, same order, same results)
+            uint32_t pg = lgg.x;
+            for (uint32_t t = 0; t < logged; ++t) {
+                const uint32_t pos = t % ILOG_PAGE;
+                if (pos == 0 && t > 0) pg = lg.next[pg];
+                const uint64_t slot = (uint64_t)pg * ILOG_PAGE + pos;
+                const uint32_t c = lg.counts[slot];
+                const int cnt = (int)(c & 0x7F);
+                if (lane < cnt) {
+                    const uint2 e = lg.entries[slot * 32 + lane];
+                    if (c & 0x80) { T.blist[lane] = e.x; T.bmask[lane] = e.y; }
+                    else { T.clist[lane] = e.x; T.cmask[lane] = e.y; }
+                }
+                __syncwarp();
+                if (c & 0x80) eval_bodies(cnt);
+                else eval_cells(cnt);
+            }
+        }
         while (sp > 0) {
             const int t = sp < 32 ? sp : 32;
             sp -= t;
@@ -435,6 +491,10 @@ __global__ void __launch_bounds__(WW * 32, ADJ ? 6 : 0) bh_walk_kernel(
         }
         if (cn > 0) eval_cells(cn);
         if (bn > 0) eval_bodies(bn);
+        if (!ADJ && lg.group && lane == 0) {
+            lg.group[g] = make_uint2(first, lok ? nt : ILOG_NONE);
+            atomicAdd(&hm->ilog_need, (nt + ILOG_PAGE - 1) / ILOG_PAGE);
+        }
         if (valid) {
             if (!ADJ) {
                 const uint32_t o = v.order[i];
@@ -536,7 +596,7 @@ __global__ void __launch_bounds__(128) bh_finish_grad_kernel(const BhView v,
 
 template <bool QUAD, bool ADJ>
 rtd_status launch_walk(rtd_bh *b, const rtd_bh_params *p, const float *g_acc, const float *g_phi,
-                       float *acc, float *phi, cudaStream_t st) {
+                       float *acc, float *phi, const IlogView &lg, cudaStream_t st) {
     int dev = 0, sms = 148, per_sm = 4;
     RTD_CUDA(cudaGetDevice(&dev));
     RTD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -558,7 +618,7 @@ rtd_status launch_walk(rtd_bh *b, const rtd_bh_params *p, const float *g_acc, co
     bh_walk_kernel<QUAD, ADJ><<<(unsigned)blocks, WW * 32, 0, st>>>(
         v, p->theta * p->theta, p->eps * p->eps, p->G, g_acc, g_phi, acc, phi,
         b->cell_grad.as<float4>(), b->gpos_flat.as<float4>(), b->stack.as<uint2>(),
-        bh_stack_entries(), h);
+        bh_stack_entries(), lg, h);
     RTD_LAUNCH_CHECK();
     return RTD_OK;
 }
@@ -566,6 +626,39 @@ rtd_status launch_walk(rtd_bh *b, const rtd_bh_params *p, const float *g_acc, co
 }  // namespace
 
 rtd_status bh_ref_forward(rtd_bh *b, const rtd_bh_params *p, float *d_out, cudaStream_t st);
+
+// The interaction log for a forward: pinned hint and event on first use,
+// the pool grown to the last logging forward's need once its copy has
+// landed (grown only), the per-group array for up to n groups, and the
+// page counters cleared.
+static rtd_status ilog_prepare(rtd_bh *b, cudaStream_t st, IlogView &lg) {
+    if (!b->ilog_hint) {
+        RTD_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&b->ilog_hint), sizeof(uint32_t),
+                               cudaHostAllocDefault));
+        *b->ilog_hint = 0;
+    }
+    if (!b->ilog_ev) RTD_CUDA(cudaEventCreateWithFlags(&b->ilog_ev, cudaEventDisableTiming));
+    const cudaError_t q = cudaEventQuery(b->ilog_ev);
+    if (q == cudaSuccess && *b->ilog_hint > b->ilog_pages) {
+        const uint64_t want = (uint64_t)*b->ilog_hint + *b->ilog_hint / 16 + 64;
+        RTD_TRY(b->ilog_entries.reserve(want * ILOG_PAGE * 32 * sizeof(uint2)));
+        RTD_TRY(b->ilog_counts.reserve(want * ILOG_PAGE));
+        RTD_TRY(b->ilog_next.reserve(want * sizeof(uint32_t)));
+        b->ilog_pages = (uint32_t)want;
+    } else if (q != cudaSuccess && q != cudaErrorNotReady) {
+        return cuda_fail(q, "cudaEventQuery");
+    }
+    cudaGetLastError();   // a not-ready query leaves no error behind
+    RTD_TRY(b->ilog_group.reserve(b->n * sizeof(uint2) + 64));
+    BhHeader *h = b->hdr.as<BhHeader>();
+    RTD_CUDA(cudaMemsetAsync(&h->ilog_used, 0, 2 * sizeof(uint32_t), st));
+    lg.entries = b->ilog_entries.as<uint2>();
+    lg.counts = b->ilog_counts.as<uint8_t>();
+    lg.next = b->ilog_next.as<uint32_t>();
+    lg.group = b->ilog_group.as<uint2>();
+    lg.pages = b->ilog_pages;
+    return RTD_OK;
+}
 
 rtd_status bh_forward(rtd_bh *b, const rtd_bh_params *p, float *d_out, float *d_phi,
                       cudaStream_t st) {
@@ -581,8 +674,21 @@ rtd_status bh_forward(rtd_bh *b, const rtd_bh_params *p, float *d_out, float *d_
         return fail(RTD_ERR_INVALID_ARGUMENT, "tree was not built for the Plummer law");
     if (p->quadrupole && !b->has_quad)
         return fail(RTD_ERR_INVALID_ARGUMENT, "tree was built without quadrupoles");
-    if (p->quadrupole) return launch_walk<true, false>(b, p, nullptr, nullptr, d_out, d_phi, st);
-    return launch_walk<false, false>(b, p, nullptr, nullptr, d_out, d_phi, st);
+    IlogView lg{};
+    if (b->backward_seen) RTD_TRY(ilog_prepare(b, st, lg));
+    b->ilog_valid = false;
+    if (p->quadrupole) RTD_TRY((launch_walk<true, false>(b, p, nullptr, nullptr, d_out, d_phi, lg, st)));
+    else RTD_TRY((launch_walk<false, false>(b, p, nullptr, nullptr, d_out, d_phi, lg, st)));
+    if (lg.group) {
+        // the pages this forward needed, for sizing the next one's pool
+        RTD_CUDA(cudaMemcpyAsync(b->ilog_hint, &b->hdr.as<BhHeader>()->ilog_need, sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, st));
+        RTD_CUDA(cudaEventRecord(b->ilog_ev, st));
+        b->ilog_valid = lg.pages > 0;
+        b->ilog_theta = p->theta;
+        b->ilog_quad = p->quadrupole;
+    }
+    return RTD_OK;
 }
 
 rtd_status bh_backward(rtd_bh *b, const rtd_bh_params *p, const float *g_acc, const float *g_phi,
@@ -605,8 +711,19 @@ rtd_status bh_backward(rtd_bh *b, const rtd_bh_params *p, const float *g_acc, co
     RTD_TRY(b->gpos_flat.reserve(n * sizeof(float4)));
     RTD_CUDA(cudaMemsetAsync(b->cell_grad.ptr, 0, n * 3 * sizeof(float4), st));
     RTD_CUDA(cudaMemsetAsync(b->gpos_flat.ptr, 0, n * sizeof(float4), st));
-    if (p->quadrupole) RTD_TRY((launch_walk<true, true>(b, p, g_acc, g_phi, nullptr, nullptr, st)));
-    else RTD_TRY((launch_walk<false, true>(b, p, g_acc, g_phi, nullptr, nullptr, st)));
+    // replay the last forward's interaction log when it was taken on this
+    // tree with these parameters; otherwise walk
+    IlogView lg{};
+    if (b->ilog_valid && b->ilog_theta == p->theta && b->ilog_quad == p->quadrupole) {
+        lg.entries = b->ilog_entries.as<uint2>();
+        lg.counts = b->ilog_counts.as<uint8_t>();
+        lg.next = b->ilog_next.as<uint32_t>();
+        lg.group = b->ilog_group.as<uint2>();
+        lg.pages = b->ilog_pages;
+    }
+    b->backward_seen = true;
+    if (p->quadrupole) RTD_TRY((launch_walk<true, true>(b, p, g_acc, g_phi, nullptr, nullptr, lg, st)));
+    else RTD_TRY((launch_walk<false, true>(b, p, g_acc, g_phi, nullptr, nullptr, lg, st)));
     const BhView v = bh_view(b);
     bh_prefix_kernel<<<1, 1024, 0, st>>>(v, b->level_nodes.as<uint32_t>(), b->cell_grad.as<float4>(),
                                           b->prefix.as<float4>());
@@ -641,7 +758,7 @@ rtd_status launch_walk_on_stack(rtd_bh *b, const rtd_bh_params *p, float *acc, f
     const BhView v = bh_view(b);
     bh_walk_kernel<QUAD, false><<<(unsigned)blocks, WW * 32, 0, st>>>(
         v, p->theta * p->theta, p->eps * p->eps, p->G, nullptr, nullptr, acc, phi, nullptr,
-        nullptr, stack, bh_stack_entries(), h);
+        nullptr, stack, bh_stack_entries(), IlogView{}, h);
     RTD_LAUNCH_CHECK();
     return RTD_OK;
 }

@@ -540,6 +540,7 @@ rtd_status bh_build(rtd_bh *b, const float *d_pos, const float *d_mass, uint64_t
     RTD_LAUNCH_CHECK();
     if (n == 0) {
         b->built = true;
+    b->ilog_valid = false;   // a new tree: the last forward's log no longer applies
         return RTD_OK;
     }
     const uint64_t n1 = n;
@@ -661,6 +662,7 @@ rtd_status bh_build(rtd_bh *b, const float *d_pos, const float *d_mass, uint64_t
         b->has_quad = quad != 0;
     }
     b->built = true;
+    b->ilog_valid = false;   // a new tree: the last forward's log no longer applies
     return RTD_OK;
 }
 

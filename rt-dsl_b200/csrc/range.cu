@@ -396,7 +396,9 @@ __global__ void __launch_bounds__(256) query_fingerprint_kernel(const float *__r
 
 // The count's pairs into their queries' segments (order within a segment
 // unspecified), unless the queries changed since the count (fingerprints
-// differ), in which case the segment fill that follows runs instead.
+// differ), in which case the segment fill that follows runs instead.  A
+// query's pairs were pushed together, so the lanes of a warp mostly share
+// queries: one atomic per query and warp reserves their slots.
 __global__ void __launch_bounds__(256) range_scatter_kernel(const uint2 *__restrict__ spec,
                                                             uint64_t n_pairs,
                                                             const uint64_t *__restrict__ offsets,
@@ -404,11 +406,20 @@ __global__ void __launch_bounds__(256) range_scatter_kernel(const uint2 *__restr
                                                             uint2 *__restrict__ out,
                                                             const IndexHeader *h) {
     if (h->qfp[0] != h->qfp[1]) return;
-    for (uint64_t t = (uint64_t)blockIdx.x * 256 + threadIdx.x; t < n_pairs;
-         t += (uint64_t)gridDim.x * 256) {
-        const uint2 pr = spec[t];
-        const uint32_t slot = atomicAdd(&qcur[pr.x], 1u);
-        out[offsets[pr.x] + slot] = pr;
+    const int lane = threadIdx.x & 31;
+    uint32_t lt;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+    for (uint64_t w = (uint64_t)blockIdx.x * 256 + (threadIdx.x & ~31u); w < n_pairs;
+         w += (uint64_t)gridDim.x * 256) {
+        const uint64_t t = w + lane;
+        const bool ok = t < n_pairs;
+        const uint2 pr = ok ? spec[t] : make_uint2(0xFFFFFFFFu, 0u);
+        const uint32_t peers = __match_any_sync(0xffffffffu, pr.x);
+        const int leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (ok && lane == leader) base = atomicAdd(&qcur[pr.x], (uint32_t)__popc(peers));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (ok) out[offsets[pr.x] + base + __popc(peers & lt)] = pr;
     }
 }
 

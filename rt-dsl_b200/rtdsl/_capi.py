@@ -154,7 +154,7 @@ class BhParams(C.Structure):
 class BhInfo(C.Structure):
     _fields_ = [("n_bodies", C.c_uint64), ("n_nodes", C.c_uint64), ("n_leaves", C.c_uint64),
                 ("depth", C.c_uint32), ("root_min", C.c_float * 3), ("root_max", C.c_float * 3),
-                ("max_stack", C.c_uint32)]
+                ("max_stack", C.c_uint32), ("log_pages", C.c_uint32)]
 
 
 class Limits(C.Structure):

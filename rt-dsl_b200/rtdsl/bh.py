@@ -93,7 +93,7 @@ class BarnesHut:
         check(self._lib.rtd_bh_info_get(self._h, C.byref(inf), _stream(stream)))
         return {"n_bodies": inf.n_bodies, "n_nodes": inf.n_nodes, "n_leaves": inf.n_leaves,
                 "depth": inf.depth, "root_min": list(inf.root_min), "root_max": list(inf.root_max),
-                "max_stack": inf.max_stack}
+                "max_stack": inf.max_stack, "log_pages": inf.log_pages}
 
     def leapfrog(self, pos, vel, mass, dt: float, steps: int,
                  params: _capi.BhParams | None = None, acc=None, stream=None):

@@ -330,3 +330,36 @@ def test_leapfrog_energy_and_chaining(orc, cuda):
     P2, V2 = torch.from_numpy(pos).cuda(), torch.from_numpy(vel).cuda()
     BarnesHut().leapfrog(P2, V2, M, 2e-3, 40, p)
     assert torch.equal(P1, P2) and torch.equal(V1, V2)
+
+
+@pytest.mark.parametrize("quad", [True, False])
+def test_plummer_adjoint_replays_the_forward_log(cuda, quad):
+    """After a first backward, forwards record their interaction tiles and
+    the next backward replays them instead of walking: the gradients are
+    bitwise those of the walking adjoint (first iteration).  With another
+    theta the handle's gradients equal a fresh handle's."""
+    pos, mass = workloads.plummer(60_000, seed=12)
+    bh, p = gpu_tree(pos, mass, law=1, theta=0.5, eps=1e-3, G=1.0, bucket=16,
+                     quadrupole=int(quad))
+    ones = torch.ones((len(pos),), device="cuda")
+    outs = []
+    for it in range(4):
+        acc, _ = bh.forward(p)
+        gp, gm = bh.backward(acc, ones, p)
+        outs.append((gp.cpu().numpy(), gm.cpu().numpy()))
+        info = bh.info()
+        if it == 0:
+            assert info["log_pages"] == 0          # no backward had run before this forward
+        if it >= 2:
+            assert info["log_pages"] > 0           # the pool was sized by the forward before
+    for gp, gm in outs[1:]:
+        np.testing.assert_array_equal(gp.view(np.uint32), outs[0][0].view(np.uint32))
+        np.testing.assert_array_equal(gm.view(np.uint32), outs[0][1].view(np.uint32))
+    # another theta
+    p2 = type(p).from_buffer_copy(p)
+    p2.theta = 0.7
+    gp_w, _ = bh.backward(bh.forward(p2)[0], ones, p2)
+    fresh, _ = gpu_tree(pos, mass, law=1, theta=0.7, eps=1e-3, G=1.0, bucket=16,
+                        quadrupole=int(quad))
+    gp_f, _ = fresh.backward(fresh.forward(p2)[0], ones, p2)
+    np.testing.assert_array_equal(gp_w.cpu().numpy().view(np.uint32), gp_f.cpu().numpy().view(np.uint32))
