@@ -402,24 +402,39 @@ __global__ void __launch_bounds__(WW * 32, ADJ ? 6 : 0) bh_walk_kernel(
             __syncwarp();
         };
 
-        if (logged != ILOG_NONE) {
+        if (logged != ILOG_NONE && logged > 0) {
             // replay: each logged tile back into the lists, evaluated as
-            // the walk evaluated it (same tiles, same order, same results)
+            // the walk evaluated it (same tiles, same order).  A page's
+            // tile counts come in one load (lane l: tile l) with the next
+            // page's id, and each tile's entries are loaded while the tile
+            // before it is evaluated.
             uint32_t pg = lgg.x;
+            uint32_t c_lane = lane < (int)ILOG_PAGE ? lg.counts[(uint64_t)pg * ILOG_PAGE + lane] : 0u;
+            uint32_t pg_next = logged > ILOG_PAGE ? lg.next[pg] : ILOG_NONE;
+            uint2 e = lg.entries[(uint64_t)pg * ILOG_PAGE * 32 + lane];
             for (uint32_t t = 0; t < logged; ++t) {
                 const uint32_t pos = t % ILOG_PAGE;
-                if (pos == 0 && t > 0) pg = lg.next[pg];
-                const uint64_t slot = (uint64_t)pg * ILOG_PAGE + pos;
-                const uint32_t c = lg.counts[slot];
+                if (pos == 0 && t > 0) {
+                    pg = pg_next;
+                    c_lane = lane < (int)ILOG_PAGE ? lg.counts[(uint64_t)pg * ILOG_PAGE + lane] : 0u;
+                    pg_next = t + ILOG_PAGE < logged ? lg.next[pg] : ILOG_NONE;
+                }
+                const uint32_t c = __shfl_sync(0xffffffffu, c_lane, (int)pos);
                 const int cnt = (int)(c & 0x7F);
+                uint2 en = make_uint2(0u, 0u);
+                if (t + 1 < logged) {
+                    const uint32_t pos1 = (t + 1) % ILOG_PAGE;
+                    const uint32_t pg1 = pos1 == 0 ? pg_next : pg;
+                    en = lg.entries[((uint64_t)pg1 * ILOG_PAGE + pos1) * 32 + lane];
+                }
                 if (lane < cnt) {
-                    const uint2 e = lg.entries[slot * 32 + lane];
                     if (c & 0x80) { T.blist[lane] = e.x; T.bmask[lane] = e.y; }
                     else { T.clist[lane] = e.x; T.cmask[lane] = e.y; }
                 }
                 __syncwarp();
                 if (c & 0x80) eval_bodies(cnt);
                 else eval_cells(cnt);
+                e = en;
             }
         }
         while (sp > 0) {

@@ -335,9 +335,11 @@ def test_leapfrog_energy_and_chaining(orc, cuda):
 @pytest.mark.parametrize("quad", [True, False])
 def test_plummer_adjoint_replays_the_forward_log(cuda, quad):
     """After a first backward, forwards record their interaction tiles and
-    the next backward replays them instead of walking: the gradients are
-    bitwise those of the walking adjoint (first iteration).  With another
-    theta the handle's gradients equal a fresh handle's."""
+    the next backward replays them instead of walking: the gradients equal
+    the walking adjoint's (first iteration) up to the order of the FP32
+    atomic sums over warps (relative norm difference below 1e-5, which the
+    walking adjoint shows between two runs too).  With another theta the
+    handle's gradients equal a fresh handle's to the same tolerance."""
     pos, mass = workloads.plummer(60_000, seed=12)
     bh, p = gpu_tree(pos, mass, law=1, theta=0.5, eps=1e-3, G=1.0, bucket=16,
                      quadrupole=int(quad))
@@ -352,9 +354,10 @@ def test_plummer_adjoint_replays_the_forward_log(cuda, quad):
             assert info["log_pages"] == 0          # no backward had run before this forward
         if it >= 2:
             assert info["log_pages"] > 0           # the pool was sized by the forward before
+    rel = lambda a, b: float(np.linalg.norm((a - b).astype(np.float64)) /   # noqa: E731
+                             np.linalg.norm(b.astype(np.float64)))
     for gp, gm in outs[1:]:
-        np.testing.assert_array_equal(gp.view(np.uint32), outs[0][0].view(np.uint32))
-        np.testing.assert_array_equal(gm.view(np.uint32), outs[0][1].view(np.uint32))
+        assert rel(gp, outs[0][0]) < 1e-5 and rel(gm, outs[0][1]) < 1e-5
     # another theta
     p2 = type(p).from_buffer_copy(p)
     p2.theta = 0.7
@@ -362,4 +365,4 @@ def test_plummer_adjoint_replays_the_forward_log(cuda, quad):
     fresh, _ = gpu_tree(pos, mass, law=1, theta=0.7, eps=1e-3, G=1.0, bucket=16,
                         quadrupole=int(quad))
     gp_f, _ = fresh.backward(fresh.forward(p2)[0], ones, p2)
-    np.testing.assert_array_equal(gp_w.cpu().numpy().view(np.uint32), gp_f.cpu().numpy().view(np.uint32))
+    assert rel(gp_w.cpu().numpy(), gp_f.cpu().numpy()) < 1e-5
