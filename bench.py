@@ -244,9 +244,10 @@ def run_ours(args, ws, rank, local):
     step_ms = []
     for _ in range(args.steps):
         flush.zero_()
-        ev0.record()
-        graph.launch()
-        ev1.record()
+        with _nvtx("knn_step"):
+            ev0.record()
+            graph.launch()
+            ev1.record()
         ev1.synchronize()
         step_ms.append(ev0.elapsed_time(ev1))
     launches = lib.rtd_launch_count() - launches0
@@ -416,12 +417,13 @@ def bench_range(args, dev, flush, P, Q, s) -> dict:
     for _ in range(args.steps):
         flush.zero_()
         e0, e1 = _events()
-        e0.record()
-        _, t = ix.range_count(Q, r, s, out_counts=counts)
-        cnt_ms.append(ix.timings()["search_ms"])
-        ix.range_fill(Q, r, t + 1024, False, s, out_pairs=pairs)
-        fill_ms.append(ix.timings()["search_ms"])
-        e1.record()
+        with _nvtx("range_step"):
+            e0.record()
+            _, t = ix.range_count(Q, r, s, out_counts=counts)
+            cnt_ms.append(ix.timings()["search_ms"])
+            ix.range_fill(Q, r, t + 1024, False, s, out_pairs=pairs)
+            fill_ms.append(ix.timings()["search_ms"])
+            e1.record()
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
     m = statistics.mean(ms)
@@ -495,6 +497,16 @@ def cpu_baseline_range(pts, q, r, sample_q: int = 20000) -> dict:
 
 
 # ----------------------------------------------------- Barnes-Hut sub-bench
+def _nvtx(name: str):
+    """An NVTX range around a timed region (for ncu --nvtx --nvtx-include)."""
+    import contextlib
+    import torch
+    try:
+        return torch.cuda.nvtx.range(name)
+    except Exception:   # noqa: BLE001
+        return contextlib.nullcontext()
+
+
 def _events():
     import torch
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -546,7 +558,8 @@ def bench_bh(args, dev, flush) -> dict:
     for _ in range(args.steps):
         flush.zero_()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-        step(ev)
+        with _nvtx("bh_step"):
+            step(ev)
         ev[3].synchronize()
         t_build.append(ev[0].elapsed_time(ev[1]))
         t_fwd.append(ev[1].elapsed_time(ev[2]))
@@ -694,7 +707,7 @@ def bench_batch(args, dev, flush) -> dict:
             ix.build(p_, plain_sched, stream=st)
             ix.knn(q_, k, plain_sched, out_ids=o, with_d2=False, stream=st)
 
-    def timed(fn, steps):
+    def timed(fn, steps, tag):
         with torch.cuda.stream(st):
             for _ in range(max(args.warmup, 3)):
                 fn()
@@ -704,17 +717,18 @@ def bench_batch(args, dev, flush) -> dict:
                 flush.zero_()
                 st.wait_stream(torch.cuda.current_stream())
                 e0, e1 = _events()
-                e0.record(st)
-                fn()
-                e1.record(st)
+                with _nvtx(tag):
+                    e0.record(st)
+                    fn()
+                    e1.record(st)
                 e1.synchronize()
                 ms.append(e0.elapsed_time(e1))
         return statistics.mean(ms)
 
-    t_batched = timed(batched, args.steps)
-    t_plain_default = timed(plain, max(3, args.steps // 3))
+    t_batched = timed(batched, args.steps, "batch_step")
+    t_plain_default = timed(plain, max(3, args.steps // 3), "plain_step")
     plain_sched = plain_tuned
-    t_plain_tuned = timed(plain, max(3, args.steps // 3))
+    t_plain_tuned = timed(plain, max(3, args.steps // 3), "plain_step")
     t_plain = min(t_plain_default, t_plain_tuned)
     torch.cuda.synchronize()
     agree = 0

@@ -245,10 +245,11 @@ rtd_status rtd_k_nn_host(rtd_context *ctx, const rtd_vec3 *data, uint64_t n,
  * own segment at the count's offsets: grouped by query in the caller's
  * order (order within a query unspecified), and RTD_ERR_INVALID_ARGUMENT if
  * the hit counts no longer match (queries changed in place).  Once an
- * earlier count has sized it, the index keeps a buffer for the count's own
- * pairs (grown only, at most 2^28 pairs, 2 GiB): such a count pushes its
- * hits there while counting, and the fill of the same queries only
- * scatters them into the segments (the queries are fingerprinted at both
+ * earlier count has sized them, the index keeps buffers for the count's own
+ * pairs (grown only, at most 2^28 pairs, 2 GiB) and for records of the
+ * subtrees that lie inside a query's ball: such a count pushes its hits and
+ * records while counting, and the fill of the same queries only scatters
+ * and expands them into the segments (the queries are fingerprinted at both
  * calls; changed queries make the fill traverse again).  Otherwise the fill
  * pushes by warp-aggregated atomics in unspecified order.  sort_pairs != 0
  * sorts by (query, id).  If capacity < total, nothing past capacity is

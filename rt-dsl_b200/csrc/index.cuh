@@ -92,8 +92,8 @@ struct rtd_index {
     // the count pass's own (query, id) pairs, kept when a buffer from an
     // earlier count is large enough (rspec_cap pairs), and the fill's
     // per-query cursors
-    rtd::DevBuf rspec, rqcur;
-    uint64_t rspec_cap = 0;
+    rtd::DevBuf rspec, rqcur, rrec;
+    uint64_t rspec_cap = 0, rrec_cap = 0;
     // DBSCAN scratch (rtd_dbscan): counts, pairs, core flags, union-find
     rtd::DevBuf db_counts, db_pairs, db_core, db_parent, db_flag, db_rank, db_nc;
     rtd::ScanScratch db_scan;
@@ -107,7 +107,8 @@ struct rtd_index {
         float radius = 0.f;
         uint64_t total = 0;
         const uint32_t *perm = nullptr;
-        bool spec = false;   // rspec holds every pair of that count
+        bool spec = false;   // rspec / rrec hold every pair of that count
+        uint64_t spec_pairs = 0, spec_recs = 0;
     } rtoken;
     // Side stream for work that overlaps the build: the radius-seed sample
     // (every build) and rtd_k_nn's query ordering

@@ -42,6 +42,11 @@ struct RangeArgs {
     uint64_t total;            // MODE_SEG: end of the last segment
     int skip_if_same;          // MODE_SEG: do nothing when the header's two query
                                // fingerprints agree (the scatter fills instead)
+    // MODE_CPUSH: every contained subtree becomes a record (query, first
+    // sorted point, points) that the fill's expansion writes out;
+    // cursor[1] counts records, cursor[2] the points they cover
+    uint4 *recs;
+    uint64_t rec_cap;
     uint32_t *err;
 };
 
@@ -233,11 +238,37 @@ __global__ void __launch_bounds__(RBLOCK, MODE == MODE_COUNT ? 10 : 8) range_ker
             if (FILL) {
                 // contained subtrees of BIG_SUB points or more: the whole
                 // warp copies each one's contiguous ids, one pair per lane
-                const uint32_t b0 = n0 >= BIG_SUB ? n0 : 0u, b1 = n1 >= BIG_SUB ? n1 : 0u;
+                // (the pushing count records every contained subtree)
+                constexpr uint32_t BIG = MODE == MODE_CPUSH ? 1u : BIG_SUB;
+                const uint32_t b0 = n0 >= BIG ? n0 : 0u, b1 = n1 >= BIG ? n1 : 0u;
                 if (MODE == MODE_CPUSH) cnt += b0 + b1;
                 if (b0) n0 = 0;
                 if (b1) n1 = 0;
-                uint32_t m = __ballot_sync(0xffffffffu, (b0 | b1) != 0);
+                if (MODE == MODE_CPUSH) {
+                    // records, not copies: a query inside a dense cluster
+                    // would keep its warp copying for thousands of steps,
+                    // while the scatter expands records with every warp
+                    const uint32_t rm0 = __ballot_sync(0xffffffffu, b0 != 0);
+                    const uint32_t rm1 = __ballot_sync(0xffffffffu, b1 != 0);
+                    const uint32_t nr = __popc(rm0) + __popc(rm1);
+                    if (nr) {
+                        uint32_t covered = b0 + b1;
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) covered += __shfl_xor_sync(0xffffffffu, covered, o);
+                        unsigned long long base = 0;
+                        if (lane == 0) {
+                            base = atomicAdd(&p.cursor[1], (unsigned long long)nr);
+                            atomicAdd(&p.cursor[2], (unsigned long long)covered);
+                        }
+                        base = __shfl_sync(0xffffffffu, base, 0);
+                        // slots: the lanes' first records in lane order, then their second ones
+                        uint64_t r = base + __popc(rm0 & lt);
+                        if (b0 && r < p.rec_cap) p.recs[r] = make_uint4((uint32_t)qi, g0, b0, 0u);
+                        r = base + __popc(rm0) + __popc(rm1 & lt);
+                        if (b1 && r < p.rec_cap) p.recs[r] = make_uint4((uint32_t)qi, g1, b1, 0u);
+                    }
+                }
+                uint32_t m = MODE == MODE_CPUSH ? 0u : __ballot_sync(0xffffffffu, (b0 | b1) != 0);
                 while (m) {
                     const int src = __ffs(m) - 1;
                     m &= m - 1;
@@ -394,6 +425,35 @@ __global__ void __launch_bounds__(256) query_fingerprint_kernel(const float *__r
     if ((threadIdx.x & 31) == 0) atomicAdd(out, (unsigned long long)acc);
 }
 
+// The count's records into their queries' segments: eight lanes per record,
+// its slots reserved with one atomic, each lane writing every 8th pair (the
+// id read from the sorted point).  Skipped like range_scatter_kernel.
+__global__ void __launch_bounds__(256) range_expand_kernel(const uint4 *__restrict__ recs,
+                                                           uint64_t n_recs,
+                                                           const uint64_t *__restrict__ offsets,
+                                                           uint32_t *__restrict__ qcur,
+                                                           const float4 *__restrict__ pts,
+                                                           uint2 *__restrict__ out,
+                                                           const IndexHeader *h) {
+    if (h->qfp[0] != h->qfp[1]) return;
+    const int lane = threadIdx.x & 31, sub = lane & 7;
+    // warp-uniform loop: four records per warp and trip
+    for (uint64_t wb = (((uint64_t)blockIdx.x * 256 + threadIdx.x) >> 5) * 4; wb < n_recs;
+         wb += (((uint64_t)gridDim.x * 256) >> 5) * 4) {
+        const uint64_t w = wb + (lane >> 3);
+        const bool ok = w < n_recs;
+        const uint4 rc = ok ? recs[w] : make_uint4(0u, 0u, 0u, 0u);
+        uint32_t base = 0;
+        if (ok && sub == 0) base = atomicAdd(&qcur[rc.x], rc.z);
+        base = __shfl_sync(0xffffffffu, base, lane & 24);
+        if (ok) {
+            const uint64_t dst = offsets[rc.x] + base;
+            for (uint32_t j = sub; j < rc.z; j += 8)
+                out[dst + j] = make_uint2(rc.x, __float_as_uint(__ldg(&pts[rc.y + j].w)));
+        }
+    }
+}
+
 // The count's pairs into their queries' segments (order within a segment
 // unspecified), unless the queries changed since the count (fingerprints
 // differ), in which case the segment fill that follows runs instead.  A
@@ -468,6 +528,8 @@ rtd_status range_args(rtd_index *idx, const float *d_q, uint64_t nq, float r,
     a.offsets = nullptr;
     a.total = 0;
     a.skip_if_same = 0;
+    a.recs = nullptr;
+    a.rec_cap = 0;
     a.err = &idx->hdr.as<IndexHeader>()->err;
     return RTD_OK;
 }
@@ -508,11 +570,13 @@ rtd_status range_count(rtd_index *idx, const float *d_q, uint64_t nq, float r,
     const bool spec = nq > 0 && idx->rspec_cap > 0;
     if (nq) {
         if (spec) {
-            RTD_TRY(idx->rcursor.reserve(sizeof(unsigned long long)));
-            RTD_CUDA(cudaMemsetAsync(idx->rcursor.ptr, 0, sizeof(unsigned long long), st));
+            RTD_TRY(idx->rcursor.reserve(3 * sizeof(unsigned long long)));
+            RTD_CUDA(cudaMemsetAsync(idx->rcursor.ptr, 0, 3 * sizeof(unsigned long long), st));
             a.pairs = idx->rspec.as<uint2>();
             a.capacity = idx->rspec_cap;
             a.cursor = idx->rcursor.as<unsigned long long>();
+            a.recs = idx->rrec.as<uint4>();
+            a.rec_cap = idx->rrec_cap;
             RTD_TRY(query_fingerprint(d_q, nq, &h->qfp[0], st));
             RTD_TRY(launch_range<MODE_CPUSH>(a, st));
         } else {
@@ -526,20 +590,27 @@ rtd_status range_count(rtd_index *idx, const float *d_q, uint64_t nq, float r,
         RTD_CUDA(cudaMemsetAsync(&h->total, 0, sizeof(uint64_t), st));
     }
     uint64_t total = 0;
-    unsigned long long pushed = 0;
+    unsigned long long cur[3] = {0, 0, 0};   // pairs pushed, records, points the records cover
     RTD_CUDA(cudaMemcpyAsync(&total, &h->total, sizeof(total), cudaMemcpyDeviceToHost, st));
     if (spec)
-        RTD_CUDA(cudaMemcpyAsync(&pushed, idx->rcursor.ptr, sizeof(pushed), cudaMemcpyDeviceToHost, st));
+        RTD_CUDA(cudaMemcpyAsync(cur, idx->rcursor.ptr, sizeof(cur), cudaMemcpyDeviceToHost, st));
     RTD_TRY(check_index_errors(idx, st));   // synchronises
     if (h_total) *h_total = total;
-    const bool spec_ok = spec && pushed == total && total <= idx->rspec_cap;
+    const bool spec_ok = spec && cur[0] + cur[2] == total && cur[0] <= idx->rspec_cap &&
+                         cur[1] <= idx->rrec_cap;
     if (!spec_ok && total > 0 && total < RSPEC_MAX) {
-        // room for the next count's pairs (grown only)
+        // room for the next count's pairs and records (grown only; a
+        // record covers at least one pair)
         uint64_t want = total + total / 8 + 4096;
         if (want > RSPEC_MAX) want = RSPEC_MAX;
         if (want > idx->rspec_cap) {
             RTD_TRY(idx->rspec.reserve(want * sizeof(uint2)));
             idx->rspec_cap = want;
+        }
+        const uint64_t want_r = (spec ? cur[1] + cur[1] / 8 : want / 4) + 4096;
+        if (want_r > idx->rrec_cap) {
+            RTD_TRY(idx->rrec.reserve(want_r * sizeof(uint4)));
+            idx->rrec_cap = want_r;
         }
     }
     // a fill of the same queries can write straight into per-query segments
@@ -550,6 +621,8 @@ rtd_status range_count(rtd_index *idx, const float *d_q, uint64_t nq, float r,
     idx->rtoken.total = total;
     idx->rtoken.perm = a.perm;
     idx->rtoken.spec = spec_ok;
+    idx->rtoken.spec_pairs = spec_ok ? cur[0] : 0;
+    idx->rtoken.spec_recs = spec_ok ? cur[1] : 0;
     return RTD_OK;
 }
 
@@ -596,9 +669,15 @@ rtd_status range_fill(rtd_index *idx, const float *d_q, uint64_t nq, float r,
         RTD_TRY(query_fingerprint(d_q, nq, &h->qfp[1], st));
         RTD_TRY(idx->rqcur.reserve(nq * sizeof(uint32_t)));
         RTD_CUDA(cudaMemsetAsync(idx->rqcur.ptr, 0, nq * sizeof(uint32_t), st));
-        if (tk.total) {
-            range_scatter_kernel<<<grid_for(tk.total, 256, 148 * 16), 256, 0, st>>>(
-                idx->rspec.as<uint2>(), tk.total, a.offsets, idx->rqcur.as<uint32_t>(), a.pairs, h);
+        if (tk.spec_pairs) {
+            range_scatter_kernel<<<grid_for(tk.spec_pairs, 256, 148 * 16), 256, 0, st>>>(
+                idx->rspec.as<uint2>(), tk.spec_pairs, a.offsets, idx->rqcur.as<uint32_t>(), a.pairs, h);
+            RTD_LAUNCH_CHECK();
+        }
+        if (tk.spec_recs) {
+            range_expand_kernel<<<grid_for((tk.spec_recs + 3) / 4 * 32, 256, 148 * 16), 256, 0, st>>>(
+                idx->rrec.as<uint4>(), tk.spec_recs, a.offsets, idx->rqcur.as<uint32_t>(),
+                a.ix.pts, a.pairs, h);
             RTD_LAUNCH_CHECK();
         }
         a.skip_if_same = 1;
