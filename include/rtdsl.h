@@ -112,7 +112,7 @@ typedef struct rtd_index rtd_index;
 rtd_status rtd_index_create(rtd_index **out);
 rtd_status rtd_index_destroy(rtd_index *idx);
 /* d_xyz: n points, x,y,z float triples (Vec3 layout) in device memory.
- * Morton codes -> onesweep radix sort -> Karras radix tree; subtrees of
+ * Morton codes -> LSD radix sort -> Karras radix tree; subtrees of
  * <= leaf_size points become leaves, and every child box is taken from a
  * pyramid of boxes over runs of 8, 64, 512 ... sorted points (no bottom-up
  * refit pass). */
@@ -144,15 +144,31 @@ rtd_status rtd_index_profile_get(rtd_index *idx, rtd_profile *out);
 /* Kernels this library has launched in this process (all handles). */
 uint64_t rtd_launch_count(void);
 
-/* Diagnostic of the bounded device waits (no reference counterpart: the
- * reference exits on any error).  Every device wait on another block's
- * progress (the look-back of the radix sort and of the scans) gives up after
- * a retry limit and reports RTD_ERR_TIMEOUT instead of hanging the GPU.
- * This call runs that same wait on a device flag: never set (flag_set = 0),
- * the wait gives up after spin_limit retries and the call returns
- * RTD_ERR_TIMEOUT with the context still usable; set (flag_set = 1), it
- * returns RTD_OK.  Synchronises. */
+/* Diagnostic of the bounded device wait (no reference counterpart: the
+ * reference exits on any error).  No kernel of this library waits on
+ * another block's progress (the radix sort and the scans run each pass as a
+ * count kernel and a scatter kernel); the bounded wait helper that any such
+ * wait must use gives up after a retry limit and reports RTD_ERR_TIMEOUT
+ * instead of hanging the GPU.  This call runs it on a device flag: never
+ * set (flag_set = 0), the wait gives up after spin_limit retries and the
+ * call returns RTD_ERR_TIMEOUT with the context still usable; set
+ * (flag_set = 1), it returns RTD_OK.  Synchronises. */
 rtd_status rtd_wait_selftest(uint32_t spin_limit, int flag_set, rtd_stream stream);
+
+/* Diagnostics of the two device primitives the index build runs (no
+ * reference counterpart), exposed so that their results can be checked
+ * against a CPU sort and scan.  rtd_radix_sort_pairs sorts n keys of
+ * key_bytes (4 or 8) bytes in place by their bits [0, end_bit) with the
+ * LSD radix sort (8-bit digits), stably, and writes to d_vals each key's index in the
+ * input (d_vals is also scratch: its input is ignored).  rtd_exclusive_scan
+ * writes d_out[i] = sum(d_in[0..i)) (32-bit; the caller guarantees the sum
+ * fits), *h_total = sum(d_in) and, when d_select != NULL and every d_in[i] is
+ * 0 or 1, d_select[d_out[i]] = i for every i with d_in[i] = 1.  Both
+ * synchronise the stream. */
+rtd_status rtd_radix_sort_pairs(void *d_keys, uint32_t key_bytes, uint32_t *d_vals, uint64_t n,
+                                uint32_t end_bit, rtd_stream stream);
+rtd_status rtd_exclusive_scan(const uint32_t *d_in, uint32_t *d_out, uint32_t *d_select,
+                              uint64_t n, uint32_t *h_total, rtd_stream stream);
 
 /* Process-wide bounds of bounded device loops.  0 keeps a field's default.
  * bh_stack_entries: traversal stack entries each warp of the Plummer-law

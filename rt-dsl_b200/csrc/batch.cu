@@ -1,7 +1,7 @@
 // batch.cu -- batched exact k-NN over many independent point clouds.
 //
 // Build: every point gets the key (cloud id << 3B) | Morton_B(point in its
-// cloud's box), B bits per axis; one onesweep sort of all keys puts each
+// cloud's box), B bits per axis; one radix sort of all keys puts each
 // cloud's points together in Morton order, and one Karras tree over the
 // whole key array is a forest whose node covering a cloud's key range is
 // that cloud's LBVH (keys sharing the cloud prefix form a subtree of a

@@ -99,10 +99,8 @@ rtd_status rtd_bh_release(rtd_bh *b) {
     b->ilog_pages = 0;
     b->ilog_valid = false;
     b->sort.hist.release();
-    b->sort.status.release();
-    b->sort.counters.release();
-    b->scan.status.release();
-    b->scan.counter.release();
+    b->sort.counts.release();
+    b->scan.sums.release();
     b->built = false;
     return RTD_OK;
 }

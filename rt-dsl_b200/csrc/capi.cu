@@ -8,6 +8,7 @@
 
 #include "bh.cuh"
 #include "index.cuh"
+#include "sort.cuh"
 
 namespace rtd {
 
@@ -184,7 +185,7 @@ rtd_context_bh *context_bh(rtd_context *ctx) {
 cudaStream_t context_stream(rtd_context *ctx) { return ctx->stream; }
 
 namespace {
-// The look-backs' bounded wait (spin_more) on one flag: waits for
+// The bounded wait helper (spin_more) on one flag: waits for
 // *flag != 0; when `limit` retries run out it sets DEVERR_TIMEOUT in *err
 // and returns.
 __global__ void wait_flag_kernel(const volatile uint32_t *flag, uint32_t limit, uint32_t *err) {
@@ -217,6 +218,58 @@ rtd_status rtd_wait_selftest(uint32_t spin_limit, int flag_set, rtd_stream strea
     RTD_CUDA(cudaMemcpyAsync(&err, w + 1, sizeof(err), cudaMemcpyDeviceToHost, st));
     RTD_CUDA(cudaStreamSynchronize(st));
     return status_from_deverr(err);
+}
+
+rtd_status rtd_radix_sort_pairs(void *d_keys, uint32_t key_bytes, uint32_t *d_vals, uint64_t n,
+                                uint32_t end_bit, rtd_stream stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    if (key_bytes != 4 && key_bytes != 8) return fail(RTD_ERR_INVALID_ARGUMENT, "key_bytes must be 4 or 8");
+    if (end_bit < 1 || end_bit > 8 * key_bytes) return fail(RTD_ERR_INVALID_ARGUMENT, "bad end_bit");
+    if (n == 0) return RTD_OK;
+    if (!d_keys || !d_vals) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL keys or values");
+    DevBuf kalt, valt, err;
+    SortScratch scr;
+    RTD_TRY(kalt.reserve(n * key_bytes));
+    RTD_TRY(valt.reserve(n * sizeof(uint32_t)));
+    RTD_TRY(err.reserve(sizeof(uint32_t)));
+    RTD_CUDA(cudaMemsetAsync(err.ptr, 0, sizeof(uint32_t), st));
+    bool in_alt = false;
+    if (key_bytes == 4)
+        RTD_TRY(radix_sort_pairs<uint32_t>(static_cast<uint32_t *>(d_keys), kalt.as<uint32_t>(),
+                                           d_vals, valt.as<uint32_t>(), true, n, 0, (int)end_bit,
+                                           scr, err.as<uint32_t>(), st, &in_alt));
+    else
+        RTD_TRY(radix_sort_pairs<uint64_t>(static_cast<uint64_t *>(d_keys), kalt.as<uint64_t>(),
+                                           d_vals, valt.as<uint32_t>(), true, n, 0, (int)end_bit,
+                                           scr, err.as<uint32_t>(), st, &in_alt));
+    if (in_alt) {
+        RTD_CUDA(cudaMemcpyAsync(d_keys, kalt.ptr, n * key_bytes, cudaMemcpyDeviceToDevice, st));
+        RTD_CUDA(cudaMemcpyAsync(d_vals, valt.ptr, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    }
+    uint32_t e = 0;
+    RTD_CUDA(cudaMemcpyAsync(&e, err.ptr, sizeof(e), cudaMemcpyDeviceToHost, st));
+    RTD_CUDA(cudaStreamSynchronize(st));
+    return status_from_deverr(e);
+}
+
+rtd_status rtd_exclusive_scan(const uint32_t *d_in, uint32_t *d_out, uint32_t *d_select, uint64_t n,
+                              uint32_t *h_total, rtd_stream stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    if (n > 0 && (!d_in || !d_out)) return fail(RTD_ERR_INVALID_ARGUMENT, "NULL input or output");
+    DevBuf words;   // total, err
+    ScanScratch scr;
+    RTD_TRY(words.reserve(2 * sizeof(uint32_t)));
+    uint32_t *w = words.as<uint32_t>();
+    RTD_CUDA(cudaMemsetAsync(w, 0, 2 * sizeof(uint32_t), st));
+    if (d_select)
+        RTD_TRY(exclusive_scan_select_u32(d_in, d_out, d_select, n, w, scr, w + 1, st));
+    else
+        RTD_TRY(exclusive_scan_u32_32(d_in, d_out, n, w, scr, w + 1, st));
+    uint32_t hw[2] = {0, 0};
+    RTD_CUDA(cudaMemcpyAsync(hw, w, sizeof(hw), cudaMemcpyDeviceToHost, st));
+    RTD_CUDA(cudaStreamSynchronize(st));
+    if (h_total) *h_total = hw[0];
+    return status_from_deverr(hw[1]);
 }
 
 rtd_status rtd_limits_set(const rtd_limits *l) {

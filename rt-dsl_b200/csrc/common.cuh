@@ -164,11 +164,12 @@ __device__ __forceinline__ uint32_t quantize(float v, float lo, float ext, float
     return (uint32_t)t;
 }
 
-// Bounded spin-waits.  Every device wait on another block's progress (the
-// look-back of the radix sort and of the scans) counts its retries with
-// spin_more, which backs off and returns false once `limit` retries have run
-// out; the waiter then sets DEVERR_TIMEOUT and stops waiting, so a wait
-// that can never complete ends the kernel instead of hanging the GPU.
+// Bounded spin-waits.  A device wait on another block's progress must count
+// its retries with spin_more, which backs off and returns false once
+// `limit` retries have run out; the waiter then sets DEVERR_TIMEOUT and
+// stops waiting, so a wait that can never complete ends the kernel instead
+// of hanging the GPU.  (The radix sort and the scans run each pass as a
+// count kernel and a scatter kernel and wait on no other block.)
 constexpr uint32_t SPIN_LIMIT = 1u << 24;
 __device__ __forceinline__ bool spin_more(uint32_t &spins, uint32_t limit) {
     if (++spins > limit) return false;

@@ -1,4 +1,4 @@
-// lbvh.cu -- LBVH builder: scene box -> Morton codes -> onesweep radix sort
+// lbvh.cu -- LBVH builder: scene box -> Morton codes -> LSD radix sort
 // -> Karras radix tree -> leaf collapse with every child box taken from a
 // pyramid of run boxes over the sorted points -> top-level staging.
 // Replaces the OptiX GAS build/refit of

@@ -1,4 +1,5 @@
-// sort.cu -- onesweep radix sort and decoupled look-back scan (see sort.cuh).
+// sort.cu -- LSD radix sort of (key, u32 value) pairs and exclusive scan,
+// both as a count kernel and a scatter kernel over fixed tiles (sort.cuh).
 #include "sort.cuh"
 
 namespace rtd {
@@ -9,9 +10,19 @@ constexpr int RS_BLOCK = 256;
 constexpr int RS_WARPS = RS_BLOCK / 32;
 constexpr int RS_ITEMS = 12;
 constexpr int RS_TILE = RS_BLOCK * RS_ITEMS;
-constexpr uint32_t FLAG_AGG = 1u << 30;
-constexpr uint32_t FLAG_INC = 2u << 30;
-constexpr uint32_t VALUE_MASK = (1u << 30) - 1;
+
+// Prefix levels of the tile counts: 32 tiles make a group, 32 groups a
+// super group.  A tile's prefix is the sum of at most 31 tile entries, 31
+// group entries and the super-group entries before it, all written by an
+// earlier kernel: no tile waits on another.
+constexpr uint32_t GROUP_TILES = 32;
+constexpr uint32_t SUPER_TILES = GROUP_TILES * 32;
+
+struct Levels {
+    uint64_t tiles, groups, supers;
+    explicit Levels(uint64_t t)
+        : tiles(t), groups(ceil_div(t, GROUP_TILES)), supers(ceil_div(t, SUPER_TILES)) {}
+};
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
@@ -20,9 +31,8 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 }
 
 // Exclusive scan of one value per thread over a 256-thread block.
-// s_warp must hold RS_WARPS entries; ends with __syncthreads().
-__device__ __forceinline__ uint32_t block_excl_scan256(uint32_t v, uint32_t *s_warp,
-                                                       uint32_t *total) {
+// s_warp must hold RS_WARPS + 1 entries; ends with __syncthreads().
+__device__ __forceinline__ uint32_t block_excl_scan256(uint32_t v, uint32_t *s_warp) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t x = v;
 #pragma unroll
@@ -45,9 +55,40 @@ __device__ __forceinline__ uint32_t block_excl_scan256(uint32_t v, uint32_t *s_w
     }
     __syncthreads();
     uint32_t r = s_warp[warp] + x - v;
-    if (total) *total = s_warp[RS_WARPS];
     __syncthreads();
     return r;
+}
+
+// Lanes of the warp whose 8-bit digit equals this lane's: one ballot per bit.
+__device__ __forceinline__ uint32_t digit_peers(uint32_t dig) {
+    uint32_t peers = 0xffffffffu;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        const bool bit = (dig >> b) & 1u;
+        const uint32_t m = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? m : ~m;
+    }
+    return peers;
+}
+
+// Sum of the 256-word rows before entry `tile` of the three levels, for
+// word d: the earlier tiles of its group, the earlier groups of its super
+// group and the earlier super groups.
+template <typename T>
+__device__ __forceinline__ T tile_prefix(const T *tcount, const T *gsum, const T *ssum,
+                                         uint64_t tile, uint32_t d, uint32_t stride) {
+    const uint64_t g = tile / GROUP_TILES, s = tile / SUPER_TILES;
+    const uint32_t rt = (uint32_t)(tile % GROUP_TILES), rg = (uint32_t)(g % 32);
+    const T *tp = tcount + g * GROUP_TILES * stride + d;
+    const T *gp = gsum + s * 32 * stride + d;
+    T a = 0, b = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < GROUP_TILES; ++j) a += j < rt ? tp[j * stride] : T(0);
+#pragma unroll
+    for (uint32_t j = 0; j < 32; ++j) b += j < rg ? gp[j * stride] : T(0);
+    T c = 0;
+    for (uint64_t j = 0; j < s; ++j) c += ssum[j * stride + d];
+    return a + b + c;
 }
 
 template <typename K>
@@ -75,16 +116,67 @@ __global__ void __launch_bounds__(RS_BLOCK) rs_hist_scan_kernel(uint32_t *hist, 
     __shared__ uint32_t s_warp[RS_WARPS + 1];
     for (int p = 0; p < passes; ++p) {
         uint32_t v = hist[p * 256 + threadIdx.x];
-        uint32_t e = block_excl_scan256(v, s_warp, nullptr);
+        uint32_t e = block_excl_scan256(v, s_warp);
         hist[p * 256 + threadIdx.x] = e;
     }
 }
 
+// Counts of one pass: the digit histogram of each tile of RS_TILE keys in
+// tcount[tile][d], added into its group's row of gsum and, when there is
+// more than one super group, into its super group's row of ssum.  Each
+// warp counts its keys in a private shared row: per key group with equal
+// digits, the lowest lane adds the group's size.
 template <typename K>
-__global__ void __launch_bounds__(RS_BLOCK) rs_pass_kernel(
+__global__ void __launch_bounds__(RS_BLOCK) rs_count_kernel(const K *__restrict__ kin, uint64_t n,
+                                                            int shift, uint32_t *__restrict__ tcount,
+                                                            uint32_t *gsum, uint32_t *ssum,
+                                                            int supers) {
+    __shared__ uint32_t s_wh[RS_WARPS][256];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < RS_WARPS * 256; i += RS_BLOCK) (&s_wh[0][0])[i] = 0;
+    const uint64_t tile = blockIdx.x;
+    const uint64_t wbase = tile * RS_TILE + (uint64_t)warp * RS_ITEMS * 32;
+    K key[RS_ITEMS];
+#pragma unroll
+    for (int i = 0; i < RS_ITEMS; ++i) {
+        const uint64_t idx = wbase + (uint64_t)i * 32 + lane;
+        key[i] = idx < n ? kin[idx] : K(0);
+    }
+    __syncthreads();
+    const uint32_t lt = lanemask_lt();
+    uint32_t *wh = s_wh[warp];
+#pragma unroll
+    for (int i = 0; i < RS_ITEMS; ++i) {
+        const bool ok = wbase + (uint64_t)i * 32 + lane < n;
+        const uint32_t dig = (uint32_t)(key[i] >> shift) & 255u;
+        const uint32_t peers = digit_peers(dig) & __ballot_sync(0xffffffffu, ok);
+        if (ok && (peers & lt) == 0) wh[dig] += __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    const uint32_t d = (uint32_t)tid;
+    uint32_t c = 0;
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; ++w) c += s_wh[w][d];
+    tcount[tile * 256 + d] = c;
+    if (c) {
+        atomicAdd(&gsum[(tile / GROUP_TILES) * 256 + d], c);
+        if (supers > 1) atomicAdd(&ssum[(tile / SUPER_TILES) * 256 + d], c);
+    }
+}
+
+// Scatter of one pass over 8 bits at `shift`: the tile's keys are ranked
+// in registers (stable: warp, item, lane order), staged in shared memory
+// grouped by digit, and each digit run is written contiguously from the
+// digit's global start plus the count of the digit in earlier tiles (the
+// count kernel's levels).  With gout set (the last pass) the value v is
+// replaced by the point gxyz[v] and v in w.
+template <typename K>
+__global__ void __launch_bounds__(RS_BLOCK) rs_scatter_kernel(
     const K *__restrict__ kin, K *__restrict__ kout, const uint32_t *__restrict__ vin,
     uint32_t *__restrict__ vout, uint64_t n, int shift, const uint32_t *__restrict__ digit_off,
-    uint32_t *status, uint32_t *tile_counter, uint32_t *d_err, const float *__restrict__ gxyz,
+    const uint32_t *__restrict__ tcount, const uint32_t *__restrict__ gsum,
+    const uint32_t *__restrict__ ssum, const float *__restrict__ gxyz,
     float4 *__restrict__ gout) {
     extern __shared__ __align__(16) unsigned char rs_smem[];
     K *s_keys = reinterpret_cast<K *>(rs_smem);
@@ -92,101 +184,57 @@ __global__ void __launch_bounds__(RS_BLOCK) rs_pass_kernel(
     uint32_t *s_wh = s_vals + RS_TILE;            // [RS_WARPS][256]
     uint32_t *s_excl = s_wh + RS_WARPS * 256;     // [256] tile-local digit start
     uint32_t *s_base = s_excl + 256;              // [256] global dest of local pos 0 (mod 2^32)
-    uint32_t *s_misc = s_base + 256;              // [RS_WARPS + 2]
+    uint32_t *s_misc = s_base + 256;              // [RS_WARPS + 1]
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) s_misc[RS_WARPS + 1] = atomicAdd(tile_counter, 1u);
     for (int i = tid; i < RS_WARPS * 256; i += RS_BLOCK) s_wh[i] = 0;
-    __syncthreads();
-    const uint32_t tile = s_misc[RS_WARPS + 1];
-    const uint64_t base = (uint64_t)tile * RS_TILE;
+    const uint64_t tile = blockIdx.x;
+    const uint64_t base = tile * RS_TILE;
 
     K key[RS_ITEMS];
-    uint32_t val[RS_ITEMS], dig[RS_ITEMS], rank[RS_ITEMS];
+    uint32_t val[RS_ITEMS], rank[RS_ITEMS];
     const uint64_t wbase = base + (uint64_t)warp * RS_ITEMS * 32;
 #pragma unroll
     for (int i = 0; i < RS_ITEMS; ++i) {
-        uint64_t idx = wbase + (uint64_t)i * 32 + lane;
-        bool ok = idx < n;
+        const uint64_t idx = wbase + (uint64_t)i * 32 + lane;
+        const bool ok = idx < n;
         key[i] = ok ? kin[idx] : ~K(0);
         val[i] = ok ? (vin ? vin[idx] : (uint32_t)idx) : 0u;
-        dig[i] = (uint32_t)(key[i] >> shift) & 255u;
     }
+    const uint32_t d = (uint32_t)tid;
+    const uint32_t before = tile_prefix(tcount, gsum, ssum, tile, d, 256u);
+    __syncthreads();
     const uint32_t lt = lanemask_lt();
     uint32_t *wh = s_wh + warp * 256;
 #pragma unroll
     for (int i = 0; i < RS_ITEMS; ++i) {
-        // lanes holding the same digit: one ballot per digit bit
-        uint32_t peers = 0xffffffffu;
-#pragma unroll
-        for (int b = 0; b < 8; ++b) {
-            const bool bit = (dig[i] >> b) & 1u;
-            const uint32_t m = __ballot_sync(0xffffffffu, bit);
-            peers &= bit ? m : ~m;
-        }
-        uint32_t before = __popc(peers & lt);
-        uint32_t cnt = wh[dig[i]];
-        rank[i] = cnt + before;
+        const uint32_t dig = (uint32_t)(key[i] >> shift) & 255u;
+        const uint32_t peers = digit_peers(dig);
+        const uint32_t below = __popc(peers & lt);
+        const uint32_t cnt = wh[dig];
+        rank[i] = cnt + below;
         __syncwarp();
-        if (before == 0) wh[dig[i]] = cnt + __popc(peers);
+        if (below == 0) wh[dig] = cnt + __popc(peers);
         __syncwarp();
     }
     __syncthreads();
 
     // Per digit (thread = digit): exclusive scan over warps, tile total.
-    const uint32_t d = (uint32_t)tid;
     uint32_t run = 0;
 #pragma unroll
     for (int w = 0; w < RS_WARPS; ++w) {
-        uint32_t t = s_wh[w * 256 + d];
+        const uint32_t t = s_wh[w * 256 + d];
         s_wh[w * 256 + d] = run;
         run += t;
     }
-    const uint32_t tile_cnt = run;
-    volatile uint32_t *st = status;
-    if (tile == 0) st[d] = FLAG_INC | tile_cnt;
-    else st[(uint64_t)tile * 256 + d] = FLAG_AGG | tile_cnt;
-
-    uint32_t excl_local = block_excl_scan256(tile_cnt, s_misc, nullptr);
+    const uint32_t excl_local = block_excl_scan256(run, s_misc);
     s_excl[d] = excl_local;
-
-    // Look back over earlier tiles, 8 status words in flight at a time:
-    // sum their counts up to the nearest inclusive prefix.
-    uint32_t prev = 0;
-    if (tile > 0) {
-        int64_t t = (int64_t)tile - 1;
-        uint32_t spins = 0;
-        while (true) {
-            uint32_t w[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j)
-                w[j] = (t - j >= 0) ? (uint32_t)st[(uint64_t)(t - j) * 256 + d] : (2u << 30);
-            int used = 0;
-            bool done = false;
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                if (done || used < j) continue;
-                uint32_t f = w[j] & ~VALUE_MASK;
-                if (f == 0) continue;          // not published yet: retry from here
-                prev += w[j] & VALUE_MASK;
-                used = j + 1;
-                if (f == FLAG_INC) done = true;
-            }
-            if (done) break;
-            t -= used;
-            if (used < 8 && !spin_more(spins, SPIN_LIMIT)) {
-                atomicOr(d_err, DEVERR_TIMEOUT);
-                break;
-            }
-        }
-        st[(uint64_t)tile * 256 + d] = FLAG_INC | ((prev + tile_cnt) & VALUE_MASK);
-    }
-    s_base[d] = digit_off[d] + prev - excl_local;
+    s_base[d] = digit_off[d] + before - excl_local;
     __syncthreads();
-
 #pragma unroll
     for (int i = 0; i < RS_ITEMS; ++i) {
-        uint32_t lp = s_excl[dig[i]] + s_wh[warp * 256 + dig[i]] + rank[i];
+        const uint32_t dig = (uint32_t)(key[i] >> shift) & 255u;
+        const uint32_t lp = s_excl[dig] + s_wh[warp * 256 + dig] + rank[i];
         s_keys[lp] = key[i];
         s_vals[lp] = val[i];
     }
@@ -194,9 +242,9 @@ __global__ void __launch_bounds__(RS_BLOCK) rs_pass_kernel(
     const uint64_t rem = n - base;
     const uint32_t valid = rem < (uint64_t)RS_TILE ? (uint32_t)rem : (uint32_t)RS_TILE;
     for (uint32_t j = tid; j < valid; j += RS_BLOCK) {
-        K k = s_keys[j];
-        uint32_t dj = (uint32_t)(k >> shift) & 255u;
-        uint32_t dst = s_base[dj] + j;
+        const K k = s_keys[j];
+        const uint32_t dj = (uint32_t)(k >> shift) & 255u;
+        const uint32_t dst = s_base[dj] + j;
         kout[dst] = k;
         const uint32_t v = s_vals[j];
         if (gout) {   // last pass with a gather: the point itself, its index in w
@@ -208,35 +256,73 @@ __global__ void __launch_bounds__(RS_BLOCK) rs_pass_kernel(
     }
 }
 
-size_t rs_pass_smem(size_t key_bytes) {
-    return RS_TILE * (key_bytes + 4) + (RS_WARPS * 256 + 512 + RS_WARPS + 2) * 4;
+size_t rs_scatter_smem(size_t key_bytes) {
+    return RS_TILE * (key_bytes + 4) + (RS_WARPS * 256 + 512 + RS_WARPS + 1) * 4;
 }
 
 // ----------------------------------------------------------------- scan
 constexpr int SC_BLOCK = 256;
 constexpr int SC_ITEMS = 8;
 constexpr int SC_TILE = SC_BLOCK * SC_ITEMS;
-constexpr uint64_t SC_AGG = 1ull << 62;
-constexpr uint64_t SC_INC = 2ull << 62;
-constexpr uint64_t SC_MASK = (1ull << 62) - 1;
 
-// With select != nullptr, also select[out[i]] = i for every i with in[i] != 0
+// Scan counts: each tile's sum in tsum[tile], added into its group's sum
+// and, with more than one super group, its super group's.
+__global__ void __launch_bounds__(SC_BLOCK) scan_count_kernel(const uint32_t *__restrict__ in,
+                                                              uint64_t n, uint64_t *__restrict__ tsum,
+                                                              unsigned long long *gsum,
+                                                              unsigned long long *ssum, int supers) {
+    __shared__ uint64_t s_warp[SC_BLOCK / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint64_t tile = blockIdx.x, base = tile * SC_TILE;
+    uint64_t sum = 0;
+#pragma unroll
+    for (int i = 0; i < SC_ITEMS; ++i) {
+        const uint64_t idx = base + (uint64_t)i * SC_BLOCK + tid;
+        if (idx < n) sum += in[idx];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0) s_warp[warp] = sum;
+    __syncthreads();
+    if (tid == 0) {
+        uint64_t t = 0;
+#pragma unroll
+        for (int w = 0; w < SC_BLOCK / 32; ++w) t += s_warp[w];
+        tsum[tile] = t;
+        if (t) {
+            atomicAdd(&gsum[tile / GROUP_TILES], (unsigned long long)t);
+            if (supers > 1) atomicAdd(&ssum[tile / SUPER_TILES], (unsigned long long)t);
+        }
+    }
+}
+
+// Scan output: out[i] = prefix of the tile (tile_prefix over the count
+// kernel's levels) + the block's exclusive scan within the tile.  With
+// select != nullptr, also select[out[i]] = i for every i with in[i] != 0
 // (stream compaction of the indices of flagged entries).
 template <typename OutT>
-__global__ void __launch_bounds__(SC_BLOCK) scan_kernel(const uint32_t *__restrict__ in,
-                                                        OutT *__restrict__ out, uint64_t n,
-                                                        OutT *d_total, uint64_t *status,
-                                                        uint32_t *counter, uint32_t ntiles,
-                                                        uint32_t *d_err, uint32_t *select) {
+__global__ void __launch_bounds__(SC_BLOCK) scan_apply_kernel(
+    const uint32_t *__restrict__ in, OutT *__restrict__ out, uint64_t n, OutT *d_total,
+    const uint64_t *__restrict__ tsum, const uint64_t *__restrict__ gsum,
+    const uint64_t *__restrict__ ssum, uint64_t ntiles, uint32_t *select) {
     __shared__ uint64_t s_io[SC_TILE];
     __shared__ uint64_t s_warp[SC_BLOCK / 32 + 1];
     __shared__ uint64_t s_prefix;
-    __shared__ uint32_t s_tile;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) s_tile = atomicAdd(counter, 1u);
-    __syncthreads();
-    const uint32_t tile = s_tile;
-    const uint64_t base = (uint64_t)tile * SC_TILE;
+    const uint64_t tile = blockIdx.x, base = tile * SC_TILE;
+    if (warp == 0) {
+        // lane j reads tile entry j and group entry j of the levels; the
+        // super groups are strided over the lanes
+        const uint64_t g = tile / GROUP_TILES, s = tile / SUPER_TILES;
+        const uint32_t rt = (uint32_t)(tile % GROUP_TILES), rg = (uint32_t)(g % 32);
+        uint64_t v = 0;
+        if ((uint32_t)lane < rt) v += tsum[g * GROUP_TILES + lane];
+        if ((uint32_t)lane < rg) v += gsum[s * 32 + lane];
+        for (uint64_t j = lane; j < s; j += 32) v += ssum[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) s_prefix = v;
+    }
     for (int i = tid; i < SC_TILE; i += SC_BLOCK) {
         uint64_t idx = base + i;
         s_io[i] = idx < n ? (uint64_t)in[idx] : 0ull;
@@ -270,48 +356,9 @@ __global__ void __launch_bounds__(SC_BLOCK) scan_kernel(const uint32_t *__restri
         if (lane == SC_BLOCK / 32 - 1) s_warp[SC_BLOCK / 32] = iw;
     }
     __syncthreads();
-    const uint64_t excl = s_warp[warp] + x - sum;
-    const uint64_t agg = s_warp[SC_BLOCK / 32];
-    // Warp-cooperative look-back: lane j reads tile (t - j); the nearest
-    // inclusive prefix ends the sum.
-    if (warp == 0) {
-        volatile uint64_t *st = status;
-        uint64_t prev = 0;
-        if (tile == 0) {
-            if (lane == 0) st[0] = SC_INC | (agg & SC_MASK);
-        } else {
-            if (lane == 0) st[tile] = SC_AGG | (agg & SC_MASK);
-            int64_t t = (int64_t)tile - 1;
-            uint32_t spins = 0;
-            while (true) {
-                const int64_t ti = t - lane;
-                uint64_t w = ti >= 0 ? (uint64_t)st[ti] : (2ull << 62);
-                while (__any_sync(0xffffffffu, (w & ~SC_MASK) == 0)) {
-                    if (!spin_more(spins, SPIN_LIMIT)) break;
-                    if ((w & ~SC_MASK) == 0) w = st[ti];
-                }
-                if (spins > SPIN_LIMIT) {
-                    if (lane == 0) atomicOr(d_err, DEVERR_TIMEOUT);
-                    break;
-                }
-                const uint32_t inc = __ballot_sync(0xffffffffu, (w & ~SC_MASK) == SC_INC);
-                const int stop = inc ? __ffs(inc) - 1 : 31;
-                uint64_t v = lane <= stop ? (w & SC_MASK) : 0ull;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                prev += v;
-                if (inc) break;
-                t -= 32;
-            }
-            if (lane == 0) st[tile] = SC_INC | ((prev + agg) & SC_MASK);
-        }
-        if (lane == 0) {
-            s_prefix = prev;
-            if (tile == ntiles - 1 && d_total) *d_total = (OutT)(prev + agg);
-        }
-    }
-    __syncthreads();
-    uint64_t run = s_prefix + excl;
+    const uint64_t prefix = s_prefix;
+    if (tid == 0 && tile == ntiles - 1 && d_total) *d_total = (OutT)(prefix + s_warp[SC_BLOCK / 32]);
+    uint64_t run = prefix + s_warp[warp] + x - sum;
 #pragma unroll
     for (int i = 0; i < SC_ITEMS; ++i) {
         s_io[tid * SC_ITEMS + i] = run;
@@ -327,20 +374,23 @@ __global__ void __launch_bounds__(SC_BLOCK) scan_kernel(const uint32_t *__restri
 
 template <typename OutT>
 rtd_status scan_impl(const uint32_t *in, OutT *out, uint64_t n, OutT *d_total, ScanScratch &scr,
-                     uint32_t *d_err, cudaStream_t stream, uint32_t *select = nullptr) {
+                     cudaStream_t stream, uint32_t *select = nullptr) {
     if (n == 0) {
         if (d_total) RTD_CUDA(cudaMemsetAsync(d_total, 0, sizeof(OutT), stream));
         return RTD_OK;
     }
-    uint64_t ntiles = ceil_div(n, SC_TILE);
-    if (ntiles >= (1ull << 31)) return fail(RTD_ERR_INVALID_ARGUMENT, "scan: input too large");
-    RTD_TRY(scr.status.reserve(ntiles * sizeof(uint64_t)));
-    RTD_TRY(scr.counter.reserve(sizeof(uint32_t)));
-    RTD_CUDA(cudaMemsetAsync(scr.status.ptr, 0, ntiles * sizeof(uint64_t), stream));
-    RTD_CUDA(cudaMemsetAsync(scr.counter.ptr, 0, sizeof(uint32_t), stream));
-    scan_kernel<OutT><<<(unsigned)ntiles, SC_BLOCK, 0, stream>>>(
-        in, out, n, d_total, scr.status.as<uint64_t>(), scr.counter.as<uint32_t>(),
-        (uint32_t)ntiles, d_err, select);
+    const Levels L(ceil_div(n, SC_TILE));
+    if (L.tiles >= (1ull << 31)) return fail(RTD_ERR_INVALID_ARGUMENT, "scan: input too large");
+    RTD_TRY(scr.sums.reserve((L.tiles + L.groups + L.supers) * sizeof(uint64_t)));
+    uint64_t *tsum = scr.sums.as<uint64_t>();
+    uint64_t *gsum = tsum + L.tiles, *ssum = gsum + L.groups;
+    RTD_CUDA(cudaMemsetAsync(gsum, 0, (L.groups + L.supers) * sizeof(uint64_t), stream));
+    scan_count_kernel<<<(unsigned)L.tiles, SC_BLOCK, 0, stream>>>(
+        in, n, tsum, reinterpret_cast<unsigned long long *>(gsum),
+        reinterpret_cast<unsigned long long *>(ssum), (int)L.supers);
+    RTD_LAUNCH_CHECK();
+    scan_apply_kernel<OutT><<<(unsigned)L.tiles, SC_BLOCK, 0, stream>>>(
+        in, out, n, d_total, tsum, gsum, ssum, L.tiles, select);
     RTD_LAUNCH_CHECK();
     return RTD_OK;
 }
@@ -352,36 +402,45 @@ rtd_status radix_sort_pairs(K *keys, K *keys_alt, uint32_t *vals, uint32_t *vals
                             bool vals_iota, uint64_t n, int begin_bit, int end_bit,
                             SortScratch &scr, uint32_t *d_err, cudaStream_t stream, bool *in_alt,
                             const float *gather_xyz, float4 *gather_out) {
+    (void)d_err;   // no pass waits on another tile: nothing can time out
     *in_alt = false;
     if (n == 0) return RTD_OK;
     if (n >= (1ull << 30)) return fail(RTD_ERR_INVALID_ARGUMENT, "radix sort: n must be < 2^30");
     const int passes = (end_bit - begin_bit + 7) / 8;
     if (passes <= 0 || passes > 8 || end_bit > (int)(8 * sizeof(K)))
         return fail(RTD_ERR_INVALID_ARGUMENT, "radix sort: bad bit range");
-    const uint64_t ntiles = ceil_div(n, RS_TILE);
+    const Levels L(ceil_div(n, RS_TILE));
+    // counts: every pass's tile rows, then every pass's group and super rows
+    // (zeroed together: the count kernels add into them)
+    const size_t trows = (size_t)passes * L.tiles, srows = (size_t)passes * (L.groups + L.supers);
     RTD_TRY(scr.hist.reserve((size_t)passes * 256 * sizeof(uint32_t)));
-    RTD_TRY(scr.status.reserve((size_t)passes * ntiles * 256 * sizeof(uint32_t)));
-    RTD_TRY(scr.counters.reserve((size_t)passes * sizeof(uint32_t)));
+    RTD_TRY(scr.counts.reserve((trows + srows) * 256 * sizeof(uint32_t)));
+    uint32_t *tc = scr.counts.as<uint32_t>(), *sc = tc + trows * 256;
     RTD_CUDA(cudaMemsetAsync(scr.hist.ptr, 0, (size_t)passes * 256 * 4, stream));
-    RTD_CUDA(cudaMemsetAsync(scr.status.ptr, 0, (size_t)passes * ntiles * 256 * 4, stream));
-    RTD_CUDA(cudaMemsetAsync(scr.counters.ptr, 0, (size_t)passes * 4, stream));
+    RTD_CUDA(cudaMemsetAsync(sc, 0, srows * 256 * 4, stream));
     rs_hist_kernel<K><<<grid_for(n, RS_BLOCK, 148 * 4), RS_BLOCK, 0, stream>>>(
         keys, n, begin_bit, passes, scr.hist.as<uint32_t>());
     RTD_LAUNCH_CHECK();
     rs_hist_scan_kernel<<<1, RS_BLOCK, 0, stream>>>(scr.hist.as<uint32_t>(), passes);
     RTD_LAUNCH_CHECK();
-    const size_t smem = rs_pass_smem(sizeof(K));
-    RTD_CUDA(cudaFuncSetAttribute(rs_pass_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
+    const size_t smem = rs_scatter_smem(sizeof(K));
+    RTD_CUDA(cudaFuncSetAttribute(rs_scatter_kernel<K>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     K *kin = keys, *kout = keys_alt;
     uint32_t *vin = vals, *vout = vals_alt;
     for (int p = 0; p < passes; ++p) {
+        const int shift = begin_bit + 8 * p;
+        uint32_t *tcount = tc + (size_t)p * L.tiles * 256;
+        uint32_t *gsum = sc + (size_t)p * (L.groups + L.supers) * 256;
+        uint32_t *ssum = gsum + L.groups * 256;
+        rs_count_kernel<K><<<(unsigned)L.tiles, RS_BLOCK, 0, stream>>>(
+            kin, n, shift, tcount, gsum, ssum, (int)L.supers);
+        RTD_LAUNCH_CHECK();
         // Pass 0 with vals_iota generates the values 0..n-1 on the fly.
-        rs_pass_kernel<K><<<(unsigned)ntiles, RS_BLOCK, smem, stream>>>(
-            kin, kout, (p == 0 && vals_iota) ? nullptr : vin, vout, n, begin_bit + 8 * p,
-            scr.hist.as<uint32_t>() + p * 256,
-            scr.status.as<uint32_t>() + (size_t)p * ntiles * 256, scr.counters.as<uint32_t>() + p,
-            d_err, gather_xyz, p == passes - 1 ? gather_out : nullptr);
+        rs_scatter_kernel<K><<<(unsigned)L.tiles, RS_BLOCK, smem, stream>>>(
+            kin, kout, (p == 0 && vals_iota) ? nullptr : vin, vout, n, shift,
+            scr.hist.as<uint32_t>() + p * 256, tcount, gsum, ssum, gather_xyz,
+            p == passes - 1 ? gather_out : nullptr);
         RTD_LAUNCH_CHECK();
         K *tk = kin; kin = kout; kout = tk;
         uint32_t *tv = vin; vin = vout; vout = tv;
@@ -401,16 +460,19 @@ template rtd_status radix_sort_pairs<uint64_t>(uint64_t *, uint64_t *, uint32_t 
 
 rtd_status exclusive_scan_u32(const uint32_t *in, uint64_t *out, uint64_t n, uint64_t *d_total,
                               ScanScratch &scr, uint32_t *d_err, cudaStream_t stream) {
-    return scan_impl<uint64_t>(in, out, n, d_total, scr, d_err, stream);
+    (void)d_err;
+    return scan_impl<uint64_t>(in, out, n, d_total, scr, stream);
 }
 rtd_status exclusive_scan_u32_32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *d_total,
                                  ScanScratch &scr, uint32_t *d_err, cudaStream_t stream) {
-    return scan_impl<uint32_t>(in, out, n, d_total, scr, d_err, stream);
+    (void)d_err;
+    return scan_impl<uint32_t>(in, out, n, d_total, scr, stream);
 }
 rtd_status exclusive_scan_select_u32(const uint32_t *in, uint32_t *out, uint32_t *select,
                                      uint64_t n, uint32_t *d_total, ScanScratch &scr,
                                      uint32_t *d_err, cudaStream_t stream) {
-    return scan_impl<uint32_t>(in, out, n, d_total, scr, d_err, stream, select);
+    (void)d_err;
+    return scan_impl<uint32_t>(in, out, n, d_total, scr, stream, select);
 }
 
 }  // namespace rtd

@@ -1,13 +1,16 @@
-// sort.cuh -- onesweep LSD radix sort of (key, u32 value) pairs and a
-// single-pass decoupled look-back exclusive scan.
+// sort.cuh -- LSD radix sort of (key, u32 value) pairs and an exclusive
+// scan, each pass as a count kernel and a scatter kernel over fixed tiles.
 //
 // Radix sort: one read of the keys builds the digit histograms of every
-// pass; each 8-bit pass is then a single kernel whose tiles (taken in order
-// from an atomic counter) rank their keys with warp match-any, publish the
-// per-digit tile count, look back over earlier tiles for the running digit
-// prefix, and scatter through shared memory so each digit run is written
-// contiguously.  Waits on earlier tiles are bounded (SPIN_LIMIT) and set
-// DEVERR_TIMEOUT instead of hanging.
+// pass (the digits' global starts).  Each 8-bit pass then runs two
+// kernels: the count kernel writes every tile's digit histogram and adds it
+// into the sums of its group (32 tiles) and super group (32 groups); the
+// scatter kernel ranks a tile's keys with warp ballots, takes the digit
+// counts of the earlier tiles from those three levels (at most 31 + 31
+// entries and the earlier super groups, all written by the count kernel),
+// and writes each digit run contiguously through shared memory.  No tile
+// waits on another, so there is nothing to time out and no chain of waits
+// when every tile is resident at once.
 #pragma once
 
 #include "common.cuh"
@@ -16,8 +19,7 @@ namespace rtd {
 
 struct SortScratch {
     DevBuf hist;      // passes * 256 u32 (counts, then exclusive offsets)
-    DevBuf status;    // passes * tiles * 256 u32 (look-back words)
-    DevBuf counters;  // passes u32 (tile tickets)
+    DevBuf counts;    // passes * (tiles + groups + super groups) * 256 u32
 };
 
 // Sorts n pairs by bits [begin_bit, end_bit) of the key.  keys/vals hold the
@@ -35,8 +37,7 @@ rtd_status radix_sort_pairs(K *keys, K *keys_alt, uint32_t *vals, uint32_t *vals
 
 // out[i] = sum(in[0..i)), out has n entries; *d_total (device) = sum(in).
 struct ScanScratch {
-    DevBuf status;    // tiles u64 look-back words
-    DevBuf counter;   // tile ticket
+    DevBuf sums;      // tiles + groups + super groups u64
 };
 rtd_status exclusive_scan_u32(const uint32_t *in, uint64_t *out, uint64_t n, uint64_t *d_total,
                               ScanScratch &scr, uint32_t *d_err, cudaStream_t stream);

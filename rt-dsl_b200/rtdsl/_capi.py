@@ -107,6 +107,8 @@ _SIGNATURES = {
     "rtd_index_profile_get": (_I, [_P, _P]),
     "rtd_launch_count": (_U64, []),
     "rtd_wait_selftest": (_I, [_U32, _I, _P]),
+    "rtd_radix_sort_pairs": (_I, [_P, _U32, _P, _U64, _U32, _P]),
+    "rtd_exclusive_scan": (_I, [_P, _P, _P, _U64, _P, _P]),
     "rtd_limits_set": (_I, [_P]),
     "rtd_limits_get": (None, [_P]),
     "rtd_bh_params_default": (None, [_P]),

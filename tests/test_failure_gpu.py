@@ -2,10 +2,9 @@
 fault: every limit here makes a loop give up early and report its status
 through the C ABI, and the context stays usable afterwards.
 
-- RTD_ERR_TIMEOUT: the look-backs' bounded wait (spin_more) run on a device
-  flag that nothing sets (rtd_wait_selftest).  The real look-backs are not
-  made to give up: a sort pass whose wait gave up leaves unwritten slots in
-  its value array, which later passes would read as indices.
+- RTD_ERR_TIMEOUT: the bounded wait helper (spin_more) run on a device flag
+  that nothing sets (rtd_wait_selftest).  No product kernel waits on
+  another block: the sort and scan passes are count + scatter kernels.
 - RTD_ERR_NOT_CONVERGED: the reference's round cap (schedule.partial_results)
   with a radius too small to reach k hits in max_rounds.  The partial lists
   must equal the oracle's k smallest keys within the last radius.
