@@ -98,7 +98,6 @@ rtd_status rtd_bh_release(rtd_bh *b) {
     b->has_quad = false;
     b->ilog_pages = 0;
     b->ilog_valid = false;
-    b->sort.hist.release();
     b->sort.counts.release();
     b->scan.sums.release();
     b->built = false;

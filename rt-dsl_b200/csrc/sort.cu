@@ -71,54 +71,40 @@ __device__ __forceinline__ uint32_t digit_peers(uint32_t dig) {
     return peers;
 }
 
-// Sum of the 256-word rows before entry `tile` of the three levels, for
-// word d: the earlier tiles of its group, the earlier groups of its super
-// group and the earlier super groups.
-template <typename T>
-__device__ __forceinline__ T tile_prefix(const T *tcount, const T *gsum, const T *ssum,
-                                         uint64_t tile, uint32_t d, uint32_t stride) {
+// For digit d of tile `tile`: the digit's count in the earlier tiles (the
+// earlier tiles of its group, the earlier groups of its super group and the
+// earlier super groups) in *before, and its count over all tiles (the sum
+// of the super-group rows, or of the group rows when there is one super
+// group) in *total.  Rows are 256 words apart.
+__device__ __forceinline__ void digit_counts(const uint32_t *tcount, const uint32_t *gsum,
+                                             const uint32_t *ssum, uint64_t tile, uint32_t groups,
+                                             uint32_t supers, uint32_t d, uint32_t *before,
+                                             uint32_t *total) {
     const uint64_t g = tile / GROUP_TILES, s = tile / SUPER_TILES;
     const uint32_t rt = (uint32_t)(tile % GROUP_TILES), rg = (uint32_t)(g % 32);
-    const T *tp = tcount + g * GROUP_TILES * stride + d;
-    const T *gp = gsum + s * 32 * stride + d;
-    T a = 0, b = 0;
+    const uint32_t *tp = tcount + g * GROUP_TILES * 256 + d;
+    uint32_t a = 0, b = 0, c = 0, t = 0;
 #pragma unroll
-    for (uint32_t j = 0; j < GROUP_TILES; ++j) a += j < rt ? tp[j * stride] : T(0);
+    for (uint32_t j = 0; j < GROUP_TILES; ++j) a += j < rt ? tp[j * 256] : 0u;
+    if (supers == 1) {
 #pragma unroll
-    for (uint32_t j = 0; j < 32; ++j) b += j < rg ? gp[j * stride] : T(0);
-    T c = 0;
-    for (uint64_t j = 0; j < s; ++j) c += ssum[j * stride + d];
-    return a + b + c;
-}
-
-template <typename K>
-__global__ void __launch_bounds__(RS_BLOCK) rs_hist_kernel(const K *__restrict__ keys, uint64_t n,
-                                                           int begin_bit, int passes,
-                                                           uint32_t *__restrict__ hist) {
-    __shared__ uint32_t sh[8][256];
-    for (int i = threadIdx.x; i < 8 * 256; i += RS_BLOCK) (&sh[0][0])[i] = 0;
-    __syncthreads();
-    for (uint64_t i = (uint64_t)blockIdx.x * RS_BLOCK + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x * RS_BLOCK) {
-        K k = keys[i];
-        for (int p = 0; p < passes; ++p)
-            atomicAdd(&sh[p][(uint32_t)(k >> (begin_bit + 8 * p)) & 255u], 1u);
+        for (uint32_t j = 0; j < 32; ++j) {
+            const uint32_t v = j < groups ? gsum[j * 256 + d] : 0u;
+            t += v;
+            b += j < rg ? v : 0u;
+        }
+    } else {
+        const uint32_t *gp = gsum + s * 32 * 256 + d;
+#pragma unroll
+        for (uint32_t j = 0; j < 32; ++j) b += j < rg ? gp[j * 256] : 0u;
+        for (uint32_t j = 0; j < supers; ++j) {
+            const uint32_t v = ssum[j * 256 + d];
+            t += v;
+            c += j < s ? v : 0u;
+        }
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < passes * 256; i += RS_BLOCK) {
-        uint32_t c = (&sh[0][0])[i];
-        if (c) atomicAdd(&hist[i], c);
-    }
-}
-
-// In place: hist[p][d] counts -> exclusive offsets.
-__global__ void __launch_bounds__(RS_BLOCK) rs_hist_scan_kernel(uint32_t *hist, int passes) {
-    __shared__ uint32_t s_warp[RS_WARPS + 1];
-    for (int p = 0; p < passes; ++p) {
-        uint32_t v = hist[p * 256 + threadIdx.x];
-        uint32_t e = block_excl_scan256(v, s_warp);
-        hist[p * 256 + threadIdx.x] = e;
-    }
+    *before = a + b + c;
+    *total = t;
 }
 
 // Counts of one pass: the digit histogram of each tile of RS_TILE keys in
@@ -174,9 +160,9 @@ __global__ void __launch_bounds__(RS_BLOCK) rs_count_kernel(const K *__restrict_
 template <typename K>
 __global__ void __launch_bounds__(RS_BLOCK) rs_scatter_kernel(
     const K *__restrict__ kin, K *__restrict__ kout, const uint32_t *__restrict__ vin,
-    uint32_t *__restrict__ vout, uint64_t n, int shift, const uint32_t *__restrict__ digit_off,
-    const uint32_t *__restrict__ tcount, const uint32_t *__restrict__ gsum,
-    const uint32_t *__restrict__ ssum, const float *__restrict__ gxyz,
+    uint32_t *__restrict__ vout, uint64_t n, int shift, const uint32_t *__restrict__ tcount,
+    const uint32_t *__restrict__ gsum, const uint32_t *__restrict__ ssum, uint32_t groups,
+    uint32_t supers, const float *__restrict__ gxyz,
     float4 *__restrict__ gout) {
     extern __shared__ __align__(16) unsigned char rs_smem[];
     K *s_keys = reinterpret_cast<K *>(rs_smem);
@@ -202,8 +188,10 @@ __global__ void __launch_bounds__(RS_BLOCK) rs_scatter_kernel(
         val[i] = ok ? (vin ? vin[idx] : (uint32_t)idx) : 0u;
     }
     const uint32_t d = (uint32_t)tid;
-    const uint32_t before = tile_prefix(tcount, gsum, ssum, tile, d, 256u);
-    __syncthreads();
+    uint32_t before, total;
+    digit_counts(tcount, gsum, ssum, tile, groups, supers, d, &before, &total);
+    // the digit's global start: exclusive scan of the digit totals
+    const uint32_t digit_start = block_excl_scan256(total, s_misc);
     const uint32_t lt = lanemask_lt();
     uint32_t *wh = s_wh + warp * 256;
 #pragma unroll
@@ -229,7 +217,7 @@ __global__ void __launch_bounds__(RS_BLOCK) rs_scatter_kernel(
     }
     const uint32_t excl_local = block_excl_scan256(run, s_misc);
     s_excl[d] = excl_local;
-    s_base[d] = digit_off[d] + before - excl_local;
+    s_base[d] = digit_start + before - excl_local;
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < RS_ITEMS; ++i) {
@@ -296,8 +284,9 @@ __global__ void __launch_bounds__(SC_BLOCK) scan_count_kernel(const uint32_t *__
     }
 }
 
-// Scan output: out[i] = prefix of the tile (tile_prefix over the count
-// kernel's levels) + the block's exclusive scan within the tile.  With
+// Scan output: out[i] = prefix of the tile (the sums of the earlier tiles
+// of its group, earlier groups of its super group and earlier super groups)
+// + the block's exclusive scan within the tile.  With
 // select != nullptr, also select[out[i]] = i for every i with in[i] != 0
 // (stream compaction of the indices of flagged entries).
 template <typename OutT>
@@ -413,16 +402,9 @@ rtd_status radix_sort_pairs(K *keys, K *keys_alt, uint32_t *vals, uint32_t *vals
     // counts: every pass's tile rows, then every pass's group and super rows
     // (zeroed together: the count kernels add into them)
     const size_t trows = (size_t)passes * L.tiles, srows = (size_t)passes * (L.groups + L.supers);
-    RTD_TRY(scr.hist.reserve((size_t)passes * 256 * sizeof(uint32_t)));
     RTD_TRY(scr.counts.reserve((trows + srows) * 256 * sizeof(uint32_t)));
     uint32_t *tc = scr.counts.as<uint32_t>(), *sc = tc + trows * 256;
-    RTD_CUDA(cudaMemsetAsync(scr.hist.ptr, 0, (size_t)passes * 256 * 4, stream));
     RTD_CUDA(cudaMemsetAsync(sc, 0, srows * 256 * 4, stream));
-    rs_hist_kernel<K><<<grid_for(n, RS_BLOCK, 148 * 4), RS_BLOCK, 0, stream>>>(
-        keys, n, begin_bit, passes, scr.hist.as<uint32_t>());
-    RTD_LAUNCH_CHECK();
-    rs_hist_scan_kernel<<<1, RS_BLOCK, 0, stream>>>(scr.hist.as<uint32_t>(), passes);
-    RTD_LAUNCH_CHECK();
     const size_t smem = rs_scatter_smem(sizeof(K));
     RTD_CUDA(cudaFuncSetAttribute(rs_scatter_kernel<K>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -438,8 +420,8 @@ rtd_status radix_sort_pairs(K *keys, K *keys_alt, uint32_t *vals, uint32_t *vals
         RTD_LAUNCH_CHECK();
         // Pass 0 with vals_iota generates the values 0..n-1 on the fly.
         rs_scatter_kernel<K><<<(unsigned)L.tiles, RS_BLOCK, smem, stream>>>(
-            kin, kout, (p == 0 && vals_iota) ? nullptr : vin, vout, n, shift,
-            scr.hist.as<uint32_t>() + p * 256, tcount, gsum, ssum, gather_xyz,
+            kin, kout, (p == 0 && vals_iota) ? nullptr : vin, vout, n, shift, tcount, gsum, ssum,
+            (uint32_t)L.groups, (uint32_t)L.supers, gather_xyz,
             p == passes - 1 ? gather_out : nullptr);
         RTD_LAUNCH_CHECK();
         K *tk = kin; kin = kout; kout = tk;

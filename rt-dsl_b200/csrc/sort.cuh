@@ -1,13 +1,13 @@
 // sort.cuh -- LSD radix sort of (key, u32 value) pairs and an exclusive
 // scan, each pass as a count kernel and a scatter kernel over fixed tiles.
 //
-// Radix sort: one read of the keys builds the digit histograms of every
-// pass (the digits' global starts).  Each 8-bit pass then runs two
-// kernels: the count kernel writes every tile's digit histogram and adds it
-// into the sums of its group (32 tiles) and super group (32 groups); the
-// scatter kernel ranks a tile's keys with warp ballots, takes the digit
-// counts of the earlier tiles from those three levels (at most 31 + 31
-// entries and the earlier super groups, all written by the count kernel),
+// Radix sort: each 8-bit pass runs two kernels.  The count kernel writes
+// every tile's digit histogram and adds it into the sums of its group (32
+// tiles) and super group (32 groups).  The scatter kernel ranks a tile's
+// keys with warp ballots, takes each digit's count in the earlier tiles
+// from those three levels (at most 31 + 31 entries and the earlier super
+// groups, all written by the count kernel) and the digit's global start
+// from a block scan of the digit totals (the group or super-group sums),
 // and writes each digit run contiguously through shared memory.  No tile
 // waits on another, so there is nothing to time out and no chain of waits
 // when every tile is resident at once.
@@ -18,7 +18,6 @@
 namespace rtd {
 
 struct SortScratch {
-    DevBuf hist;      // passes * 256 u32 (counts, then exclusive offsets)
     DevBuf counts;    // passes * (tiles + groups + super groups) * 256 u32
 };
 
