@@ -82,9 +82,12 @@ struct rtd_index {
     rtd::DevBuf pyramid;    // run boxes over the sorted points (2 float4 per run)
     rtd::SortScratch sort;
     rtd::ScanScratch scan;
-    // radius-seed data kept from the build: stride sample of the points in
-    // input order (<= 1000 x float4) and the 4096-point 1-NN scratch
+    // radius-seed data kept from the build: stride samples of the points in
+    // input order (<= 1000 + 4096 float4) and the 1-NN scratch; nn_seeded:
+    // the sampled 1-NN seed (IndexHeader::nn95_key) has been computed for
+    // this build
     rtd::DevBuf sample, seed;
+    bool nn_seeded = false;
     // search scratch
     rtd::DevBuf qkeys, qkeys_alt, qperm, qperm_alt;
     const void *skeys = nullptr;   // the points' sorted Morton keys (in keys or keys_alt)
@@ -111,10 +114,12 @@ struct rtd_index {
         uint64_t spec_pairs = 0, spec_recs = 0;
     } rtoken;
     // Side stream for work that overlaps the build: the radius-seed sample
-    // (every build) and rtd_k_nn's query ordering
-    cudaStream_t side_stream = nullptr;
+    // (every build) and rtd_k_nn's query ordering; tree stream: the box
+    // pyramid, beside the Karras flags and their scan
+    cudaStream_t side_stream = nullptr, tree_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_seed_fork = nullptr,
-                ev_seed_join = nullptr, ev_sorted = nullptr;
+                ev_seed_join = nullptr, ev_sorted = nullptr, ev_tree_fork = nullptr,
+                ev_tree_join = nullptr;
     rtd::DevBuf wpos;       // queries' Morton positions for the window seed
     rtd::DevBuf wide;       // per-warp list slabs of the k > 2048 search
     rtd::QueryOrderScratch qorder;
@@ -130,9 +135,11 @@ struct rtd_index {
     ~rtd_index() {
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
-        for (cudaEvent_t e : {ev_fork, ev_join, ev_seed_fork, ev_seed_join, ev_sorted})
+        for (cudaEvent_t e : {ev_fork, ev_join, ev_seed_fork, ev_seed_join, ev_sorted,
+                              ev_tree_fork, ev_tree_join})
             if (e) cudaEventDestroy(e);
         if (side_stream) cudaStreamDestroy(side_stream);
+        if (tree_stream) cudaStreamDestroy(tree_stream);
     }
 };
 
@@ -223,8 +230,12 @@ inline uint64_t chunk_begin(uint64_t nq, uint32_t chunks, uint32_t c) {
     return (c * nq + chunks - 1) / chunks;
 }
 
-// Creates the index's side stream and its events on first use.
+// Creates the index's side and tree streams and their events on first use.
 rtd_status ensure_side_stream(rtd_index *idx);
+
+// The sampled 1-NN seed of the last build (IndexHeader::nn95_key), computed
+// on stream st unless it already has been (lbvh.cu).
+rtd_status ensure_nn_seed(rtd_index *idx, cudaStream_t st);
 
 // LBVH build over n device points (lbvh.cu).
 rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd_schedule *s,

@@ -65,11 +65,17 @@ __device__ __forceinline__ uint32_t morton_position(const IndexHeader *h, const 
 
 // Every query's position, in processing order, ahead of the search (so the
 // search's dependent loads do not include the binary search).
-__global__ void __launch_bounds__(256) window_pos_kernel(const IndexHeader *h, const void *skeys,
+__global__ void __launch_bounds__(256) window_pos_kernel(IndexHeader *h, const void *skeys,
                                                          uint32_t n, int key64, float scale,
                                                          const float *__restrict__ q,
                                                          const uint32_t *__restrict__ perm,
-                                                         uint64_t nq, uint32_t *__restrict__ pos) {
+                                                         uint64_t nq, uint32_t *__restrict__ pos,
+                                                         IndexHeader *qh) {
+    // the query ordering's error flags move into the index's here
+    if (qh && blockIdx.x == 0 && threadIdx.x == 0 && qh->err) {
+        atomicOr(&h->err, qh->err);
+        qh->err = 0;
+    }
     for (uint64_t t = (uint64_t)blockIdx.x * 256 + threadIdx.x; t < nq;
          t += (uint64_t)gridDim.x * 256) {
         const uint64_t qi = perm ? perm[t] : t;
@@ -371,9 +377,11 @@ rtd_status seed_radius(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t k
             d_q, nq, k, s.radius_heuristic == RTD_RADIUS_SAMPLED_MAX ? 1.0f : s.radius_param,
             idx->sample.as<float4>(), h);
         break;
-    case RTD_RADIUS_FIXED:
     case RTD_RADIUS_SAMPLED_NN:
     case RTD_RADIUS_MORTON_WINDOW:
+        RTD_TRY(ensure_nn_seed(idx, st));
+        [[fallthrough]];
+    case RTD_RADIUS_FIXED:
         seed_set_kernel<<<1, 1, 0, st>>>(
             h, s.radius_heuristic == RTD_RADIUS_FIXED ? RTD_RADIUS_FIXED : RTD_RADIUS_SAMPLED_NN,
             s.radius_param);
@@ -452,7 +460,8 @@ rtd_status knn_search_ex(rtd_index *idx, const float *d_q, uint64_t nq, uint32_t
         return fail(RTD_ERR_INVALID_ARGUMENT, "fixed radius must be > 0");
     for (int e = EV_SEARCH0; e <= EV_SEARCH1; ++e) idx->ev_set[e] = false;
     idx->mark(EV_SEARCH0, st);
-    RTD_TRY(seed_radius(idx, d_q, nq, k, s, st));
+    // the Morton-window search runs one unbounded round: no initial radius
+    if (!uses_window(idx, s, k)) RTD_TRY(seed_radius(idx, d_q, nq, k, s, st));
     idx->mark(EV_SEEDED, st);
     const uint32_t *perm = given_perm;
     if (!have_perm) RTD_TRY(order_queries(idx, d_q, nq, s.use_morton_lbv != 0, &perm, st));
@@ -554,7 +563,8 @@ rtd_status k_nn_device(rtd_index *idx, const float *d_points, uint64_t n, const 
             window_pos_kernel<<<grid_for(nq, 256, 148 * 8), 256, 0, side>>>(
                 idx->hdr.as<IndexHeader>(), idx->skeys, (uint32_t)idx->n, idx->morton_bits != 30,
                 idx->morton_bits == 30 ? 1023.0f : (float)((1u << (idx->morton_bits / 3)) - 1u),
-                d_q, perm, nq, idx->wpos.as<uint32_t>());
+                d_q, perm, nq, idx->wpos.as<uint32_t>(),
+                perm ? idx->qorder.hdr.as<IndexHeader>() : nullptr);
             RTD_LAUNCH_CHECK();
             RTD_CUDA(cudaEventRecord(idx->ev_join, side));
             wpos = idx->wpos.as<uint32_t>();
@@ -563,7 +573,7 @@ rtd_status k_nn_device(rtd_index *idx, const float *d_points, uint64_t n, const 
     RTD_CUDA(cudaStreamWaitEvent(st, idx->ev_join, 0));   // also on the error paths
     RTD_TRY(ord);
     RTD_TRY(r);
-    if (perm) {
+    if (perm && !wpos) {   // (window_pos_kernel has folded them otherwise)
         fold_errors_kernel<<<1, 1, 0, st>>>(idx->hdr.as<IndexHeader>(), idx->qorder.hdr.as<IndexHeader>());
         RTD_LAUNCH_CHECK();
     }

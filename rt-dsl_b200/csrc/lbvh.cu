@@ -425,8 +425,11 @@ __global__ void __launch_bounds__(32) stage_top_kernel(IndexHeader *h,
 }
 
 // ------------------------------------------------ radius-seed sample data
-// Stride sample of <= 1000 points in input order, kept for the k_nn!
-// sampled-percentile seed (gprt-macros/src/lib.rs:433-434).
+// Two stride samples of the points in input order, kept with the index:
+// <= 1000 points (sample[0..n_sample)) for the k_nn! sampled-percentile seed
+// (gprt-macros/src/lib.rs:433-434), and S = min(n, 4096) points, index
+// b*n/S (sample[SEED_PCT_POINTS + b]), for the sampled 1-NN seed, which is
+// computed from them on the first search that needs it (ensure_nn_seed).
 __global__ void seed_sample_kernel(const float *__restrict__ xyz, uint64_t n, float4 *sample,
                                    IndexHeader *h) {
     uint64_t pstep = n / SEED_PCT_POINTS > 1 ? n / SEED_PCT_POINTS : 1;
@@ -436,30 +439,35 @@ __global__ void seed_sample_kernel(const float *__restrict__ xyz, uint64_t n, fl
         uint64_t i = t * pstep;
         sample[t] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], 0.0f);
     }
+    const uint32_t S = n < SEED_NN_SAMPLE ? (uint32_t)n : (uint32_t)SEED_NN_SAMPLE;
+    for (uint32_t b = threadIdx.x; b < S; b += blockDim.x) {
+        const uint64_t i = (uint64_t)b * n / S;
+        sample[SEED_PCT_POINTS + b] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], 0.0f);
+    }
     if (threadIdx.x == 0) h->n_sample = (uint32_t)cnt;
 }
 
-// Squared 1-NN distance of each of S = min(n, 4096) stride-sampled points
-// (index a*n/S) among the other sample points.  Grid (a-tiles x b-chunks);
-// each thread folds its chunk's minimum into out[a] (order-preserving u32,
-// pre-set to 0xFFFFFFFF).  The minimum does not depend on the order.
+// Squared 1-NN distance of each of the S sample points p[a] among the other
+// sample points.  Grid (a-tiles x b-chunks); each thread folds its chunk's
+// minimum into out[a] (order-preserving u32, pre-set to 0xFFFFFFFF).  The
+// minimum does not depend on the order.
 constexpr int SEED_CHUNK = 256;
-__global__ void __launch_bounds__(128) seed_nn_kernel(const float *__restrict__ xyz, uint64_t n,
-                                                      uint32_t S, uint32_t *__restrict__ out) {
+__global__ void __launch_bounds__(128) seed_nn_kernel(const float4 *__restrict__ p, uint32_t S,
+                                                      uint32_t *__restrict__ out) {
     __shared__ float3 s_p[SEED_CHUNK];
     const uint32_t a = blockIdx.x * 128 + threadIdx.x;
     const uint32_t b0 = blockIdx.y * SEED_CHUNK;
     for (uint32_t t = threadIdx.x; t < SEED_CHUNK; t += 128) {
         uint32_t b = b0 + t;
         if (b < S) {
-            uint64_t ib = (uint64_t)b * n / S;
-            s_p[t] = make_float3(xyz[3 * ib], xyz[3 * ib + 1], xyz[3 * ib + 2]);
+            const float4 v = p[b];
+            s_p[t] = make_float3(v.x, v.y, v.z);
         }
     }
     __syncthreads();
     if (a >= S) return;
-    const uint64_t ia = (uint64_t)a * n / S;
-    const float ax = xyz[3 * ia], ay = xyz[3 * ia + 1], az = xyz[3 * ia + 2];
+    const float4 va = p[a];
+    const float ax = va.x, ay = va.y, az = va.z;
     const uint32_t lim = S - b0 < (uint32_t)SEED_CHUNK ? S - b0 : (uint32_t)SEED_CHUNK;
     float best = INFINITY;
     for (uint32_t j = 0; j < lim; ++j) {
@@ -513,23 +521,34 @@ __global__ void __launch_bounds__(1024) seed_nn_select_kernel(const uint32_t *__
 
 rtd_status build_seed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStream_t st) {
     IndexHeader *h = idx->hdr.as<IndexHeader>();
-    RTD_TRY(idx->sample.reserve(SEED_PCT_POINTS * sizeof(float4)));
+    RTD_TRY(idx->sample.reserve((SEED_PCT_POINTS + SEED_NN_SAMPLE) * sizeof(float4)));
     RTD_TRY(idx->seed.reserve(SEED_NN_SAMPLE * sizeof(float)));
     seed_sample_kernel<<<1, 256, 0, st>>>(d_xyz, n, idx->sample.as<float4>(), h);
     RTD_LAUNCH_CHECK();
-    if (n >= 2) {
-        uint32_t S = n < SEED_NN_SAMPLE ? (uint32_t)n : (uint32_t)SEED_NN_SAMPLE;
-        RTD_CUDA(cudaMemsetAsync(idx->seed.ptr, 0xFF, S * sizeof(uint32_t), st));
-        dim3 grid((S + 127) / 128, (S + SEED_CHUNK - 1) / SEED_CHUNK);
-        seed_nn_kernel<<<grid, 128, 0, st>>>(d_xyz, n, S, idx->seed.as<uint32_t>());
-        RTD_LAUNCH_CHECK();
-        seed_nn_select_kernel<<<1, 1024, 0, st>>>(idx->seed.as<uint32_t>(), S, h);
-        RTD_LAUNCH_CHECK();
-    }
+    idx->nn_seeded = false;
     return RTD_OK;
 }
 
 }  // namespace
+
+rtd_status ensure_nn_seed(rtd_index *idx, cudaStream_t st) {
+    if (idx->nn_seeded || idx->n < 2) return RTD_OK;
+    IndexHeader *h = idx->hdr.as<IndexHeader>();
+    const uint32_t S = idx->n < SEED_NN_SAMPLE ? (uint32_t)idx->n : (uint32_t)SEED_NN_SAMPLE;
+    RTD_CUDA(cudaMemsetAsync(idx->seed.ptr, 0xFF, S * sizeof(uint32_t), st));
+    dim3 grid((S + 127) / 128, (S + SEED_CHUNK - 1) / SEED_CHUNK);
+    seed_nn_kernel<<<grid, 128, 0, st>>>(idx->sample.as<float4>() + SEED_PCT_POINTS, S,
+                                         idx->seed.as<uint32_t>());
+    RTD_LAUNCH_CHECK();
+    seed_nn_select_kernel<<<1, 1024, 0, st>>>(idx->seed.as<uint32_t>(), S, h);
+    RTD_LAUNCH_CHECK();
+    // Inside a stream capture the kernels run at each launch of the graph,
+    // not now: an eager search afterwards must still compute the seed.
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    RTD_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (cs == cudaStreamCaptureStatusNone) idx->nn_seeded = true;
+    return RTD_OK;
+}
 
 namespace {
 
@@ -592,22 +611,38 @@ rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStr
     P.pyr = pyr;
     float4 *lv[PYR_MAX + 1] = {};
     for (int j = 1; j <= nlev; ++j) lv[j] = pyr + 2 * offs[j];
+    // The pyramid (from the points) runs on the tree stream while the flags
+    // and their scan (from the keys) run on st; the node kernel needs both.
+    RTD_TRY(ensure_side_stream(idx));
+    cudaStream_t ts = idx->tree_stream;
+    RTD_CUDA(cudaEventRecord(idx->ev_tree_fork, st));
+    RTD_CUDA(cudaStreamWaitEvent(ts, idx->ev_tree_fork, 0));
     // three levels per launch: 1-3 from the points, 4-6 from level 3, ...
-    for (int j = 1; j <= nlev; j += 3) {
+    cudaError_t pe = cudaSuccess;
+    for (int j = 1; j <= nlev && pe == cudaSuccess; j += 3) {
         float4 *o2 = j + 1 <= nlev ? lv[j + 1] : nullptr;
         float4 *o3 = j + 2 <= nlev ? lv[j + 2] : nullptr;
         const unsigned g = (unsigned)ceil_div(sizes[j - 1], 512);
-        if (j == 1) pyramid_fold_kernel<true><<<g, 512, 0, st>>>(P.pts, n, lv[1], o2, o3);
-        else pyramid_fold_kernel<false><<<g, 512, 0, st>>>(lv[j - 1], sizes[j - 1], lv[j], o2, o3);
-        RTD_LAUNCH_CHECK();
+        if (j == 1) pyramid_fold_kernel<true><<<g, 512, 0, ts>>>(P.pts, n, lv[1], o2, o3);
+        else pyramid_fold_kernel<false><<<g, 512, 0, ts>>>(lv[j - 1], sizes[j - 1], lv[j], o2, o3);
+        note_launch();
+        pe = cudaGetLastError();
     }
+    RTD_CUDA(cudaEventRecord(idx->ev_tree_join, ts));
     const int gi = grid_for(ni, BLOCK, 148 * 8);
     karras_flag_kernel<K><<<gi, BLOCK, 0, st>>>(skeys, (int64_t)n, idx->leaf_size,
                                                 idx->flags.as<uint32_t>());
-    RTD_LAUNCH_CHECK();
-    RTD_TRY(exclusive_scan_select_u32(idx->flags.as<uint32_t>(), idx->cidx.as<uint32_t>(),
-                                      idx->csel.as<uint32_t>(), ni, &h->n_internal, idx->scan,
-                                      d_err, st));
+    note_launch();
+    cudaError_t fe = cudaGetLastError();
+    const rtd_status sr =
+        fe != cudaSuccess ? RTD_OK
+                          : exclusive_scan_select_u32(idx->flags.as<uint32_t>(), idx->cidx.as<uint32_t>(),
+                                                      idx->csel.as<uint32_t>(), ni, &h->n_internal,
+                                                      idx->scan, d_err, st);
+    RTD_CUDA(cudaStreamWaitEvent(st, idx->ev_tree_join, 0));   // also on the error paths
+    if (pe != cudaSuccess) return cuda_fail(pe, "pyramid_fold_kernel launch");
+    if (fe != cudaSuccess) return cuda_fail(fe, "karras_flag_kernel launch");
+    RTD_TRY(sr);
     // grid for about (n - 1) / leaf_size kept nodes, the count of a balanced
     // tree; the kernel strides over however many there are (up to
     // n - 1 - leaf_size in a chain-shaped tree)
@@ -627,10 +662,12 @@ template rtd_status build_tree_sorted<uint64_t>(rtd_index *, const uint64_t *, u
 
 rtd_status ensure_side_stream(rtd_index *idx) {
     if (idx->side_stream) return RTD_OK;
-    RTD_CUDA(cudaStreamCreateWithFlags(&idx->side_stream, cudaStreamNonBlocking));
+    RTD_CUDA(cudaStreamCreateWithFlags(&idx->tree_stream, cudaStreamNonBlocking));
     for (cudaEvent_t *e : {&idx->ev_fork, &idx->ev_join, &idx->ev_seed_fork, &idx->ev_seed_join,
-                           &idx->ev_sorted})
+                           &idx->ev_sorted, &idx->ev_tree_fork, &idx->ev_tree_join})
         RTD_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    // created last: its presence means every stream and event exists
+    RTD_CUDA(cudaStreamCreateWithFlags(&idx->side_stream, cudaStreamNonBlocking));
     return RTD_OK;
 }
 
