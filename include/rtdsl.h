@@ -159,7 +159,10 @@ rtd_status rtd_wait_selftest(uint32_t spin_limit, int flag_set, rtd_stream strea
  * reference counterpart), exposed so that their results can be checked
  * against a CPU sort and scan.  rtd_radix_sort_pairs sorts n keys of
  * key_bytes (4 or 8) bytes in place by their bits [0, end_bit) with the
- * LSD radix sort (8-bit digits), stably, and writes to d_vals each key's index in the
+ * LSD radix sort (8-bit digits; 8-byte keys with 32 < end_bit <= 48 as the
+ * index build sorts its Morton codes: the low end_bit - 32 bits as 8-byte
+ * keys, then the top 32 bits as 4-byte keys), stably, and writes to d_vals
+ * each key's index in the
  * input (d_vals is also scratch: its input is ignored).  rtd_exclusive_scan
  * writes d_out[i] = sum(d_in[0..i)) (32-bit; the caller guarantees the sum
  * fits), *h_total = sum(d_in) and, when d_select != NULL and every d_in[i] is

@@ -234,7 +234,20 @@ rtd_status rtd_radix_sort_pairs(void *d_keys, uint32_t key_bytes, uint32_t *d_va
     RTD_TRY(err.reserve(sizeof(uint32_t)));
     RTD_CUDA(cudaMemsetAsync(err.ptr, 0, sizeof(uint32_t), st));
     bool in_alt = false;
-    if (key_bytes == 4)
+    if (key_bytes == 8 && end_bit > 32 && end_bit <= 48) {
+        // the split sort the index build runs on keys of this width
+        DevBuf k32;
+        RTD_TRY(k32.reserve(2 * n * sizeof(uint32_t)));
+        uint32_t *sv = nullptr;
+        RTD_TRY(radix_sort_split64(static_cast<const uint64_t *>(d_keys), kalt.as<uint64_t>(),
+                                   k32.as<uint32_t>(), k32.as<uint32_t>() + n, d_vals,
+                                   valt.as<uint32_t>(), n, (int)end_bit, scr, st, nullptr, nullptr,
+                                   kalt.as<uint64_t>(), &sv));
+        RTD_CUDA(cudaMemcpyAsync(d_keys, kalt.ptr, n * key_bytes, cudaMemcpyDeviceToDevice, st));
+        if (sv != d_vals)
+            RTD_CUDA(cudaMemcpyAsync(d_vals, sv, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+        RTD_CUDA(cudaStreamSynchronize(st));   // k32 is freed on return
+    } else if (key_bytes == 4)
         RTD_TRY(radix_sort_pairs<uint32_t>(static_cast<uint32_t *>(d_keys), kalt.as<uint32_t>(),
                                            d_vals, valt.as<uint32_t>(), true, n, 0, (int)end_bit,
                                            scr, err.as<uint32_t>(), st, &in_alt));

@@ -75,6 +75,7 @@ struct rtd_index {
     rtd::DevBuf top;        // BvhNode * TOP_MAX
     // build scratch
     rtd::DevBuf keys, keys_alt, vals, vals_alt;
+    rtd::DevBuf k32a, k32b;   // 32-bit top keys of the split sort
     // Karras node flags (1: the node keeps more than leaf_size points),
     // compact indices, the list of kept nodes, and (forest builds) the kept
     // nodes' first and last points by Karras index

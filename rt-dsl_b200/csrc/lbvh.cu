@@ -435,16 +435,17 @@ __global__ void seed_sample_kernel(const float *__restrict__ xyz, uint64_t n, fl
     uint64_t pstep = n / SEED_PCT_POINTS > 1 ? n / SEED_PCT_POINTS : 1;
     uint64_t cnt = (n + pstep - 1) / pstep;
     if (cnt > SEED_PCT_POINTS) cnt = SEED_PCT_POINTS;
-    for (uint64_t t = threadIdx.x; t < cnt; t += blockDim.x) {
+    const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    for (uint64_t t = t0; t < cnt; t += stride) {
         uint64_t i = t * pstep;
         sample[t] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], 0.0f);
     }
     const uint32_t S = n < SEED_NN_SAMPLE ? (uint32_t)n : (uint32_t)SEED_NN_SAMPLE;
-    for (uint32_t b = threadIdx.x; b < S; b += blockDim.x) {
+    for (uint32_t b = t0; b < S; b += stride) {
         const uint64_t i = (uint64_t)b * n / S;
         sample[SEED_PCT_POINTS + b] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], 0.0f);
     }
-    if (threadIdx.x == 0) h->n_sample = (uint32_t)cnt;
+    if (t0 == 0) h->n_sample = (uint32_t)cnt;
 }
 
 // Squared 1-NN distance of each of the S sample points p[a] among the other
@@ -523,7 +524,8 @@ rtd_status build_seed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStream
     IndexHeader *h = idx->hdr.as<IndexHeader>();
     RTD_TRY(idx->sample.reserve((SEED_PCT_POINTS + SEED_NN_SAMPLE) * sizeof(float4)));
     RTD_TRY(idx->seed.reserve(SEED_NN_SAMPLE * sizeof(float)));
-    seed_sample_kernel<<<1, 256, 0, st>>>(d_xyz, n, idx->sample.as<float4>(), h);
+    seed_sample_kernel<<<(SEED_NN_SAMPLE + 255) / 256, 256, 0, st>>>(d_xyz, n,
+                                                                    idx->sample.as<float4>(), h);
     RTD_LAUNCH_CHECK();
     idx->nn_seeded = false;
     return RTD_OK;
@@ -565,12 +567,27 @@ rtd_status build_typed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStrea
     const int g = grid_for(n, BLOCK, 148 * 8);
     morton_kernel<K><<<g, BLOCK, 0, st>>>(d_xyz, n, h, scale, idx->keys.as<K>());
     RTD_LAUNCH_CHECK();
-    bool in_alt = false;
     // the last pass gathers the points into idx->pts in key order
-    RTD_TRY(radix_sort_pairs<K>(idx->keys.as<K>(), idx->keys_alt.as<K>(), idx->vals.as<uint32_t>(),
-                                idx->vals_alt.as<uint32_t>(), true, n, 0, kbits, idx->sort, d_err,
-                                st, &in_alt, d_xyz, idx->pts.as<float4>()));
-    K *skeys = in_alt ? idx->keys_alt.as<K>() : idx->keys.as<K>();
+    K *skeys;
+    if (sizeof(K) == 8 && kbits > 32 && kbits <= 48) {
+        // 64-bit keys of up to 48 bits: the low bits as 64-bit keys, then
+        // four passes over the top 32 bits as 32-bit keys
+        RTD_TRY(idx->k32a.reserve(n * sizeof(uint32_t)));
+        RTD_TRY(idx->k32b.reserve(n * sizeof(uint32_t)));
+        RTD_TRY(radix_sort_split64(reinterpret_cast<const uint64_t *>(idx->keys.ptr),
+                                   idx->keys_alt.as<uint64_t>(), idx->k32a.as<uint32_t>(),
+                                   idx->k32b.as<uint32_t>(), idx->vals.as<uint32_t>(),
+                                   idx->vals_alt.as<uint32_t>(), n, kbits, idx->sort, st, d_xyz,
+                                   idx->pts.as<float4>(), idx->keys_alt.as<uint64_t>()));
+        skeys = idx->keys_alt.as<K>();
+    } else {
+        bool in_alt = false;
+        RTD_TRY(radix_sort_pairs<K>(idx->keys.as<K>(), idx->keys_alt.as<K>(),
+                                    idx->vals.as<uint32_t>(), idx->vals_alt.as<uint32_t>(), true, n,
+                                    0, kbits, idx->sort, d_err, st, &in_alt, d_xyz,
+                                    idx->pts.as<float4>()));
+        skeys = in_alt ? idx->keys_alt.as<K>() : idx->keys.as<K>();
+    }
     idx->skeys = skeys;
     idx->mark(EV_BUILD_SORTED, st);
     // the sorted keys are ready: side-stream work may wait on this

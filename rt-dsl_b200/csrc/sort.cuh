@@ -34,6 +34,21 @@ rtd_status radix_sort_pairs(K *keys, K *keys_alt, uint32_t *vals, uint32_t *vals
                             SortScratch &scr, uint32_t *d_err, cudaStream_t stream, bool *in_alt,
                             const float *gather_xyz = nullptr, float4 *gather_out = nullptr);
 
+// Sorts n 64-bit keys of key_bits bits, 32 < key_bits <= 48, with their
+// indices as values (stable): one or two passes over the low key_bits - 32
+// bits move the 64-bit keys, whose last writes the top 32 bits to k32a, and
+// four passes over those 32-bit keys (k32a / k32b) finish the order.  The
+// last pass writes sorted_keys[i] = keys[v] for the i-th sorted index v,
+// and the index itself to *sorted_vals (one of vals / vals_alt) or, with
+// gather_out, the point gather_xyz[v] with v in w (as radix_sort_pairs).
+// keys is not modified; keys_alt is scratch for two low passes; all
+// buffers hold n entries.
+rtd_status radix_sort_split64(const uint64_t *keys, uint64_t *keys_alt, uint32_t *k32a,
+                              uint32_t *k32b, uint32_t *vals, uint32_t *vals_alt, uint64_t n,
+                              int key_bits, SortScratch &scr, cudaStream_t stream,
+                              const float *gather_xyz, float4 *gather_out,
+                              uint64_t *sorted_keys, uint32_t **sorted_vals = nullptr);
+
 // out[i] = sum(in[0..i)), out has n entries; *d_total (device) = sum(in).
 struct ScanScratch {
     DevBuf sums;      // tiles + groups + super groups u64

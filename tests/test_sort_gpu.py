@@ -1,9 +1,12 @@
 """The two device primitives of the index build, through their diagnostic
-entry points: the onesweep radix sort (rtd_radix_sort_pairs) against
-numpy's stable argsort, and the exclusive scan with stream compaction
-(rtd_exclusive_scan) against numpy's cumsum and nonzero.  The sizes cross
-the tile (3,072 keys for the sort, 2,048 entries for the scan) and look-back
-group (32 tiles) boundaries and reach several waves of resident tiles."""
+entry points: the radix sort (rtd_radix_sort_pairs) against numpy's stable
+argsort, and the exclusive scan with stream compaction (rtd_exclusive_scan)
+against numpy's cumsum and nonzero.  64-bit keys of 33 to 48 bits take the
+split sort the index build runs (one or two passes over the low bits, then
+four over the top 32 bits as 32-bit keys); wider ones and 32-bit keys the
+plain passes.  The sizes cross the tile (3,072 keys for the sort, 2,048
+entries for the scan), group (32 tiles) and super-group (1,024 tiles)
+boundaries."""
 import ctypes as C
 
 import numpy as np
@@ -49,7 +52,8 @@ SIZES = [1, 2, 100, SORT_TILE - 1, SORT_TILE, SORT_TILE + 1, GROUP * SORT_TILE -
 
 
 @pytest.mark.parametrize("n", SIZES)
-@pytest.mark.parametrize("dtype,bits", [(np.uint64, 39), (np.uint32, 30)])
+@pytest.mark.parametrize("dtype,bits", [(np.uint64, 39), (np.uint64, 33), (np.uint64, 41),
+                                        (np.uint64, 56), (np.uint32, 30)])
 def test_radix_sort_sizes(rtd, cuda, n, dtype, bits):
     rng = np.random.default_rng(n + bits)
     keys = _keys(rng, n, bits, "uniform", dtype)
