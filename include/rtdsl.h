@@ -60,7 +60,7 @@ typedef enum rtd_radius_heuristic {
     RTD_RADIUS_FIXED = 2,               /* param = radius */
     RTD_RADIUS_SAMPLED_MAX = 3,         /* percentile 1.0 */
     RTD_RADIUS_MORTON_WINDOW = 4        /* no radius rounds: each query's list starts with the
-                                           2k points around it in the index's Morton order and
+                                           4k points around it in the index's Morton order and
                                            one unbounded round follows (thread-per-query search;
                                            elsewhere as RTD_RADIUS_SAMPLED_NN with param) */
 } rtd_radius_heuristic;

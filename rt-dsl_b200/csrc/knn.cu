@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(256) window_pos_kernel(IndexHeader *h, const v
     }
 }
 
-// Seeds a query's list with the 2k points around its position in the
+// Seeds a query's list with the 4k points around its position in the
 // points' Morton order (given in wpos, else found by binary search over the
 // sorted keys); returns that window [w0, w1) of sorted indices.
 template <int KC>
@@ -93,8 +93,8 @@ __device__ __forceinline__ void morton_window_seed(const KnnArgs &p, uint64_t t,
     const uint32_t n = (uint32_t)p.ix.n;
     const uint32_t lo = p.wpos ? p.wpos[t]
                                : morton_position(p.ix.hdr, p.skeys, n, p.key64, p.scale, qx, qy, qz);
-    const uint32_t w = 2u * (uint32_t)kk < n ? 2u * (uint32_t)kk : n;
-    w0 = lo > (uint32_t)kk ? lo - (uint32_t)kk : 0u;
+    const uint32_t w = 4u * (uint32_t)kk < n ? 4u * (uint32_t)kk : n;
+    w0 = lo > w / 2u ? lo - w / 2u : 0u;
     if (w0 + w > n) w0 = n - w;
     w1 = w0 + w;
     for (uint32_t j = w0; j < w1; ++j) {

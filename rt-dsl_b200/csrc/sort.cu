@@ -1,6 +1,7 @@
 // sort.cu -- LSD radix sort of (key, u32 value) pairs and exclusive scan,
 // both as a count kernel and a scatter kernel over fixed tiles (sort.cuh).
 #include "sort.cuh"
+#include "scan.cuh"
 
 namespace rtd {
 
@@ -10,19 +11,6 @@ constexpr int RS_BLOCK = 256;
 constexpr int RS_WARPS = RS_BLOCK / 32;
 constexpr int RS_ITEMS = 12;
 constexpr int RS_TILE = RS_BLOCK * RS_ITEMS;
-
-// Prefix levels of the tile counts: 32 tiles make a group, 32 groups a
-// super group.  A tile's prefix is the sum of at most 31 tile entries, 31
-// group entries and the super-group entries before it, all written by an
-// earlier kernel: no tile waits on another.
-constexpr uint32_t GROUP_TILES = 32;
-constexpr uint32_t SUPER_TILES = GROUP_TILES * 32;
-
-struct Levels {
-    uint64_t tiles, groups, supers;
-    explicit Levels(uint64_t t)
-        : tiles(t), groups(ceil_div(t, GROUP_TILES)), supers(ceil_div(t, SUPER_TILES)) {}
-};
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
@@ -281,142 +269,6 @@ size_t rs_scatter_smem(size_t key_bytes) {
     return RS_TILE * (key_bytes + 4) + (RS_WARPS * 256 + 512 + RS_WARPS + 1) * 4;
 }
 
-// ----------------------------------------------------------------- scan
-constexpr int SC_BLOCK = 256;
-constexpr int SC_ITEMS = 8;
-constexpr int SC_TILE = SC_BLOCK * SC_ITEMS;
-
-// Scan counts: each tile's sum in tsum[tile], added into its group's sum
-// and, with more than one super group, its super group's.
-__global__ void __launch_bounds__(SC_BLOCK) scan_count_kernel(const uint32_t *__restrict__ in,
-                                                              uint64_t n, uint64_t *__restrict__ tsum,
-                                                              unsigned long long *gsum,
-                                                              unsigned long long *ssum, int supers) {
-    __shared__ uint64_t s_warp[SC_BLOCK / 32];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint64_t tile = blockIdx.x, base = tile * SC_TILE;
-    uint64_t sum = 0;
-#pragma unroll
-    for (int i = 0; i < SC_ITEMS; ++i) {
-        const uint64_t idx = base + (uint64_t)i * SC_BLOCK + tid;
-        if (idx < n) sum += in[idx];
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    if (lane == 0) s_warp[warp] = sum;
-    __syncthreads();
-    if (tid == 0) {
-        uint64_t t = 0;
-#pragma unroll
-        for (int w = 0; w < SC_BLOCK / 32; ++w) t += s_warp[w];
-        tsum[tile] = t;
-        if (t) {
-            atomicAdd(&gsum[tile / GROUP_TILES], (unsigned long long)t);
-            if (supers > 1) atomicAdd(&ssum[tile / SUPER_TILES], (unsigned long long)t);
-        }
-    }
-}
-
-// Scan output: out[i] = prefix of the tile (the sums of the earlier tiles
-// of its group, earlier groups of its super group and earlier super groups)
-// + the block's exclusive scan within the tile.  With
-// select != nullptr, also select[out[i]] = i for every i with in[i] != 0
-// (stream compaction of the indices of flagged entries).
-template <typename OutT>
-__global__ void __launch_bounds__(SC_BLOCK) scan_apply_kernel(
-    const uint32_t *__restrict__ in, OutT *__restrict__ out, uint64_t n, OutT *d_total,
-    const uint64_t *__restrict__ tsum, const uint64_t *__restrict__ gsum,
-    const uint64_t *__restrict__ ssum, uint64_t ntiles, uint32_t *select) {
-    __shared__ uint64_t s_io[SC_TILE];
-    __shared__ uint64_t s_warp[SC_BLOCK / 32 + 1];
-    __shared__ uint64_t s_prefix;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint64_t tile = blockIdx.x, base = tile * SC_TILE;
-    if (warp == 0) {
-        // lane j reads tile entry j and group entry j of the levels; the
-        // super groups are strided over the lanes
-        const uint64_t g = tile / GROUP_TILES, s = tile / SUPER_TILES;
-        const uint32_t rt = (uint32_t)(tile % GROUP_TILES), rg = (uint32_t)(g % 32);
-        uint64_t v = 0;
-        if ((uint32_t)lane < rt) v += tsum[g * GROUP_TILES + lane];
-        if ((uint32_t)lane < rg) v += gsum[s * 32 + lane];
-        for (uint64_t j = lane; j < s; j += 32) v += ssum[j];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) s_prefix = v;
-    }
-    for (int i = tid; i < SC_TILE; i += SC_BLOCK) {
-        uint64_t idx = base + i;
-        s_io[i] = idx < n ? (uint64_t)in[idx] : 0ull;
-    }
-    __syncthreads();
-    uint64_t v[SC_ITEMS];
-    uint64_t sum = 0;
-#pragma unroll
-    for (int i = 0; i < SC_ITEMS; ++i) {
-        v[i] = s_io[tid * SC_ITEMS + i];
-        sum += v[i];
-    }
-    // block exclusive scan of 64-bit sums
-    uint64_t x = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) s_warp[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        uint64_t w = lane < SC_BLOCK / 32 ? s_warp[lane] : 0ull;
-        uint64_t iw = w;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint64_t y = __shfl_up_sync(0xffffffffu, iw, o);
-            if (lane >= o) iw += y;
-        }
-        if (lane < SC_BLOCK / 32) s_warp[lane] = iw - w;
-        if (lane == SC_BLOCK / 32 - 1) s_warp[SC_BLOCK / 32] = iw;
-    }
-    __syncthreads();
-    const uint64_t prefix = s_prefix;
-    if (tid == 0 && tile == ntiles - 1 && d_total) *d_total = (OutT)(prefix + s_warp[SC_BLOCK / 32]);
-    uint64_t run = prefix + s_warp[warp] + x - sum;
-#pragma unroll
-    for (int i = 0; i < SC_ITEMS; ++i) {
-        s_io[tid * SC_ITEMS + i] = run;
-        if (select && v[i]) select[run] = (uint32_t)(base + (uint64_t)tid * SC_ITEMS + i);
-        run += v[i];
-    }
-    __syncthreads();
-    for (int i = tid; i < SC_TILE; i += SC_BLOCK) {
-        uint64_t idx = base + i;
-        if (idx < n) out[idx] = (OutT)s_io[i];
-    }
-}
-
-template <typename OutT>
-rtd_status scan_impl(const uint32_t *in, OutT *out, uint64_t n, OutT *d_total, ScanScratch &scr,
-                     cudaStream_t stream, uint32_t *select = nullptr) {
-    if (n == 0) {
-        if (d_total) RTD_CUDA(cudaMemsetAsync(d_total, 0, sizeof(OutT), stream));
-        return RTD_OK;
-    }
-    const Levels L(ceil_div(n, SC_TILE));
-    if (L.tiles >= (1ull << 31)) return fail(RTD_ERR_INVALID_ARGUMENT, "scan: input too large");
-    RTD_TRY(scr.sums.reserve((L.tiles + L.groups + L.supers) * sizeof(uint64_t)));
-    uint64_t *tsum = scr.sums.as<uint64_t>();
-    uint64_t *gsum = tsum + L.tiles, *ssum = gsum + L.groups;
-    RTD_CUDA(cudaMemsetAsync(gsum, 0, (L.groups + L.supers) * sizeof(uint64_t), stream));
-    scan_count_kernel<<<(unsigned)L.tiles, SC_BLOCK, 0, stream>>>(
-        in, n, tsum, reinterpret_cast<unsigned long long *>(gsum),
-        reinterpret_cast<unsigned long long *>(ssum), (int)L.supers);
-    RTD_LAUNCH_CHECK();
-    scan_apply_kernel<OutT><<<(unsigned)L.tiles, SC_BLOCK, 0, stream>>>(
-        in, out, n, d_total, tsum, gsum, ssum, L.tiles, select);
-    RTD_LAUNCH_CHECK();
-    return RTD_OK;
-}
-
 // Count rows for `passes` passes over n keys: every pass's tile rows, then
 // every pass's group and super rows (zeroed together: the count kernels add
 // into them).
@@ -564,18 +416,18 @@ template rtd_status radix_sort_pairs<uint64_t>(uint64_t *, uint64_t *, uint32_t 
 rtd_status exclusive_scan_u32(const uint32_t *in, uint64_t *out, uint64_t n, uint64_t *d_total,
                               ScanScratch &scr, uint32_t *d_err, cudaStream_t stream) {
     (void)d_err;
-    return scan_impl<uint64_t>(in, out, n, d_total, scr, stream);
+    return scan_impl<ArrayIn, uint64_t>(ArrayIn{in}, out, n, d_total, scr, stream);
 }
 rtd_status exclusive_scan_u32_32(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *d_total,
                                  ScanScratch &scr, uint32_t *d_err, cudaStream_t stream) {
     (void)d_err;
-    return scan_impl<uint32_t>(in, out, n, d_total, scr, stream);
+    return scan_impl<ArrayIn, uint32_t>(ArrayIn{in}, out, n, d_total, scr, stream);
 }
 rtd_status exclusive_scan_select_u32(const uint32_t *in, uint32_t *out, uint32_t *select,
                                      uint64_t n, uint32_t *d_total, ScanScratch &scr,
                                      uint32_t *d_err, cudaStream_t stream) {
     (void)d_err;
-    return scan_impl<uint32_t>(in, out, n, d_total, scr, stream, select);
+    return scan_impl<ArrayIn, uint32_t>(ArrayIn{in}, out, n, d_total, scr, stream, select);
 }
 
 }  // namespace rtd

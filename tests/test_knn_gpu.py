@@ -90,7 +90,7 @@ def test_knn_radius_heuristics_do_not_change_results(rtd, orc, cuda, heur, param
 @pytest.mark.parametrize("k", [1, 5, 16, 40])
 @pytest.mark.parametrize("bits", [30, 42, 63])
 def test_knn_morton_window_seed(rtd, orc, cuda, k, bits):
-    """RTD_RADIUS_MORTON_WINDOW: lists seeded with each query's 2k Morton
+    """RTD_RADIUS_MORTON_WINDOW: lists seeded with each query's 4k Morton
     neighbours, then one unbounded round that skips them; ids and keys equal
     the oracle's for every key width, for duplicates, far queries and tiny
     clouds (k = 40 takes the warp path, where the heuristic is the sampled
@@ -103,7 +103,7 @@ def test_knn_morton_window_seed(rtd, orc, cuda, k, bits):
                          leaf_size=8)
     oi, od = orc.knn(pts, q, k)
     assert_same(oi, od, ids, d2)
-    for n in (1, 3, 2 * k + 1):
+    for n in (1, 3, 2 * k + 1, 4 * k + 1):
         ids, d2, _ = gpu_knn(rtd, pts[:n], q[:50], k, radius_heuristic=4, morton_bits=bits)
         oi, od = orc.knn(pts[:n], q[:50], k)
         assert_same(oi, od, ids, d2)
