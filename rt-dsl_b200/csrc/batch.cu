@@ -272,7 +272,7 @@ __host__ __device__ constexpr int k_class(uint32_t k) {
 // Shared memory of one warp, reused by whichever class its current item
 // has: the thread classes' short stacks (SHORT_STACK x 32 entries, one
 // column per lane) or the warp classes' stack, list scratch and rank words.
-constexpr int WARP_SMEM = SHORT_STACK * 32;   // uint2 entries (4 KB)
+constexpr int WARP_SMEM = SHORT_STACK * 32;   // uint2 entries (3 KB)
 static_assert(STACK_MAX + 256 + 16 <= WARP_SMEM, "warp classes fit the thread stacks' space");
 
 __global__ void __launch_bounds__(SWARPS * 32) batch_knn_kernel(const BatchArgs a) {

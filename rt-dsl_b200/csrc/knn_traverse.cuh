@@ -16,7 +16,7 @@
 
 namespace rtd {
 
-constexpr int SHORT_STACK = 16;   // per-thread stack entries kept in shared memory
+constexpr int SHORT_STACK = 12;   // per-thread stack entries kept in shared memory
 constexpr int STACK_MAX = 104;    // >= maximal tree depth (63 key bits + 32 index bits)
 
 // One tree to search: a whole index, or one cloud's subtree of a forest.

@@ -136,6 +136,25 @@ __global__ void __launch_bounds__(RS_BLOCK) rs_count_kernel(const K *__restrict_
     }
 }
 
+// Values of the split sort with the low key bits packed above the index:
+// with bits != 0, the first pass makes v = index | (key & low_mask) << bits
+// (index < 2^bits), and the last pass takes the index and rebuilds the full
+// key (top << low) | (v >> bits) without reading the keys again.  With
+// bits = 0 values are plain indices.
+struct ValuePack {
+    uint32_t bits = 0, low = 0;
+    uint64_t low_mask = 0;
+    __device__ __forceinline__ uint32_t make(uint64_t idx, uint64_t key) const {
+        return bits ? (uint32_t)idx | ((uint32_t)(key & low_mask) << bits) : (uint32_t)idx;
+    }
+    __device__ __forceinline__ uint32_t index(uint32_t v) const {
+        return bits ? v & ((1u << bits) - 1u) : v;
+    }
+    __device__ __forceinline__ uint64_t key(uint64_t top, uint32_t v) const {
+        return (top << low) | (uint64_t)(v >> bits);
+    }
+};
+
 // Scatter of one pass over 8 bits at `shift`: the tile's keys are ranked
 // in registers (stable: warp, item, lane order), staged in shared memory
 // grouped by digit, and each digit run is written contiguously from the
@@ -152,7 +171,7 @@ __global__ void __launch_bounds__(RS_BLOCK) rs_scatter_kernel(
     const uint32_t *__restrict__ gsum, const uint32_t *__restrict__ ssum, uint32_t groups,
     uint32_t supers, const float *__restrict__ gxyz, float4 *__restrict__ gout,
     uint32_t *__restrict__ kout32, int shift32, const uint64_t *__restrict__ gk_in,
-    uint64_t *__restrict__ gk_out) {
+    uint64_t *__restrict__ gk_out, const ValuePack pk) {
     extern __shared__ __align__(16) unsigned char rs_smem[];
     K *s_keys = reinterpret_cast<K *>(rs_smem);
     uint32_t *s_vals = reinterpret_cast<uint32_t *>(s_keys + RS_TILE);
@@ -174,7 +193,7 @@ __global__ void __launch_bounds__(RS_BLOCK) rs_scatter_kernel(
         const uint64_t idx = wbase + (uint64_t)i * 32 + lane;
         const bool ok = idx < n;
         key[i] = ok ? kin[idx] : ~K(0);
-        val[i] = ok ? (vin ? vin[idx] : (uint32_t)idx) : 0u;
+        val[i] = ok ? (vin ? vin[idx] : pk.make(idx, (uint64_t)key[i])) : 0u;
     }
     const uint32_t d = (uint32_t)tid;
     uint32_t before, total;
@@ -232,12 +251,13 @@ __global__ void __launch_bounds__(RS_BLOCK) rs_scatter_kernel(
                 const uint32_t jj = j < valid ? j : j0;   // a repeat of slot j0: not stored
                 const K k = s_keys[jj];
                 dst[u] = s_base[(uint32_t)(k >> shift) & 255u] + jj;
-                v[u] = s_vals[jj];
+                const uint32_t w = s_vals[jj];
+                v[u] = pk.index(w);
                 const uint64_t o = v[u];
                 x[u] = gxyz[3 * o];
                 y[u] = gxyz[3 * o + 1];
                 z[u] = gxyz[3 * o + 2];
-                gk[u] = gk_out ? gk_in[o] : 0ull;
+                gk[u] = !gk_out ? 0ull : pk.bits ? pk.key((uint64_t)k, w) : gk_in[o];
                 if (j < valid) {
                     if (kout) kout[dst[u]] = k;
                     if (kout32) kout32[dst[u]] = (uint32_t)((uint64_t)k >> shift32);
@@ -259,9 +279,14 @@ __global__ void __launch_bounds__(RS_BLOCK) rs_scatter_kernel(
         const uint32_t dst = s_base[dj] + j;
         if (kout) kout[dst] = k;
         if (kout32) kout32[dst] = (uint32_t)((uint64_t)k >> shift32);
-        const uint32_t v = s_vals[j];
-        if (gk_out) gk_out[dst] = gk_in[v];
-        vout[dst] = v;
+        const uint32_t w = s_vals[j];
+        if (gk_out) {   // the last pass: full keys, values unpacked
+            const uint32_t v = pk.index(w);
+            gk_out[dst] = pk.bits ? pk.key((uint64_t)k, w) : gk_in[v];
+            vout[dst] = v;
+        } else {
+            vout[dst] = w;
+        }
     }
 }
 
@@ -295,6 +320,7 @@ template <typename K> struct PassOut {
     float4 *gout = nullptr;
     const uint64_t *gk_in = nullptr;
     uint64_t *gk_out = nullptr;
+    ValuePack pk;
 };
 
 // Count + scatter of pass p (its count rows) over bits [shift, shift + 8).
@@ -313,7 +339,7 @@ rtd_status run_pass(const PassRows &R, int p, const K *kin, const uint32_t *vin,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     rs_scatter_kernel<K><<<(unsigned)L.tiles, RS_BLOCK, smem, stream>>>(
         kin, o.kout, vin, vout, n, shift, tcount, gsum, ssum, (uint32_t)L.groups,
-        (uint32_t)L.supers, o.gxyz, o.gout, o.kout32, o.shift32, o.gk_in, o.gk_out);
+        (uint32_t)L.supers, o.gxyz, o.gout, o.kout32, o.shift32, o.gk_in, o.gk_out, o.pk);
     RTD_LAUNCH_CHECK();
     return RTD_OK;
 }
@@ -364,6 +390,15 @@ rtd_status radix_sort_split64(const uint64_t *keys, uint64_t *keys_alt, uint32_t
         return fail(RTD_ERR_INVALID_ARGUMENT, "split radix sort: key_bits must be in (32, 48]");
     const int low = key_bits - 32;          // bits [0, low) sort as 64-bit keys
     const int lp = (low + 7) / 8;           // 1 or 2 passes
+    // the low key bits ride above the index in the values when they fit
+    ValuePack pk;
+    uint32_t ib = 1;
+    while (ib < 32 && (1ull << ib) < n) ++ib;
+    if (ib + (uint32_t)low <= 32) {
+        pk.bits = ib;
+        pk.low = (uint32_t)low;
+        pk.low_mask = (1ull << low) - 1ull;
+    }
     PassRows R(n);
     RTD_TRY(R.reserve(scr, lp + 4, stream));
     const uint32_t *vin = nullptr;          // pass 0: values 0..n-1 on the fly
@@ -372,6 +407,7 @@ rtd_status radix_sort_split64(const uint64_t *keys, uint64_t *keys_alt, uint32_t
     const uint64_t *kin = keys;
     for (int p = 0; p < lp; ++p) {
         PassOut<uint64_t> o;
+        if (p == 0) o.pk = pk;   // makes the values
         if (p == lp - 1) {
             o.kout32 = k32a;
             o.shift32 = low;
@@ -392,6 +428,7 @@ rtd_status radix_sort_split64(const uint64_t *keys, uint64_t *keys_alt, uint32_t
             o.gout = gather_out;
             o.gk_in = keys;
             o.gk_out = sorted_keys;
+            o.pk = pk;   // unpacks the values, rebuilds the keys
         } else {
             o.kout = k32out;
         }
