@@ -12,6 +12,9 @@ namespace {
 
 constexpr int BLOCK = 256;
 
+// Whether a device array can be read as float4.
+inline int aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0 ? 1 : 0; }
+
 __global__ void hdr_init_kernel(IndexHeader *h) {
     h->root = CHILD_NONE;
     h->root_count = 0;
@@ -28,12 +31,37 @@ __global__ void hdr_init_kernel(IndexHeader *h) {
     h->n_sample = 0;
 }
 
-// Scene box, NaN-ignoring (fminf/fmaxf), as order-preserving atomics.
+// Points 4g .. 4g+3 of a 16-byte aligned xyz array: three float4 loads.
+__device__ __forceinline__ void load_point4(const float *__restrict__ xyz, uint64_t g,
+                                            float (&x)[4], float (&y)[4], float (&z)[4]) {
+    const float4 *p = reinterpret_cast<const float4 *>(xyz) + 3 * g;
+    const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+    x[0] = a.x; y[0] = a.y; z[0] = a.z;
+    x[1] = a.w; y[1] = b.x; z[1] = b.y;
+    x[2] = b.z; y[2] = b.w; z[2] = c.x;
+    x[3] = c.y; y[3] = c.z; z[3] = c.w;
+}
+
+// Scene box, NaN-ignoring (fminf/fmaxf), as order-preserving atomics.  With
+// vec4 (a 16-byte aligned array) whole groups of 4 points are read as three
+// float4 each; the last n % 4 points, or all of them without vec4, one
+// coordinate at a time.
 __global__ void __launch_bounds__(BLOCK) bbox_kernel(const float *__restrict__ xyz, uint64_t n,
-                                                     IndexHeader *h) {
+                                                     IndexHeader *h, int vec4) {
     float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    for (uint64_t i = (uint64_t)blockIdx.x * BLOCK + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x * BLOCK) {
+    const uint64_t t0 = (uint64_t)blockIdx.x * BLOCK + threadIdx.x, stride = (uint64_t)gridDim.x * BLOCK;
+    const uint64_t groups = vec4 ? n / 4 : 0;
+    for (uint64_t g = t0; g < groups; g += stride) {
+        float x[4], y[4], z[4];
+        load_point4(xyz, g, x, y, z);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            lo[0] = fminf(lo[0], x[u]); hi[0] = fmaxf(hi[0], x[u]);
+            lo[1] = fminf(lo[1], y[u]); hi[1] = fmaxf(hi[1], y[u]);
+            lo[2] = fminf(lo[2], z[u]); hi[2] = fmaxf(hi[2], z[u]);
+        }
+    }
+    for (uint64_t i = 4 * groups + t0; i < n; i += stride) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             float v = xyz[3 * i + a];
@@ -65,23 +93,32 @@ __global__ void __launch_bounds__(BLOCK) bbox_kernel(const float *__restrict__ x
 // extent per axis; wider codes (B = bits / 3 per axis, scale = 2^B - 1,
 // B <= 21, interleaved in the low 3B bits of a u64) use one cubic extent.
 template <typename K>
+__device__ __forceinline__ K morton_key(const SceneNorm &s, float scale, float x, float y, float z) {
+    if (sizeof(K) == 4)
+        return (K)morton30(quantize(x, s.lo[0], s.ext[0], 1023.0f),
+                           quantize(y, s.lo[1], s.ext[1], 1023.0f),
+                           quantize(z, s.lo[2], s.ext[2], 1023.0f));
+    return (K)morton63(quantize(x, s.lo[0], s.ext[0], scale), quantize(y, s.lo[1], s.ext[1], scale),
+                       quantize(z, s.lo[2], s.ext[2], scale));
+}
+
+// Keys of the points; with vec4 (as bbox_kernel) whole groups of 4 points
+// are read as three float4 each.
+template <typename K>
 __global__ void __launch_bounds__(BLOCK) morton_kernel(const float *__restrict__ xyz, uint64_t n,
                                                        const IndexHeader *h, float scale,
-                                                       K *__restrict__ keys) {
+                                                       K *__restrict__ keys, int vec4) {
     const SceneNorm s = sizeof(K) == 4 ? scene_norm(h) : scene_norm_cubic(h);
-    for (uint64_t i = (uint64_t)blockIdx.x * BLOCK + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x * BLOCK) {
-        float x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
-        if (sizeof(K) == 4) {
-            keys[i] = (K)morton30(quantize(x, s.lo[0], s.ext[0], 1023.0f),
-                                  quantize(y, s.lo[1], s.ext[1], 1023.0f),
-                                  quantize(z, s.lo[2], s.ext[2], 1023.0f));
-        } else {
-            keys[i] = (K)morton63(quantize(x, s.lo[0], s.ext[0], scale),
-                                  quantize(y, s.lo[1], s.ext[1], scale),
-                                  quantize(z, s.lo[2], s.ext[2], scale));
-        }
+    const uint64_t t0 = (uint64_t)blockIdx.x * BLOCK + threadIdx.x, stride = (uint64_t)gridDim.x * BLOCK;
+    const uint64_t groups = vec4 ? n / 4 : 0;
+    for (uint64_t g = t0; g < groups; g += stride) {
+        float x[4], y[4], z[4];
+        load_point4(xyz, g, x, y, z);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) keys[4 * g + u] = morton_key<K>(s, scale, x[u], y[u], z[u]);
     }
+    for (uint64_t i = 4 * groups + t0; i < n; i += stride)
+        keys[i] = morton_key<K>(s, scale, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
 }
 
 // Common-prefix length of sorted keys i and j (ki = keys[i]), ties broken
@@ -113,15 +150,35 @@ __device__ __forceinline__ void karras_dir(const K *__restrict__ keys, int64_t n
 // split searches run afterwards for the kept nodes alone, packed densely by
 // the scan of these flags (node_kernel), so no warp carries idle lanes of
 // collapsed nodes through them.
+// A block takes FLAG_TILE consecutive nodes and first stages their keys
+// with a halo of leaf_size + 1 on each side in shared memory (one
+// coalesced read), so that the four keys of each test come from there.
+constexpr int FLAG_TILE = 2048;
+constexpr int FLAG_HALO = 65;   // leaf_size (<= 64) + 1
 template <typename K>
 __global__ void __launch_bounds__(BLOCK) karras_flag_kernel(const K *__restrict__ keys, int64_t n,
                                                             uint32_t leaf_size, uint32_t *flags) {
-    for (int64_t i = (int64_t)blockIdx.x * BLOCK + threadIdx.x; i < n - 1;
-         i += (int64_t)gridDim.x * BLOCK) {
-        const K ki = keys[i];
-        int dir, dmin;
-        karras_dir(keys, n, ki, i, dir, dmin);
-        flags[i] = delta(keys, n, ki, i, i + (int64_t)leaf_size * dir) > dmin ? 1u : 0u;
+    __shared__ K s_k[FLAG_TILE + 2 * FLAG_HALO];
+    const int64_t b0 = (int64_t)blockIdx.x * FLAG_TILE, base = b0 - FLAG_HALO;
+    for (int t = threadIdx.x; t < FLAG_TILE + 2 * FLAG_HALO; t += BLOCK) {
+        const int64_t j = base + t;
+        if (j >= 0 && j < n) s_k[t] = keys[j];
+    }
+    __syncthreads();
+    // delta on the staged keys (j within the halo whenever j is in [0, n))
+    auto dl = [&](K ki, int64_t i, int64_t j) -> int {
+        if (j < 0 || j >= n) return -1;
+        const K b = s_k[j - base];
+        if (ki == b) return (int)(8 * sizeof(K)) + __clz((uint32_t)(i ^ j));
+        return sizeof(K) == 8 ? __clzll((unsigned long long)(ki ^ b)) : __clz((uint32_t)(ki ^ b));
+    };
+    for (int t = threadIdx.x; t < FLAG_TILE; t += BLOCK) {
+        const int64_t i = b0 + t;
+        if (i >= n - 1) break;
+        const K ki = s_k[i - base];
+        const int dir = (dl(ki, i, i + 1) - dl(ki, i, i - 1)) >= 0 ? 1 : -1;
+        const int dmin = dl(ki, i, i - dir);
+        flags[i] = dl(ki, i, i + (int64_t)leaf_size * dir) > dmin ? 1u : 0u;
     }
 }
 
@@ -565,7 +622,8 @@ rtd_status build_typed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStrea
     RTD_TRY(idx->vals.reserve(n * sizeof(uint32_t)));
     RTD_TRY(idx->vals_alt.reserve(n * sizeof(uint32_t)));
     const int g = grid_for(n, BLOCK, 148 * 8);
-    morton_kernel<K><<<g, BLOCK, 0, st>>>(d_xyz, n, h, scale, idx->keys.as<K>());
+    morton_kernel<K><<<g, BLOCK, 0, st>>>(d_xyz, n, h, scale, idx->keys.as<K>(),
+                                           aligned16(d_xyz));
     RTD_LAUNCH_CHECK();
     // the last pass gathers the points into idx->pts in key order
     K *skeys;
@@ -646,7 +704,7 @@ rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStr
         pe = cudaGetLastError();
     }
     RTD_CUDA(cudaEventRecord(idx->ev_tree_join, ts));
-    const int gi = grid_for(ni, BLOCK, 148 * 8);
+    const unsigned gi = (unsigned)ceil_div(ni, (uint64_t)FLAG_TILE);
     karras_flag_kernel<K><<<gi, BLOCK, 0, st>>>(skeys, (int64_t)n, idx->leaf_size,
                                                 idx->flags.as<uint32_t>());
     note_launch();
@@ -720,7 +778,7 @@ rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd
     hdr_init_kernel<<<1, 1, 0, st>>>(h);
     RTD_LAUNCH_CHECK();
     if (n > 0) {
-        bbox_kernel<<<grid_for(n, BLOCK, 148 * 4), BLOCK, 0, st>>>(d_xyz, n, h);
+        bbox_kernel<<<grid_for(n, BLOCK, 148 * 4), BLOCK, 0, st>>>(d_xyz, n, h, aligned16(d_xyz));
         RTD_LAUNCH_CHECK();
         // the radius-seed sample reads only the input points: it runs on the
         // side stream while the keys are made and sorted
@@ -799,7 +857,7 @@ rtd_status order_queries_own(QueryOrderScratch &qs, const float *d_q, uint64_t n
     IndexHeader *h = qs.hdr.as<IndexHeader>();
     hdr_init_kernel<<<1, 1, 0, st>>>(h);
     RTD_LAUNCH_CHECK();
-    bbox_kernel<<<grid_for(nq, BLOCK, 148 * 4), BLOCK, 0, st>>>(d_q, nq, h);
+    bbox_kernel<<<grid_for(nq, BLOCK, 148 * 4), BLOCK, 0, st>>>(d_q, nq, h, aligned16(d_q));
     RTD_LAUNCH_CHECK();
     int cbits = 0;
     while ((1u << cbits) < chunks) ++cbits;
