@@ -6,6 +6,7 @@
 #include <stdint.h>
 #include <string.h>
 #include <string>
+#include <utility>
 
 #include "rtdsl.h"
 
@@ -35,6 +36,38 @@ void note_launch();
     do {                                                                \
         rtd_status s_ = (call);                                         \
         if (s_ != RTD_OK) return s_;                                    \
+    } while (0)
+
+// ------------------------------------------------------- chained launches
+// The kernels of one dependent chain (the index build, the search) launch
+// with programmatic stream serialization: a kernel's blocks may be
+// scheduled while the previous kernel in the stream finishes, and wait in
+// chain_wait() (griddepcontrol.wait) until that kernel has completed and
+// its writes are visible.  A kernel launched this way calls chain_wait()
+// before it reads or writes anything; launched the plain way, the wait
+// returns at once.
+__device__ __forceinline__ void chain_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                  cudaStream_t st, Args &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+#define RTD_LAUNCH_CHAINED(kernel, grid, block, smem, st, ...)                           \
+    do {                                                                                \
+        ::rtd::note_launch();                                                           \
+        cudaError_t e_ = ::rtd::launch_chained(kernel, grid, block, smem, st, __VA_ARGS__); \
+        if (e_ != cudaSuccess) return ::rtd::cuda_fail(e_, "kernel launch");           \
     } while (0)
 
 // Device-side error flags (bit mask), written by kernels whose bounded

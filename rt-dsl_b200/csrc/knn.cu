@@ -109,6 +109,7 @@ __device__ __forceinline__ void morton_window_seed(const KnnArgs &p, uint64_t t,
 // SM (48 registers a thread); longer lists take the registers they need.
 template <int KC, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, KC <= 5 ? 1280 / BLOCK : 0) knn_thread_kernel(const KnnArgs p) {
+    chain_wait();
     __shared__ BvhNode s_top[TOP_MAX];
     __shared__ uint2 s_stack[SHORT_STACK][BLOCK];
     const IndexHeader *h = p.ix.hdr;
@@ -303,13 +304,15 @@ __global__ void seed_set_kernel(IndexHeader *h, int mode, float param) {
 template <int KC>
 rtd_status launch_thread(const KnnArgs &a, uint32_t block, cudaStream_t st) {
     if (block == 256) {
-        knn_thread_kernel<KC, 256><<<grid_for(a.nq, 256, 1 << 20), 256, 0, st>>>(a);
+        RTD_LAUNCH_CHAINED((knn_thread_kernel<KC, 256>), dim3(grid_for(a.nq, 256, 1 << 20)), dim3(256),
+                           0, st, a);
     } else if (block == 64) {
-        knn_thread_kernel<KC, 64><<<grid_for(a.nq, 64, 1 << 20), 64, 0, st>>>(a);
+        RTD_LAUNCH_CHAINED((knn_thread_kernel<KC, 64>), dim3(grid_for(a.nq, 64, 1 << 20)), dim3(64),
+                           0, st, a);
     } else {
-        knn_thread_kernel<KC, 128><<<grid_for(a.nq, 128, 1 << 20), 128, 0, st>>>(a);
+        RTD_LAUNCH_CHAINED((knn_thread_kernel<KC, 128>), dim3(grid_for(a.nq, 128, 1 << 20)), dim3(128),
+                           0, st, a);
     }
-    RTD_LAUNCH_CHECK();
     return RTD_OK;
 }
 

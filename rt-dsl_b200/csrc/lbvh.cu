@@ -16,6 +16,7 @@ constexpr int BLOCK = 256;
 inline int aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0 ? 1 : 0; }
 
 __global__ void hdr_init_kernel(IndexHeader *h) {
+    chain_wait();
     h->root = CHILD_NONE;
     h->root_count = 0;
     h->n_internal = 0;
@@ -48,6 +49,7 @@ __device__ __forceinline__ void load_point4(const float *__restrict__ xyz, uint6
 // coordinate at a time.
 __global__ void __launch_bounds__(BLOCK) bbox_kernel(const float *__restrict__ xyz, uint64_t n,
                                                      IndexHeader *h, int vec4) {
+    chain_wait();
     float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
     const uint64_t t0 = (uint64_t)blockIdx.x * BLOCK + threadIdx.x, stride = (uint64_t)gridDim.x * BLOCK;
     const uint64_t groups = vec4 ? n / 4 : 0;
@@ -108,6 +110,7 @@ template <typename K>
 __global__ void __launch_bounds__(BLOCK) morton_kernel(const float *__restrict__ xyz, uint64_t n,
                                                        const IndexHeader *h, float scale,
                                                        K *__restrict__ keys, int vec4) {
+    chain_wait();
     const SceneNorm s = sizeof(K) == 4 ? scene_norm(h) : scene_norm_cubic(h);
     const uint64_t t0 = (uint64_t)blockIdx.x * BLOCK + threadIdx.x, stride = (uint64_t)gridDim.x * BLOCK;
     const uint64_t groups = vec4 ? n / 4 : 0;
@@ -158,6 +161,7 @@ constexpr int FLAG_HALO = 65;   // leaf_size (<= 64) + 1
 template <typename K>
 __global__ void __launch_bounds__(BLOCK) karras_flag_kernel(const K *__restrict__ keys, int64_t n,
                                                             uint32_t leaf_size, uint32_t *flags) {
+    chain_wait();
     __shared__ K s_k[FLAG_TILE + 2 * FLAG_HALO];
     const int64_t b0 = (int64_t)blockIdx.x * FLAG_TILE, base = b0 - FLAG_HALO;
     for (int t = threadIdx.x; t < FLAG_TILE + 2 * FLAG_HALO; t += BLOCK) {
@@ -398,6 +402,7 @@ __global__ void __launch_bounds__(BLOCK) node_kernel(
     const K *__restrict__ keys, uint64_t n, const IndexHeader *h, const uint32_t *__restrict__ sel,
     const uint32_t *__restrict__ cidx, uint32_t leaf_size, const Pyramid P, BvhNode *nodes,
     uint32_t *kfirst, uint32_t *klast) {
+    chain_wait();
     const uint32_t n_int = h->n_internal;
     for (uint32_t c = blockIdx.x * BLOCK + threadIdx.x; c < n_int && c + 1 < n;
          c += gridDim.x * BLOCK) {
@@ -434,6 +439,7 @@ __global__ void __launch_bounds__(32) stage_top_kernel(IndexHeader *h,
                                                        const BvhNode *__restrict__ nodes,
                                                        BvhNode *top, uint64_t n,
                                                        uint32_t leaf_size) {
+    chain_wait();
     const int lane = threadIdx.x;
     if (n == 0 || n == 1 || n <= leaf_size) {
         if (lane == 0) {
@@ -622,9 +628,8 @@ rtd_status build_typed(rtd_index *idx, const float *d_xyz, uint64_t n, cudaStrea
     RTD_TRY(idx->vals.reserve(n * sizeof(uint32_t)));
     RTD_TRY(idx->vals_alt.reserve(n * sizeof(uint32_t)));
     const int g = grid_for(n, BLOCK, 148 * 8);
-    morton_kernel<K><<<g, BLOCK, 0, st>>>(d_xyz, n, h, scale, idx->keys.as<K>(),
-                                           aligned16(d_xyz));
-    RTD_LAUNCH_CHECK();
+    RTD_LAUNCH_CHAINED(morton_kernel<K>, dim3(g), dim3(BLOCK), 0, st, d_xyz, n,
+                       (const IndexHeader *)h, scale, idx->keys.as<K>(), aligned16(d_xyz));
     // the last pass gathers the points into idx->pts in key order
     K *skeys;
     if (sizeof(K) == 8 && kbits > 32 && kbits <= 48) {
@@ -705,10 +710,9 @@ rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStr
     }
     RTD_CUDA(cudaEventRecord(idx->ev_tree_join, ts));
     const unsigned gi = (unsigned)ceil_div(ni, (uint64_t)FLAG_TILE);
-    karras_flag_kernel<K><<<gi, BLOCK, 0, st>>>(skeys, (int64_t)n, idx->leaf_size,
-                                                idx->flags.as<uint32_t>());
     note_launch();
-    cudaError_t fe = cudaGetLastError();
+    cudaError_t fe = launch_chained(karras_flag_kernel<K>, dim3(gi), dim3(BLOCK), 0, st, skeys,
+                                    (int64_t)n, idx->leaf_size, idx->flags.as<uint32_t>());
     const rtd_status sr =
         fe != cudaSuccess ? RTD_OK
                           : exclusive_scan_select_u32(idx->flags.as<uint32_t>(), idx->cidx.as<uint32_t>(),
@@ -722,11 +726,11 @@ rtd_status build_tree_sorted(rtd_index *idx, const K *skeys, uint64_t n, cudaStr
     // tree; the kernel strides over however many there are (up to
     // n - 1 - leaf_size in a chain-shaped tree)
     const uint64_t kept_max = ni / idx->leaf_size + 1 < ni ? ni / idx->leaf_size + 1 : ni;
-    node_kernel<K><<<grid_for(kept_max, BLOCK, 148 * 8), BLOCK, 0, st>>>(
-        skeys, n, h, idx->csel.as<uint32_t>(), idx->cidx.as<uint32_t>(), idx->leaf_size, P,
-        idx->nodes.as<BvhNode>(), ranges ? idx->kfirst.as<uint32_t>() : nullptr,
-        ranges ? idx->klast.as<uint32_t>() : nullptr);
-    RTD_LAUNCH_CHECK();
+    RTD_LAUNCH_CHAINED(node_kernel<K>, dim3(grid_for(kept_max, BLOCK, 148 * 8)), dim3(BLOCK), 0, st,
+                       skeys, n, (const IndexHeader *)h, (const uint32_t *)idx->csel.as<uint32_t>(),
+                       (const uint32_t *)idx->cidx.as<uint32_t>(), idx->leaf_size, P,
+                       idx->nodes.as<BvhNode>(), ranges ? idx->kfirst.as<uint32_t>() : nullptr,
+                       ranges ? idx->klast.as<uint32_t>() : nullptr);
     return RTD_OK;
 }
 
@@ -775,11 +779,10 @@ rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd
     IndexHeader *h = idx->hdr.as<IndexHeader>();
     for (bool &e : idx->ev_set) e = false;
     idx->mark(EV_BUILD0, st);
-    hdr_init_kernel<<<1, 1, 0, st>>>(h);
-    RTD_LAUNCH_CHECK();
+    RTD_LAUNCH_CHAINED(hdr_init_kernel, dim3(1), dim3(1), 0, st, h);
     if (n > 0) {
-        bbox_kernel<<<grid_for(n, BLOCK, 148 * 4), BLOCK, 0, st>>>(d_xyz, n, h, aligned16(d_xyz));
-        RTD_LAUNCH_CHECK();
+        RTD_LAUNCH_CHAINED(bbox_kernel, dim3(grid_for(n, BLOCK, 148 * 4)), dim3(BLOCK), 0, st, d_xyz,
+                           n, h, aligned16(d_xyz));
         // the radius-seed sample reads only the input points: it runs on the
         // side stream while the keys are made and sorted
         RTD_TRY(ensure_side_stream(idx));
@@ -793,9 +796,9 @@ rtd_status index_build(rtd_index *idx, const float *d_xyz, uint64_t n, const rtd
         RTD_TRY(rs);
         RTD_TRY(rb);
     }
-    stage_top_kernel<<<1, 32, 0, st>>>(h, idx->nodes.as<BvhNode>(), idx->top.as<BvhNode>(), n,
-                                      idx->leaf_size);
-    RTD_LAUNCH_CHECK();
+    RTD_LAUNCH_CHAINED(stage_top_kernel, dim3(1), dim3(32), 0, st, h,
+                       (const BvhNode *)idx->nodes.as<BvhNode>(), idx->top.as<BvhNode>(), n,
+                       idx->leaf_size);
     idx->mark(EV_BUILD1, st);
     return RTD_OK;
 }

@@ -43,6 +43,7 @@ __global__ void __launch_bounds__(SC_BLOCK) scan_count_kernel(const In in, uint6
                                                               uint64_t *__restrict__ tsum,
                                                               unsigned long long *gsum,
                                                               unsigned long long *ssum, int supers) {
+    chain_wait();
     __shared__ uint64_t s_warp[SC_BLOCK / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint64_t tile = blockIdx.x, base = tile * SC_TILE;
@@ -78,6 +79,7 @@ __global__ void __launch_bounds__(SC_BLOCK) scan_apply_kernel(
     const In in, OutT *__restrict__ out, uint64_t n, OutT *d_total,
     const uint64_t *__restrict__ tsum, const uint64_t *__restrict__ gsum,
     const uint64_t *__restrict__ ssum, uint64_t ntiles, uint32_t *select) {
+    chain_wait();
     __shared__ uint64_t s_io[SC_TILE];
     __shared__ uint64_t s_warp[SC_BLOCK / 32 + 1];
     __shared__ uint64_t s_prefix;
@@ -160,13 +162,12 @@ rtd_status scan_impl(const In in, OutT *out, uint64_t n, OutT *d_total, ScanScra
     uint64_t *tsum = scr.sums.as<uint64_t>();
     uint64_t *gsum = tsum + L.tiles, *ssum = gsum + L.groups;
     RTD_CUDA(cudaMemsetAsync(gsum, 0, (L.groups + L.supers) * sizeof(uint64_t), stream));
-    scan_count_kernel<In><<<(unsigned)L.tiles, SC_BLOCK, 0, stream>>>(
-        in, n, tsum, reinterpret_cast<unsigned long long *>(gsum),
-        reinterpret_cast<unsigned long long *>(ssum), (int)L.supers);
-    RTD_LAUNCH_CHECK();
-    scan_apply_kernel<In, OutT><<<(unsigned)L.tiles, SC_BLOCK, 0, stream>>>(
-        in, out, n, d_total, tsum, gsum, ssum, L.tiles, select);
-    RTD_LAUNCH_CHECK();
+    RTD_LAUNCH_CHAINED(scan_count_kernel<In>, dim3((unsigned)L.tiles), dim3(SC_BLOCK), 0, stream, in,
+                       n, tsum, reinterpret_cast<unsigned long long *>(gsum),
+                       reinterpret_cast<unsigned long long *>(ssum), (int)L.supers);
+    RTD_LAUNCH_CHAINED((scan_apply_kernel<In, OutT>), dim3((unsigned)L.tiles), dim3(SC_BLOCK), 0,
+                       stream, in, out, n, d_total, (const uint64_t *)tsum, (const uint64_t *)gsum,
+                       (const uint64_t *)ssum, L.tiles, select);
     return RTD_OK;
 }
 

@@ -105,6 +105,7 @@ __global__ void __launch_bounds__(RS_BLOCK) rs_count_kernel(const K *__restrict_
                                                             int shift, uint32_t *__restrict__ tcount,
                                                             uint32_t *gsum, uint32_t *ssum,
                                                             int supers) {
+    chain_wait();
     __shared__ uint32_t s_wh[RS_WARPS][256];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int i = tid; i < RS_WARPS * 256; i += RS_BLOCK) (&s_wh[0][0])[i] = 0;
@@ -172,6 +173,7 @@ __global__ void __launch_bounds__(RS_BLOCK) rs_scatter_kernel(
     uint32_t supers, const float *__restrict__ gxyz, float4 *__restrict__ gout,
     uint32_t *__restrict__ kout32, int shift32, const uint64_t *__restrict__ gk_in,
     uint64_t *__restrict__ gk_out, const ValuePack pk) {
+    chain_wait();
     extern __shared__ __align__(16) unsigned char rs_smem[];
     K *s_keys = reinterpret_cast<K *>(rs_smem);
     uint32_t *s_vals = reinterpret_cast<uint32_t *>(s_keys + RS_TILE);
@@ -331,16 +333,15 @@ rtd_status run_pass(const PassRows &R, int p, const K *kin, const uint32_t *vin,
     uint32_t *tcount = R.tc + (size_t)p * L.tiles * 256;
     uint32_t *gsum = R.sc + (size_t)p * (L.groups + L.supers) * 256;
     uint32_t *ssum = gsum + L.groups * 256;
-    rs_count_kernel<K><<<(unsigned)L.tiles, RS_BLOCK, 0, stream>>>(kin, n, shift, tcount, gsum,
-                                                                    ssum, (int)L.supers);
-    RTD_LAUNCH_CHECK();
+    RTD_LAUNCH_CHAINED(rs_count_kernel<K>, dim3((unsigned)L.tiles), dim3(RS_BLOCK), 0, stream, kin,
+                       n, shift, tcount, gsum, ssum, (int)L.supers);
     const size_t smem = rs_scatter_smem(sizeof(K));
     RTD_CUDA(cudaFuncSetAttribute(rs_scatter_kernel<K>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    rs_scatter_kernel<K><<<(unsigned)L.tiles, RS_BLOCK, smem, stream>>>(
-        kin, o.kout, vin, vout, n, shift, tcount, gsum, ssum, (uint32_t)L.groups,
-        (uint32_t)L.supers, o.gxyz, o.gout, o.kout32, o.shift32, o.gk_in, o.gk_out, o.pk);
-    RTD_LAUNCH_CHECK();
+    RTD_LAUNCH_CHAINED(rs_scatter_kernel<K>, dim3((unsigned)L.tiles), dim3(RS_BLOCK), smem, stream,
+                       kin, o.kout, vin, vout, n, shift, tcount, gsum, ssum, (uint32_t)L.groups,
+                       (uint32_t)L.supers, o.gxyz, o.gout, o.kout32, o.shift32, o.gk_in, o.gk_out,
+                       o.pk);
     return RTD_OK;
 }
 
