@@ -308,7 +308,7 @@ struct PassRows {
         RTD_TRY(scr.counts.reserve((trows + srows) * 256 * sizeof(uint32_t)));
         tc = scr.counts.as<uint32_t>();
         sc = tc + trows * 256;
-        RTD_CUDA(cudaMemsetAsync(sc, 0, srows * 256 * 4, stream));
+        RTD_TRY(zero_words(sc, srows * 256, stream));
         return RTD_OK;
     }
 };
