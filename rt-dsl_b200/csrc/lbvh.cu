@@ -136,12 +136,14 @@ __device__ __forceinline__ int delta(const K *__restrict__ keys, int64_t n, K ki
     return sizeof(K) == 8 ? __clzll((unsigned long long)(ki ^ b)) : __clz((uint32_t)(ki ^ b));
 }
 
-// Direction of Karras node i and the lower bound on its common prefix.
+// Direction of Karras node i and the lower bound on its common prefix (the
+// prefix shared with the neighbour away from the direction).
 template <typename K>
 __device__ __forceinline__ void karras_dir(const K *__restrict__ keys, int64_t n, K ki, int64_t i,
                                            int &dir, int &dmin) {
-    dir = (delta(keys, n, ki, i, i + 1) - delta(keys, n, ki, i, i - 1)) >= 0 ? 1 : -1;
-    dmin = delta(keys, n, ki, i, i - dir);
+    const int dp = delta(keys, n, ki, i, i + 1), dm = delta(keys, n, ki, i, i - 1);
+    dir = (dp - dm) >= 0 ? 1 : -1;
+    dmin = dir > 0 ? dm : dp;
 }
 
 // Karras nodes.  Only nodes with more than leaf_size points are kept (the
