@@ -78,6 +78,21 @@ def test_invalid_arguments_without_device(rtd):
     assert lib.rtd_index_destroy(h) == 0
 
 
+def test_sort_and_scan_diagnostics_reject_bad_arguments_without_device(rtd):
+    """rtd_radix_sort_pairs / rtd_exclusive_scan check their arguments on
+    the host before any device call; n = 0 is a no-op."""
+    lib = rtd.load()
+    p = C.c_void_p(16)   # never dereferenced: each call fails or returns first
+    assert lib.rtd_radix_sort_pairs(p, 2, p, 4, 8, None) == 1          # key_bytes
+    assert lib.rtd_radix_sort_pairs(p, 8, p, 4, 0, None) == 1          # end_bit 0
+    assert lib.rtd_radix_sort_pairs(p, 4, p, 4, 33, None) == 1         # end_bit > 32
+    assert lib.rtd_radix_sort_pairs(None, 8, p, 4, 39, None) == 1      # NULL keys
+    assert lib.rtd_radix_sort_pairs(p, 8, None, 4, 39, None) == 1      # NULL values
+    assert lib.rtd_radix_sort_pairs(None, 8, None, 0, 39, None) == 0   # nothing to sort
+    assert lib.rtd_exclusive_scan(None, p, None, 5, None, None) == 1   # NULL input
+    assert lib.rtd_exclusive_scan(p, None, None, 5, None, None) == 1   # NULL output
+
+
 def test_python_api_rejects_bad_shapes(rtd):
     from rtdsl.api import _as_vec3
     with pytest.raises(ValueError):
