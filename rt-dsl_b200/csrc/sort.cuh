@@ -27,7 +27,9 @@ struct SortScratch {
 // and vals is not read.  On return *in_alt tells whether the sorted result
 // is in the *_alt buffers.  n must be < 2^30.  With gather_out, the last
 // pass writes gather_out[i] = (x, y, z, bits of v) of the i-th sorted value
-// v from the xyz triples gather_xyz instead of the sorted values.
+// v from the xyz triples gather_xyz instead of the sorted values.  d_err
+// (the caller's device error word) is not written: no pass waits on
+// another tile, so none can give up.
 template <typename K>
 rtd_status radix_sort_pairs(K *keys, K *keys_alt, uint32_t *vals, uint32_t *vals_alt,
                             bool vals_iota, uint64_t n, int begin_bit, int end_bit,
@@ -50,6 +52,7 @@ rtd_status radix_sort_split64(const uint64_t *keys, uint64_t *keys_alt, uint32_t
                               uint64_t *sorted_keys, uint32_t **sorted_vals = nullptr);
 
 // out[i] = sum(in[0..i)), out has n entries; *d_total (device) = sum(in).
+// As for the sort, d_err is not written.
 struct ScanScratch {
     DevBuf sums;      // tiles + groups + super groups u64
 };
